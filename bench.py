@@ -1,0 +1,337 @@
+#!/usr/bin/env python3
+"""Benchmark of the fused MUSCL-Hancock step on Kelvin-Helmholtz 2048^2.
+
+Workload: 2-D Cartesian KH on [0,1]^2, 2048x2048 cells, periodic, gamma=1.4,
+van Leer slopes, HLLC, CFL 0.4 (synthetic seeded initial state).  A "step" is
+one time step of the whole grid.  The headline arm is the FP32-mixed fused
+step; the plain FP64 fused step is measured in the same run, and the relative
+L1 density error of the mixed result against the FP64 result after the timed
+steps (same dt sequence) is reported.
+
+Metric: Mcell-updates/s = steps x interior cells / time (src/main.cpp:570-581).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --gpus N > 1 under torchrun each rank runs an independent replica of the
+single-domain step ("replicas only"); value is the sum over ranks, timing the
+max over ranks.  --impl reference times the CPU oracle (the reference's FP64
+algorithm restated in C, OpenMP on the host cores) on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+NX = 2048
+CELLS = NX * NX
+BYTES_PER_CELL = 2 * (2 + 2) * 8  # one FP64 read + one FP64 write of (rho, rhou_x, rhou_y, E)
+WORKLOAD = "kelvin_helmholtz_2d_2048x2048_vanleer_hllc_cfl0.4_periodic"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=1000)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--e2e-chunk", type=int, default=100, help="steps per C-ABI call in the end-to-end arm")
+    p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU oracle work for cpu_baseline")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def kh_domain(precision):
+    from heraclespp_b200 import Domain, setups
+
+    d = Domain(2, [NX, NX], gamma=1.4, limiter="VanLeer", riemann="HLLC", bc=["Periodic"] * 4, precision=precision)
+    grid = setups.Grid.from_domain(d)
+    prim = setups.kelvin_helmholtz(grid)
+    return d, prim
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([s.strip() for s in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        smax = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, nm in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def time_fused(torch, d, steps, warmup):
+    """Device time of `steps` fused steps (CUDA events on the library's stream)."""
+    stream = torch.cuda.ExternalStream(d.stream_handle())
+    d.run(cfl=0.4, nsteps=warmup)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    r = d.run(cfl=0.4, nsteps=steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) * 1e-3, r
+
+
+def read_traffic():
+    """DRAM bytes per launch of the fused mixed kernel, from the committed ncu summary."""
+    f = ROOT / "profiles" / "fused_step_mixed_kh2048.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return json.loads(f.read_text()), "measured"
+        except Exception:
+            pass
+    return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def cpu_baseline(budget_s, cells_full=CELLS):
+    """The CPU oracle (reference FP64 algorithm) on the full KH 2048^2 grid,
+    OpenMP over all host cores, for as many steps as fit in budget_s."""
+    from heraclespp_b200 import setups
+    from oracle import Oracle
+
+    ncores = os.cpu_count() or 1
+    Oracle.set_threads(ncores)
+    o = Oracle(2, [NX, NX], gamma=1.4, limiter="VanLeer", riemann="HLLC", bc=["Periodic"] * 4)
+    grid = setups.Grid.from_domain(o)
+    rho, u, P = setups.kelvin_helmholtz(grid)
+    rho, rhou, E, fx = o.init_from_prim(rho, u, P)
+    t0 = time.perf_counter()
+    o.run(rho, rhou, E, fx, cfl=0.4, max_iter=1)
+    one = time.perf_counter() - t0
+    n = max(1, int(budget_s / max(one, 1e-3)))
+    t0 = time.perf_counter()
+    o.run(rho, rhou, E, fx, cfl=0.4, max_iter=n)
+    el = time.perf_counter() - t0
+    return {"value": n * cells_full / el * 1e-6, "unit": "Mcell-updates/s", "cores": Oracle.get_threads(),
+            "kind": "port",
+            "sample": f"{n} full steps of KH 2048^2 (FP64 oracle, {Oracle.get_threads()} OpenMP threads), {el:.1f} s"}
+
+
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def run_reference(args):
+    world, rank, local = dist_setup(args)
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    base = cpu_baseline(min(args.cpu_budget * 3, 60.0))
+    line = {"metric": "Mcell-updates/s", "value": base["value"], "unit": "Mcell-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": CELLS, "precision": "fp64"},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_setup(args)
+    import heraclespp_b200 as hb
+
+    dev_index = local
+    os.environ.setdefault("CUDA_DEVICE_ORDER", "PCI_BUS_ID")
+    torch.cuda.set_device(dev_index)
+    peaks, peaks_kind = measured_peaks()
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+
+    # ---- FP32-mixed headline --------------------------------------------
+    d, prim = kh_domain("fp32_mixed")
+    d.h  # noqa: B018
+    d.set_state_from_prim(*prim)
+    launches0 = hb.kernel_launch_count()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    with ClockSampler(int(os.environ.get("HCL_NVSMI_INDEX", dev_index))) as clk:
+        el_mixed, r_mixed = time_fused(torch, d, args.steps, args.warmup)
+    launches = hb.kernel_launch_count() - launches0 - args.warmup
+    dts = d.dt_log()
+    rho_mixed = d.get_state()[0]
+
+    # ---- FP64 fused step, same workload and the same dt sequence ----------
+    d64, _ = kh_domain("fp64")
+    d64.set_state_from_prim(*prim)
+    el_64, _ = time_fused(torch, d64, args.steps, args.warmup)
+    # accuracy of mixed vs FP64 with identical dts over warmup+steps steps
+    d64.set_state_from_prim(*prim)
+    d64.run(nsteps=len(dts), dts=dts)
+    rho64 = d64.get_state()[0]
+    ng = 2
+    a = rho_mixed[ng:-ng, ng:-ng]
+    b = rho64[ng:-ng, ng:-ng]
+    l1 = float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
+    linf = float(np.max(np.abs(a - b) / np.abs(b)))
+    d64.close()
+
+    # ---- end to end through the C ABI with host buffers ----------------------
+    pinned = [torch.empty(s, dtype=torch.float64).pin_memory() for s in (d.shape3, (2,) + d.shape3, d.shape3)]
+    host = d.get_state()
+    for t_, h_ in zip(pinned, host):
+        t_.numpy()[...] = h_
+    chunk = args.e2e_chunk
+    reps = max(1, args.steps // chunk)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(d.stream_handle())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        d.set_state(*[t_.numpy() for t_ in pinned])
+        d.run(cfl=0.4, nsteps=chunk)
+        d.get_state(out=tuple(t_.numpy() for t_ in pinned))
+    e1.record(stream)
+    e1.synchronize()
+    el_e2e = e0.elapsed_time(e1) * 1e-3
+    state_bytes = sum(int(np.prod(t_.shape)) * 8 for t_ in pinned)
+
+    # ---- cross-rank aggregation -------------------------------------------
+    el_max, el64_max, e2e_max = el_mixed, el_64, el_e2e
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([el_mixed, el_64, el_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el_max, el64_max, e2e_max = (float(v) for v in t.tolist())
+
+    value = world * args.steps * CELLS / el_max * 1e-6
+    value64 = world * args.steps * CELLS / el64_max * 1e-6
+    e2e_val = world * reps * chunk * CELLS / e2e_max * 1e-6
+    ms_per_step = el_max / args.steps * 1e3
+    achieved = BYTES_PER_CELL * CELLS / (el_mixed / args.steps) * 1e-9  # GB/s per launch
+    traffic = read_traffic()
+    line = {
+        "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32-mixed (f32 fluxes, f64 state)", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells": CELLS, "precision": "fp32_mixed", "parallelism": "replicas",
+                   "l2": "inputs larger than L2 (state 134 MB read + 134 MB written per step)",
+                   "e2e_steps_per_call": chunk},
+        "fp64": {"value": value64, "ms_per_step": el64_max / args.steps * 1e3, "unit": "Mcell-updates/s"},
+        "speedup_mixed_vs_fp64": value / value64,
+        "accuracy": {"rel_l1_rho_mixed_vs_fp64": l1, "rel_linf_rho_mixed_vs_fp64": linf,
+                     "steps_compared": int(len(dts))},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": traffic,
+                     "peak_source": f"{peaks_kind} (MEASURED_PEAKS.json hbm_gbs)" if peaks_kind == "measured"
+                     else "fallback 6.65 TB/s",
+                     "bytes_per_cell": BYTES_PER_CELL, "cells_per_launch": CELLS},
+        "e2e": {"value": e2e_val, "unit": "Mcell-updates/s", "h2d_bytes_per_step": state_bytes / chunk,
+                "d2h_bytes_per_step": state_bytes / chunk + 96},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(args.cpu_budget)
+    d.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,226 @@
+"""heraclespp_b200 -- B200-native MUSCL-Hancock step of HERACLES++.
+
+Python view of the C ABI (include/heracles_b200.h).  ``Domain`` wraps one
+handle: one grid on one GPU with the physics plugins chosen by the same
+keys as the reference's factories (``Minmod``, ``HLLC``, ``NullGradient``,
+...).  Host arrays are numpy float64 arrays in the reference's LayoutLeft
+order, i.e. numpy shape (n2, n1, n0) for rho and (ndim, n2, n1, n0) for rhou.
+Stage methods take torch CUDA tensors laid out the same way.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._native import (BCS, GEOMS, GRAVITY, LIMITERS, PRECISION, RIEMANN, Config, DomainError, HclError,
+                      RunParams, RunResult, check, lib)
+
+__all__ = ["Domain", "HclError", "DomainError", "lib", "kernel_launch_count"]
+
+
+def kernel_launch_count() -> int:
+    return int(lib().hcl_kernel_launch_count())
+
+
+def _key(mapping, v, what):
+    if isinstance(v, (int, np.integer)):
+        return int(v)
+    try:
+        return mapping[v]
+    except KeyError:
+        raise HclError(1, f"Unknown {what}: {v}.") from None
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        assert t.dtype == np.float64 and t.flags["C_CONTIGUOUS"]
+        return t.ctypes.data_as(C.c_void_p)
+    return C.c_void_p(t.data_ptr())
+
+
+class Domain:
+    """One domain on one GPU (hcl_create)."""
+
+    def __init__(self, ndim, nx, *, nghost=2, nfx=0, geometry="Cartesian", gamma=5.0 / 3.0, mmw=1.0,
+                 limiter="VanLeer", riemann="HLL", bc=("Periodic",) * 6, gravity="Uniform", g=(0.0, 0.0, 0.0),
+                 central_mass=1.0, xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0), nodes=None, precision="fp64",
+                 device=0):
+        L = lib()
+        cfg = Config()
+        L.hcl_config_default(C.byref(cfg))
+        cfg.ndim = int(ndim)
+        nx = list(nx) + [1, 1, 1]
+        for d in range(3):
+            cfg.nx[d] = int(nx[d]) if d < ndim else 1
+            cfg.g[d] = float(g[d])
+            cfg.xmin[d] = float(xmin[d])
+            cfg.xmax[d] = float(xmax[d])
+        cfg.nghost = int(nghost)
+        cfg.nfx = int(nfx)
+        cfg.geometry = _key(GEOMS, geometry, "geometry")
+        cfg.gamma = float(gamma)
+        cfg.mmw = float(mmw)
+        cfg.limiter = _key(LIMITERS, limiter, "face reconstruction algorithm")
+        cfg.riemann = _key(RIEMANN, riemann, "riemann solver")
+        bcs = list(bc) + ["Periodic"] * 6
+        for f in range(6):
+            cfg.bc[f] = _key(BCS, bcs[f], "boundary condition")
+        cfg.gravity = _key(GRAVITY, gravity, "gravity")
+        cfg.central_mass = float(central_mass)
+        cfg.precision = _key(PRECISION, precision, "precision")
+        cfg.device = int(device)
+        self._nodes = None
+        if nodes is not None:
+            self._nodes = [np.ascontiguousarray(x, dtype=np.float64) for x in nodes]
+            for d in range(3):
+                cfg.nodes[d] = self._nodes[d].ctypes.data
+        self.cfg = cfg
+        h = C.c_void_p()
+        check(L.hcl_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.ndim = int(ndim)
+        self.nfx = int(nfx)
+        n = (C.c_int * 3)()
+        nc = C.c_int64()
+        check(L.hcl_get_extents(h, n, C.byref(nc)))
+        self.n = tuple(n)
+        self.ncells = int(nc.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hcl_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape3(self):
+        return (self.n[2], self.n[1], self.n[0])
+
+    def zeros(self, ncomp=None):
+        return np.zeros(self.shape3 if ncomp is None else (ncomp,) + self.shape3)
+
+    # ---- grid --------------------------------------------------------
+    def grid(self):
+        x = [np.zeros(self.n[d] + 1) for d in range(3)]
+        dx = [np.zeros(self.n[d]) for d in range(3)]
+        xc = [np.zeros(self.n[d]) for d in range(3)]
+        ds = np.zeros((3,) + self.shape3)
+        dv = np.zeros(self.shape3)
+        arr = lambda a: (C.c_void_p * 3)(*[v.ctypes.data for v in a])  # noqa: E731
+        check(lib().hcl_get_grid(self.h, arr(x), arr(dx), arr(xc), _ptr(ds), _ptr(dv)))
+        out = {"ds": ds, "dv": dv}
+        for d in range(3):
+            out[f"x{d}"] = x[d]
+            out[f"dx{d}"] = dx[d]
+            out[f"x{d}c"] = xc[d]
+        return out
+
+    # ---- stage entry points (device tensors) ---------------------------
+    def conv_prim_to_cons(self, ng_eff, rho, u, P, rhou, E, stream=None):
+        check(lib().hcl_conv_prim_to_cons(self.h, ng_eff, _ptr(rho), _ptr(u), _ptr(P), _ptr(rhou), _ptr(E), stream))
+
+    def conv_cons_to_prim(self, ng_eff, rho, rhou, E, u, P, stream=None):
+        check(lib().hcl_conv_cons_to_prim(self.h, ng_eff, _ptr(rho), _ptr(rhou), _ptr(E), _ptr(u), _ptr(P), stream))
+
+    def face_reconstruction(self, ng_eff, var, var_rec, stream=None):
+        check(lib().hcl_face_reconstruction(self.h, ng_eff, _ptr(var), _ptr(var_rec), stream))
+
+    def hydro_reconstruction(self, ng_eff, dt, rho, u, P, fx, rho_rec, rhou_rec, E_rec, fx_rec, u_rec=None,
+                             P_rec=None, stream=None):
+        check(lib().hcl_hydro_reconstruction(self.h, ng_eff, float(dt), _ptr(rho), _ptr(u), _ptr(P), _ptr(fx),
+                                             _ptr(rho_rec), _ptr(rhou_rec), _ptr(E_rec), _ptr(fx_rec), _ptr(u_rec),
+                                             _ptr(P_rec), stream))
+
+    def godunov_scheme(self, ng_eff, dt, rho, rhou, E, fx, rho_rec, rhou_rec, E_rec, fx_rec, rho_new, rhou_new,
+                       E_new, fx_new, stream=None):
+        check(lib().hcl_godunov_scheme(self.h, ng_eff, float(dt), _ptr(rho), _ptr(rhou), _ptr(E), _ptr(fx),
+                                       _ptr(rho_rec), _ptr(rhou_rec), _ptr(E_rec), _ptr(fx_rec), _ptr(rho_new),
+                                       _ptr(rhou_new), _ptr(E_new), _ptr(fx_new), stream))
+
+    def boundary_conditions(self, rho, rhou, E, fx=None, stream=None):
+        check(lib().hcl_boundary_conditions(self.h, _ptr(rho), _ptr(rhou), _ptr(E), _ptr(fx), stream))
+
+    def time_step(self, ng_eff, rho, u, P, stream=None):
+        out = C.c_double()
+        check(lib().hcl_time_step(self.h, ng_eff, _ptr(rho), _ptr(u), _ptr(P), C.byref(out), stream))
+        return out.value
+
+    def minimum_internal_energy(self, rho, rhou, E, stream=None):
+        out = C.c_double()
+        check(lib().hcl_minimum_internal_energy(self.h, _ptr(rho), _ptr(rhou), _ptr(E), C.byref(out), stream))
+        return out.value
+
+    def integrate(self, var, stream=None):
+        out = C.c_double()
+        check(lib().hcl_integrate(self.h, _ptr(var), C.byref(out), stream))
+        return out.value
+
+    # ---- handle-owned state -------------------------------------------
+    def set_state(self, rho, rhou, E, fx=None, device=False):
+        if not device:
+            rho, rhou, E = (np.ascontiguousarray(a, dtype=np.float64) for a in (rho, rhou, E))
+        check(lib().hcl_set_state(self.h, _ptr(rho), _ptr(rhou), _ptr(E), _ptr(fx), 1 if device else 0))
+
+    def get_state(self, out=None, device=False):
+        if out is None:
+            out = (self.zeros(), self.zeros(self.ndim), self.zeros())
+        rho, rhou, E = out
+        check(lib().hcl_get_state(self.h, _ptr(rho), _ptr(rhou), _ptr(E), None, 1 if device else 0))
+        return out
+
+    def set_state_from_prim(self, rho, u, P):
+        rho, u, P = (np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, P))
+        check(lib().hcl_set_state_from_prim(self.h, _ptr(rho), _ptr(u), _ptr(P), None))
+
+    def reset_clock(self, t_ini=0.0):
+        check(lib().hcl_reset_clock(self.h, float(t_ini)))
+
+    def run(self, *, cfl=0.4, t_end=1e300, max_iter=2 ** 31 - 1, iter_frequency=0, time_frequency=0.0,
+            time_first_output=None, nsteps=0, graph_chunk=0, dts=None, check_status=True):
+        p = RunParams()
+        p.cfl = cfl
+        p.t_end = t_end
+        p.max_iter = int(max_iter)
+        p.iter_frequency = int(iter_frequency)
+        p.time_frequency = float(time_frequency)
+        p.time_first_output = float(time_frequency if time_first_output is None else time_first_output)
+        p.nsteps = int(nsteps)
+        p.graph_chunk = int(graph_chunk)
+        keep = None
+        if dts is not None:
+            keep = np.ascontiguousarray(dts, dtype=np.float64)
+            p.fixed_dt = 1
+            p.dts = keep.ctypes.data_as(C.POINTER(C.c_double))
+        r = RunResult()
+        rc = lib().hcl_run(self.h, C.byref(p), C.byref(r))
+        if check_status:
+            check(rc)
+        return r
+
+    def step_fixed_dt(self, dt, stream=None):
+        check(lib().hcl_step_fixed_dt(self.h, float(dt), stream))
+
+    def dt_log(self, max_count=1 << 20):
+        buf = np.zeros(max_count)
+        cnt = C.c_int()
+        check(lib().hcl_get_dt_log(self.h, _ptr(buf), max_count, C.byref(cnt)))
+        return buf[: cnt.value].copy()
+
+    def stream_handle(self) -> int:
+        """cudaStream_t of the handle (for timing events on the launching stream)."""
+        s = C.c_void_p()
+        check(lib().hcl_get_stream(self.h, C.byref(s)))
+        return int(s.value or 0)
+
+    def conservation_sums(self):
+        out = np.zeros(self.ndim + 2)
+        check(lib().hcl_conservation_sums(self.h, _ptr(out)))
+        return out

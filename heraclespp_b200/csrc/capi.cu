@@ -1,0 +1,1218 @@
+// capi.cu -- implementation of the C ABI declared in include/heracles_b200.h.
+//
+// Owns the per-domain handle: configuration, the grid arrays built on the
+// host exactly as Grid::set_grid builds them (mesh/grid.cpp:134-155,
+// mesh/geometry.cpp:32-126, mesh/grid_type.cpp:151-186), their device copies,
+// the fused-path state buffers and control block, and the CUDA graphs that
+// replay chunks of fused steps.  No entry point throws; failures return a
+// status and set the thread's last-error message.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <climits>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "heracles_b200.h"
+#include "hcl_device.cuh"
+#include "stages.hpp"
+
+using hcl::GridDev;
+using hcl::RunParamsDev;
+using hcl::StepCtl;
+using hcl::fused::StateDev;
+
+namespace {
+
+thread_local std::string t_last_error;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    t_last_error = buf;
+    return code;
+}
+
+#define HCL_CUDA(call)                                                                                         \
+    do {                                                                                                       \
+        cudaError_t e_ = (call);                                                                               \
+        if (e_ != cudaSuccess) {                                                                               \
+            return fail(HCL_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+        }                                                                                                      \
+    } while (0)
+
+#define HCL_LAUNCH_CHECK()                                                                                  \
+    do {                                                                                                    \
+        cudaError_t e_ = cudaGetLastError();                                                                \
+        if (e_ != cudaSuccess) {                                                                            \
+            return fail(HCL_ERR_CUDA, "kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                                          \
+        }                                                                                                   \
+    } while (0)
+
+template <class T>
+int dalloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) {
+        return HCL_OK;
+    }
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(HCL_ERR_CUDA, "cudaMalloc of %zu bytes failed: %s", sizeof(T) * count, cudaGetErrorString(e));
+    }
+    return HCL_OK;
+}
+
+struct GraphKey {
+    int k;
+    int precision;
+    int shape;
+    RunParamsDev rp;
+    bool operator<(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) < 0; }
+};
+
+} // namespace
+
+namespace hcl::host {
+// Shared with the host-only entry points (host/capi_host.cpp).
+int set_error(int code, std::string const& msg)
+{
+    t_last_error = msg;
+    return code;
+}
+} // namespace hcl::host
+
+struct hcl_handle {
+    hcl_config cfg{};
+    GridDev g{};
+    // host grid arrays
+    std::vector<double> hx[3], hdx[3], hxc[3], hds, hdv, hgr, hcot, hsin1, hsinxc1;
+    // device grid arrays
+    double *dx_nodes[3] = {}, *ddx[3] = {}, *dxc[3] = {}, *dds = nullptr, *ddv = nullptr, *dgr = nullptr;
+    double *dcot = nullptr, *dsin1 = nullptr, *dsinxc1 = nullptr;
+    // stage-path scratch (MUSCLHancockHydroReconstruction's P_rec/u_rec, fx_rec_old)
+    double *u_rec = nullptr, *P_rec = nullptr, *fx_rec_old = nullptr;
+    // reductions
+    unsigned long long* red_bits = nullptr;
+    int* red_flag = nullptr;
+    double* red_partials = nullptr;
+    double* red_out = nullptr;
+    // fused state
+    double* state_mem[2] = {nullptr, nullptr};
+    StateDev st[2]{};
+    StepCtl* ctl = nullptr;
+    StepCtl* ctl_tune = nullptr;
+    int64_t counter = 0;   // fused steps launched since the last prologue
+    int state_valid = 0;
+    int cur = 0;           // buffer holding the current state when not running
+    double t_base = 0.0;
+    int iter_base = 0;
+    int stopped = 0;
+    int mixed_shape = -1;  // autotuned tile shape of the mixed 2-D kernel
+    // dt log
+    double* dt_log = nullptr;
+    int dt_log_cap = 0;
+    double* d_dts = nullptr;
+    int d_dts_cap = 0;
+    // stream and graphs
+    cudaStream_t stream = nullptr;
+    std::map<GraphKey, cudaGraphExec_t> graphs;
+};
+
+namespace {
+
+void free_handle(hcl_handle* h)
+{
+    if (!h) {
+        return;
+    }
+    for (auto& kv : h->graphs) {
+        cudaGraphExecDestroy(kv.second);
+    }
+    for (int d = 0; d < 3; ++d) {
+        cudaFree(h->dx_nodes[d]);
+        cudaFree(h->ddx[d]);
+        cudaFree(h->dxc[d]);
+    }
+    cudaFree(h->dds);
+    cudaFree(h->ddv);
+    cudaFree(h->dgr);
+    cudaFree(h->dcot);
+    cudaFree(h->dsin1);
+    cudaFree(h->dsinxc1);
+    cudaFree(h->u_rec);
+    cudaFree(h->P_rec);
+    cudaFree(h->fx_rec_old);
+    cudaFree(h->red_bits);
+    cudaFree(h->red_flag);
+    cudaFree(h->red_partials);
+    cudaFree(h->red_out);
+    cudaFree(h->state_mem[0]);
+    cudaFree(h->state_mem[1]);
+    cudaFree(h->ctl);
+    cudaFree(h->ctl_tune);
+    cudaFree(h->dt_log);
+    cudaFree(h->d_dts);
+    if (h->stream) {
+        cudaStreamDestroy(h->stream);
+    }
+    delete h;
+}
+
+// Regular mesh (mesh/grid_type.cpp:151-186), cell sizes and centres
+// (mesh/grid.cpp:31-44), ds/dv (mesh/geometry.cpp:32-126), point-mass
+// gravity (gravity/gravity.cpp:49-55), on the host with libm.
+void build_grid_host(hcl_handle* h)
+{
+    const hcl_config& c = h->cfg;
+    const int nd = c.ndim;
+    int n[3], nx[3];
+    for (int d = 0; d < 3; ++d) {
+        nx[d] = d < nd ? c.nx[d] : 1;
+        n[d] = nx[d] + (d < nd ? 2 * c.nghost : 0);
+    }
+    for (int d = 0; d < 3; ++d) {
+        h->hx[d].assign((size_t)n[d] + 1, 0.0);
+        if (c.nodes[d]) {
+            std::memcpy(h->hx[d].data(), c.nodes[d], sizeof(double) * ((size_t)n[d] + 1));
+        } else {
+            const int ngd = d < nd ? c.nghost : 0;
+            const double dxd = (c.xmax[d] - c.xmin[d]) / nx[d];
+            for (int i = 0; i < n[d] + 1; ++i) {
+                h->hx[d][i] = c.xmin[d] + ((i - ngd) * dxd);
+            }
+        }
+        h->hdx[d].assign(n[d], 0.0);
+        h->hxc[d].assign(n[d], 0.0);
+        for (int i = 0; i < n[d]; ++i) {
+            h->hdx[d][i] = h->hx[d][i + 1] - h->hx[d][i];
+            h->hxc[d][i] = (h->hx[d][i] + h->hx[d][i + 1]) / 2;
+        }
+    }
+    const int64_t N = (int64_t)n[0] * n[1] * n[2];
+    h->hds.assign((size_t)N * 3, 0.0);
+    h->hdv.assign((size_t)N, 0.0);
+    const double pi = hcl::kPi;
+    const std::vector<double>& x0 = h->hx[0];
+    const std::vector<double>& x1 = h->hx[1];
+    for (int k = 0; k < n[2]; ++k) {
+        for (int j = 0; j < n[1]; ++j) {
+            for (int i = 0; i < n[0]; ++i) {
+                const int64_t id = i + (int64_t)n[0] * (j + (int64_t)n[1] * k);
+                const double dx0 = h->hdx[0][i], dx1 = h->hdx[1][j], dx2 = h->hdx[2][k];
+                if (c.geometry == HCL_GEOM_CARTESIAN) {
+                    for (int idim = 0; idim < 3; ++idim) {
+                        double a[3] = {dx0, dx1, dx2};
+                        a[idim] = 1;
+                        h->hds[id + N * idim] = a[0] * a[1] * a[2];
+                    }
+                    h->hdv[id] = dx0 * dx1 * dx2;
+                } else if (nd == 1) {
+                    h->hds[id] = 4 * pi * x0[i] * x0[i];
+                    h->hdv[id] = (4 * pi * ((x0[i + 1] * x0[i + 1] * x0[i + 1]) - (x0[i] * x0[i] * x0[i]))) / 3;
+                } else if (nd == 2) {
+                    const double dcos = std::cos(x1[j]) - std::cos(x1[j + 1]);
+                    h->hds[id] = 2 * pi * x0[i] * x0[i] * dcos;
+                    h->hds[id + N] = (2 * pi / 2) * ((x0[i + 1] * x0[i + 1]) - (x0[i] * x0[i])) * std::sin(x1[j]);
+                    h->hdv[id] = (2 * pi / 3) * ((x0[i + 1] * x0[i + 1] * x0[i + 1]) - (x0[i] * x0[i] * x0[i])) * dcos;
+                } else {
+                    const double dcos = std::cos(x1[j]) - std::cos(x1[j + 1]);
+                    h->hds[id] = x0[i] * x0[i] * dcos * dx2;
+                    h->hds[id + N] = (1. / 2) * ((x0[i + 1] * x0[i + 1]) - (x0[i] * x0[i])) * std::sin(x1[j]) * dx2;
+                    h->hds[id + 2 * N] = x0[i] * dx0 * dx1;
+                    h->hdv[id] = (1. / 3) * ((x0[i + 1] * x0[i + 1] * x0[i + 1]) - (x0[i] * x0[i] * x0[i])) * dcos * dx2;
+                }
+            }
+        }
+    }
+    if (c.gravity == HCL_GRAVITY_POINT_MASS) {
+        h->hgr.assign(n[0], 0.0);
+        for (int i = 0; i < n[0]; ++i) {
+            h->hgr[i] = -hcl::kG * c.central_mass / (h->hxc[0][i] * h->hxc[0][i]);
+        }
+    }
+    // spherical trig factors per index (source_terms.hpp:38, :58-59, time_step.hpp:67)
+    h->hcot.assign(n[1], 0.0);
+    h->hsin1.assign((size_t)n[1] + 1, 0.0);
+    h->hsinxc1.assign(n[1], 0.0);
+    for (int j = 0; j < n[1]; ++j) {
+        h->hcot[j] = std::cos((x1[j] + x1[j + 1]) / 2) / std::sin((x1[j] + x1[j + 1]) / 2);
+        h->hsinxc1[j] = std::sin(h->hxc[1][j]);
+    }
+    for (int j = 0; j < n[1] + 1; ++j) {
+        h->hsin1[j] = std::sin(x1[j]);
+    }
+
+    GridDev& g = h->g;
+    g.ndim = nd;
+    g.ng = c.nghost;
+    g.nfx = c.nfx;
+    for (int d = 0; d < 3; ++d) {
+        g.n[d] = n[d];
+        g.nx[d] = nx[d];
+        g.g[d] = c.g[d];
+    }
+    g.N = N;
+    g.geom = c.geometry;
+    g.limiter = c.limiter;
+    g.riemann = c.riemann;
+    for (int f = 0; f < 6; ++f) {
+        g.bc[f] = c.bc[f];
+    }
+    g.gravity = c.gravity;
+    g.gamma = c.gamma;
+    g.gamma_m1 = c.gamma - 1;
+    g.mmw = c.mmw;
+    // uniform Cartesian spacing (to 1e-12 relative) enables the fast forms of
+    // the mixed kernel
+    int uniform = c.geometry == HCL_GEOM_CARTESIAN;
+    for (int d = 0; d < nd && uniform; ++d) {
+        const double ref = h->hdx[d][c.nghost];
+        for (int i = 0; i < n[d]; ++i) {
+            if (std::fabs(h->hdx[d][i] - ref) > 1e-12 * std::fabs(ref)) {
+                uniform = 0;
+                break;
+            }
+        }
+        g.inv_dx[d] = 1.0 / ref;
+    }
+    g.uniform_cart = uniform;
+}
+
+int validate(const hcl_config* c)
+{
+    if (!c) {
+        return fail(HCL_ERR_ARGUMENT, "null config");
+    }
+    if (c->ndim < 1 || c->ndim > 3) {
+        return fail(HCL_ERR_CONFIG, "ndim must be 1, 2 or 3 (got %d)", c->ndim);
+    }
+    // thermodynamics/perfect_gas.cpp:15-21
+    if (!std::isfinite(c->gamma) || c->gamma <= 1) {
+        return fail(HCL_ERR_DOMAIN, "Invalid gamma");
+    }
+    if (!std::isfinite(c->mmw) || c->mmw <= 0) {
+        return fail(HCL_ERR_DOMAIN, "Invalid mmw");
+    }
+    if (c->nghost < 2 || c->nghost > 4) {
+        return fail(HCL_ERR_CONFIG, "Nghost must be in [2, 4] (got %d)", c->nghost);
+    }
+    for (int d = 0; d < c->ndim; ++d) {
+        if (c->nx[d] < c->nghost) {
+            return fail(HCL_ERR_CONFIG, "Nx%d_glob = %d is smaller than Nghost", d, c->nx[d]);
+        }
+    }
+    if (c->limiter < 0 || c->limiter > 3) {
+        return fail(HCL_ERR_CONFIG, "Unknown face reconstruction algorithm id %d.", c->limiter);
+    }
+    if (c->riemann < 0 || c->riemann > 2) {
+        return fail(HCL_ERR_CONFIG, "Invalid riemann solver id %d.", c->riemann);
+    }
+    for (int f = 0; f < 2 * c->ndim; ++f) {
+        if (c->bc[f] < 0 || c->bc[f] > 2) {
+            return fail(HCL_ERR_CONFIG, "Unknown boundary condition id %d on face %d.", c->bc[f], f);
+        }
+        // periodicity is a property of the pair of faces (ghost_sync wraps both)
+    }
+    if (c->geometry != HCL_GEOM_CARTESIAN && c->geometry != HCL_GEOM_SPHERICAL) {
+        return fail(HCL_ERR_CONFIG, "Unknown geometry id %d", c->geometry);
+    }
+    if (c->gravity != HCL_GRAVITY_UNIFORM && c->gravity != HCL_GRAVITY_POINT_MASS) {
+        return fail(HCL_ERR_CONFIG, "Unknown gravity id %d", c->gravity);
+    }
+    if (c->precision != HCL_FP64 && c->precision != HCL_FP32_MIXED) {
+        return fail(HCL_ERR_CONFIG, "Unknown precision id %d", c->precision);
+    }
+    if (c->nfx < 0) {
+        return fail(HCL_ERR_CONFIG, "nfx must be >= 0");
+    }
+    return HCL_OK;
+}
+
+cudaStream_t pick(hcl_handle* h, void* s)
+{
+    return s ? (cudaStream_t)s : h->stream;
+}
+
+int upload(double** dst, const std::vector<double>& src)
+{
+    int rc = dalloc(dst, src.size());
+    if (rc) {
+        return rc;
+    }
+    if (!src.empty()) {
+        HCL_CUDA(cudaMemcpy(*dst, src.data(), sizeof(double) * src.size(), cudaMemcpyHostToDevice));
+    }
+    return HCL_OK;
+}
+
+int ensure_dt_log(hcl_handle* h, int need)
+{
+    if (need <= h->dt_log_cap) {
+        return HCL_OK;
+    }
+    int cap = std::max(need, std::max(1024, 2 * h->dt_log_cap));
+    double* p = nullptr;
+    int rc = dalloc(&p, (size_t)cap);
+    if (rc) {
+        return rc;
+    }
+    if (h->dt_log && h->dt_log_cap > 0) {
+        HCL_CUDA(cudaMemcpyAsync(p, h->dt_log, sizeof(double) * h->dt_log_cap, cudaMemcpyDeviceToDevice, h->stream));
+        HCL_CUDA(cudaStreamSynchronize(h->stream));
+        cudaFree(h->dt_log);
+    }
+    h->dt_log = p;
+    h->dt_log_cap = cap;
+    return HCL_OK;
+}
+
+int read_ctl(hcl_handle* h, StepCtl* out)
+{
+    HCL_CUDA(cudaMemcpyAsync(out, h->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, h->stream));
+    HCL_CUDA(cudaStreamSynchronize(h->stream));
+    return HCL_OK;
+}
+
+void launch_step(hcl_handle* h, const RunParamsDev& rp, int64_t counter, StepCtl* ctl, int in_buf, int shape,
+                 cudaStream_t s)
+{
+    const int slot = (int)(counter % 6);
+    const int out_buf = in_buf ^ 1;
+    if (h->cfg.precision == HCL_FP64) {
+        hcl::fused::step_exact(h->g, h->st[in_buf], h->st[out_buf], ctl, rp, slot, out_buf, s);
+    } else {
+        hcl::fused::step_mixed(h->g, h->st[in_buf], h->st[out_buf], ctl, rp, slot, out_buf, shape, s);
+    }
+}
+
+// Picks the fastest tile shape of the mixed 2-D kernel by timing a few steps
+// that read the current state and write the other buffer with a scratch
+// control block (the current state is not modified).
+int autotune_mixed(hcl_handle* h)
+{
+    const int nshapes = hcl::fused::mixed_shape_count(h->g.ndim);
+    h->mixed_shape = 0;
+    if (nshapes <= 1) {
+        return HCL_OK;
+    }
+    const char* env = std::getenv("HCL_MIXED_SHAPE");
+    if (env) {
+        h->mixed_shape = std::max(0, std::min(nshapes - 1, std::atoi(env)));
+        return HCL_OK;
+    }
+    if (h->g.N < 65536) {
+        return HCL_OK;
+    }
+    RunParamsDev rp;
+    std::memset(&rp, 0, sizeof(rp));
+    rp.cfl = 0.4;
+    rp.t_end = 1e300;
+    rp.max_iter = INT_MAX;
+    rp.fixed_dt = 2;
+    rp.dt_value = 0.0;
+    cudaEvent_t e0, e1;
+    HCL_CUDA(cudaEventCreate(&e0));
+    HCL_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    for (int sh = 0; sh < nshapes; ++sh) {
+        hcl::fused::prologue(h->g, h->st[h->cur], h->ctl_tune, 0.0, 0, h->stream);
+        // warm-up, then time 4 launches that all read the same input
+        for (int r = 0; r < 2; ++r) {
+            launch_step(h, rp, 0, h->ctl_tune, h->cur, sh, h->stream);
+        }
+        HCL_CUDA(cudaEventRecord(e0, h->stream));
+        for (int r = 0; r < 4; ++r) {
+            launch_step(h, rp, 0, h->ctl_tune, h->cur, sh, h->stream);
+        }
+        HCL_CUDA(cudaEventRecord(e1, h->stream));
+        HCL_CUDA(cudaEventSynchronize(e1));
+        HCL_LAUNCH_CHECK();
+        float ms = 0;
+        HCL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+            best = ms;
+            h->mixed_shape = sh;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return HCL_OK;
+}
+
+int get_graph(hcl_handle* h, const RunParamsDev& rp, int k, cudaGraphExec_t* out)
+{
+    GraphKey key;
+    std::memset(&key, 0, sizeof(key));
+    key.k = k;
+    key.precision = h->cfg.precision;
+    key.shape = h->mixed_shape;
+    key.rp = rp;
+    auto it = h->graphs.find(key);
+    if (it != h->graphs.end()) {
+        *out = it->second;
+        return HCL_OK;
+    }
+    cudaGraph_t graph;
+    HCL_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = hcl::g_launches.load();
+    for (int s = 0; s < k; ++s) {
+        launch_step(h, rp, s, h->ctl, s & 1, h->mixed_shape, h->stream);
+    }
+    hcl::g_launches = before; // counted at replay
+    HCL_CUDA(cudaStreamEndCapture(h->stream, &graph));
+    cudaGraphExec_t exec;
+    HCL_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    h->graphs[key] = exec;
+    *out = exec;
+    return HCL_OK;
+}
+
+// Normalises the fused state after a finished run so that it sits in buffer 0
+// with a fresh control block (t and iteration carried over).
+int restart_clock(hcl_handle* h, double t, int iter)
+{
+    if (h->cur != 0) {
+        const size_t bytes = sizeof(double) * (size_t)h->st[0].plane * (h->g.ndim + 2);
+        HCL_CUDA(cudaMemcpyAsync(h->st[0].q, h->st[1].q, bytes, cudaMemcpyDeviceToDevice, h->stream));
+        h->cur = 0;
+    }
+    hcl::fused::prologue(h->g, h->st[0], h->ctl, t, iter, h->stream);
+    HCL_LAUNCH_CHECK();
+    h->counter = 0;
+    h->stopped = 0;
+    h->t_base = t;
+    h->iter_base = iter;
+    return HCL_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int hcl_abi_version(void)
+{
+    return HCL_ABI_VERSION;
+}
+
+const char* hcl_last_error(void)
+{
+    return t_last_error.c_str();
+}
+
+int64_t hcl_kernel_launch_count(void)
+{
+    return hcl::g_launches.load();
+}
+
+int hcl_get_stream(const hcl_handle* h, void** stream)
+{
+    if (!h || !stream) {
+        return fail(HCL_ERR_ARGUMENT, "null argument");
+    }
+    *stream = (void*)h->stream;
+    return HCL_OK;
+}
+
+void hcl_config_default(hcl_config* c)
+{
+    if (!c) {
+        return;
+    }
+    std::memset(c, 0, sizeof(*c));
+    // utils/param.cpp:14-73
+    c->ndim = 1;
+    c->nx[0] = c->nx[1] = c->nx[2] = 1;
+    c->nghost = 2;
+    c->nfx = 0;
+    c->geometry = HCL_GEOM_CARTESIAN;
+    c->gamma = 5. / 3;
+    c->mmw = 1.;
+    c->limiter = HCL_LIMITER_VANLEER;
+    c->riemann = HCL_RIEMANN_HLL;
+    for (int f = 0; f < 6; ++f) {
+        c->bc[f] = HCL_BC_PERIODIC;
+    }
+    c->gravity = HCL_GRAVITY_UNIFORM;
+    c->central_mass = 1.0;
+    for (int d = 0; d < 3; ++d) {
+        c->xmin[d] = 0.0;
+        c->xmax[d] = 1.0;
+    }
+    c->precision = HCL_FP64;
+    c->device = 0;
+}
+
+int hcl_create(const hcl_config* cfg, hcl_handle** out)
+{
+    if (!out) {
+        return fail(HCL_ERR_ARGUMENT, "null output handle");
+    }
+    *out = nullptr;
+    int rc = validate(cfg);
+    if (rc) {
+        return rc;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return fail(HCL_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) {
+        return fail(HCL_ERR_CONFIG, "device %d out of range (%d devices)", cfg->device, ndev);
+    }
+    HCL_CUDA(cudaSetDevice(cfg->device));
+    hcl::fused::configure_exact();
+    hcl::fused::configure_mixed();
+    HCL_CUDA(cudaGetLastError());
+    hcl_handle* h = new hcl_handle();
+    h->cfg = *cfg;
+    for (int d = 0; d < 3; ++d) {
+        h->cfg.nodes[d] = nullptr; // not retained
+    }
+    hcl_config tmp = *cfg;
+    h->cfg = tmp;
+    build_grid_host(h);
+    for (int d = 0; d < 3; ++d) {
+        h->cfg.nodes[d] = nullptr;
+    }
+    auto bail = [&](int code) {
+        free_handle(h);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        return bail(fail(HCL_ERR_CUDA, "cudaStreamCreate failed"));
+    }
+    GridDev& g = h->g;
+    for (int d = 0; d < 3; ++d) {
+        if ((rc = upload(&h->dx_nodes[d], h->hx[d])) || (rc = upload(&h->ddx[d], h->hdx[d])) ||
+            (rc = upload(&h->dxc[d], h->hxc[d]))) {
+            return bail(rc);
+        }
+        g.x[d] = h->dx_nodes[d];
+        g.dx[d] = h->ddx[d];
+        g.xc[d] = h->dxc[d];
+    }
+    if ((rc = upload(&h->dds, h->hds)) || (rc = upload(&h->ddv, h->hdv)) || (rc = upload(&h->dgr, h->hgr)) ||
+        (rc = upload(&h->dcot, h->hcot)) || (rc = upload(&h->dsin1, h->hsin1)) ||
+        (rc = upload(&h->dsinxc1, h->hsinxc1))) {
+        return bail(rc);
+    }
+    g.ds = h->dds;
+    g.dv = h->ddv;
+    g.g_r = h->dgr;
+    g.cot_mid1 = h->dcot;
+    g.sin1 = h->dsin1;
+    g.sin_xc1 = h->dsinxc1;
+
+    const int nd = g.ndim;
+    const int nv = nd + 2;
+    if ((rc = dalloc(&h->red_bits, 4)) || (rc = dalloc(&h->red_flag, 4)) ||
+        (rc = dalloc(&h->red_partials,
+                     (size_t)std::max(2 * hcl::stage::integrate_blocks(), hcl::fused::conservation_partials_doubles(nd)))) ||
+        (rc = dalloc(&h->red_out, 16))) {
+        return bail(rc);
+    }
+    // fused state: nv planes of n2*n1*pitch doubles, pitch a multiple of 16
+    const int pitch = (g.n[0] + 15) / 16 * 16;
+    const int64_t plane = (int64_t)pitch * g.n[1] * g.n[2];
+    for (int b = 0; b < 2; ++b) {
+        if ((rc = dalloc(&h->state_mem[b], (size_t)plane * nv))) {
+            return bail(rc);
+        }
+        HCL_CUDA(cudaMemset(h->state_mem[b], 0, sizeof(double) * (size_t)plane * nv));
+        h->st[b].q = h->state_mem[b];
+        h->st[b].plane = plane;
+        h->st[b].pitch = pitch;
+    }
+    if ((rc = dalloc(&h->ctl, 1)) || (rc = dalloc(&h->ctl_tune, 1))) {
+        return bail(rc);
+    }
+    HCL_CUDA(cudaMemset(h->ctl, 0, sizeof(StepCtl)));
+    *out = h;
+    return HCL_OK;
+}
+
+int hcl_destroy(hcl_handle* h)
+{
+    if (h) {
+        cudaSetDevice(h->cfg.device);
+        cudaStreamSynchronize(h->stream);
+    }
+    free_handle(h);
+    return HCL_OK;
+}
+
+int hcl_get_extents(const hcl_handle* h, int n_wg[3], int64_t* ncells)
+{
+    if (!h) {
+        return fail(HCL_ERR_ARGUMENT, "null handle");
+    }
+    for (int d = 0; d < 3; ++d) {
+        if (n_wg) {
+            n_wg[d] = h->g.n[d];
+        }
+    }
+    if (ncells) {
+        *ncells = h->g.N;
+    }
+    return HCL_OK;
+}
+
+int hcl_get_interior(const hcl_handle* h, int nx[3], int* nghost)
+{
+    if (!h) {
+        return fail(HCL_ERR_ARGUMENT, "null handle");
+    }
+    for (int d = 0; d < 3; ++d) {
+        if (nx) {
+            nx[d] = h->g.nx[d];
+        }
+    }
+    if (nghost) {
+        *nghost = h->g.ng;
+    }
+    return HCL_OK;
+}
+
+int hcl_get_grid(const hcl_handle* h, double* x[3], double* dx[3], double* xc[3], double* ds, double* dv)
+{
+    if (!h) {
+        return fail(HCL_ERR_ARGUMENT, "null handle");
+    }
+    for (int d = 0; d < 3; ++d) {
+        if (x && x[d]) {
+            std::memcpy(x[d], h->hx[d].data(), sizeof(double) * h->hx[d].size());
+        }
+        if (dx && dx[d]) {
+            std::memcpy(dx[d], h->hdx[d].data(), sizeof(double) * h->hdx[d].size());
+        }
+        if (xc && xc[d]) {
+            std::memcpy(xc[d], h->hxc[d].data(), sizeof(double) * h->hxc[d].size());
+        }
+    }
+    if (ds) {
+        std::memcpy(ds, h->hds.data(), sizeof(double) * h->hds.size());
+    }
+    if (dv) {
+        std::memcpy(dv, h->hdv.data(), sizeof(double) * h->hdv.size());
+    }
+    return HCL_OK;
+}
+
+int hcl_get_grid_device(const hcl_handle* h, const double* dx[3], const double** ds, const double** dv)
+{
+    if (!h) {
+        return fail(HCL_ERR_ARGUMENT, "null handle");
+    }
+    for (int d = 0; d < 3; ++d) {
+        if (dx) {
+            dx[d] = h->ddx[d];
+        }
+    }
+    if (ds) {
+        *ds = h->dds;
+    }
+    if (dv) {
+        *dv = h->ddv;
+    }
+    return HCL_OK;
+}
+
+// ---- stage entry points ----------------------------------------------------
+#define HCL_CHECK_HANDLE(h)                              \
+    do {                                                 \
+        if (!(h)) {                                      \
+            return fail(HCL_ERR_ARGUMENT, "null handle"); \
+        }                                                \
+        HCL_CUDA(cudaSetDevice((h)->cfg.device));        \
+    } while (0)
+
+#define HCL_CHECK_NGEFF(h, ng_eff)                                                                    \
+    do {                                                                                             \
+        if ((ng_eff) < 0 || (ng_eff) > (h)->g.ng) {                                                  \
+            return fail(HCL_ERR_CONFIG, "NgEff > Ng"); /* range.cpp:370-372 */                        \
+        }                                                                                            \
+    } while (0)
+
+int hcl_conv_prim_to_cons(hcl_handle* h, int ng_eff, const double* rho, const double* u, const double* P,
+                          double* rhou, double* E, void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    HCL_CHECK_NGEFF(h, ng_eff);
+    if (!rho || !u || !P || !rhou || !E) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    hcl::stage::conv_prim_to_cons(h->g, ng_eff, rho, u, P, rhou, E, pick(h, stream));
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
+int hcl_conv_cons_to_prim(hcl_handle* h, int ng_eff, const double* rho, const double* rhou, const double* E,
+                          double* u, double* P, void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    HCL_CHECK_NGEFF(h, ng_eff);
+    if (!rho || !u || !P || !rhou || !E) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    hcl::stage::conv_cons_to_prim(h->g, ng_eff, rho, rhou, E, u, P, pick(h, stream));
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
+int hcl_face_reconstruction(hcl_handle* h, int ng_eff, const double* var, double* var_rec, void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    HCL_CHECK_NGEFF(h, ng_eff);
+    if (ng_eff > h->g.ng - 1) {
+        return fail(HCL_ERR_CONFIG, "face reconstruction needs one ghost layer beyond the range");
+    }
+    if (!var || !var_rec) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    hcl::stage::face_reconstruction(h->g, ng_eff, var, var_rec, pick(h, stream));
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
+int hcl_hydro_reconstruction(hcl_handle* h, int ng_eff, double dt, const double* rho, const double* u,
+                             const double* P, const double* fx, double* rho_rec, double* rhou_rec, double* E_rec,
+                             double* fx_rec, double* u_rec, double* P_rec, void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    HCL_CHECK_NGEFF(h, ng_eff);
+    if (ng_eff > h->g.ng - 1) {
+        return fail(HCL_ERR_CONFIG, "reconstruction needs one ghost layer beyond the range");
+    }
+    if (!rho || !u || !P || !rho_rec || !rhou_rec || !E_rec) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    if (h->g.nfx > 0 && (!fx || !fx_rec)) {
+        return fail(HCL_ERR_ARGUMENT, "nfx > 0 needs fx and fx_rec");
+    }
+    const int nd = h->g.ndim;
+    const size_t N = (size_t)h->g.N;
+    int rc;
+    if (!u_rec) {
+        if (!h->u_rec && (rc = dalloc(&h->u_rec, N * 2 * nd * nd))) {
+            return rc;
+        }
+        u_rec = h->u_rec;
+    }
+    if (!P_rec) {
+        if (!h->P_rec && (rc = dalloc(&h->P_rec, N * 2 * nd))) {
+            return rc;
+        }
+        P_rec = h->P_rec;
+    }
+    if (h->g.nfx > 0 && !h->fx_rec_old && (rc = dalloc(&h->fx_rec_old, N * 2 * nd * h->g.nfx))) {
+        return rc;
+    }
+    hcl::stage::hydro_reconstruction(h->g, ng_eff, dt, rho, u, P, fx, rho_rec, rhou_rec, E_rec, fx_rec, u_rec, P_rec,
+                                     h->fx_rec_old, pick(h, stream));
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
+int hcl_godunov_scheme(hcl_handle* h, int ng_eff, double dt, const double* rho, const double* rhou,
+                       const double* E, const double* fx, const double* rho_rec, const double* rhou_rec,
+                       const double* E_rec, const double* fx_rec, double* rho_new, double* rhou_new, double* E_new,
+                       double* fx_new, void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    HCL_CHECK_NGEFF(h, ng_eff);
+    if (ng_eff > h->g.ng - 2 + 0 && ng_eff > 0) {
+        return fail(HCL_ERR_CONFIG, "the Godunov update reads face states one cell beyond the range");
+    }
+    if (!rho || !rhou || !E || !rho_rec || !rhou_rec || !E_rec || !rho_new || !rhou_new || !E_new) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    if (h->g.nfx > 0 && (!fx || !fx_rec || !fx_new)) {
+        return fail(HCL_ERR_ARGUMENT, "nfx > 0 needs fx, fx_rec and fx_new");
+    }
+    hcl::stage::godunov(h->g, ng_eff, dt, rho, rhou, E, fx, rho_rec, rhou_rec, E_rec, fx_rec, rho_new, rhou_new, E_new,
+                        fx_new, pick(h, stream));
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
+int hcl_boundary_conditions(hcl_handle* h, double* rho, double* rhou, double* E, double* fx, void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!rho || !rhou || !E || (h->g.nfx > 0 && !fx)) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    hcl::stage::boundaries(h->g, rho, rhou, E, fx, pick(h, stream));
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
+int hcl_time_step(hcl_handle* h, int ng_eff, const double* rho, const double* u, const double* P, double* dt_out,
+                  void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    HCL_CHECK_NGEFF(h, ng_eff);
+    if (!rho || !u || !P || !dt_out) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    cudaStream_t s = pick(h, stream);
+    HCL_CUDA(cudaMemsetAsync(h->red_bits, 0, sizeof(unsigned long long), s));
+    hcl::stage::time_step_inv(h->g, ng_eff, rho, u, P, h->red_bits, s);
+    HCL_LAUNCH_CHECK();
+    unsigned long long bits = 0;
+    HCL_CUDA(cudaMemcpyAsync(&bits, h->red_bits, sizeof(bits), cudaMemcpyDeviceToHost, s));
+    HCL_CUDA(cudaStreamSynchronize(s));
+    double inv;
+    std::memcpy(&inv, &bits, sizeof(inv));
+    *dt_out = 1 / inv; // time_step.hpp:82
+    return HCL_OK;
+}
+
+int hcl_minimum_internal_energy(hcl_handle* h, const double* rho, const double* rhou, const double* E, double* out,
+                                void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!rho || !rhou || !E || !out) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    cudaStream_t s = pick(h, stream);
+    HCL_CUDA(cudaMemsetAsync(h->red_bits, 0xff, sizeof(unsigned long long), s));
+    HCL_CUDA(cudaMemsetAsync(h->red_flag, 0, sizeof(int), s));
+    hcl::stage::min_internal_energy(h->g, rho, rhou, E, h->red_bits, h->red_flag, s);
+    HCL_LAUNCH_CHECK();
+    unsigned long long key = 0;
+    int nanf = 0;
+    HCL_CUDA(cudaMemcpyAsync(&key, h->red_bits, sizeof(key), cudaMemcpyDeviceToHost, s));
+    HCL_CUDA(cudaMemcpyAsync(&nanf, h->red_flag, sizeof(nanf), cudaMemcpyDeviceToHost, s));
+    HCL_CUDA(cudaStreamSynchronize(s));
+    *out = nanf ? NAN : hcl::stage::decode_min_key(key);
+    return HCL_OK;
+}
+
+int hcl_integrate(hcl_handle* h, const double* var, double* out, void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!var || !out) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    cudaStream_t s = pick(h, stream);
+    hcl::stage::integrate(h->g, var, h->red_partials, h->red_out, s);
+    HCL_LAUNCH_CHECK();
+    double res[2];
+    HCL_CUDA(cudaMemcpyAsync(res, h->red_out, sizeof(res), cudaMemcpyDeviceToHost, s));
+    HCL_CUDA(cudaStreamSynchronize(s));
+    *out = res[0];
+    return HCL_OK;
+}
+
+// ---- handle-owned state ----------------------------------------------------
+int hcl_set_state(hcl_handle* h, const double* rho, const double* rhou, const double* E, const double* fx,
+                  int memory)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!rho || !rhou || !E) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    if (h->g.nfx > 0) {
+        return fail(HCL_ERR_CONFIG, "the fused path does not carry passive scalars (nfx > 0); use the stage entry points");
+    }
+    (void)fx;
+    const cudaMemcpyKind kind = memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    hcl::fused::pack_state(h->g, h->st[0], rho, rhou, E, kind, h->stream);
+    HCL_CUDA(cudaGetLastError());
+    h->cur = 0;
+    h->state_valid = 1;
+    return restart_clock(h, 0.0, 0);
+}
+
+int hcl_get_state(hcl_handle* h, double* rho, double* rhou, double* E, double* fx, int memory)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!rho || !rhou || !E) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    (void)fx;
+    if (!h->state_valid) {
+        return fail(HCL_ERR_CONFIG, "no state set");
+    }
+    const cudaMemcpyKind kind = memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    hcl::fused::unpack_state(h->g, h->st[h->cur], rho, rhou, E, kind, h->stream);
+    HCL_CUDA(cudaGetLastError());
+    HCL_CUDA(cudaStreamSynchronize(h->stream));
+    return HCL_OK;
+}
+
+int hcl_set_state_from_prim(hcl_handle* h, const double* rho, const double* u, const double* P, const double* fx)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!rho || !u || !P) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    if (h->g.nfx > 0) {
+        return fail(HCL_ERR_CONFIG, "the fused path does not carry passive scalars (nfx > 0)");
+    }
+    (void)fx;
+    const int nd = h->g.ndim;
+    const size_t N = (size_t)h->g.N;
+    double *d_rho = nullptr, *d_u = nullptr, *d_P = nullptr, *d_m = nullptr, *d_E = nullptr;
+    int rc;
+    if ((rc = dalloc(&d_rho, N)) || (rc = dalloc(&d_u, N * nd)) || (rc = dalloc(&d_P, N)) ||
+        (rc = dalloc(&d_m, N * nd)) || (rc = dalloc(&d_E, N))) {
+        cudaFree(d_rho);
+        cudaFree(d_u);
+        cudaFree(d_P);
+        cudaFree(d_m);
+        cudaFree(d_E);
+        return rc;
+    }
+    cudaStream_t s = h->stream;
+    cudaMemcpyAsync(d_rho, rho, sizeof(double) * N, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_u, u, sizeof(double) * N * nd, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_P, P, sizeof(double) * N, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(d_m, 0, sizeof(double) * N * nd, s);
+    cudaMemsetAsync(d_E, 0, sizeof(double) * N, s);
+    // main.cpp:305-307: conv_prim_to_cons(no_ghosts) then the boundaries
+    hcl::stage::conv_prim_to_cons(h->g, 0, d_rho, d_u, d_P, d_m, d_E, s);
+    hcl::stage::boundaries(h->g, d_rho, d_m, d_E, nullptr, s);
+    hcl::fused::pack_state(h->g, h->st[0], d_rho, d_m, d_E, cudaMemcpyDeviceToDevice, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    cudaFree(d_rho);
+    cudaFree(d_u);
+    cudaFree(d_P);
+    cudaFree(d_m);
+    cudaFree(d_E);
+    if (e != cudaSuccess) {
+        return fail(HCL_ERR_CUDA, "initial state: %s", cudaGetErrorString(e));
+    }
+    h->cur = 0;
+    h->state_valid = 1;
+    return restart_clock(h, 0.0, 0);
+}
+
+int hcl_reset_clock(hcl_handle* h, double t_ini)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!h->state_valid) {
+        return fail(HCL_ERR_CONFIG, "no state set");
+    }
+    return restart_clock(h, t_ini, 0);
+}
+
+int hcl_run(hcl_handle* h, const hcl_run_params* p, hcl_run_result* r)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!p) {
+        return fail(HCL_ERR_ARGUMENT, "null run parameters");
+    }
+    if (!h->state_valid) {
+        return fail(HCL_ERR_CONFIG, "no state set");
+    }
+    int rc;
+    StepCtl ctl;
+    if (h->stopped) {
+        // resume after a finished run: carry t and iteration over
+        if ((rc = read_ctl(h, &ctl))) {
+            return rc;
+        }
+        if (ctl.err) {
+            return fail(HCL_ERR_INVALID_STATE, "the state is invalid; set a new state");
+        }
+        if ((rc = restart_clock(h, ctl.t[h->counter & 1], ctl.iter[h->counter & 1]))) {
+            return rc;
+        }
+    }
+    if (h->cfg.precision == HCL_FP32_MIXED && h->mixed_shape < 0) {
+        if ((rc = autotune_mixed(h))) {
+            return rc;
+        }
+    }
+    RunParamsDev rp;
+    std::memset(&rp, 0, sizeof(rp));
+    rp.cfl = p->cfl;
+    rp.t_end = p->t_end;
+    rp.max_iter = p->max_iter;
+    rp.iter_frequency = p->iter_frequency;
+    rp.time_frequency = p->time_frequency;
+    rp.time_first_output = p->time_first_output;
+    rp.fixed_dt = p->fixed_dt ? 1 : 0;
+    const int nsteps = p->nsteps;
+    if ((rc = read_ctl(h, &ctl))) {
+        return rc;
+    }
+    const int iter_now = ctl.iter[h->counter & 1];
+    const int horizon = nsteps > 0 ? iter_now + nsteps : std::min(p->max_iter, iter_now + (1 << 20));
+    if ((rc = ensure_dt_log(h, horizon + 8))) {
+        return rc;
+    }
+    rp.dt_log = h->dt_log;
+    rp.dt_log_cap = h->dt_log_cap;
+    if (p->fixed_dt) {
+        if (!p->dts || nsteps <= 0) {
+            return fail(HCL_ERR_ARGUMENT, "fixed_dt needs dts and nsteps > 0");
+        }
+        if (h->d_dts_cap < horizon + 8) {
+            cudaFree(h->d_dts);
+            h->d_dts = nullptr;
+            h->d_dts_cap = 0;
+            if ((rc = dalloc(&h->d_dts, (size_t)horizon + 8))) {
+                return rc;
+            }
+            h->d_dts_cap = horizon + 8;
+        }
+        HCL_CUDA(cudaMemsetAsync(h->d_dts, 0, sizeof(double) * h->d_dts_cap, h->stream));
+        HCL_CUDA(cudaMemcpyAsync(h->d_dts + iter_now, p->dts, sizeof(double) * nsteps, cudaMemcpyHostToDevice,
+                                 h->stream));
+        rp.dts = h->d_dts;
+    }
+    const int K = p->graph_chunk > 0 ? (p->graph_chunk + 5) / 6 * 6 : 60;
+    const int shape = h->mixed_shape < 0 ? 0 : h->mixed_shape;
+
+    auto single = [&]() {
+        launch_step(h, rp, h->counter, h->ctl, (int)(h->counter & 1), shape, h->stream);
+        ++h->counter;
+    };
+    int done = 0;
+    bool finished = false;
+    while (!finished) {
+        // align to the graph's slot phase with single launches
+        while (h->counter % 6 != 0 && (nsteps <= 0 || done < nsteps)) {
+            single();
+            ++done;
+        }
+        const int remaining = nsteps > 0 ? nsteps - done : K;
+        if (remaining >= K) {
+            cudaGraphExec_t exec;
+            if ((rc = get_graph(h, rp, K, &exec))) {
+                return rc;
+            }
+            HCL_CUDA(cudaGraphLaunch(exec, h->stream));
+            hcl::g_launches += K;
+            h->counter += K;
+            done += K;
+        } else {
+            while (done < nsteps) {
+                single();
+                ++done;
+            }
+        }
+        HCL_LAUNCH_CHECK();
+        if (nsteps > 0) {
+            finished = done >= nsteps;
+        } else {
+            if ((rc = read_ctl(h, &ctl))) {
+                return rc;
+            }
+            finished = ctl.stop[h->counter & 1] || ctl.errflag[h->counter & 1] || ctl.err;
+        }
+    }
+    if ((rc = read_ctl(h, &ctl))) {
+        return rc;
+    }
+    const int q = (int)(h->counter & 1);
+    const bool stop = ctl.stop[q] || ctl.err;
+    h->cur = stop ? ctl.final_buf : q;
+    h->stopped = stop ? 1 : 0;
+    if (r) {
+        r->t = ctl.t[q];
+        r->iter = ctl.iter[q];
+        r->status = ctl.err;
+        r->bad_cell = ctl.bad_cell == ~0ull ? -1 : (int64_t)ctl.bad_cell;
+        r->finished = ctl.stop[q] ? 1 : 0;
+        r->last_dt = ctl.last_dt;
+    }
+    if (ctl.err == HCL_ERR_INVALID_STATE) {
+        return fail(HCL_ERR_INVALID_STATE, "detected invalid volumic internal energy at cell %lld",
+                    (long long)(ctl.bad_cell == ~0ull ? -1 : (long long)ctl.bad_cell));
+    }
+    if (ctl.err == HCL_ERR_NEGATIVE_DT) {
+        return fail(HCL_ERR_NEGATIVE_DT, "Error: the time step is negative");
+    }
+    return HCL_OK;
+}
+
+int hcl_step_fixed_dt(hcl_handle* h, double dt, void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!h->state_valid) {
+        return fail(HCL_ERR_CONFIG, "no state set");
+    }
+    if (h->stopped) {
+        StepCtl ctl;
+        int rc = read_ctl(h, &ctl);
+        if (rc) {
+            return rc;
+        }
+        if ((rc = restart_clock(h, ctl.t[h->counter & 1], ctl.iter[h->counter & 1]))) {
+            return rc;
+        }
+    }
+    if (h->cfg.precision == HCL_FP32_MIXED && h->mixed_shape < 0) {
+        int rc = autotune_mixed(h);
+        if (rc) {
+            return rc;
+        }
+    }
+    RunParamsDev rp;
+    std::memset(&rp, 0, sizeof(rp));
+    rp.cfl = 0.4;
+    rp.t_end = 1e300;
+    rp.max_iter = INT_MAX;
+    rp.fixed_dt = 2;
+    rp.dt_value = dt;
+    cudaStream_t s = pick(h, stream);
+    launch_step(h, rp, h->counter, h->ctl, (int)(h->counter & 1), h->mixed_shape < 0 ? 0 : h->mixed_shape, s);
+    ++h->counter;
+    h->cur = (int)(h->counter & 1);
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
+int hcl_get_dt_log(hcl_handle* h, double* dts, int max_count, int* count)
+{
+    HCL_CHECK_HANDLE(h);
+    StepCtl ctl;
+    int rc = read_ctl(h, &ctl);
+    if (rc) {
+        return rc;
+    }
+    const int n = std::min(max_count, std::min(ctl.iter[h->counter & 1], h->dt_log_cap));
+    if (n > 0 && dts) {
+        HCL_CUDA(cudaMemcpy(dts, h->dt_log, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    }
+    if (count) {
+        *count = n;
+    }
+    return HCL_OK;
+}
+
+int hcl_conservation_sums(hcl_handle* h, double* out)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!out) {
+        return fail(HCL_ERR_ARGUMENT, "null output");
+    }
+    if (!h->state_valid) {
+        return fail(HCL_ERR_CONFIG, "no state set");
+    }
+    hcl::fused::conservation_sums(h->g, h->st[h->cur], h->red_partials, h->red_out, h->stream);
+    HCL_LAUNCH_CHECK();
+    HCL_CUDA(cudaMemcpyAsync(out, h->red_out, sizeof(double) * (h->g.ndim + 2), cudaMemcpyDeviceToHost, h->stream));
+    HCL_CUDA(cudaStreamSynchronize(h->stream));
+    return HCL_OK;
+}
+
+} // extern "C"

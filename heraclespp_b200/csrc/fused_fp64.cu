@@ -1,0 +1,283 @@
+// fused_fp64.cu -- the FP64 fused step with the reference's arithmetic
+// (compiled with --fmad=false), plus the pieces of the fused path that must
+// round like the reference: the prologue CFL reduction of the initial state,
+// state packing and the compensated conservation sums.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fused_step.cuh"
+#include "physics_exact.cuh"
+#include "stages.hpp"
+
+namespace hcl::fused {
+
+void step_exact(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                int slot, int out_buf, cudaStream_t s)
+{
+    switch (g.ndim) {
+    case 1:
+        FusedLauncher<1, true, 128, 1, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        break;
+    case 2:
+        FusedLauncher<2, true, 16, 16, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        break;
+    default:
+        FusedLauncher<3, true, 8, 4, 4>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        break;
+    }
+}
+
+void configure_exact()
+{
+    FusedLauncher<1, true, 128, 1, 1>::configure();
+    FusedLauncher<2, true, 16, 16, 1>::configure();
+    FusedLauncher<3, true, 8, 4, 4>::configure();
+}
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kRedBlocks = 296;
+
+__device__ __forceinline__ void two_sum_acc(double& s, double& e, double v)
+{
+    const double t = s + v;
+    const double bp = t - s;
+    e += (s - (t - bp)) + (v - bp);
+    s = t;
+}
+
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+// time_step.hpp:55-77 over all_ghosts of the fused state, and the
+// minimum_internal_energy check of main.cpp:397-425 over no_ghosts.
+template <int ND>
+__global__ void k_prologue(GridDev g, StateDev st, StepCtl* ctl)
+{
+    const exact::Eos eos{g.gamma, g.gamma_m1, g.mmw};
+    double local = 0;
+    bool nan_seen = false;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < g.N; c += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % g.n[0]);
+        const int64_t r = c / g.n[0];
+        const int j = (int)(r % g.n[1]);
+        const int k = (int)(r / g.n[1]);
+        const int64_t o = (int64_t)i + (int64_t)st.pitch * ((int64_t)j + (int64_t)g.n[1] * k);
+        double q[ND + 2], p[ND + 2];
+#pragma unroll
+        for (int v = 0; v < ND + 2; ++v) {
+            q[v] = st.q[o + st.plane * v];
+        }
+        exact::to_prim<ND>(eos, q, p);
+        const double sound = exact::sound(eos, p[0], p[1 + ND]);
+        double dxg[3] = {g.dx[0][i], g.dx[1][j], g.dx[2][k]};
+        if (g.geom == GEOM_SPHERICAL) {
+            if (ND == 2) {
+                dxg[1] *= g.xc[0][i];
+            }
+            if (ND == 3) {
+                dxg[1] *= g.xc[0][i];
+                dxg[2] *= g.xc[0][i] * g.sin_xc1[j];
+            }
+        }
+        double cell = 0;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            cell += (fabs(p[1 + d]) + sound) / dxg[d];
+        }
+        nan_seen |= isnan(cell);
+        local = local > cell ? local : cell;
+        bool interior = true;
+        const int idx[3] = {i, j, k};
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            interior &= idx[d] >= g.ng && idx[d] < g.n[d] - g.ng;
+        }
+        if (interior) {
+            const double evol = q[1 + ND] - exact::ek_cons<ND>(q);
+            if (!(evol >= 0.0)) {
+                atomicMin(&ctl->bad_cell, (unsigned long long)lidx(g, i, j, k));
+                ctl->err = 4;
+                ctl->errflag[0] = 1;
+                ctl->final_buf = 0;
+            }
+        }
+    }
+    local = warp_max(local);
+    __shared__ double red[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[w] = local;
+    }
+    __syncthreads();
+    if (w == 0) {
+        local = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+        local = warp_max(local);
+        if (lane == 0) {
+            atomicMax(&ctl->inv_dt_bits[0], dbl_bits(local));
+        }
+    }
+    if (nan_seen) {
+        atomicMax(&ctl->inv_dt_bits[0], 0x7ff8000000000000ull);
+    }
+}
+
+__global__ void k_ctl_init(StepCtl* ctl, double t_ini, int iter0)
+{
+    ctl->inv_dt_bits[0] = 0ull;
+    ctl->inv_dt_bits[1] = 0ull;
+    ctl->inv_dt_bits[2] = 0ull;
+    ctl->t[0] = ctl->t[1] = t_ini;
+    ctl->iter[0] = ctl->iter[1] = iter0;
+    // an initial output bumps both ids (main.cpp:315-316, 207-209): the
+    // loop starts with iter_output_id = time_output_id = -1 and the host
+    // adjusts them through hcl_run's parameters
+    ctl->time_output_id[0] = ctl->time_output_id[1] = -1;
+    ctl->iter_output_id[0] = ctl->iter_output_id[1] = -1;
+    ctl->stop[0] = ctl->stop[1] = 0;
+    ctl->errflag[0] = ctl->errflag[1] = 0;
+    ctl->final_buf = 0;
+    ctl->err = 0;
+    ctl->bad_cell = ~0ull;
+    ctl->last_dt = 0.0;
+}
+
+template <int ND>
+__global__ void k_cons_partial(GridDev g, StateDev st, double* partials)
+{
+    constexpr int NV = ND + 2;
+    double s[NV], e[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        s[v] = 0;
+        e[v] = 0;
+    }
+    const int w0 = g.nx[0], w1 = g.nx[1];
+    const int64_t count = (int64_t)g.nx[0] * g.nx[1] * g.nx[2];
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < count;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (ND >= 1 ? g.ng : 0) + (int)(idx % w0);
+        const int64_t r = idx / w0;
+        const int j = (ND >= 2 ? g.ng : 0) + (int)(r % w1);
+        const int k = (ND >= 3 ? g.ng : 0) + (int)(r / w1);
+        const int64_t o = (int64_t)i + (int64_t)st.pitch * ((int64_t)j + (int64_t)g.n[1] * k);
+        const double dv = g.dv[lidx(g, i, j, k)];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            two_sum_acc(s[v], e[v], st.q[o + st.plane * v] * dv);
+        }
+    }
+    __shared__ double ss[NV][kThreads];
+    __shared__ double se[NV][kThreads];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        ss[v][threadIdx.x] = s[v];
+        se[v][threadIdx.x] = e[v];
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        const int v = threadIdx.x;
+        double S = 0, Ec = 0;
+        for (int t = 0; t < (int)blockDim.x; ++t) {
+            two_sum_acc(S, Ec, ss[v][t]);
+            Ec += se[v][t];
+        }
+        partials[(2 * blockIdx.x) * NV + v] = S;
+        partials[(2 * blockIdx.x + 1) * NV + v] = Ec;
+    }
+}
+
+__global__ void k_cons_final(const double* partials, int nblocks, int nv, double* out)
+{
+    const int v = threadIdx.x;
+    if (v < nv) {
+        double S = 0, Ec = 0;
+        for (int b = 0; b < nblocks; ++b) {
+            two_sum_acc(S, Ec, partials[(2 * b) * nv + v]);
+            Ec += partials[(2 * b + 1) * nv + v];
+        }
+        out[v] = S + Ec;
+    }
+}
+
+} // namespace
+
+void prologue(const GridDev& g, const StateDev& st, StepCtl* ctl, double t_ini, int iter0, cudaStream_t s)
+{
+    k_ctl_init<<<1, 1, 0, s>>>(ctl, t_ini, iter0);
+    int blocks = (int)((g.N + kThreads - 1) / kThreads);
+    if (blocks > 148 * 8) {
+        blocks = 148 * 8;
+    }
+    switch (g.ndim) {
+    case 1:
+        k_prologue<1><<<blocks, kThreads, 0, s>>>(g, st, ctl);
+        break;
+    case 2:
+        k_prologue<2><<<blocks, kThreads, 0, s>>>(g, st, ctl);
+        break;
+    default:
+        k_prologue<3><<<blocks, kThreads, 0, s>>>(g, st, ctl);
+        break;
+    }
+    g_launches += 2;
+}
+
+void conservation_sums(const GridDev& g, const StateDev& st, double* partials, double* out_dev, cudaStream_t s)
+{
+    const int nv = g.ndim + 2;
+    switch (g.ndim) {
+    case 1:
+        k_cons_partial<1><<<kRedBlocks, kThreads, 0, s>>>(g, st, partials);
+        break;
+    case 2:
+        k_cons_partial<2><<<kRedBlocks, kThreads, 0, s>>>(g, st, partials);
+        break;
+    default:
+        k_cons_partial<3><<<kRedBlocks, kThreads, 0, s>>>(g, st, partials);
+        break;
+    }
+    k_cons_final<<<1, 32, 0, s>>>(partials, kRedBlocks, nv, out_dev);
+    g_launches += 2;
+}
+
+int conservation_partials_doubles(int ndim)
+{
+    return 2 * kRedBlocks * (ndim + 2);
+}
+
+void pack_state(const GridDev& g, const StateDev& st, const double* rho, const double* rhou, const double* E,
+                cudaMemcpyKind kind, cudaStream_t s)
+{
+    const size_t w = sizeof(double) * (size_t)g.n[0];
+    const size_t rows = (size_t)g.n[1] * g.n[2];
+    const size_t dp = sizeof(double) * (size_t)st.pitch;
+    cudaMemcpy2DAsync(st.q, dp, rho, w, w, rows, kind, s);
+    for (int d = 0; d < g.ndim; ++d) {
+        cudaMemcpy2DAsync(st.q + st.plane * (1 + d), dp, rhou + g.N * d, w, w, rows, kind, s);
+    }
+    cudaMemcpy2DAsync(st.q + st.plane * (1 + g.ndim), dp, E, w, w, rows, kind, s);
+}
+
+void unpack_state(const GridDev& g, const StateDev& st, double* rho, double* rhou, double* E, cudaMemcpyKind kind,
+                  cudaStream_t s)
+{
+    const size_t w = sizeof(double) * (size_t)g.n[0];
+    const size_t rows = (size_t)g.n[1] * g.n[2];
+    const size_t dp = sizeof(double) * (size_t)st.pitch;
+    cudaMemcpy2DAsync(rho, w, st.q, dp, w, rows, kind, s);
+    for (int d = 0; d < g.ndim; ++d) {
+        cudaMemcpy2DAsync(rhou + g.N * d, w, st.q + st.plane * (1 + d), dp, w, rows, kind, s);
+    }
+    cudaMemcpy2DAsync(E, w, st.q + st.plane * (1 + g.ndim), dp, w, rows, kind, s);
+}
+
+} // namespace hcl::fused

@@ -1,0 +1,49 @@
+// fused_mixed.cu -- the FP32-mixed fused step (compiled with FMA contraction,
+// -ftz=true -prec-div=false -prec-sqrt=false): FP32 primitives, slopes,
+// face states and fluxes; FP64 stored state, internal-energy recovery,
+// update accumulation and dt.
+#include <cuda_runtime.h>
+
+#include "fused_step.cuh"
+#include "stages.hpp"
+
+namespace hcl::fused {
+
+// Tile shapes selectable at run time for 2-D (the autotuner picks one).
+int mixed_shape_count(int ndim)
+{
+    return ndim == 2 ? 3 : 1;
+}
+
+void configure_mixed()
+{
+    FusedLauncher<1, false, 256, 1, 1>::configure();
+    FusedLauncher<2, false, 16, 16, 1>::configure();
+    FusedLauncher<2, false, 32, 8, 1>::configure();
+    FusedLauncher<2, false, 32, 16, 1>::configure();
+    FusedLauncher<3, false, 8, 8, 4>::configure();
+}
+
+void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                int slot, int out_buf, int shape, cudaStream_t s)
+{
+    switch (g.ndim) {
+    case 1:
+        FusedLauncher<1, false, 256, 1, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        break;
+    case 2:
+        if (shape == 1) {
+            FusedLauncher<2, false, 32, 8, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        } else if (shape == 2) {
+            FusedLauncher<2, false, 32, 16, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        } else {
+            FusedLauncher<2, false, 16, 16, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        }
+        break;
+    default:
+        FusedLauncher<3, false, 8, 8, 4>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        break;
+    }
+}
+
+} // namespace hcl::fused

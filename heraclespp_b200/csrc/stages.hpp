@@ -1,0 +1,84 @@
+// stages.hpp -- host-side launchers of the stage kernels and of the fused
+// step, shared between the translation units of the library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+
+#include "hcl_device.cuh"
+
+namespace hcl {
+
+// Count of kernel launches issued by this library (reported by
+// hcl_kernel_launch_count()).
+extern std::atomic<int64_t> g_launches;
+
+namespace stage {
+
+void conv_prim_to_cons(const GridDev& g, int ng_eff, const double* rho, const double* u, const double* P,
+                       double* rhou, double* E, cudaStream_t s);
+void conv_cons_to_prim(const GridDev& g, int ng_eff, const double* rho, const double* rhou, const double* E,
+                       double* u, double* P, cudaStream_t s);
+void face_reconstruction(const GridDev& g, int ng_eff, const double* var, double* var_rec, cudaStream_t s);
+void hydro_reconstruction(const GridDev& g, int ng_eff, double dt, const double* rho, const double* u,
+                          const double* P, const double* fx, double* rho_rec, double* rhou_rec, double* E_rec,
+                          double* fx_rec, double* u_rec, double* P_rec, double* fx_rec_old, cudaStream_t s);
+void godunov(const GridDev& g, int ng_eff, double dt, const double* rho, const double* rhou, const double* E,
+             const double* fx, const double* rho_rec, const double* rhou_rec, const double* E_rec,
+             const double* fx_rec, double* rho_new, double* rhou_new, double* E_new, double* fx_new,
+             cudaStream_t s);
+void boundaries(const GridDev& g, double* rho, double* rhou, double* E, double* fx, cudaStream_t s);
+// writes the bits of max_cells(sum_d (|u_d|+c)/dx_d) into *inv_bits (device),
+// which must hold 0 before the call
+void time_step_inv(const GridDev& g, int ng_eff, const double* rho, const double* u, const double* P,
+                   unsigned long long* inv_bits, cudaStream_t s);
+// min over interior cells of E - ek; *key must hold ~0ull, *nan_flag 0
+void min_internal_energy(const GridDev& g, const double* rho, const double* rhou, const double* E,
+                         unsigned long long* key, int* nan_flag, cudaStream_t s);
+double decode_min_key(unsigned long long key);
+// compensated sum of var*dv over the interior: partials must hold
+// 2*integrate_blocks() doubles; result (sum, compensation) in out[0..1]
+int integrate_blocks();
+void integrate(const GridDev& g, const double* var, double* partials, double* out, cudaStream_t s);
+
+} // namespace stage
+
+namespace fused {
+
+// State buffers of the fused path: nvar planes, each n2*n1*pitch doubles with
+// the x0 row padded to `pitch` (a multiple of 16 doubles).
+struct StateDev {
+    double* q;        // base of plane 0
+    int64_t plane;    // doubles per plane
+    int pitch;        // doubles per x0 row
+};
+
+// Computes 1/dt of the current state into ctl->inv_dt_bits[0], clears the
+// other slots, sets t, iteration counters and flags for step 0.
+void prologue(const GridDev& g, const StateDev& st, StepCtl* ctl, double t_ini, int iter0, cudaStream_t s);
+
+// One fused step.  `slot` is the step counter modulo 6 (selects the control
+// slots); out_buf is the index of the output state buffer.
+void step_exact(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                int slot, int out_buf, cudaStream_t s);
+void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                int slot, int out_buf, int shape, cudaStream_t s);
+int mixed_shape_count(int ndim);
+void configure_exact();
+void configure_mixed();
+int conservation_partials_doubles(int ndim);
+
+// Copies between the reference layout (contiguous LayoutLeft) and StateDev.
+void pack_state(const GridDev& g, const StateDev& st, const double* rho, const double* rhou, const double* E,
+                cudaMemcpyKind kind, cudaStream_t s);
+void unpack_state(const GridDev& g, const StateDev& st, double* rho, double* rhou, double* E, cudaMemcpyKind kind,
+                  cudaStream_t s);
+
+// Compensated conservation sums of the fused state: out[0..ndim+1].
+void conservation_sums(const GridDev& g, const StateDev& st, double* partials, double* out_dev, cudaStream_t s);
+
+} // namespace fused
+
+} // namespace hcl

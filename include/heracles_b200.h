@@ -1,0 +1,261 @@
+/*
+ * heracles_b200.h -- C ABI of the B200-native MUSCL-Hancock step.
+ *
+ * One shared library (libheracles_b200.so) exports these entry points.  They
+ * take plain pointers, sizes and enums; no C++ or torch types cross the ABI.
+ * Every call returns an int status (HCL_OK = 0) and never throws; the message
+ * of the last failure on the calling thread is hcl_last_error().
+ *
+ * Arrays follow the reference's Kokkos::LayoutLeft Views exactly
+ * (src/utils/kokkos_shortcut.hpp:22-41): x0 index fastest, trailing component
+ * indices slowest, extents including Nghost ghost cells on active dimensions
+ * (src/mesh/grid.cpp:56-58,119).  With N = n0*n1*n2:
+ *   rho(i,j,k)             rho[c],   c = i + n0*(j + n1*k)
+ *   rhou(i,j,k,d)          rhou[c + N*d]
+ *   var_rec(i,j,k,s,d)     rec[c + N*(s + 2*d)]
+ *   rhou_rec(i,j,k,s,d,r)  rec[c + N*(s + 2*(d + ndim*r))]
+ *
+ * The stage entry points (hcl_conv_*, hcl_face_reconstruction,
+ * hcl_hydro_reconstruction, hcl_godunov_scheme, hcl_boundary_conditions,
+ * hcl_time_step, ...) operate on caller-owned DEVICE arrays in that layout, so
+ * each one can replace one plugin of the reference's time loop
+ * (src/main.cpp:354-531).  The fused entry points (hcl_run, hcl_step, ...)
+ * operate on a state owned by the handle and are the fast path.
+ *
+ * Reference citations are path:line inside the HERACLES++ project.
+ */
+#ifndef HERACLES_B200_H
+#define HERACLES_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HCL_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum hcl_status {
+    HCL_OK = 0,
+    HCL_ERR_CONFIG = 1,        /* invalid configuration (maps to std::runtime_error) */
+    HCL_ERR_DOMAIN = 2,        /* invalid EOS parameter (maps to std::domain_error, perfect_gas.cpp:15-21) */
+    HCL_ERR_CUDA = 3,          /* CUDA runtime error */
+    HCL_ERR_INVALID_STATE = 4, /* NaN or negative internal energy (main.cpp:397-425) */
+    HCL_ERR_NEGATIVE_DT = 5,   /* main.cpp:368-371 */
+    HCL_ERR_TIMEOUT = 6,       /* a device-side wait gave up (bounded spin) */
+    HCL_ERR_NO_DEVICE = 7,     /* no CUDA device / library built without the device code */
+    HCL_ERR_ARGUMENT = 8       /* null pointer, wrong size, unknown name */
+};
+
+/* ---- enumerations (factory keys of the reference) ----------------------- */
+enum hcl_limiter {             /* hydro/face_reconstruction.cpp:31-50 */
+    HCL_LIMITER_CONSTANT = 0,
+    HCL_LIMITER_VANLEER = 1,
+    HCL_LIMITER_MINMOD = 2,
+    HCL_LIMITER_VANALBADA = 3
+};
+enum hcl_riemann {             /* hydro/godunov_scheme.hpp:305-321 */
+    HCL_RIEMANN_HLL = 0,
+    HCL_RIEMANN_HLLC = 1,
+    HCL_RIEMANN_LOW_MACH = 2   /* "Low Mach" = Splitting */
+};
+enum hcl_bc {                  /* boundary_factory.hpp:31-47 */
+    HCL_BC_NULLGRADIENT = 0,
+    HCL_BC_PERIODIC = 1,
+    HCL_BC_REFLEXIVE = 2
+};
+enum hcl_geometry { HCL_GEOM_CARTESIAN = 0, HCL_GEOM_SPHERICAL = 1 };   /* utils/geom.hpp.in:17-25 */
+enum hcl_gravity { HCL_GRAVITY_UNIFORM = 0, HCL_GRAVITY_POINT_MASS = 1 }; /* main.cpp:73-96 */
+enum hcl_precision {
+    HCL_FP64 = 0,              /* reference arithmetic, bitwise-comparable to the FP64 CPU build */
+    HCL_FP32_MIXED = 1         /* FP32 prim/slopes/faces/fluxes, FP64 state, energy recovery, dt, sums */
+};
+enum hcl_memory { HCL_HOST = 0, HCL_DEVICE = 1 };
+
+/* ---- configuration ------------------------------------------------------ */
+/* Everything Param (utils/param.cpp:14-73), Grid (mesh/grid.cpp:48-76), the
+ * EOS (thermodynamics/perfect_gas.cpp:13-22), the gravity plugin
+ * (gravity/gravity.cpp:29-55) and the factories decide for the hot path. */
+typedef struct hcl_config {
+    int ndim;                 /* 1, 2 or 3 (utils/ndim.hpp.in) */
+    int nx[3];                /* [Grid] Nx{0,1,2}_glob; set inactive dims to 1 */
+    int nghost;               /* [Grid] Nghost (2; the MUSCL stencil needs >= 2) */
+    int nfx;                  /* [Passive Scalar] nfx */
+    int geometry;             /* enum hcl_geometry */
+    double gamma;             /* [Perfect Gas] gamma */
+    double mmw;               /* [Perfect Gas] mu */
+    int limiter;              /* enum hcl_limiter   ([Hydro] reconstruction) */
+    int riemann;              /* enum hcl_riemann   ([Hydro] riemann_solver) */
+    int bc[6];                /* enum hcl_bc, index 2*idim + iface (main.cpp:174-185) */
+    int gravity;              /* enum hcl_gravity */
+    double g[3];              /* [Gravity] gx0..gx2 (uniform) */
+    double central_mass;      /* [Gravity] M (point mass) */
+    double xmin[3], xmax[3];  /* [Grid] x{0,1,2}{min,max} for the Regular grid */
+    const double* nodes[3];   /* optional host node coordinates (length n_d + 1) for a
+                                 UserDefined grid; NULL selects Regular (grid_type.cpp:151-186) */
+    int precision;            /* enum hcl_precision, fused path */
+    int device;               /* CUDA device ordinal */
+} hcl_config;
+
+typedef struct hcl_handle hcl_handle;
+
+/* Fills *cfg with the reference's defaults (utils/param.cpp:14-73). */
+void hcl_config_default(hcl_config* cfg);
+
+/* Creates a solver for one domain on one GPU.  Builds the grid arrays
+ * (x, dx, centres, ds, dv, point-mass g) on the host exactly as Grid::set_grid
+ * does (mesh/grid.cpp:134-155, mesh/geometry.cpp:32-126) and uploads them.
+ * Replaces the construction block of main.cpp:138-289. */
+int hcl_create(const hcl_config* cfg, hcl_handle** out);
+int hcl_destroy(hcl_handle* h);
+const char* hcl_last_error(void);
+int hcl_abi_version(void);
+
+/* Extents with ghosts (Nx_local_wg, grid.cpp:119) and cell count. */
+int hcl_get_extents(const hcl_handle* h, int n_wg[3], int64_t* ncells);
+/* Interior extents (Nx_glob_ng; 1 on inactive dims) and ghost width. */
+int hcl_get_interior(const hcl_handle* h, int nx[3], int* nghost);
+/* Host copies of the grid arrays: x_d (n_d+1), dx_d (n_d), xc_d (n_d) for d<3,
+ * ds (N*3) and dv (N); any pointer may be NULL. */
+int hcl_get_grid(const hcl_handle* h, double* x[3], double* dx[3], double* xc[3], double* ds, double* dv);
+/* Device pointers of the handle's grid arrays (Grid::dx0.., ds, dv). */
+int hcl_get_grid_device(const hcl_handle* h, const double* dx[3], const double** ds, const double** dv);
+
+/* ---- stage entry points: one per reference plugin ----------------------- */
+/* All arrays are DEVICE pointers in the layout above; ng_eff selects
+ * Range::with_ghosts(ng_eff) (mesh/range.cpp:367-403).  stream may be NULL
+ * (the handle's stream).  None of these synchronise. */
+
+/* conv_prim_to_cons (hydro/array_conversion.hpp:32-104) */
+int hcl_conv_prim_to_cons(hcl_handle* h, int ng_eff, const double* rho, const double* u, const double* P,
+                          double* rhou, double* E, void* stream);
+/* conv_cons_to_prim (hydro/array_conversion.hpp:106-172) */
+int hcl_conv_cons_to_prim(hcl_handle* h, int ng_eff, const double* rho, const double* rhou, const double* E,
+                          double* u, double* P, void* stream);
+/* IFaceReconstruction::execute (hydro/face_reconstruction.hpp:40-43,
+ * limited_linear_reconstruction.hpp:46-64): var -> var_rec(.., 2, ndim) */
+int hcl_face_reconstruction(hcl_handle* h, int ng_eff, const double* var, double* var_rec, void* stream);
+/* IHydroReconstruction::execute (hydro/hydro_reconstruction.hpp:46-58,85-129)
+ * including HancockExtrapolationReconstruction (extrapolation_reconstruction.hpp:65-338).
+ * dt is the reconstruction time step (the reference passes dt/2, main.cpp:427-439).
+ * u_rec/P_rec are the scratch views MUSCLHancockHydroReconstruction owns
+ * (hydro_reconstruction.hpp:67-68); pass NULL to use the handle's own.
+ * fx/fx_rec may be NULL when nfx == 0. */
+int hcl_hydro_reconstruction(hcl_handle* h, int ng_eff, double dt, const double* rho, const double* u,
+                             const double* P, const double* fx, double* rho_rec, double* rhou_rec, double* E_rec,
+                             double* fx_rec, double* u_rec, double* P_rec, void* stream);
+/* IGodunovScheme::execute (hydro/godunov_scheme.hpp:47-63,77-302) with the
+ * Riemann solver chosen at hcl_create (factory_godunov_scheme, :305-321). */
+int hcl_godunov_scheme(hcl_handle* h, int ng_eff, double dt, const double* rho, const double* rhou,
+                       const double* E, const double* fx, const double* rho_rec, const double* rhou_rec,
+                       const double* E_rec, const double* fx_rec, double* rho_new, double* rhou_new,
+                       double* E_new, double* fx_new, void* stream);
+/* DistributedBoundaryCondition::operator() on one rank
+ * (boundary_distribute.hpp:42-76) + every IBoundaryCondition::execute
+ * (boundary.hpp:81-87, boundary.cpp:221-296): fills all ghost cells in place. */
+int hcl_boundary_conditions(hcl_handle* h, double* rho, double* rhou, double* E, double* fx, void* stream);
+/* time_step (hydro/time_step.hpp:35-82): writes 1/max_cells(sum_d (|u_d|+c)/dx_d)
+ * to *dt_out (host), i.e. the value the reference returns before main
+ * multiplies by cfl.  Synchronises the stream. */
+int hcl_time_step(hcl_handle* h, int ng_eff, const double* rho, const double* u, const double* P, double* dt_out,
+                  void* stream);
+/* minimum_internal_energy (analysis/internal_energy.cpp:20-45), no_ghosts. Synchronises. */
+int hcl_minimum_internal_energy(hcl_handle* h, const double* rho, const double* rhou, const double* E,
+                                double* out, void* stream);
+/* integrate (analysis/integration.cpp:22-37): sum var*dv over no_ghosts,
+ * compensated and deterministic.  Synchronises. */
+int hcl_integrate(hcl_handle* h, const double* var, double* out, void* stream);
+
+/* ---- handle-owned state and the fused step ------------------------------ */
+/* Copies the conserved state in (rho, rhou, E, fx: full arrays with ghosts,
+ * layout above) from host or device memory. fx may be NULL when nfx == 0. */
+int hcl_set_state(hcl_handle* h, const double* rho, const double* rhou, const double* E, const double* fx,
+                  int memory);
+int hcl_get_state(hcl_handle* h, double* rho, double* rhou, double* E, double* fx, int memory);
+/* Initial state from primitives on the interior (what a setup plugin's
+ * InitializationSetup::execute writes, initialization_interface.hpp:33-39),
+ * then conv_prim_to_cons + boundaries (main.cpp:305-307).  Host arrays of
+ * full extent; ghost entries are ignored. */
+int hcl_set_state_from_prim(hcl_handle* h, const double* rho, const double* u, const double* P,
+                            const double* fx);
+
+/* Parameters of the time loop (utils/param.cpp:40-50, main.cpp:354-385). */
+typedef struct hcl_run_params {
+    double cfl;               /* [Run] cfl */
+    double t_end;             /* [Run] t_end */
+    int max_iter;             /* [Output] max_iter (absolute iteration bound) */
+    int iter_frequency;       /* [Output] iter_frequency (0 = off) */
+    double time_frequency;    /* [Output] time_frequency (0 = off): dt is clamped to output times */
+    double time_first_output; /* [Output] time_first_output */
+    int nsteps;               /* steps to take in this call (<= 0: until t_end / max_iter) */
+    int graph_chunk;          /* steps per CUDA-graph replay (0 = default) */
+    int fixed_dt;             /* 1: use dts[] (host, one per step) instead of the CFL dt */
+    const double* dts;
+} hcl_run_params;
+
+typedef struct hcl_run_result {
+    double t;                 /* time after the last step */
+    int iter;                 /* iterations done since the state was set */
+    int status;               /* HCL_OK, HCL_ERR_INVALID_STATE, HCL_ERR_NEGATIVE_DT */
+    int64_t bad_cell;         /* first cell with NaN / negative internal energy, or -1 */
+    int finished;             /* 1 when t_end or max_iter was reached */
+    double last_dt;
+} hcl_run_result;
+
+/* Runs the reference time loop (main.cpp:354-531) with the fused step kernel,
+ * everything on the device: CFL dt reduced inside the step kernel, dt clamps,
+ * health check and ghost filling in place; steps are replayed from CUDA graphs.
+ * Synchronises at the end (and between graph chunks when nsteps <= 0). */
+int hcl_run(hcl_handle* h, const hcl_run_params* p, hcl_run_result* r);
+/* One step of the fused kernel with the given dt (no CFL clamp logic, no
+ * synchronisation): the building block the adapters use. */
+int hcl_step_fixed_dt(hcl_handle* h, double dt, void* stream);
+/* Resets time/iteration counters (t = t_ini) without touching the state. */
+int hcl_reset_clock(hcl_handle* h, double t_ini);
+/* Records the dt of each step taken by hcl_run into a device log that
+ * hcl_get_dt_log copies out (adjoint and parity tools). */
+int hcl_get_dt_log(hcl_handle* h, double* dts, int max_count, int* count);
+
+/* Compensated FP64 sums over no_ghosts: out[0] = sum rho dv, out[1..ndim] =
+ * sum rhou_d dv, out[ndim+1] = sum E dv.  Deterministic. */
+int hcl_conservation_sums(hcl_handle* h, double* out);
+
+/* Number of kernels of this library launched by the calling process so far
+ * (host-side counter of launches issued). */
+int64_t hcl_kernel_launch_count(void);
+
+/* The CUDA stream (cudaStream_t) the handle launches on, so callers can order
+ * their own work or record timing events on it. */
+int hcl_get_stream(const hcl_handle* h, void** stream);
+
+/* ---- .ini front end (host only) ------------------------------------------ */
+/* Compile-time choices of the reference (CMake Heraclespp_NDIM, _GEOM,
+ * _GRAVITY, _SETUP; CMakeLists.txt:11-79) given at run time. */
+typedef struct hcl_build_options {
+    int ndim;                 /* 0: infer from Nx1_glob/Nx2_glob > 1 */
+    int geometry;             /* enum hcl_geometry */
+    int gravity;              /* enum hcl_gravity */
+    int precision;            /* enum hcl_precision */
+    int device;
+    const char* setup;        /* setup plugin name, e.g. "shock_tube" */
+} hcl_build_options;
+
+/* Initial primitives of a setup plugin (InitializationSetup::execute,
+ * initialization_interface.hpp:33-39) on the interior cells, parameterised by
+ * the [Initialisation] keys of ini_path (NULL: the setup's defaults).  Host
+ * arrays of full extent n_wg; xc_d are the cell centres (Grid::x{d}_center). */
+int hcl_setup_initial_prim(const char* setup, const char* ini_path, int ndim, const int n_wg[3], int nghost,
+                           const double* xc0, const double* xc1, const double* xc2, double* rho, double* u,
+                           double* P);
+
+/* Everything main.cpp:138-311 does before the time loop, from an .ini file:
+ * Param, BC resolution and factories, grid, setup plugin, prim->cons and
+ * boundaries; fills *run from [Run]/[Output] (nsteps = 0: run to t_end). */
+int hcl_create_from_ini(const char* ini_path, const hcl_build_options* opt, hcl_handle** out, hcl_run_params* run);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HERACLES_B200_H */
