@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--e2e-chunk", type=int, default=100, help="steps per C-ABI call in the end-to-end arm")
     p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU oracle work for cpu_baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     return p.parse_args()
 
 
@@ -171,6 +172,45 @@ def cpu_baseline(budget_s, cells_full=CELLS):
             "sample": f"{n} full steps of KH 2048^2 (FP64 oracle, {Oracle.get_threads()} OpenMP threads), {el:.1f} s"}
 
 
+def adjoint_cost(torch, nsteps=400, n=512, k=32):
+    """Gresho 512^2, 400 steps, checkpoint every 32: device time of one
+    gradient (adjoint forward + backward) against one forward run."""
+    from heraclespp_b200 import Domain, setups
+
+    kw = dict(gamma=5.0 / 3.0, limiter="VanLeer", riemann="HLLC", bc=["Periodic"] * 4)
+    out = {"config": f"gresho_vortex_2d_{n}x{n}_{nsteps}steps_checkpoint{k}"}
+    for prec in ("fp64", "fp32_mixed"):
+        d = Domain(2, [n, n], precision=prec, **kw)
+        prim = setups.gresho_vortex(setups.Grid.from_domain(d))
+        d.set_state_from_prim(*prim)
+        d.run(cfl=0.4, nsteps=nsteps)
+        dts = d.dt_log()[:nsteps]
+        lam = np.zeros((4,) + d.shape3)
+        lam[0] = 1.0
+        stream = torch.cuda.ExternalStream(d.stream_handle())
+
+        def timed(fn):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1)
+
+        d.set_state_from_prim(*prim)
+        d.run(nsteps=nsteps, dts=dts)  # warm the graphs
+        d.set_state_from_prim(*prim)
+        fwd = timed(lambda: d.run(nsteps=nsteps, dts=dts))
+        d.set_state_from_prim(*prim)
+        adj = timed(lambda: (d.adjoint_forward(nsteps, dts=dts, precision=prec, checkpoint_every=k),
+                             d.adjoint_backward(lam)))
+        out[prec] = {"forward_ms": fwd, "gradient_ms": adj, "adj_over_fwd": adj / fwd}
+        d.close()
+    return out
+
+
 def dist_setup(args):
     import torch
 
@@ -250,8 +290,8 @@ def run_ours(args):
     d64.run(nsteps=len(dts), dts=dts)
     rho64 = d64.get_state()[0]
     ng = 2
-    a = rho_mixed[ng:-ng, ng:-ng]
-    b = rho64[ng:-ng, ng:-ng]
+    a = rho_mixed[0, ng:-ng, ng:-ng]
+    b = rho64[0, ng:-ng, ng:-ng]
     l1 = float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
     linf = float(np.max(np.abs(a - b) / np.abs(b)))
     d64.close()
@@ -313,6 +353,8 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if rank == 0 and not args.no_adjoint:
+        line["adjoint"] = adjoint_cost(torch)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.cpu_budget)
     d.close()

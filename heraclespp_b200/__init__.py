@@ -214,6 +214,47 @@ class Domain:
         check(lib().hcl_get_dt_log(self.h, _ptr(buf), max_count, C.byref(cnt)))
         return buf[: cnt.value].copy()
 
+    # ---- discrete adjoint ----------------------------------------------
+    def adjoint_forward(self, nsteps, *, dts=None, cfl=0.4, checkpoint_every=32, precision="fp64"):
+        """Runs nsteps steps from the current state, checkpointing; returns the dts used."""
+        from ._native import AdjointParams
+
+        p = AdjointParams()
+        p.nsteps = int(nsteps)
+        keep = None
+        if dts is not None:
+            keep = np.ascontiguousarray(dts, dtype=np.float64)
+            p.dts = keep.ctypes.data_as(C.POINTER(C.c_double))
+        p.cfl = float(cfl)
+        p.checkpoint_every = int(checkpoint_every)
+        p.precision = _key(PRECISION, precision, "precision")
+        check(lib().hcl_adjoint_forward(self.h, C.byref(p)))
+        out = np.zeros(int(nsteps))
+        cnt = C.c_int()
+        check(lib().hcl_adjoint_dts(self.h, _ptr(out), int(nsteps), C.byref(cnt)))
+        return out[: cnt.value]
+
+    def adjoint_backward(self, lam_final, grad=None, device=False):
+        """lam_final, grad: one contiguous buffer of (ndim+2)*N doubles (rho, rhou, E)."""
+        if grad is None:
+            grad = np.zeros(((self.ndim + 2),) + self.shape3)
+        if not device:
+            lam_final = np.ascontiguousarray(lam_final, dtype=np.float64)
+        check(lib().hcl_adjoint_backward(self.h, _ptr(lam_final), _ptr(grad), 1 if device else 0))
+        return grad
+
+    def set_schedule(self, schedule):
+        """Forces a schedule of the mixed kernel (-1: autotune); returns the one in use."""
+        used = C.c_int()
+        check(lib().hcl_set_schedule(self.h, int(schedule), C.byref(used)))
+        return used.value
+
+    def interior(self):
+        nx = (C.c_int * 3)()
+        ng = C.c_int()
+        check(lib().hcl_get_interior(self.h, nx, C.byref(ng)))
+        return tuple(nx), ng.value
+
     def stream_handle(self) -> int:
         """cudaStream_t of the handle (for timing events on the launching stream)."""
         s = C.c_void_p()

@@ -33,7 +33,8 @@ EXPORTS = [
     "hcl_face_reconstruction", "hcl_hydro_reconstruction", "hcl_godunov_scheme", "hcl_boundary_conditions",
     "hcl_time_step", "hcl_minimum_internal_energy", "hcl_integrate", "hcl_set_state", "hcl_get_state",
     "hcl_set_state_from_prim", "hcl_run", "hcl_step_fixed_dt", "hcl_reset_clock", "hcl_get_dt_log",
-    "hcl_conservation_sums", "hcl_kernel_launch_count", "hcl_get_stream",
+    "hcl_conservation_sums", "hcl_kernel_launch_count", "hcl_get_stream", "hcl_get_interior",
+    "hcl_adjoint_forward", "hcl_adjoint_backward", "hcl_adjoint_dts", "hcl_set_schedule",
 ]
 
 
@@ -82,6 +83,16 @@ class RunParams(C.Structure):
         ("graph_chunk", C.c_int),
         ("fixed_dt", C.c_int),
         ("dts", C.POINTER(C.c_double)),
+    ]
+
+
+class AdjointParams(C.Structure):
+    _fields_ = [
+        ("nsteps", C.c_int),
+        ("dts", C.POINTER(C.c_double)),
+        ("cfl", C.c_double),
+        ("checkpoint_every", C.c_int),
+        ("precision", C.c_int),
     ]
 
 
@@ -140,6 +151,11 @@ def lib():
     L.hcl_conservation_sums.argtypes = [H, vp]
     L.hcl_kernel_launch_count.restype = C.c_int64
     L.hcl_get_stream.argtypes = [H, C.POINTER(vp)]
+    L.hcl_get_interior.argtypes = [H, C.c_int * 3, C.POINTER(i)]
+    L.hcl_adjoint_forward.argtypes = [H, C.POINTER(AdjointParams)]
+    L.hcl_adjoint_backward.argtypes = [H, vp, vp, i]
+    L.hcl_adjoint_dts.argtypes = [H, vp, i, C.POINTER(i)]
+    L.hcl_set_schedule.argtypes = [H, i, C.POINTER(i)]
     _LIB = L
     return L
 

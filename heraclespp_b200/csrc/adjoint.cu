@@ -1,0 +1,131 @@
+// adjoint.cu -- launchers of the discrete-adjoint kernels (FP64 and FP32-mixed
+// reverse sweeps; the stored state and the adjoint state are FP64).
+#include <cuda_runtime.h>
+
+#include "adjoint_step.cuh"
+#include "stages.hpp"
+
+namespace hcl::adjoint {
+
+namespace {
+
+template <int ND, class R, int TX, int TY, int TZ>
+struct Launcher {
+    using S = Shape<ND, TX, TY, TZ>;
+    static size_t smem() { return AdjShape<ND, R, TX, TY, TZ>::smem(); }
+    static void configure()
+    {
+        cudaFuncSetAttribute(k_adjoint_step<ND, R, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
+    }
+    static void launch(const GridDev& g, const StateDev& U, const StateDev& lo, const StateDev& li, double dt,
+                       cudaStream_t s)
+    {
+        const int nt0 = (g.nx[0] + S::T0 - 1) / S::T0;
+        const int nt1 = (g.nx[1] + S::T1 - 1) / S::T1;
+        const int nt2 = (g.nx[2] + S::T2 - 1) / S::T2;
+        k_adjoint_step<ND, R, TX, TY, TZ><<<nt0 * nt1 * nt2, S::TVOL, smem(), s>>>(g, U, lo, li, dt);
+        ++g_launches;
+    }
+};
+
+using L1d = Launcher<1, double, 128, 1, 1>;
+using L2d = Launcher<2, double, 16, 16, 1>;
+using L3d = Launcher<3, double, 8, 4, 4>;
+using L1f = Launcher<1, float, 128, 1, 1>;
+using L2f = Launcher<2, float, 16, 16, 1>;
+using L3f = Launcher<3, float, 8, 4, 4>;
+
+} // namespace
+
+void configure()
+{
+    L1d::configure();
+    L2d::configure();
+    L3d::configure();
+    L1f::configure();
+    L2f::configure();
+    L3f::configure();
+}
+
+void step(const GridDev& g, const StateDev& U, const StateDev& lam_out, const StateDev& lam_in, double dt, bool fp64,
+          cudaStream_t s)
+{
+    if (fp64) {
+        if (g.ndim == 1) {
+            L1d::launch(g, U, lam_out, lam_in, dt, s);
+        } else if (g.ndim == 2) {
+            L2d::launch(g, U, lam_out, lam_in, dt, s);
+        } else {
+            L3d::launch(g, U, lam_out, lam_in, dt, s);
+        }
+    } else {
+        if (g.ndim == 1) {
+            L1f::launch(g, U, lam_out, lam_in, dt, s);
+        } else if (g.ndim == 2) {
+            L2f::launch(g, U, lam_out, lam_in, dt, s);
+        } else {
+            L3f::launch(g, U, lam_out, lam_in, dt, s);
+        }
+    }
+}
+
+namespace {
+template <int ND>
+__global__ void k_zero_ghosts(GridDev g, StateDev lam)
+{
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < g.N; c += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % g.n[0]);
+        const int64_t r = c / g.n[0];
+        const int j = (int)(r % g.n[1]);
+        const int k = (int)(r / g.n[1]);
+        const int idx[3] = {i, j, k};
+        bool ghost = false;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            ghost |= idx[d] < g.ng || idx[d] >= g.n[d] - g.ng;
+        }
+        if (ghost) {
+            const int64_t o = sidx(lam, g.n[1], i, j, k);
+#pragma unroll
+            for (int v = 0; v < ND + 2; ++v) {
+                lam.q[o + lam.plane * v] = 0.0;
+            }
+        }
+    }
+}
+} // namespace
+
+void zero_ghosts(const GridDev& g, const StateDev& lam, cudaStream_t s)
+{
+    int blocks = (int)((g.N + 255) / 256);
+    if (blocks > 148 * 8) {
+        blocks = 148 * 8;
+    }
+    if (g.ndim == 1) {
+        k_zero_ghosts<1><<<blocks, 256, 0, s>>>(g, lam);
+    } else if (g.ndim == 2) {
+        k_zero_ghosts<2><<<blocks, 256, 0, s>>>(g, lam);
+    } else {
+        k_zero_ghosts<3><<<blocks, 256, 0, s>>>(g, lam);
+    }
+    ++g_launches;
+}
+
+void fold(const GridDev& g, const StateDev& lam, cudaStream_t s)
+{
+    const int64_t count = (int64_t)g.nx[0] * g.nx[1] * g.nx[2];
+    int blocks = (int)((count + 255) / 256);
+    if (blocks > 148 * 8) {
+        blocks = 148 * 8;
+    }
+    if (g.ndim == 1) {
+        k_fold_ghosts<1><<<blocks, 256, 0, s>>>(g, lam);
+    } else if (g.ndim == 2) {
+        k_fold_ghosts<2><<<blocks, 256, 0, s>>>(g, lam);
+    } else {
+        k_fold_ghosts<3><<<blocks, 256, 0, s>>>(g, lam);
+    }
+    ++g_launches;
+}
+
+} // namespace hcl::adjoint

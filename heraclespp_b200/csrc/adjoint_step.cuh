@@ -1,0 +1,513 @@
+// adjoint_step.cuh -- discrete adjoint of one fused MUSCL-Hancock step.
+//
+// Forward step (Cartesian, uniform spacing, uniform gravity):
+//   U'_c = U_c + sum_d c_d (F_{c-1/2,d} - F_{c+1/2,d}) + dt g-terms(U_c),
+//   F_{f,d} = Riemann(H_{L,d}, H_{R,d}),  H = Hancock face states built from the
+//   limited slopes of the primitive stencil of each cell, and ghosts of U' are
+//   images of interior cells.  dt is held fixed (recorded by the forward run).
+//
+// One CTA owns a tile.  It recomputes the forward face states of the tile on
+// chip, then runs the reverse sweep: the adjoint of each face it owns (its
+// cells' left faces) through the Riemann solver, of the Hancock predictor and
+// the limited slopes of every cell it touched, and of the primitive recovery,
+// and adds the result for every cell of its halo-extended tile into lam_in
+// with atomics (neighbouring tiles overlap by the stencil width).  The
+// transpose of the boundary fill (ghost adjoints folded onto their interior
+// sources) is a separate gather kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "adjoint_cell.cuh"
+#include "fused_step.cuh"
+#include "hcl_device.cuh"
+#include "stages.hpp"
+
+namespace hcl::adjoint {
+
+using fused::Shape;
+using fused::sidx;
+using fused::StateDev;
+
+template <int ND, class R, int TX, int TY, int TZ>
+struct AdjShape {
+    using S = Shape<ND, TX, TY, TZ>;
+    static constexpr size_t smem()
+    {
+        // W, Wb, lam: [NV][NP]; A, Ab: A_TOTAL each
+        return sizeof(R) * (2 * (size_t)S::NV * S::NP + 2 * (size_t)S::A_TOTAL) + sizeof(double) * (size_t)S::NV * S::NP;
+    }
+};
+
+template <int ND, class R, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1))
+k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt)
+{
+    using S = Shape<ND, TX, TY, TZ>;
+    constexpr int NV = S::NV;
+    constexpr int NT = S::TVOL;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sl = reinterpret_cast<double*>(smem_raw);       // lambda' [NV][NP] (FP64)
+    R* sw = reinterpret_cast<R*>(sl + NV * S::NP);          // primitives [NV][NP]
+    R* swb = sw + NV * S::NP;                               // primitive adjoints [NV][NP]
+    R* sa = swb + NV * S::NP;                               // face states per d [2][NV][A_d]
+    R* sab = sa + S::A_TOTAL;                               // face-state adjoints
+
+    const int tid = threadIdx.x;
+    const adj::Eos<R> eos{(R)g.gamma, (R)g.gamma_m1, (R)(1.0 / g.gamma_m1)};
+    const double dth = dt / 2;
+    R cth[3], cfull[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        cth[d] = (R)(dth * g.inv_dx[d]);
+        cfull[d] = (R)(dt * g.inv_dx[d]);
+    }
+
+    int ntile[2];
+    ntile[0] = (g.nx[0] + S::T0 - 1) / S::T0;
+    ntile[1] = (g.nx[1] + S::T1 - 1) / S::T1;
+    int tc[3];
+    {
+        int b = blockIdx.x;
+        tc[0] = b % ntile[0];
+        b /= ntile[0];
+        tc[1] = b % ntile[1];
+        tc[2] = b / ntile[1];
+    }
+    const int t0[3] = {tc[0] * S::T0, tc[1] * S::T1, tc[2] * S::T2};
+    const int gorg[3] = {g.ng + t0[0], ND >= 2 ? g.ng + t0[1] : 0, ND >= 3 ? g.ng + t0[2] : 0};
+    const int lstride[3] = {1, S::L0, S::L0 * S::L1};
+
+    // ---- phase 1: primitives, lambda', zero adjoint buffers --------------
+    for (int p = tid; p < S::NP; p += NT) {
+        const int lx = p % S::L0;
+        const int ly = (p / S::L0) % S::L1;
+        const int lz = p / (S::L0 * S::L1);
+        const int ri = gorg[0] - 2 + lx;
+        const int rj = ND >= 2 ? gorg[1] - 2 + ly : 0;
+        const int rk = ND >= 3 ? gorg[2] - 2 + lz : 0;
+        const int gi = min(max(ri, 0), g.n[0] - 1);
+        const int gj = min(max(rj, 0), g.n[1] - 1);
+        const int gk = min(max(rk, 0), g.n[2] - 1);
+        const int64_t o = sidx(U, g.n[1], gi, gj, gk);
+        R q[NV], w[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            q[v] = (R)U.q[o + U.plane * v];
+        }
+        adj::prim_from_cons<ND>(eos, q, w);
+        // lambda' lives on output (interior) cells only
+        bool out_cell = ri >= g.ng && ri < g.n[0] - g.ng;
+        if (ND >= 2) {
+            out_cell = out_cell && rj >= g.ng && rj < g.n[1] - g.ng;
+        }
+        if (ND >= 3) {
+            out_cell = out_cell && rk >= g.ng && rk < g.n[2] - g.ng;
+        }
+        const int64_t ol = sidx(lam_out, g.n[1], gi, gj, gk);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            sw[v * S::NP + p] = w[v];
+            swb[v * S::NP + p] = R(0);
+            sl[v * S::NP + p] = out_cell ? lam_out.q[ol + lam_out.plane * v] : 0.0;
+        }
+    }
+    for (int a = tid; a < S::A_TOTAL; a += NT) {
+        sab[a] = R(0);
+    }
+    __syncthreads();
+
+    // helper: decode the a-th cell of the union H (interior + one slab per side and dim)
+    auto decode_h = [&](int h, int x[3], int& own) {
+        x[0] = x[1] = x[2] = 0;
+        own = -1;
+        int r = h;
+        if (r < S::TVOL) {
+            x[0] = r % S::T0;
+            x[1] = (r / S::T0) % S::T1;
+            x[2] = r / (S::T0 * S::T1);
+            return;
+        }
+        r -= S::TVOL;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const int slab = S::TVOL / S::T(d);
+            if (own < 0) {
+                if (r < 2 * slab) {
+                    own = d;
+                    const int side = r / slab;
+                    int rr = r % slab;
+#pragma unroll
+                    for (int e = 0; e < 3; ++e) {
+                        if (e == d) {
+                            continue;
+                        }
+                        x[e] = rr % S::T(e);
+                        rr /= S::T(e);
+                    }
+                    x[d] = side == 0 ? -1 : S::T(d);
+                } else {
+                    r -= 2 * slab;
+                }
+            }
+        }
+    };
+    auto lcell = [&](const int x[3]) {
+        return (x[0] + 2) + S::L0 * ((ND >= 2 ? x[1] + 2 : 0) + S::L1 * (ND >= 3 ? x[2] + 2 : 0));
+    };
+
+    // ---- phase 2: forward Hancock face states (recomputed) -----------------
+    for (int h = tid; h < S::HCOUNT; h += NT) {
+        int x[3], own;
+        decode_h(h, x, own);
+        const int lc = lcell(x);
+        R fp[2][ND][NV];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const R wc = sw[v * S::NP + lc];
+                R gR, gL;
+                const R phi = adj::limiter(g.limiter, sw[v * S::NP + lc + lstride[d]] - wc,
+                                           wc - sw[v * S::NP + lc - lstride[d]], &gR, &gL);
+                fp[0][d][v] = wc - R(0.5) * phi;
+                fp[1][d][v] = wc + R(0.5) * phi;
+            }
+        }
+        R fc[2][ND][NV];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                adj::cons_from_prim<ND>(eos, fp[s][d], fc[s][d]);
+            }
+        }
+        R inc[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            inc[v] = R(0);
+        }
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            R fL[NV], fR[NV];
+            adj::flux_prim<ND>(eos, fp[0][d], d, fL);
+            adj::flux_prim<ND>(eos, fp[1][d], d, fR);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                inc[v] += cth[d] * (fL[v] - fR[v]);
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            if (own >= 0 && own != d) {
+                continue;
+            }
+            const int ax = x[0] + (d == 0), ay = x[1] + (d == 1), az = x[2] + (d == 2);
+            const int a = ax + S::Adim(d, 0) * (ay + S::Adim(d, 1) * az);
+            R* base = sa + S::Aoff(d);
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                R hs[NV];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    hs[v] = fc[s][d][v] + inc[v];
+                }
+#pragma unroll
+                for (int e = 0; e < ND; ++e) {
+                    const R gg = (R)(dth * g.g[e]);
+                    hs[1 + e] += gg * fc[s][d][0];
+                    hs[1 + ND] += gg * fc[s][d][1 + e];
+                }
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    base[(s * NV + v) * S::Asize(d) + a] = hs[v];
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- phase 3: adjoint of each owned face through the Riemann solver ---------
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        const R* base = sa + S::Aoff(d);
+        R* bb = sab + S::Aoff(d);
+        constexpr int dummy = 0;
+        (void)dummy;
+        const int nf = S::TVOL; // owned faces: the left face of every interior cell
+        for (int f = tid; f < nf; f += NT) {
+            int x[3];
+            x[0] = f % S::T0;
+            x[1] = (f / S::T0) % S::T1;
+            x[2] = f / (S::T0 * S::T1);
+            // cells R = x (interior) and L = x - e_d
+            const int lcR = lcell(x);
+            const int lcL = lcR - lstride[d];
+            R Fb[NV];
+            bool nz = false;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                Fb[v] = (R)(cfull[d] * (sl[v * S::NP + lcR] - sl[v * S::NP + lcL]));
+                nz |= Fb[v] != R(0);
+            }
+            if (!nz) {
+                continue;
+            }
+            // A coordinates: left state = cell x_d - 1 (A index x_d), right = cell x_d (A index x_d + 1)
+            const int ax = x[0] + (d == 0 ? 0 : 0), ay = x[1], az = x[2];
+            const int aL = ax + S::Adim(d, 0) * (ay + S::Adim(d, 1) * az);
+            const int stepd = d == 0 ? 1 : (d == 1 ? S::Adim(d, 0) : S::Adim(d, 0) * S::Adim(d, 1));
+            // for d != 0 the cell's own coordinate along d is stored shifted by 1
+            const int aLd = d == 0 ? aL : aL; // x_d (not +1) is the left cell's A index along d
+            const int aRd = aLd + stepd;
+            R UL[NV], UR[NV], ULb[NV], URb[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                UL[v] = base[(NV + v) * S::Asize(d) + aLd];
+                UR[v] = base[v * S::Asize(d) + aRd];
+                ULb[v] = URb[v] = R(0);
+            }
+            adj::riemann_rev<ND>(eos, g.riemann == 0 ? 0 : 1, UL, UR, d, Fb, ULb, URb);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                bb[(NV + v) * S::Asize(d) + aLd] = ULb[v];
+                bb[v * S::Asize(d) + aRd] = URb[v];
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- phase 4: reverse Hancock + slopes of every cell with face adjoints ------
+    for (int h = tid; h < S::HCOUNT; h += NT) {
+        int x[3], own;
+        decode_h(h, x, own);
+        const int lc = lcell(x);
+        // gather this cell's face-state adjoints
+        R Hb[2][ND][NV];
+        bool any = false;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const bool has = own < 0 || own == d;
+            const int ax = x[0] + (d == 0), ay = x[1] + (d == 1), az = x[2] + (d == 2);
+            const int a = ax + S::Adim(d, 0) * (ay + S::Adim(d, 1) * az);
+            const R* bb = sab + S::Aoff(d);
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    Hb[s][d][v] = has ? bb[(s * NV + v) * S::Asize(d) + a] : R(0);
+                    any |= Hb[s][d][v] != R(0);
+                }
+            }
+        }
+        if (!any) {
+            continue;
+        }
+        // recompute slopes and face primitives
+        R fp[2][ND][NV], gRs[ND][NV], gLs[ND][NV];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const R wc = sw[v * S::NP + lc];
+                const R phi = adj::limiter(g.limiter, sw[v * S::NP + lc + lstride[d]] - wc,
+                                           wc - sw[v * S::NP + lc - lstride[d]], &gRs[d][v], &gLs[d][v]);
+                fp[0][d][v] = wc - R(0.5) * phi;
+                fp[1][d][v] = wc + R(0.5) * phi;
+            }
+        }
+        R fpb[2][ND][NV];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    fpb[s][d][v] = R(0);
+                }
+            }
+        }
+        // H[s][ipos] = cons(fp[s][ipos]) + sum_d cth_d (F(fp[0][d]) - F(fp[1][d])) + gravity(cons(fp[s][ipos]))
+        R Sb[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            Sb[v] = R(0);
+        }
+#pragma unroll
+        for (int ip = 0; ip < ND; ++ip) {
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                R cb[NV];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    cb[v] = Hb[s][ip][v];
+                    Sb[v] += Hb[s][ip][v];
+                }
+#pragma unroll
+                for (int e = 0; e < ND; ++e) {
+                    const R gg = (R)(dth * g.g[e]);
+                    cb[0] += gg * Hb[s][ip][1 + e];
+                    cb[1 + e] += gg * Hb[s][ip][1 + ND];
+                }
+                adj::cons_from_prim_rev<ND>(eos, fp[s][ip], cb, fpb[s][ip]);
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            R Fb0[NV], Fb1[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                Fb0[v] = cth[d] * Sb[v];
+                Fb1[v] = -cth[d] * Sb[v];
+            }
+            adj::flux_prim_rev<ND>(eos, fp[0][d], d, Fb0, fpb[0][d]);
+            adj::flux_prim_rev<ND>(eos, fp[1][d], d, Fb1, fpb[1][d]);
+        }
+        // slopes: fp[0/1][d][v] = w_c -/+ phi/2, phi = limiter(w_{c+1} - w_c, w_c - w_{c-1})
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const R phib = R(0.5) * (fpb[1][d][v] - fpb[0][d][v]);
+                const R dRb = phib * gRs[d][v];
+                const R dLb = phib * gLs[d][v];
+                atomicAdd(&swb[v * S::NP + lc], fpb[0][d][v] + fpb[1][d][v] - dRb + dLb);
+                if (dRb != R(0)) {
+                    atomicAdd(&swb[v * S::NP + lc + lstride[d]], dRb);
+                }
+                if (dLb != R(0)) {
+                    atomicAdd(&swb[v * S::NP + lc - lstride[d]], -dLb);
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- phase 5: primitive recovery reverse, identity and gravity terms ---------
+    for (int p = tid; p < S::NP; p += NT) {
+        const int lx = p % S::L0;
+        const int ly = (p / S::L0) % S::L1;
+        const int lz = p / (S::L0 * S::L1);
+        const int ri = gorg[0] - 2 + lx;
+        const int rj = ND >= 2 ? gorg[1] - 2 + ly : 0;
+        const int rk = ND >= 3 ? gorg[2] - 2 + lz : 0;
+        if (ri < 0 || ri >= g.n[0] || rj < 0 || rj >= g.n[1] || rk < 0 || rk >= g.n[2]) {
+            continue;
+        }
+        // owned output cell of this tile (identity + Godunov gravity terms)
+        const int x0 = lx - 2, x1 = ly - 2, x2 = lz - 2;
+        bool own_cell = x0 >= 0 && x0 < S::T0 && ri < g.n[0] - g.ng;
+        if (ND >= 2) {
+            own_cell = own_cell && x1 >= 0 && x1 < S::T1 && rj < g.n[1] - g.ng;
+        }
+        if (ND >= 3) {
+            own_cell = own_cell && x2 >= 0 && x2 < S::T2 && rk < g.n[2] - g.ng;
+        }
+        R wb[NV];
+        bool nz = own_cell;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            wb[v] = swb[v * S::NP + p];
+            nz |= wb[v] != R(0);
+        }
+        if (!nz) {
+            continue;
+        }
+        const int64_t o = sidx(U, g.n[1], ri, rj, rk);
+        R q[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            q[v] = (R)U.q[o + U.plane * v];
+        }
+        R ub[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            ub[v] = R(0);
+        }
+        adj::prim_from_cons_rev<ND>(eos, q, wb, ub);
+        double outv[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            outv[v] = (double)ub[v];
+        }
+        if (own_cell) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                outv[v] += sl[v * S::NP + p];
+            }
+#pragma unroll
+            for (int e = 0; e < ND; ++e) {
+                // U'_m_e += dt g_e rho ; U'_E += dt g_e m_e   (godunov_scheme.hpp:258-260)
+                outv[0] += dt * g.g[e] * sl[(1 + e) * S::NP + p];
+                outv[1 + e] += dt * g.g[e] * sl[(1 + ND) * S::NP + p];
+            }
+        }
+        const int64_t oo = sidx(lam_in, g.n[1], ri, rj, rk);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            if (outv[v] != 0.0) {
+                atomicAdd(&lam_in.q[oo + lam_in.plane * v], outv[v]);
+            }
+        }
+    }
+}
+
+// Transpose of the boundary fill: every interior cell gathers the adjoints of
+// its ghost images (sign-flipped momentum for Reflexive faces).
+template <int ND>
+__global__ void k_fold_ghosts(GridDev g, StateDev lam)
+{
+    const int64_t count = (int64_t)g.nx[0] * g.nx[1] * g.nx[2];
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < count;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int ii = (int)(idx % g.nx[0]);
+        const int64_t r = idx / g.nx[0];
+        const int jj = (int)(r % g.nx[1]);
+        const int kk = (int)(r / g.nx[1]);
+        const int gidx[3] = {g.ng + ii, ND >= 2 ? g.ng + jj : 0, ND >= 3 ? g.ng + kk : 0};
+        int pos[3][9], flp[3][9], cnt[3] = {1, 1, 1};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            pos[d][0] = gidx[d];
+            flp[d][0] = 0;
+            if (d < ND) {
+                cnt[d] += fused::ghost_images(gidx[d], g.n[d], g.ng, g.bc[2 * d], g.bc[2 * d + 1], &pos[d][1], &flp[d][1]);
+            }
+        }
+        if (cnt[0] * cnt[1] * cnt[2] == 1) {
+            continue;
+        }
+        double acc[ND + 2];
+        const int64_t oc = sidx(lam, g.n[1], gidx[0], gidx[1], gidx[2]);
+#pragma unroll
+        for (int v = 0; v < ND + 2; ++v) {
+            acc[v] = lam.q[oc + lam.plane * v];
+        }
+        for (int a2 = 0; a2 < cnt[2]; ++a2) {
+            for (int a1 = 0; a1 < cnt[1]; ++a1) {
+                for (int a0 = 0; a0 < cnt[0]; ++a0) {
+                    if (a0 == 0 && a1 == 0 && a2 == 0) {
+                        continue;
+                    }
+                    const int64_t og = sidx(lam, g.n[1], pos[0][a0], pos[1][a1], pos[2][a2]);
+                    const int fl[3] = {flp[0][a0], flp[1][a1], flp[2][a2]};
+                    acc[0] += lam.q[og];
+#pragma unroll
+                    for (int d = 0; d < ND; ++d) {
+                        const double v = lam.q[og + lam.plane * (1 + d)];
+                        acc[1 + d] += fl[d] ? -v : v;
+                    }
+                    acc[1 + ND] += lam.q[og + lam.plane * (1 + ND)];
+                }
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < ND + 2; ++v) {
+            lam.q[oc + lam.plane * v] = acc[v];
+        }
+    }
+}
+
+} // namespace hcl::adjoint

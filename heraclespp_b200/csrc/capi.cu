@@ -129,6 +129,19 @@ struct hcl_handle {
     // stream and graphs
     cudaStream_t stream = nullptr;
     std::map<GraphKey, cudaGraphExec_t> graphs;
+    // discrete adjoint: checkpoints, segment states, adjoint state, dts
+    double* adj_ckpt = nullptr;   // nck states
+    double* adj_seg = nullptr;    // k+1 states
+    double* adj_lam = nullptr;    // 2 states
+    double* adj_ddts = nullptr;   // device copy of the dts
+    StepCtl* adj_ctl = nullptr;
+    std::vector<double> adj_dts;
+    int adj_k = 0;
+    int adj_nck = 0;
+    int adj_cap_ck = 0;
+    int adj_cap_seg = 0;
+    int adj_prec = 0;
+    int adj_ready = 0;
 };
 
 namespace {
@@ -165,6 +178,11 @@ void free_handle(hcl_handle* h)
     cudaFree(h->ctl_tune);
     cudaFree(h->dt_log);
     cudaFree(h->d_dts);
+    cudaFree(h->adj_ckpt);
+    cudaFree(h->adj_seg);
+    cudaFree(h->adj_lam);
+    cudaFree(h->adj_ddts);
+    cudaFree(h->adj_ctl);
     if (h->stream) {
         cudaStreamDestroy(h->stream);
     }
@@ -411,6 +429,9 @@ int autotune_mixed(hcl_handle* h)
     const char* env = std::getenv("HCL_MIXED_SHAPE");
     if (env) {
         h->mixed_shape = std::max(0, std::min(nshapes - 1, std::atoi(env)));
+        if (!hcl::fused::mixed_shape_valid(h->g, h->mixed_shape)) {
+            h->mixed_shape = 0;
+        }
         return HCL_OK;
     }
     if (h->g.N < 65536) {
@@ -428,6 +449,9 @@ int autotune_mixed(hcl_handle* h)
     HCL_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
     for (int sh = 0; sh < nshapes; ++sh) {
+        if (!hcl::fused::mixed_shape_valid(h->g, sh)) {
+            continue;
+        }
         hcl::fused::prologue(h->g, h->st[h->cur], h->ctl_tune, 0.0, 0, h->stream);
         // warm-up, then time 4 launches that all read the same input
         for (int r = 0; r < 2; ++r) {
@@ -577,6 +601,7 @@ int hcl_create(const hcl_config* cfg, hcl_handle** out)
     HCL_CUDA(cudaSetDevice(cfg->device));
     hcl::fused::configure_exact();
     hcl::fused::configure_mixed();
+    hcl::adjoint::configure();
     HCL_CUDA(cudaGetLastError());
     hcl_handle* h = new hcl_handle();
     h->cfg = *cfg;
@@ -1181,6 +1206,22 @@ int hcl_step_fixed_dt(hcl_handle* h, double dt, void* stream)
     return HCL_OK;
 }
 
+int hcl_set_schedule(hcl_handle* h, int schedule, int* used)
+{
+    HCL_CHECK_HANDLE(h);
+    if (schedule >= hcl::fused::mixed_shape_count(h->g.ndim)) {
+        return fail(HCL_ERR_ARGUMENT, "schedule %d out of range", schedule);
+    }
+    if (schedule >= 0 && !hcl::fused::mixed_shape_valid(h->g, schedule)) {
+        return fail(HCL_ERR_CONFIG, "schedule %d needs a uniform Cartesian 2-D grid", schedule);
+    }
+    h->mixed_shape = schedule < 0 ? -1 : schedule;
+    if (used) {
+        *used = h->mixed_shape;
+    }
+    return HCL_OK;
+}
+
 int hcl_get_dt_log(hcl_handle* h, double* dts, int max_count, int* count)
 {
     HCL_CHECK_HANDLE(h);
@@ -1212,6 +1253,193 @@ int hcl_conservation_sums(hcl_handle* h, double* out)
     HCL_LAUNCH_CHECK();
     HCL_CUDA(cudaMemcpyAsync(out, h->red_out, sizeof(double) * (h->g.ndim + 2), cudaMemcpyDeviceToHost, h->stream));
     HCL_CUDA(cudaStreamSynchronize(h->stream));
+    return HCL_OK;
+}
+
+// ---- discrete adjoint -------------------------------------------------------
+int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!p || p->nsteps <= 0) {
+        return fail(HCL_ERR_ARGUMENT, "adjoint needs nsteps > 0");
+    }
+    if (!h->state_valid) {
+        return fail(HCL_ERR_CONFIG, "no state set");
+    }
+    const GridDev& g = h->g;
+    if (g.geom != HCL_GEOM_CARTESIAN || !g.uniform_cart || g.gravity != HCL_GRAVITY_UNIFORM ||
+        g.riemann == HCL_RIEMANN_LOW_MACH || g.nfx > 0) {
+        return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian uniform grids, uniform gravity, HLL/HLLC, nfx = 0");
+    }
+    int rc;
+    StepCtl ctl;
+    if ((rc = read_ctl(h, &ctl))) {
+        return rc;
+    }
+    if (h->stopped) {
+        if ((rc = restart_clock(h, ctl.t[h->counter & 1], ctl.iter[h->counter & 1]))) {
+            return rc;
+        }
+        if ((rc = read_ctl(h, &ctl))) {
+            return rc;
+        }
+    }
+    const int N = p->nsteps;
+    const int k = p->checkpoint_every > 0 ? p->checkpoint_every : 32;
+    const int nck = (N + k - 1) / k;
+    const size_t sz = (size_t)h->st[0].plane * (g.ndim + 2);
+    if (h->adj_cap_ck < nck) {
+        cudaFree(h->adj_ckpt);
+        h->adj_ckpt = nullptr;
+        h->adj_cap_ck = 0;
+        if ((rc = dalloc(&h->adj_ckpt, sz * nck))) {
+            return rc;
+        }
+        h->adj_cap_ck = nck;
+    }
+    const int iter0 = ctl.iter[h->counter & 1];
+    int done = 0;
+    for (int s = 0; s < nck; ++s) {
+        const int cur = h->cur;
+        HCL_CUDA(cudaMemcpyAsync(h->adj_ckpt + sz * s, h->st[cur].q, sizeof(double) * sz, cudaMemcpyDeviceToDevice,
+                                 h->stream));
+        hcl_run_params rp;
+        std::memset(&rp, 0, sizeof(rp));
+        rp.cfl = p->cfl > 0 ? p->cfl : 0.4;
+        rp.t_end = 1e300;
+        rp.max_iter = INT_MAX;
+        rp.nsteps = std::min(k, N - done);
+        rp.graph_chunk = 6;
+        if (p->dts) {
+            rp.fixed_dt = 1;
+            rp.dts = p->dts + done;
+        }
+        hcl_run_result rr;
+        if ((rc = hcl_run(h, &rp, &rr))) {
+            return rc;
+        }
+        done += rp.nsteps;
+    }
+    // dts of the steps just taken
+    std::vector<double> all((size_t)iter0 + N);
+    int cnt = 0;
+    if ((rc = hcl_get_dt_log(h, all.data(), iter0 + N, &cnt))) {
+        return rc;
+    }
+    if (cnt < iter0 + N) {
+        return fail(HCL_ERR_CONFIG, "dt log shorter than the forward run");
+    }
+    h->adj_dts.assign(all.begin() + iter0, all.begin() + iter0 + N);
+    h->adj_k = k;
+    h->adj_nck = nck;
+    h->adj_prec = p->precision;
+    h->adj_ready = 1;
+    return HCL_OK;
+}
+
+int hcl_adjoint_dts(const hcl_handle* h, double* dts, int max_count, int* count)
+{
+    if (!h) {
+        return fail(HCL_ERR_ARGUMENT, "null handle");
+    }
+    const int n = std::min(max_count, (int)h->adj_dts.size());
+    if (dts && n > 0) {
+        std::memcpy(dts, h->adj_dts.data(), sizeof(double) * n);
+    }
+    if (count) {
+        *count = n;
+    }
+    return HCL_OK;
+}
+
+int hcl_adjoint_backward(hcl_handle* h, const double* lam_final, double* grad, int memory)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!h->adj_ready) {
+        return fail(HCL_ERR_CONFIG, "call hcl_adjoint_forward first");
+    }
+    if (!lam_final || !grad) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    const GridDev& g = h->g;
+    const int nd = g.ndim;
+    const int N = (int)h->adj_dts.size();
+    const int k = h->adj_k;
+    const size_t sz = (size_t)h->st[0].plane * (nd + 2);
+    int rc;
+    if (h->adj_cap_seg < k + 1) {
+        cudaFree(h->adj_seg);
+        h->adj_seg = nullptr;
+        h->adj_cap_seg = 0;
+        if ((rc = dalloc(&h->adj_seg, sz * (size_t)(k + 1)))) {
+            return rc;
+        }
+        h->adj_cap_seg = k + 1;
+    }
+    if (!h->adj_lam && (rc = dalloc(&h->adj_lam, sz * 2))) {
+        return rc;
+    }
+    if (!h->adj_ctl && (rc = dalloc(&h->adj_ctl, 1))) {
+        return rc;
+    }
+    cudaFree(h->adj_ddts);
+    h->adj_ddts = nullptr;
+    if ((rc = dalloc(&h->adj_ddts, (size_t)N + 8))) {
+        return rc;
+    }
+    cudaStream_t s = h->stream;
+    HCL_CUDA(cudaMemcpyAsync(h->adj_ddts, h->adj_dts.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    auto state_at = [&](double* base, size_t idx) {
+        StateDev st = h->st[0];
+        st.q = base + sz * idx;
+        return st;
+    };
+    StateDev lam[2] = {state_at(h->adj_lam, 0), state_at(h->adj_lam, 1)};
+    HCL_CUDA(cudaMemsetAsync(h->adj_lam, 0, sizeof(double) * sz * 2, s));
+    hcl::fused::pack_state(g, lam[0], lam_final, lam_final + g.N, lam_final + g.N * (nd + 1),
+                           memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
+    // the reference layout packs rho, rhou (nd planes), E contiguously: rhou at +N, E at +N*(nd+1)
+    hcl::adjoint::fold(g, lam[0], s);
+    RunParamsDev rp;
+    std::memset(&rp, 0, sizeof(rp));
+    rp.cfl = 0.4;
+    rp.t_end = 1e300;
+    rp.max_iter = INT_MAX;
+    rp.fixed_dt = 1;
+    rp.dts = h->adj_ddts;
+    const bool fp64_sweep = h->adj_prec == HCL_FP64;
+    int cur = 0;
+    for (int sg = h->adj_nck - 1; sg >= 0; --sg) {
+        const int first = sg * k;
+        const int len = std::min(k, N - first);
+        // recompute U^{first} .. U^{first+len-1} into the segment buffer
+        HCL_CUDA(cudaMemcpyAsync(h->adj_seg, h->adj_ckpt + sz * sg, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s));
+        hcl::fused::prologue(g, state_at(h->adj_seg, 0), h->adj_ctl, 0.0, first, s);
+        for (int j = 0; j + 1 < len; ++j) {
+            if (h->cfg.precision == HCL_FP64) {
+                hcl::fused::step_exact(g, state_at(h->adj_seg, j), state_at(h->adj_seg, j + 1), h->adj_ctl, rp, j % 6,
+                                       1, s);
+            } else {
+                hcl::fused::step_mixed(g, state_at(h->adj_seg, j), state_at(h->adj_seg, j + 1), h->adj_ctl, rp, j % 6,
+                                       1, h->mixed_shape < 0 ? 0 : h->mixed_shape, s);
+            }
+        }
+        // backward through the segment
+        for (int j = len - 1; j >= 0; --j) {
+            const int n = first + j;
+            HCL_CUDA(cudaMemsetAsync(lam[cur ^ 1].q, 0, sizeof(double) * sz, s));
+            hcl::adjoint::step(g, state_at(h->adj_seg, j), lam[cur], lam[cur ^ 1], h->adj_dts[n], fp64_sweep, s);
+            hcl::adjoint::fold(g, lam[cur ^ 1], s);
+            cur ^= 1;
+        }
+    }
+    HCL_LAUNCH_CHECK();
+    // the gradient lives on the interior cells; ghost entries are zero
+    hcl::adjoint::zero_ghosts(g, lam[cur], s);
+    hcl::fused::unpack_state(g, lam[cur], grad, grad + g.N, grad + g.N * (nd + 1),
+                             memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
+    HCL_CUDA(cudaStreamSynchronize(s));
+    HCL_LAUNCH_CHECK();
     return HCL_OK;
 }
 

@@ -9,10 +9,17 @@
 
 namespace hcl::fused {
 
-// Tile shapes selectable at run time for 2-D (the autotuner picks one).
+// Schedules selectable at run time for 2-D (the autotuner picks one):
+// 0-2 shared-memory tiles 16x16, 32x8, 32x16; 3-5 warp strips of 32, 64,
+// 128 rows (uniform Cartesian grids only).
 int mixed_shape_count(int ndim)
 {
-    return ndim == 2 ? 3 : 1;
+    return ndim == 2 ? 6 : 1;
+}
+
+bool mixed_shape_valid(const GridDev& g, int shape)
+{
+    return shape < 3 || strip2d_eligible(g);
 }
 
 void configure_mixed()
@@ -32,7 +39,9 @@ void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepC
         FusedLauncher<1, false, 256, 1, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
         break;
     case 2:
-        if (shape == 1) {
+        if (shape >= 3 && strip2d_eligible(g)) {
+            step_strip2d(g, in, out, ctl, rp, slot, out_buf, shape == 3 ? 32 : (shape == 4 ? 64 : 128), s);
+        } else if (shape == 1) {
             FusedLauncher<2, false, 32, 8, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
         } else if (shape == 2) {
             FusedLauncher<2, false, 32, 16, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);

@@ -1,0 +1,63 @@
+// fused_strip.cu -- instantiations of the warp-strip 2-D mixed step for every
+// limiter x Riemann solver pair (same flags as fused_mixed.cu).
+#include <cuda_runtime.h>
+
+#include "fused_strip2d.cuh"
+#include "stages.hpp"
+
+namespace hcl::fused {
+
+bool strip2d_eligible(const GridDev& g)
+{
+    return g.ndim == 2 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM;
+}
+
+namespace {
+
+template <int LIM, int RS>
+void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp, int slot,
+               int out_buf, int L, cudaStream_t s)
+{
+    const int ncolw = (g.nx[0] + kStripLanesOut - 1) / kStripLanesOut;
+    const int nstrip = (g.nx[1] + L - 1) / L;
+    const int warps = ncolw * nstrip;
+    const int blocks = (warps + 3) / 4;
+    k_strip2d<LIM, RS><<<blocks, 128, 0, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
+}
+
+template <int LIM>
+void launch_l(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp, int slot,
+              int out_buf, int L, cudaStream_t s)
+{
+    if (g.riemann == RS_HLL) {
+        launch_lr<LIM, RS_HLL>(g, in, out, ctl, rp, slot, out_buf, L, s);
+    } else if (g.riemann == RS_HLLC) {
+        launch_lr<LIM, RS_HLLC>(g, in, out, ctl, rp, slot, out_buf, L, s);
+    } else {
+        launch_lr<LIM, RS_SPLITTING>(g, in, out, ctl, rp, slot, out_buf, L, s);
+    }
+}
+
+} // namespace
+
+void step_strip2d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                  int slot, int out_buf, int L, cudaStream_t s)
+{
+    switch (g.limiter) {
+    case LIM_CONSTANT:
+        launch_l<LIM_CONSTANT>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        break;
+    case LIM_VANLEER:
+        launch_l<LIM_VANLEER>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        break;
+    case LIM_MINMOD:
+        launch_l<LIM_MINMOD>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        break;
+    default:
+        launch_l<LIM_VANALBADA>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        break;
+    }
+    ++g_launches;
+}
+
+} // namespace hcl::fused

@@ -66,6 +66,10 @@ void step_exact(const GridDev& g, const StateDev& in, const StateDev& out, StepC
 void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                 int slot, int out_buf, int shape, cudaStream_t s);
 int mixed_shape_count(int ndim);
+bool mixed_shape_valid(const GridDev& g, int shape);
+bool strip2d_eligible(const GridDev& g);
+void step_strip2d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                  int slot, int out_buf, int L, cudaStream_t s);
 void configure_exact();
 void configure_mixed();
 int conservation_partials_doubles(int ndim);
@@ -80,5 +84,18 @@ void unpack_state(const GridDev& g, const StateDev& st, double* rho, double* rho
 void conservation_sums(const GridDev& g, const StateDev& st, double* partials, double* out_dev, cudaStream_t s);
 
 } // namespace fused
+
+namespace adjoint {
+
+void configure();
+// One adjoint step: lam_in (zeroed by the caller) += (dU^{n+1}/dU^n)^T lam_out,
+// with U = U^n and lam_out already folded onto interior cells.
+void step(const GridDev& g, const fused::StateDev& U, const fused::StateDev& lam_out, const fused::StateDev& lam_in,
+          double dt, bool fp64, cudaStream_t s);
+// Transpose of the boundary fill, in place on interior cells.
+void fold(const GridDev& g, const fused::StateDev& lam, cudaStream_t s);
+void zero_ghosts(const GridDev& g, const fused::StateDev& lam, cudaStream_t s);
+
+} // namespace adjoint
 
 } // namespace hcl

@@ -218,6 +218,12 @@ int hcl_reset_clock(hcl_handle* h, double t_ini);
  * hcl_get_dt_log copies out (adjoint and parity tools). */
 int hcl_get_dt_log(hcl_handle* h, double* dts, int max_count, int* count);
 
+/* Schedule of the FP32-mixed fused kernel.  -1 (default): autotuned on the
+ * first run.  2-D: 0-2 shared-memory tiles (16x16, 32x8, 32x16), 3-5 warp
+ * strips of 32/64/128 rows (uniform Cartesian grids).  Returns the schedule
+ * in use through *used (may be NULL). */
+int hcl_set_schedule(hcl_handle* h, int schedule, int* used);
+
 /* Compensated FP64 sums over no_ghosts: out[0] = sum rho dv, out[1..ndim] =
  * sum rhou_d dv, out[ndim+1] = sum E dv.  Deterministic. */
 int hcl_conservation_sums(hcl_handle* h, double* out);
@@ -229,6 +235,35 @@ int64_t hcl_kernel_launch_count(void);
 /* The CUDA stream (cudaStream_t) the handle launches on, so callers can order
  * their own work or record timing events on it. */
 int hcl_get_stream(const hcl_handle* h, void** stream);
+
+/* ---- discrete adjoint of the fused step ------------------------------------ */
+/* Reverse-mode derivative of nsteps fused steps with dt held fixed per step
+ * (recorded by the forward pass or given).  Supported: Cartesian uniform
+ * grids, uniform gravity, HLL/HLLC, every limiter.  Branches (limiter sign
+ * tests, wave-speed min/max, HLLC switches) are differentiated along the
+ * branch the forward evaluation took.  No reference counterpart: the
+ * reference has no adjoint (BASELINE north_star asks for one). */
+typedef struct hcl_adjoint_params {
+    int nsteps;
+    const double* dts;        /* host, nsteps values; NULL: CFL dt of this forward run (recorded) */
+    double cfl;               /* CFL number when dts == NULL */
+    int checkpoint_every;     /* store the state every k steps (0: 32) */
+    int precision;            /* reverse sweep: HCL_FP64 or HCL_FP32_MIXED (state and adjoint stay FP64) */
+} hcl_adjoint_params;
+
+/* Forward pass: runs nsteps fused steps from the current state U^0 (in the
+ * handle's precision), checkpointing the state every k steps.  The handle's
+ * state becomes U^N; dts used are available through hcl_adjoint_dts. */
+int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p);
+/* Reverse pass: given lam_final = dJ/dU^N, writes grad = dJ/dU^0 for the
+ * interior cells (ghost entries are zero: ghosts are functions of the
+ * interior).  Both are one contiguous buffer of (ndim+2)*N doubles holding
+ * the full arrays rho, rhou (ndim planes), E in the layout above.  Each
+ * checkpoint segment is recomputed forward on the device, then swept
+ * backward step by step. */
+int hcl_adjoint_backward(hcl_handle* h, const double* lam_final, double* grad, int memory);
+/* The dt of each step of the last hcl_adjoint_forward (host array of nsteps). */
+int hcl_adjoint_dts(const hcl_handle* h, double* dts, int max_count, int* count);
 
 /* ---- .ini front end (host only) ------------------------------------------ */
 /* Compile-time choices of the reference (CMake Heraclespp_NDIM, _GEOM,

@@ -172,7 +172,7 @@ def test_invalid_state_reports_error_and_gpu_stays_usable():
 
     o, d, (rho0, u0, P0) = make_pair("kh_2d", "fp64")
     P0 = P0.copy()
-    P0[2 + 10, 2 + 7] = -1.0  # host-side injected bad pressure
+    P0[0, 2 + 10, 2 + 7] = -1.0  # host-side injected bad pressure
     d.set_state_from_prim(rho0, u0, P0)
     with pytest.raises(HclError, match="invalid"):
         d.run(cfl=0.4, max_iter=10)
