@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU oracle work for cpu_baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
+    p.add_argument("--no-ensemble", action="store_true", help="skip the batched ensemble measurement")
     return p.parse_args()
 
 
@@ -211,6 +212,77 @@ def adjoint_cost(torch, nsteps=400, n=512, k=32):
     return out
 
 
+ENSEMBLE_SIDES = (128, 256, 512, 1024)
+
+
+def ensemble_cost(torch, nprob=96, nsteps=300, k=20, seed=2024):
+    """96 independent 2-D four-quadrant Riemann problems (sides drawn from
+    {128, 256, 512, 1024}, seeded), outflow, Minmod, HLLC, FP32-mixed,
+    300 steps: one persistent graph-replayed launch against looping the
+    single-problem step (each problem's own hcl_run), then the adjoint of
+    the sum of the final total energies.  Wall-clock of synchronous calls."""
+    from heraclespp_b200 import Domain, Ensemble, setups
+
+    rng = np.random.default_rng(seed)
+    sides = [(int(rng.choice(ENSEMBLE_SIDES)), int(rng.choice(ENSEMBLE_SIDES))) for _ in range(nprob)]
+    cells = sum(a * b for a, b in sides)
+    kw = dict(gamma=1.4, limiter="Minmod", riemann="HLLC", bc=["NullGradient"] * 4)
+    ens = Ensemble([dict(nx=list(s), **kw) for s in sides])
+    prims = [setups.four_quadrant(setups.Grid.from_domain(d), seed=1000 + p) for p, d in enumerate(ens.domains)]
+
+    def reset(doms):
+        for d, prim in zip(doms, prims):
+            d.set_state_from_prim(*prim)
+
+    def wall(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, out
+
+    reset(ens.domains)
+    ens.run(nsteps)  # autotune, capture
+    reset(ens.domains)
+    t_ens, r = wall(lambda: ens.run(nsteps))
+    out = {"config": f"{nprob} four-quadrant problems, sides from {list(ENSEMBLE_SIDES)} (seed {seed}), "
+                     f"{cells} cells, {nsteps} steps, Minmod, HLLC, outflow, fp32_mixed",
+           "cells": cells,
+           "ensemble": {"ms": t_ens * 1e3, "mcups": cells * nsteps / t_ens * 1e-6, "strip_rows": r.strip_rows,
+                        "blocks_per_sm": r.blocks_per_sm, "grid": r.grid, "launches": r.launches,
+                        "graph": bool(r.graph)}}
+    # looping the single-problem step (each problem graph-replays its own steps)
+    doms = [Domain(2, list(s), precision="fp32_mixed", **kw) for s in sides]
+    reset(doms)
+    for d in doms:
+        d.run(cfl=0.4, nsteps=nsteps)  # autotune, capture
+    reset(doms)
+    t_loop, _ = wall(lambda: [d.run(cfl=0.4, nsteps=nsteps) for d in doms])
+    out["loop"] = {"ms": t_loop * 1e3, "mcups": cells * nsteps / t_loop * 1e-6}
+    out["ensemble_over_loop"] = t_loop / t_ens
+    for d in doms:
+        d.close()
+    # adjoint of J = sum_p sum_cells E dV
+    lams = []
+    for d in ens.domains:
+        lam = torch.zeros((4,) + d.shape3, dtype=torch.float64, device="cuda")
+        dv = torch.from_numpy(d.grid()["dv"]).cuda()
+        lam[3, :, 2:-2, 2:-2] = dv[:, 2:-2, 2:-2]
+        lams.append(lam)
+    grads = [torch.empty_like(x) for x in lams]
+    for prec in ("fp64", "fp32_mixed"):
+        reset(ens.domains)
+        ens.run(nsteps, checkpoint_every=k, adjoint_precision=prec)
+        ens.adjoint(lams, grads)  # allocate the sweep buffers
+        reset(ens.domains)
+        t_f, _ = wall(lambda: ens.run(nsteps, checkpoint_every=k, adjoint_precision=prec))
+        t_b, _ = wall(lambda: ens.adjoint(lams, grads))
+        out[f"adjoint_{prec}"] = {"forward_ckpt_ms": t_f * 1e3, "backward_ms": t_b * 1e3,
+                                  "adj_over_fwd": (t_f + t_b) / t_ens, "checkpoint_every": k}
+    ens.close()
+    return out
+
+
 def dist_setup(args):
     import torch
 
@@ -355,6 +427,8 @@ def run_ours(args):
     }
     if rank == 0 and not args.no_adjoint:
         line["adjoint"] = adjoint_cost(torch)
+    if rank == 0 and not args.no_ensemble:
+        line["ensemble"] = ensemble_cost(torch)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.cpu_budget)
     d.close()

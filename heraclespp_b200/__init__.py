@@ -16,7 +16,7 @@ import numpy as np
 from ._native import (BCS, GEOMS, GRAVITY, LIMITERS, PRECISION, RIEMANN, Config, DomainError, HclError,
                       RunParams, RunResult, check, lib)
 
-__all__ = ["Domain", "HclError", "DomainError", "lib", "kernel_launch_count"]
+__all__ = ["Domain", "Ensemble", "make_config", "HclError", "DomainError", "lib", "kernel_launch_count"]
 
 
 def kernel_launch_count() -> int:
@@ -41,6 +41,42 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr())
 
 
+def make_config(ndim, nx, *, nghost=2, nfx=0, geometry="Cartesian", gamma=5.0 / 3.0, mmw=1.0, limiter="VanLeer",
+                riemann="HLL", bc=("Periodic",) * 6, gravity="Uniform", g=(0.0, 0.0, 0.0), central_mass=1.0,
+                xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0), nodes=None, precision="fp64", device=0):
+    """hcl_config from the reference's plugin keys; returns (config, node arrays kept alive)."""
+    L = lib()
+    cfg = Config()
+    L.hcl_config_default(C.byref(cfg))
+    cfg.ndim = int(ndim)
+    nx = list(nx) + [1, 1, 1]
+    for d in range(3):
+        cfg.nx[d] = int(nx[d]) if d < ndim else 1
+        cfg.g[d] = float(g[d])
+        cfg.xmin[d] = float(xmin[d])
+        cfg.xmax[d] = float(xmax[d])
+    cfg.nghost = int(nghost)
+    cfg.nfx = int(nfx)
+    cfg.geometry = _key(GEOMS, geometry, "geometry")
+    cfg.gamma = float(gamma)
+    cfg.mmw = float(mmw)
+    cfg.limiter = _key(LIMITERS, limiter, "face reconstruction algorithm")
+    cfg.riemann = _key(RIEMANN, riemann, "riemann solver")
+    bcs = list(bc) + ["Periodic"] * 6
+    for f in range(6):
+        cfg.bc[f] = _key(BCS, bcs[f], "boundary condition")
+    cfg.gravity = _key(GRAVITY, gravity, "gravity")
+    cfg.central_mass = float(central_mass)
+    cfg.precision = _key(PRECISION, precision, "precision")
+    cfg.device = int(device)
+    _nodes = None
+    if nodes is not None:
+        _nodes = [np.ascontiguousarray(x, dtype=np.float64) for x in nodes]
+        for d in range(3):
+            cfg.nodes[d] = _nodes[d].ctypes.data
+    return cfg, _nodes
+
+
 class Domain:
     """One domain on one GPU (hcl_create)."""
 
@@ -48,51 +84,39 @@ class Domain:
                  limiter="VanLeer", riemann="HLL", bc=("Periodic",) * 6, gravity="Uniform", g=(0.0, 0.0, 0.0),
                  central_mass=1.0, xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0), nodes=None, precision="fp64",
                  device=0):
-        L = lib()
-        cfg = Config()
-        L.hcl_config_default(C.byref(cfg))
-        cfg.ndim = int(ndim)
-        nx = list(nx) + [1, 1, 1]
-        for d in range(3):
-            cfg.nx[d] = int(nx[d]) if d < ndim else 1
-            cfg.g[d] = float(g[d])
-            cfg.xmin[d] = float(xmin[d])
-            cfg.xmax[d] = float(xmax[d])
-        cfg.nghost = int(nghost)
-        cfg.nfx = int(nfx)
-        cfg.geometry = _key(GEOMS, geometry, "geometry")
-        cfg.gamma = float(gamma)
-        cfg.mmw = float(mmw)
-        cfg.limiter = _key(LIMITERS, limiter, "face reconstruction algorithm")
-        cfg.riemann = _key(RIEMANN, riemann, "riemann solver")
-        bcs = list(bc) + ["Periodic"] * 6
-        for f in range(6):
-            cfg.bc[f] = _key(BCS, bcs[f], "boundary condition")
-        cfg.gravity = _key(GRAVITY, gravity, "gravity")
-        cfg.central_mass = float(central_mass)
-        cfg.precision = _key(PRECISION, precision, "precision")
-        cfg.device = int(device)
-        self._nodes = None
-        if nodes is not None:
-            self._nodes = [np.ascontiguousarray(x, dtype=np.float64) for x in nodes]
-            for d in range(3):
-                cfg.nodes[d] = self._nodes[d].ctypes.data
-        self.cfg = cfg
+        cfg, self._nodes = make_config(ndim, nx, nghost=nghost, nfx=nfx, geometry=geometry, gamma=gamma, mmw=mmw,
+                                       limiter=limiter, riemann=riemann, bc=bc, gravity=gravity, g=g,
+                                       central_mass=central_mass, xmin=xmin, xmax=xmax, nodes=nodes,
+                                       precision=precision, device=device)
         h = C.c_void_p()
-        check(L.hcl_create(C.byref(cfg), C.byref(h)))
+        check(lib().hcl_create(C.byref(cfg), C.byref(h)))
+        self._owned = True
+        self._attach(h, cfg)
+
+    @classmethod
+    def _view(cls, h, cfg):
+        """Domain over a handle owned by someone else (an Ensemble)."""
+        self = cls.__new__(cls)
+        self._nodes = None
+        self._owned = False
+        self._attach(h, cfg)
+        return self
+
+    def _attach(self, h, cfg):
+        self.cfg = cfg
         self.h = h
-        self.ndim = int(ndim)
-        self.nfx = int(nfx)
+        self.ndim = int(cfg.ndim)
+        self.nfx = int(cfg.nfx)
         n = (C.c_int * 3)()
         nc = C.c_int64()
-        check(L.hcl_get_extents(h, n, C.byref(nc)))
+        check(lib().hcl_get_extents(h, n, C.byref(nc)))
         self.n = tuple(n)
         self.ncells = int(nc.value)
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and getattr(self, "_owned", False):
             lib().hcl_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -265,3 +289,80 @@ class Domain:
         out = np.zeros(self.ndim + 2)
         check(lib().hcl_conservation_sums(self.h, _ptr(out)))
         return out
+
+
+class Ensemble:
+    """A batch of independent 2-D FP32-mixed problems stepped by one persistent
+    cooperative launch (hcl_ensemble_*).  ``configs`` is a list of keyword
+    dicts for :func:`make_config`; ``domains[p]`` is a :class:`Domain` view of
+    problem p's handle (set its state, read its results)."""
+
+    def __init__(self, configs):
+        from ._native import EnsembleParams  # noqa: F401  (checks the binding)
+
+        cfgs = (Config * len(configs))()
+        self._nodes = []
+        for p, kw in enumerate(configs):
+            kw = dict(kw)
+            kw.setdefault("precision", "fp32_mixed")
+            cfg, nodes = make_config(2, kw.pop("nx"), **kw)
+            cfgs[p] = cfg
+            self._nodes.append(nodes)
+        e = C.c_void_p()
+        check(lib().hcl_ensemble_create(cfgs, len(configs), C.byref(e)))
+        self.e = e
+        self.domains = []
+        for p in range(len(configs)):
+            h = C.c_void_p()
+            check(lib().hcl_ensemble_handle(e, p, C.byref(h)))
+            self.domains.append(Domain._view(h, cfgs[p]))
+        self.result = None
+
+    def close(self):
+        if getattr(self, "e", None):
+            for d in self.domains:
+                d.h = None
+            lib().hcl_ensemble_destroy(self.e)
+            self.e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.domains)
+
+    def stream_handle(self) -> int:
+        s = C.c_void_p()
+        check(lib().hcl_ensemble_stream(self.e, C.byref(s)))
+        return int(s.value or 0)
+
+    def run(self, nsteps, *, cfl=0.4, checkpoint_every=0, strip_rows=0, blocks_per_sm=0, use_graph=True,
+            adjoint_precision="fp64", check_status=True):
+        from ._native import EnsembleParams, EnsembleResult
+
+        p = EnsembleParams()
+        p.nsteps = int(nsteps)
+        p.cfl = float(cfl)
+        p.checkpoint_every = int(checkpoint_every)
+        p.strip_rows = int(strip_rows)
+        p.blocks_per_sm = int(blocks_per_sm)
+        p.use_graph = 1 if use_graph else 0
+        p.adjoint_precision = _key(PRECISION, adjoint_precision, "precision")
+        r = EnsembleResult()
+        rc = lib().hcl_ensemble_run(self.e, C.byref(p), C.byref(r))
+        if check_status:
+            check(rc)
+        self.result = r
+        return r
+
+    def adjoint(self, lam_finals, grads, device=True):
+        """Reverse pass of the last run (checkpoint_every > 0); per problem one
+        contiguous (ndim+2)*N buffer for lam_final and for the gradient."""
+        n = len(self.domains)
+        lam = (C.c_void_p * n)(*[_ptr(t).value for t in lam_finals])
+        out = (C.c_void_p * n)(*[_ptr(t).value for t in grads])
+        check(lib().hcl_ensemble_adjoint(self.e, lam, out, 1 if device else 0))
+        return grads

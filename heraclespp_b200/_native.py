@@ -35,6 +35,8 @@ EXPORTS = [
     "hcl_set_state_from_prim", "hcl_run", "hcl_step_fixed_dt", "hcl_reset_clock", "hcl_get_dt_log",
     "hcl_conservation_sums", "hcl_kernel_launch_count", "hcl_get_stream", "hcl_get_interior",
     "hcl_adjoint_forward", "hcl_adjoint_backward", "hcl_adjoint_dts", "hcl_set_schedule",
+    "hcl_ensemble_create", "hcl_ensemble_destroy", "hcl_ensemble_handle", "hcl_ensemble_stream",
+    "hcl_ensemble_run", "hcl_ensemble_adjoint",
 ]
 
 
@@ -93,6 +95,30 @@ class AdjointParams(C.Structure):
         ("cfl", C.c_double),
         ("checkpoint_every", C.c_int),
         ("precision", C.c_int),
+    ]
+
+
+class EnsembleParams(C.Structure):
+    _fields_ = [
+        ("nsteps", C.c_int),
+        ("cfl", C.c_double),
+        ("checkpoint_every", C.c_int),
+        ("strip_rows", C.c_int),
+        ("blocks_per_sm", C.c_int),
+        ("use_graph", C.c_int),
+        ("adjoint_precision", C.c_int),
+    ]
+
+
+class EnsembleResult(C.Structure):
+    _fields_ = [
+        ("status", C.c_int),
+        ("strip_rows", C.c_int),
+        ("blocks_per_sm", C.c_int),
+        ("grid", C.c_int),
+        ("launches", C.c_int),
+        ("graph", C.c_int),
+        ("cells", C.c_int64),
     ]
 
 
@@ -156,6 +182,12 @@ def lib():
     L.hcl_adjoint_backward.argtypes = [H, vp, vp, i]
     L.hcl_adjoint_dts.argtypes = [H, vp, i, C.POINTER(i)]
     L.hcl_set_schedule.argtypes = [H, i, C.POINTER(i)]
+    L.hcl_ensemble_create.argtypes = [C.POINTER(Config), i, C.POINTER(vp)]
+    L.hcl_ensemble_destroy.argtypes = [vp]
+    L.hcl_ensemble_handle.argtypes = [vp, i, C.POINTER(H)]
+    L.hcl_ensemble_stream.argtypes = [vp, C.POINTER(vp)]
+    L.hcl_ensemble_run.argtypes = [vp, C.POINTER(EnsembleParams), C.POINTER(EnsembleResult)]
+    L.hcl_ensemble_adjoint.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), i]
     _LIB = L
     return L
 

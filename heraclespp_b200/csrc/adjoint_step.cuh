@@ -79,6 +79,7 @@ k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double 
     const int t0[3] = {tc[0] * S::T0, tc[1] * S::T1, tc[2] * S::T2};
     const int gorg[3] = {g.ng + t0[0], ND >= 2 ? g.ng + t0[1] : 0, ND >= 3 ? g.ng + t0[2] : 0};
     const int lstride[3] = {1, S::L0, S::L0 * S::L1};
+    auto ntile_d = [&](int d) { return (g.nx[d] + S::T(d) - 1) / S::T(d); };
 
     // ---- phase 1: primitives, lambda', zero adjoint buffers --------------
     for (int p = tid; p < S::NP; p += NT) {
@@ -230,19 +231,23 @@ k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double 
     __syncthreads();
 
     // ---- phase 3: adjoint of each owned face through the Riemann solver ---------
+    // A tile owns the left face of each of its interior cells; the last tile
+    // along d also owns the domain's last face (the right face of the last
+    // interior cell), so every face an interior update uses has one owner.
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
         const R* base = sa + S::Aoff(d);
         R* bb = sab + S::Aoff(d);
-        constexpr int dummy = 0;
-        (void)dummy;
-        const int nf = S::TVOL; // owned faces: the left face of every interior cell
-        for (int f = tid; f < nf; f += NT) {
+        const bool last_d = tc[d] == ntile_d(d) - 1;
+        for (int f = tid; f < S::Fsize(d); f += NT) {
             int x[3];
-            x[0] = f % S::T0;
-            x[1] = (f / S::T0) % S::T1;
-            x[2] = f / (S::T0 * S::T1);
-            // cells R = x (interior) and L = x - e_d
+            x[0] = f % S::Fdim(d, 0);
+            x[1] = (f / S::Fdim(d, 0)) % S::Fdim(d, 1);
+            x[2] = f / (S::Fdim(d, 0) * S::Fdim(d, 1));
+            if (x[d] == S::T(d) && !last_d) {
+                continue; // owned by the next tile along d
+            }
+            // cells R = x and L = x - e_d (R may be the slab cell x_d = T_d)
             const int lcR = lcell(x);
             const int lcL = lcR - lstride[d];
             R Fb[NV];
@@ -255,12 +260,9 @@ k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double 
             if (!nz) {
                 continue;
             }
-            // A coordinates: left state = cell x_d - 1 (A index x_d), right = cell x_d (A index x_d + 1)
-            const int ax = x[0] + (d == 0 ? 0 : 0), ay = x[1], az = x[2];
-            const int aL = ax + S::Adim(d, 0) * (ay + S::Adim(d, 1) * az);
+            // A coordinates: the left cell x_d - 1 has A index x_d along d, the right cell x_d + 1
+            const int aLd = x[0] + S::Adim(d, 0) * (x[1] + S::Adim(d, 1) * x[2]);
             const int stepd = d == 0 ? 1 : (d == 1 ? S::Adim(d, 0) : S::Adim(d, 0) * S::Adim(d, 1));
-            // for d != 0 the cell's own coordinate along d is stored shifted by 1
-            const int aLd = d == 0 ? aL : aL; // x_d (not +1) is the left cell's A index along d
             const int aRd = aLd + stepd;
             R UL[NV], UR[NV], ULb[NV], URb[NV];
 #pragma unroll

@@ -142,7 +142,10 @@ struct hcl_handle {
     int adj_cap_seg = 0;
     int adj_prec = 0;
     int adj_ready = 0;
+    int adj_ddts_cap = 0;
 };
+
+static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double* grad, int memory);
 
 namespace {
 
@@ -1354,6 +1357,20 @@ int hcl_adjoint_dts(const hcl_handle* h, double* dts, int max_count, int* count)
 
 int hcl_adjoint_backward(hcl_handle* h, const double* lam_final, double* grad, int memory)
 {
+    int rc = adjoint_backward_impl(h, lam_final, grad, memory);
+    if (rc) {
+        return rc;
+    }
+    HCL_CUDA(cudaStreamSynchronize(h->stream));
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
+} // extern "C"
+
+// Reverse pass without the final synchronisation (the ensemble runs many concurrently).
+static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double* grad, int memory)
+{
     HCL_CHECK_HANDLE(h);
     if (!h->adj_ready) {
         return fail(HCL_ERR_CONFIG, "call hcl_adjoint_forward first");
@@ -1382,10 +1399,14 @@ int hcl_adjoint_backward(hcl_handle* h, const double* lam_final, double* grad, i
     if (!h->adj_ctl && (rc = dalloc(&h->adj_ctl, 1))) {
         return rc;
     }
-    cudaFree(h->adj_ddts);
-    h->adj_ddts = nullptr;
-    if ((rc = dalloc(&h->adj_ddts, (size_t)N + 8))) {
-        return rc;
+    if (h->adj_ddts_cap < N + 8) {
+        cudaFree(h->adj_ddts);
+        h->adj_ddts = nullptr;
+        h->adj_ddts_cap = 0;
+        if ((rc = dalloc(&h->adj_ddts, (size_t)N + 8))) {
+            return rc;
+        }
+        h->adj_ddts_cap = N + 8;
     }
     cudaStream_t s = h->stream;
     HCL_CUDA(cudaMemcpyAsync(h->adj_ddts, h->adj_dts.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
@@ -1438,7 +1459,416 @@ int hcl_adjoint_backward(hcl_handle* h, const double* lam_final, double* grad, i
     hcl::adjoint::zero_ghosts(g, lam[cur], s);
     hcl::fused::unpack_state(g, lam[cur], grad, grad + g.N, grad + g.N * (nd + 1),
                              memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
-    HCL_CUDA(cudaStreamSynchronize(s));
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
+// ---- batched ensemble ----------------------------------------------------------
+struct hcl_ensemble {
+    std::vector<hcl_handle*> h;
+    std::vector<hcl::ensemble::Prob> probs;
+    hcl::ensemble::Prob* d_probs = nullptr;
+    hcl::ensemble::Prob* d_probs_tune = nullptr;
+    int* d_items = nullptr;
+    int nitems = 0;
+    int items_L = 0;
+    unsigned int* d_barrier = nullptr;
+    int* d_status = nullptr;
+    cudaStream_t stream = nullptr;
+    int lim = 0, rs = 0;
+    int L = 0, bps = 0; // tuned schedule
+    int64_t cells = 0;
+    std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs; // (nsteps, step0, L, bps)
+};
+
+namespace {
+
+void free_ensemble(hcl_ensemble* e)
+{
+    if (!e) {
+        return;
+    }
+    for (auto& kv : e->graphs) {
+        cudaGraphExecDestroy(kv.second);
+    }
+    cudaFree(e->d_probs);
+    cudaFree(e->d_probs_tune);
+    cudaFree(e->d_items);
+    cudaFree(e->d_barrier);
+    cudaFree(e->d_status);
+    if (e->stream) {
+        cudaStreamDestroy(e->stream);
+    }
+    for (hcl_handle* h : e->h) {
+        free_handle(h);
+    }
+    delete e;
+}
+
+// Work list of warp strips of L rows over every problem.
+int ensemble_build_items(hcl_ensemble* e, int L)
+{
+    if (e->items_L == L) {
+        return HCL_OK;
+    }
+    std::vector<int> items;
+    for (size_t p = 0; p < e->h.size(); ++p) {
+        hcl::ensemble::Prob& P = e->probs[p];
+        P.ncolw = (P.g.nx[0] + hcl::fused::kStripLanesOut - 1) / hcl::fused::kStripLanesOut;
+        P.nstrip = (P.g.nx[1] + L - 1) / L;
+        P.item0 = (int)items.size();
+        items.insert(items.end(), (size_t)P.ncolw * P.nstrip, (int)p);
+    }
+    cudaFree(e->d_items);
+    e->d_items = nullptr;
+    int rc = dalloc(&e->d_items, items.size());
+    if (rc) {
+        return rc;
+    }
+    HCL_CUDA(cudaMemcpy(e->d_items, items.data(), sizeof(int) * items.size(), cudaMemcpyHostToDevice));
+    e->nitems = (int)items.size();
+    e->items_L = L;
+    // device copies of the problem table (live control blocks and tuning copies)
+    std::vector<hcl::ensemble::Prob> tune = e->probs;
+    for (size_t p = 0; p < e->h.size(); ++p) {
+        tune[p].ctl = e->h[p]->ctl_tune;
+        tune[p].dt_log = nullptr;
+    }
+    HCL_CUDA(cudaMemcpy(e->d_probs, e->probs.data(), sizeof(hcl::ensemble::Prob) * e->probs.size(),
+                        cudaMemcpyHostToDevice));
+    HCL_CUDA(cudaMemcpy(e->d_probs_tune, tune.data(), sizeof(hcl::ensemble::Prob) * tune.size(), cudaMemcpyHostToDevice));
+    return HCL_OK;
+}
+
+int ensemble_launch(hcl_ensemble* e, const hcl::ensemble::Prob* probs, int nsteps, int step0, int L, int bps,
+                    int use_graph, double cfl, int* graphed)
+{
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->h[0]->cfg.device);
+    const int grid = bps * nsm;
+    hcl::ensemble::Params ep;
+    std::memset(&ep, 0, sizeof(ep));
+    ep.cfl = cfl;
+    ep.nsteps = nsteps;
+    ep.step0 = step0;
+    ep.L = L;
+    ep.nitems = e->nitems;
+    ep.nprob = (int)e->h.size();
+    auto issue = [&]() -> cudaError_t {
+        cudaError_t err = cudaMemsetAsync(e->d_barrier, 0, sizeof(unsigned int), e->stream);
+        if (err == cudaSuccess) {
+            err = cudaMemsetAsync(e->d_status, 0, sizeof(int), e->stream);
+        }
+        if (err == cudaSuccess) {
+            err = hcl::ensemble::launch(e->lim, e->rs, grid, probs, e->d_items, ep, e->d_barrier, e->d_status, e->stream);
+        }
+        return err;
+    };
+    *graphed = 0;
+    if (use_graph && probs == e->d_probs) {
+        const auto key = std::make_tuple(nsteps, step0, L, bps);
+        auto it = e->graphs.find(key);
+        if (it == e->graphs.end()) {
+            cudaGraph_t graph;
+            HCL_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+            const cudaError_t err = issue();
+            cudaError_t err2 = cudaStreamEndCapture(e->stream, &graph);
+            if (err == cudaSuccess && err2 == cudaSuccess) {
+                cudaGraphExec_t exec;
+                if (cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+                    it = e->graphs.emplace(key, exec).first;
+                }
+                cudaGraphDestroy(graph);
+            }
+            cudaGetLastError(); // a failed capture falls back to a direct launch
+        }
+        if (it != e->graphs.end()) {
+            HCL_CUDA(cudaGraphLaunch(it->second, e->stream));
+            *graphed = 1;
+            return HCL_OK;
+        }
+    }
+    HCL_CUDA(issue());
+    return HCL_OK;
+}
+
+// Picks (strip rows, CTAs per SM) by timing one step of every candidate on the
+// tuning control blocks (reads buffer 0, writes buffer 1; the state is kept).
+int ensemble_autotune(hcl_ensemble* e, double cfl)
+{
+    const int maxb = hcl::ensemble::max_blocks_per_sm(e->lim, e->rs);
+    if (maxb <= 0) {
+        return fail(HCL_ERR_CUDA, "ensemble kernel cannot be resident");
+    }
+    cudaEvent_t e0, e1;
+    HCL_CUDA(cudaEventCreate(&e0));
+    HCL_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    const int Ls[3] = {32, 64, 128};
+    for (int L : Ls) {
+        int rc = ensemble_build_items(e, L);
+        if (rc) {
+            return rc;
+        }
+        for (int bps = maxb; bps >= 1 && bps >= maxb - 2; --bps) {
+            float tot = 0;
+            for (int r = 0; r < 3; ++r) {
+                for (hcl_handle* h : e->h) {
+                    hcl::fused::prologue(h->g, h->st[0], h->ctl_tune, 0.0, 0, e->stream);
+                }
+                int graphed = 0;
+                HCL_CUDA(cudaEventRecord(e0, e->stream));
+                if ((rc = ensemble_launch(e, e->d_probs_tune, 1, 0, L, bps, 0, cfl, &graphed))) {
+                    return rc;
+                }
+                HCL_CUDA(cudaEventRecord(e1, e->stream));
+                HCL_CUDA(cudaEventSynchronize(e1));
+                float ms = 0;
+                HCL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (r > 0) {
+                    tot += ms;
+                }
+            }
+            if (tot < best) {
+                best = tot;
+                e->L = L;
+                e->bps = bps;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return ensemble_build_items(e, e->L);
+}
+
+} // namespace
+
+extern "C" {
+
+int hcl_ensemble_create(const hcl_config* cfgs, int nprob, hcl_ensemble** out)
+{
+    if (!cfgs || nprob <= 0 || !out) {
+        return fail(HCL_ERR_ARGUMENT, "ensemble needs configurations");
+    }
+    *out = nullptr;
+    hcl_ensemble* e = new hcl_ensemble();
+    auto bail = [&](int rc) {
+        free_ensemble(e);
+        return rc;
+    };
+    for (int p = 0; p < nprob; ++p) {
+        const hcl_config& c = cfgs[p];
+        if (c.ndim != 2 || c.precision != HCL_FP32_MIXED || c.geometry != HCL_GEOM_CARTESIAN ||
+            c.gravity != HCL_GRAVITY_UNIFORM || c.nfx != 0 || c.limiter != cfgs[0].limiter ||
+            c.riemann != cfgs[0].riemann) {
+            return bail(fail(HCL_ERR_CONFIG, "ensemble problem %d: needs 2-D Cartesian FP32-mixed, uniform gravity, "
+                                             "and the limiter and Riemann solver of problem 0", p));
+        }
+        hcl_handle* h = nullptr;
+        int rc = hcl_create(&c, &h);
+        if (rc) {
+            return bail(rc);
+        }
+        e->h.push_back(h);
+        if (!h->g.uniform_cart) {
+            return bail(fail(HCL_ERR_CONFIG, "ensemble problem %d: the grid must be uniform", p));
+        }
+        hcl::ensemble::Prob P;
+        std::memset(&P, 0, sizeof(P));
+        P.g = h->g;
+        P.q[0] = h->st[0].q;
+        P.q[1] = h->st[1].q;
+        P.plane = h->st[0].plane;
+        P.pitch = h->st[0].pitch;
+        P.ctl = h->ctl;
+        e->probs.push_back(P);
+        e->cells += (int64_t)h->g.nx[0] * h->g.nx[1];
+    }
+    e->lim = cfgs[0].limiter;
+    e->rs = cfgs[0].riemann;
+    HCL_CUDA(cudaSetDevice(cfgs[0].device));
+    int rc;
+    if ((rc = dalloc(&e->d_probs, (size_t)nprob)) || (rc = dalloc(&e->d_probs_tune, (size_t)nprob)) ||
+        (rc = dalloc(&e->d_barrier, 1)) || (rc = dalloc(&e->d_status, 1))) {
+        return bail(rc);
+    }
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        return bail(fail(HCL_ERR_CUDA, "cudaStreamCreate failed"));
+    }
+    *out = e;
+    return HCL_OK;
+}
+
+int hcl_ensemble_destroy(hcl_ensemble* e)
+{
+    if (e) {
+        cudaStreamSynchronize(e->stream);
+    }
+    free_ensemble(e);
+    return HCL_OK;
+}
+
+int hcl_ensemble_handle(hcl_ensemble* e, int p, hcl_handle** h)
+{
+    if (!e || !h || p < 0 || p >= (int)e->h.size()) {
+        return fail(HCL_ERR_ARGUMENT, "bad ensemble index");
+    }
+    *h = e->h[p];
+    return HCL_OK;
+}
+
+int hcl_ensemble_stream(const hcl_ensemble* e, void** stream)
+{
+    if (!e || !stream) {
+        return fail(HCL_ERR_ARGUMENT, "null argument");
+    }
+    *stream = (void*)e->stream;
+    return HCL_OK;
+}
+
+int hcl_ensemble_run(hcl_ensemble* e, const hcl_ensemble_params* p, hcl_ensemble_result* r)
+{
+    if (!e || !p || p->nsteps <= 0) {
+        return fail(HCL_ERR_ARGUMENT, "ensemble run needs nsteps > 0");
+    }
+    HCL_CUDA(cudaSetDevice(e->h[0]->cfg.device));
+    const int N = p->nsteps;
+    int rc;
+    // every problem: state in buffer 0, fresh control block at its current t and iteration
+    std::vector<int> iter0(e->h.size());
+    for (size_t q = 0; q < e->h.size(); ++q) {
+        hcl_handle* h = e->h[q];
+        if (!h->state_valid) {
+            return fail(HCL_ERR_CONFIG, "ensemble problem %zu has no state", q);
+        }
+        StepCtl ctl;
+        if ((rc = read_ctl(h, &ctl))) {
+            return rc;
+        }
+        if (ctl.err) {
+            return fail(HCL_ERR_INVALID_STATE, "ensemble problem %zu holds an invalid state", q);
+        }
+        const int qq = (int)(h->counter & 1);
+        if ((rc = restart_clock(h, ctl.t[qq], ctl.iter[qq]))) {
+            return rc;
+        }
+        iter0[q] = ctl.iter[qq];
+        if ((rc = ensure_dt_log(h, iter0[q] + N + 8))) {
+            return rc;
+        }
+        e->probs[q].dt_log = h->dt_log;
+        e->probs[q].dt_cap = h->dt_log_cap;
+        HCL_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    if (p->strip_rows != 0 && p->strip_rows != 32 && p->strip_rows != 64 && p->strip_rows != 128) {
+        return fail(HCL_ERR_ARGUMENT, "strip_rows must be 0 (autotune), 32, 64 or 128");
+    }
+    const int maxb = hcl::ensemble::max_blocks_per_sm(e->lim, e->rs);
+    if (p->blocks_per_sm < 0 || p->blocks_per_sm > maxb) {
+        return fail(HCL_ERR_ARGUMENT, "blocks_per_sm must be in [0, %d] for a co-resident launch", maxb);
+    }
+    e->items_L = 0; // the table carries the dt logs: rebuild it
+    if (p->strip_rows > 0 || p->blocks_per_sm > 0) {
+        e->L = p->strip_rows > 0 ? p->strip_rows : 64;
+        e->bps = p->blocks_per_sm > 0 ? p->blocks_per_sm : hcl::ensemble::max_blocks_per_sm(e->lim, e->rs);
+    } else if (e->L == 0) {
+        if ((rc = ensemble_autotune(e, p->cfl))) {
+            return rc;
+        }
+    }
+    if ((rc = ensemble_build_items(e, e->L))) {
+        return rc;
+    }
+    const int k = p->checkpoint_every > 0 ? p->checkpoint_every : N;
+    const int nseg = (N + k - 1) / k;
+    if (p->checkpoint_every > 0) {
+        for (hcl_handle* h : e->h) {
+            const size_t sz = (size_t)h->st[0].plane * (h->g.ndim + 2);
+            if (h->adj_cap_ck < nseg) {
+                cudaFree(h->adj_ckpt);
+                h->adj_ckpt = nullptr;
+                h->adj_cap_ck = 0;
+                if ((rc = dalloc(&h->adj_ckpt, sz * nseg))) {
+                    return rc;
+                }
+                h->adj_cap_ck = nseg;
+            }
+        }
+    }
+    int graphed_all = 1;
+    int done = 0;
+    for (int sgm = 0; sgm < nseg; ++sgm) {
+        const int len = std::min(k, N - done);
+        if (p->checkpoint_every > 0) {
+            for (hcl_handle* h : e->h) {
+                const size_t sz = (size_t)h->st[0].plane * (h->g.ndim + 2);
+                HCL_CUDA(cudaMemcpyAsync(h->adj_ckpt + sz * sgm, h->st[done & 1].q, sizeof(double) * sz,
+                                         cudaMemcpyDeviceToDevice, e->stream));
+            }
+        }
+        int graphed = 0;
+        if ((rc = ensemble_launch(e, e->d_probs, len, done, e->L, e->bps, p->use_graph, p->cfl, &graphed))) {
+            return rc;
+        }
+        graphed_all &= graphed;
+        done += len;
+    }
+    int status = 0;
+    HCL_CUDA(cudaMemcpyAsync(&status, e->d_status, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    HCL_CUDA(cudaStreamSynchronize(e->stream));
+    HCL_LAUNCH_CHECK();
+    for (size_t q = 0; q < e->h.size(); ++q) {
+        hcl_handle* h = e->h[q];
+        h->counter = N;
+        h->cur = N & 1;
+        h->stopped = 0;
+        // later single-problem steps (and the adjoint's recomputation) use the
+        // same warp-strip code as the ensemble
+        h->mixed_shape = e->L == 32 ? 3 : (e->L == 64 ? 4 : 5);
+        if (p->checkpoint_every > 0) {
+            std::vector<double> all((size_t)iter0[q] + N);
+            HCL_CUDA(cudaMemcpy(all.data(), h->dt_log, sizeof(double) * all.size(), cudaMemcpyDeviceToHost));
+            h->adj_dts.assign(all.begin() + iter0[q], all.end());
+            h->adj_k = k;
+            h->adj_nck = nseg;
+            h->adj_prec = p->adjoint_precision;
+            h->adj_ready = 1;
+        }
+    }
+    if (r) {
+        r->status = status;
+        r->strip_rows = e->L;
+        r->blocks_per_sm = e->bps;
+        int nsm = 0;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->h[0]->cfg.device);
+        r->grid = e->bps * nsm;
+        r->launches = nseg;
+        r->graph = graphed_all;
+        r->cells = e->cells;
+    }
+    if (status == HCL_ERR_TIMEOUT) {
+        return fail(HCL_ERR_TIMEOUT, "ensemble grid barrier timed out");
+    }
+    if (status == HCL_ERR_INVALID_STATE) {
+        return fail(HCL_ERR_INVALID_STATE, "detected invalid volumic internal energy in the ensemble");
+    }
+    return HCL_OK;
+}
+
+int hcl_ensemble_adjoint(hcl_ensemble* e, const double* const* lam_final, double* const* grads, int memory)
+{
+    if (!e || !lam_final || !grads) {
+        return fail(HCL_ERR_ARGUMENT, "null argument");
+    }
+    for (size_t q = 0; q < e->h.size(); ++q) {
+        int rc = adjoint_backward_impl(e->h[q], lam_final[q], grads[q], memory);
+        if (rc) {
+            return rc;
+        }
+    }
+    for (hcl_handle* h : e->h) {
+        HCL_CUDA(cudaStreamSynchronize(h->stream));
+    }
     HCL_LAUNCH_CHECK();
     return HCL_OK;
 }

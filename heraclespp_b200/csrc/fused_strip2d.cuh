@@ -6,14 +6,17 @@
 //  * a warp owns 28 output columns x L output rows.  Lane l holds column
 //    c0 - 2 + l, so x-neighbours (slopes, the left state of an x-face, the
 //    right flux of a cell) come from warp shuffles; lanes 2..29 write output;
-//  * the warp marches up its rows with a register window: at row r it loads
-//    state row r+2, converts it to primitives (FP64 internal-energy recovery),
-//    builds the Hancock face states of row r+1, solves the y-face r+1/2 and
-//    the x-faces of row r, and updates row r in FP64.  Every primitive,
-//    Hancock state and face flux is computed once per lane (plus a 4-row
-//    start-up and the 4 halo lanes), with no shared memory and no barriers;
+//  * the warp marches up its rows with a register window: at row r it turns
+//    the prefetched state row r+2 into primitives (FP64 internal-energy
+//    recovery) and issues the load of row r+3, builds the Hancock face states
+//    of row r+1, solves the y-face r+1/2 and the x-faces of row r, and updates
+//    row r in FP64.  Every primitive, Hancock state and face flux is computed
+//    once per lane (plus a 4-row start-up and the 4 halo lanes), with no
+//    shared memory and no barriers;
 //  * ghost images, the internal-energy check and the CFL max of the new
-//    state are done in the same pass (one atomic per warp).
+//    state are done in the same pass.
+// strip_work() is the per-strip body shared by the single-domain kernel and
+// the persistent ensemble kernel.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -23,10 +26,9 @@
 #include "fused_step.cuh"
 #include "hcl_device.cuh"
 #include "physics_fast.cuh"
+#include "stages.hpp"
 
 namespace hcl::fused {
-
-constexpr int kStripLanesOut = 28;
 
 template <int LIM>
 __device__ __forceinline__ float lim_fast(float dR, float dL)
@@ -49,14 +51,16 @@ __device__ __forceinline__ float lim_fast(float dR, float dL)
 
 struct StripCtx {
     fast::Eos eos;
-    float cthx, cthy;   // (dt/2)/dx, (dt/2)/dy
-    float dgx, dgy;     // (dt/2) g
+    float cthx, cthy; // (dt/2)/dx, (dt/2)/dy
+    float dgx, dgy;   // (dt/2) g
 };
 
-// FP64 state row -> FP32 primitives, internal energy recovered in FP64
+// FP64 state -> FP32 primitives, internal energy recovered in FP64 (the
+// reciprocal starts from the hardware approximation and takes one FP64
+// Newton step: ~1e-14 relative)
 __device__ __forceinline__ void strip_prim(double gm1, const double q[4], float w[4])
 {
-    double r = (double)__frcp_rn((float)q[0]);
+    double r = (double)__fdividef(1.f, (float)q[0]);
     r = r * (2.0 - q[0] * r);
     const double u = q[1] * r;
     const double v = q[2] * r;
@@ -65,6 +69,26 @@ __device__ __forceinline__ void strip_prim(double gm1, const double q[4], float 
     w[1] = (float)u;
     w[2] = (float)v;
     w[3] = (float)(gm1 * fma(-0.5, mu, q[3]));
+}
+
+// conservative state and physical flux of a face primitive state along l
+// (hydro/euler_equations.hpp:72-86, :124-134), sharing the products
+__device__ __forceinline__ void cons_and_flux(const fast::Eos& e, const float w[4], int l, float U[4], float F[4])
+{
+    const float m0 = w[0] * w[1];
+    const float m1 = w[0] * w[2];
+    const float Et = fmaf(0.5f, fmaf(m0, w[1], m1 * w[2]), w[3] * e.inv_gm1);
+    U[0] = w[0];
+    U[1] = m0;
+    U[2] = m1;
+    U[3] = Et;
+    const float ml = l == 0 ? m0 : m1;
+    const float ul = l == 0 ? w[1] : w[2];
+    F[0] = ml;
+    F[1] = ml * w[1];
+    F[2] = ml * w[2];
+    F[1 + l] += w[3];
+    F[3] = ul * (Et + w[3]);
 }
 
 // Hancock face states of one cell: x-left, x-right, y-bottom, y-top (conservative)
@@ -84,30 +108,26 @@ __device__ __forceinline__ void strip_hancock(const StripCtx& c, const float wd[
         fyB[v] = wc[v] - sy;
         fyT[v] = wc[v] + sy;
     }
-    float a[4], b[4], inc[4];
-    fast::flux_prim<2>(c.eos, fxL, 0, a);
-    fast::flux_prim<2>(c.eos, fxR, 0, b);
+    float FxL[4], FxR[4], FyB[4], FyT[4];
+    cons_and_flux(c.eos, fxL, 0, hxL, FxL);
+    cons_and_flux(c.eos, fxR, 0, hxR, FxR);
+    cons_and_flux(c.eos, fyB, 1, hyB, FyB);
+    cons_and_flux(c.eos, fyT, 1, hyT, FyT);
+    float inc[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        inc[v] = c.cthx * (a[v] - b[v]);
-    }
-    fast::flux_prim<2>(c.eos, fyB, 1, a);
-    fast::flux_prim<2>(c.eos, fyT, 1, b);
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        inc[v] = fmaf(c.cthy, a[v] - b[v], inc[v]);
+        inc[v] = fmaf(c.cthx, FxL[v] - FxR[v], c.cthy * (FyB[v] - FyT[v]));
     }
     float* outs[4] = {hxL, hxR, hyB, hyT};
-    const float* ins[4] = {fxL, fxR, fyB, fyT};
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-        float u[4];
-        fast::to_cons<2>(c.eos, ins[f], u);
+        float* u = outs[f];
         // gravity on the face state (extrapolation_reconstruction.hpp:306-312)
-        outs[f][0] = u[0] + inc[0];
-        outs[f][1] = fmaf(c.dgx, u[0], u[1] + inc[1]);
-        outs[f][2] = fmaf(c.dgy, u[0], u[2] + inc[2]);
-        outs[f][3] = fmaf(c.dgx, u[1], fmaf(c.dgy, u[2], u[3] + inc[3]));
+        const float r0 = u[0], m0 = u[1], m1 = u[2];
+        u[0] = r0 + inc[0];
+        u[1] = fmaf(c.dgx, r0, m0 + inc[1]);
+        u[2] = fmaf(c.dgy, r0, m1 + inc[2]);
+        u[3] = fmaf(c.dgx, m0, fmaf(c.dgy, m1, u[3] + inc[3]));
     }
 }
 
@@ -117,56 +137,14 @@ __device__ __forceinline__ void strip_riemann(const fast::Eos& e, const float* L
     fast::riemann<2>(e, RS, L, R, l, F);
 }
 
+// One strip (28 columns x rows [r0, r1)) of one domain: reads qin, writes qout.
+// Accumulates the CFL max and the first bad cell of the lanes' output cells.
 template <int LIM, int RS>
-__global__ void __launch_bounds__(128)
-k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
+__device__ __forceinline__ void strip_work(const GridDev& g, const double* __restrict__ qin, double* __restrict__ qout,
+                                           int64_t plane, int pitch, double dt, int sx, int sy, int L, double& inv_max,
+                                           int64_t& bad_cell)
 {
     const int lane = threadIdx.x & 31;
-    const Decision dec = decide(ctl, slot, rp);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const int q = (slot + 1) & 1;
-        if (!dec.noop) {
-            ctl->t[q] = dec.t + dec.dt;
-            ctl->iter[q] = dec.iter + 1;
-            ctl->time_output_id[q] = dec.toid_next;
-            ctl->iter_output_id[q] = dec.ioid_next;
-            ctl->stop[q] = dec.stop;
-            ctl->last_dt = dec.dt;
-            if (dec.stop) {
-                ctl->final_buf = out_buf;
-            }
-            if (dec.neg_dt) {
-                ctl->err = 5;
-                ctl->errflag[q] = 1;
-                ctl->t[q] = dec.t;
-                ctl->iter[q] = dec.iter;
-                ctl->final_buf = out_buf ^ 1;
-            }
-            if (rp.dt_log && dec.iter < rp.dt_log_cap && !dec.neg_dt) {
-                rp.dt_log[dec.iter] = dec.dt;
-            }
-        } else {
-            ctl->t[q] = dec.t;
-            ctl->iter[q] = dec.iter;
-            ctl->time_output_id[q] = dec.toid_next;
-            ctl->iter_output_id[q] = dec.ioid_next;
-            ctl->stop[q] = 1;
-            ctl->errflag[q] = ctl->errflag[slot & 1];
-        }
-        ctl->inv_dt_bits[(slot + 2) % 3] = 0ull;
-    }
-    if (dec.noop || dec.neg_dt) {
-        return;
-    }
-    const double dt = dec.dt;
-    const int ncolw = (g.nx[0] + kStripLanesOut - 1) / kStripLanesOut;
-    const int nstrip = (g.nx[1] + L - 1) / L;
-    const int wg = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (wg >= ncolw * nstrip) {
-        return;
-    }
-    const int sx = wg % ncolw;
-    const int sy = wg / ncolw;
     const int n0 = g.n[0], n1 = g.n[1];
     const int c0 = g.ng + kStripLanesOut * sx;
     const int col = c0 - 2 + lane;
@@ -186,9 +164,6 @@ k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     const double dgx = dt * g.g[0];
     const double dgy = dt * g.g[1];
     const double gm1 = g.gamma_m1;
-    const double* __restrict__ qin = in.q;
-    const int64_t plane = in.plane;
-    const int pitch = in.pitch;
 
     auto load_row = [&](int r, double q[4]) {
         const int rc = min(max(r, 0), n1 - 1);
@@ -200,68 +175,78 @@ k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     };
 
     // preamble: rows r0-2 .. r0+1 -> primitives; Hancock of rows r0-1 and r0
-    double qA[4], qB[4], qC[4], qD[4];
-    float wA[4], wB[4], wC[4], wD[4];
-    load_row(r0 - 2, qA);
-    load_row(r0 - 1, qB);
-    load_row(r0, qC);
-    load_row(r0 + 1, qD);
-    strip_prim(gm1, qA, wA);
-    strip_prim(gm1, qB, wB);
-    strip_prim(gm1, qC, wC);
-    strip_prim(gm1, qD, wD);
-    float hxL[4], hxR[4], hyB[4], hyT[4];
-    float G_lo[4];
+    float wB[4], wC[4], wD[4];
+    float hxL[4], hxR[4], hyT[4];
+    double Glo[4];
+    double qPre[4];
     {
-        float t0[4], t1[4], t2[4];
-        strip_hancock<LIM>(c, wA, wB, wC, t0, t1, t2, hyT); // row r0-1: keep its top face
-        strip_hancock<LIM>(c, wB, wC, wD, hxL, hxR, hyB, t0); // row r0
-        strip_riemann<RS>(c.eos, hyT, hyB, 1, G_lo);
-        hyT[0] = t0[0];
-        hyT[1] = t0[1];
-        hyT[2] = t0[2];
-        hyT[3] = t0[3];
+        double q[4];
+        float wA[4], hyB[4];
+        load_row(r0 - 2, q);
+        strip_prim(gm1, q, wA);
+        load_row(r0 - 1, q);
+        strip_prim(gm1, q, wB);
+        load_row(r0, q);
+        strip_prim(gm1, q, wC);
+        load_row(r0 + 1, q);
+        strip_prim(gm1, q, wD);
+        load_row(r0 + 2, qPre);
+        float t0[4], t1[4], t2[4], tT[4];
+        strip_hancock<LIM>(c, wA, wB, wC, t0, t1, t2, tT); // row r0-1: keep its top face
+        strip_hancock<LIM>(c, wB, wC, wD, hxL, hxR, hyB, hyT); // row r0
+        float G[4];
+        strip_riemann<RS>(c.eos, tT, hyB, 1, G);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            Glo[v] = (double)G[v];
+        }
     }
-    // window: wm = P[r-1] (wB), wc = P[r] (wC), wp = P[r+1] (wD); qc = U[r] (qC), qn = U[r+1] (qD)
-    double inv_max = 0.0;
-    bool bad = false;
-    int64_t bad_cell = -1;
+    // window: wC = P[r], wD = P[r+1]; qPre = U[r+2] (in flight)
     for (int r = r0; r < r1; ++r) {
-        double qN[4];
         float wN[4];
-        load_row(r + 2, qN);
-        strip_prim(gm1, qN, wN);
+        strip_prim(gm1, qPre, wN);
+        load_row(r + 3, qPre); // prefetch for the next row
         // Hancock of row r+1
         float nxL[4], nxR[4], nyB[4], nyT[4];
         strip_hancock<LIM>(c, wC, wD, wN, nxL, nxR, nyB, nyT);
         // y-face r+1/2
-        float G_hi[4];
-        strip_riemann<RS>(c.eos, hyT, nyB, 1, G_hi);
+        float G[4];
+        strip_riemann<RS>(c.eos, hyT, nyB, 1, G);
+        double Ghi[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            Ghi[v] = (double)G[v];
+        }
         // x-faces of row r: left face at this lane, right face from lane+1
-        float uL[4], Fl[4], Fr[4];
+        float uL[4], Fl[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             uL[v] = __shfl_up_sync(0xffffffffu, hxR[v], 1);
         }
         strip_riemann<RS>(c.eos, uL, hxL, 0, Fl);
+        double Fld[4], Frd[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            Fr[v] = __shfl_down_sync(0xffffffffu, Fl[v], 1);
+            Fld[v] = (double)Fl[v];
+            Frd[v] = __shfl_down_sync(0xffffffffu, Fld[v], 1);
         }
-        // Godunov update of row r in FP64 (godunov_scheme.hpp:159-163, 258-260)
-        double qn[4];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const double fx = (double)Fl[v] - (double)Fr[v];
-            const double fy = (double)G_lo[v] - (double)G_hi[v];
-            qn[v] = qC[v] + fma(cx, fx, cy * fy);
-        }
-        qn[1] = fma(dgx, qC[0], qn[1]);
-        qn[2] = fma(dgy, qC[0], qn[2]);
-        qn[3] = fma(dgx, qC[1], fma(dgy, qC[2], qn[3]));
         if (out_lane) {
+            // Godunov update of row r in FP64 (godunov_scheme.hpp:159-163, 258-260)
+            double q[4], qn[4];
+            const int64_t oo = (int64_t)r * pitch + col;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                q[v] = __ldg(qin + oo + plane * v);
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                qn[v] = q[v] + fma(cx, Fld[v] - Frd[v], cy * (Glo[v] - Ghi[v]));
+            }
+            qn[1] = fma(dgx, q[0], qn[1]);
+            qn[2] = fma(dgy, q[0], qn[2]);
+            qn[3] = fma(dgx, q[1], fma(dgy, q[2], qn[3]));
             // health check (main.cpp:397-425) and CFL (time_step.hpp:55-77) of the new state
-            double rr = (double)__frcp_rn((float)qn[0]);
+            double rr = (double)__fdividef(1.f, (float)qn[0]);
             rr = rr * (2.0 - qn[0] * rr);
             const double u = qn[1] * rr;
             const double vv = qn[2] * rr;
@@ -272,14 +257,12 @@ k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             const double snd = c2 * y;
             const double cell = fma(fabs(u) + snd, g.inv_dx[0], (fabs(vv) + snd) * g.inv_dx[1]);
             inv_max = cell > inv_max ? cell : (isnan(cell) ? cell : inv_max);
-            if (!(evol >= 0.0)) {
-                bad = true;
+            if (!(evol >= 0.0) && bad_cell < 0) {
                 bad_cell = lidx(g, col, r, 0);
             }
-            const int64_t oo = (int64_t)r * pitch + col;
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
-                out.q[oo + plane * v] = qn[v];
+                qout[oo + plane * v] = qn[v];
             }
             // ghost images of border cells (boundary_distribute.hpp:42-76)
             if (!(col >= 2 * g.ng && col < n0 - 2 * g.ng && r >= 2 * g.ng && r < n1 - 2 * g.ng)) {
@@ -296,30 +279,87 @@ k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
                             continue;
                         }
                         const int64_t og = (int64_t)py[b] * pitch + px[a];
-                        out.q[og] = qn[0];
-                        out.q[og + plane] = fx[a] ? -qn[1] : qn[1];
-                        out.q[og + 2 * plane] = fy[b] ? -qn[2] : qn[2];
-                        out.q[og + 3 * plane] = qn[3];
+                        qout[og] = qn[0];
+                        qout[og + plane] = fx[a] ? -qn[1] : qn[1];
+                        qout[og + 2 * plane] = fy[b] ? -qn[2] : qn[2];
+                        qout[og + 3 * plane] = qn[3];
                     }
                 }
             }
         }
-        // rotate the window
+        // slide the window
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            wB[v] = wC[v];
             wC[v] = wD[v];
             wD[v] = wN[v];
-            qC[v] = qD[v];
-            qD[v] = qN[v];
             hxL[v] = nxL[v];
             hxR[v] = nxR[v];
             hyT[v] = nyT[v];
-            G_lo[v] = G_hi[v];
+            Glo[v] = Ghi[v];
         }
     }
+    (void)wB;
+}
+
+// time-loop control of one step, published by one thread (main.cpp:354-385)
+__device__ __forceinline__ void publish_decision(StepCtl* ctl, const Decision& dec, const RunParamsDev& rp, int slot,
+                                                 int out_buf)
+{
+    const int q = (slot + 1) & 1;
+    if (!dec.noop) {
+        ctl->t[q] = dec.t + dec.dt;
+        ctl->iter[q] = dec.iter + 1;
+        ctl->time_output_id[q] = dec.toid_next;
+        ctl->iter_output_id[q] = dec.ioid_next;
+        ctl->stop[q] = dec.stop;
+        ctl->last_dt = dec.dt;
+        if (dec.stop) {
+            ctl->final_buf = out_buf;
+        }
+        if (dec.neg_dt) {
+            ctl->err = 5;
+            ctl->errflag[q] = 1;
+            ctl->t[q] = dec.t;
+            ctl->iter[q] = dec.iter;
+            ctl->final_buf = out_buf ^ 1;
+        }
+        if (rp.dt_log && dec.iter < rp.dt_log_cap && !dec.neg_dt) {
+            rp.dt_log[dec.iter] = dec.dt;
+        }
+    } else {
+        ctl->t[q] = dec.t;
+        ctl->iter[q] = dec.iter;
+        ctl->time_output_id[q] = dec.toid_next;
+        ctl->iter_output_id[q] = dec.ioid_next;
+        ctl->stop[q] = 1;
+        ctl->errflag[q] = ctl->errflag[slot & 1];
+    }
+    ctl->inv_dt_bits[(slot + 2) % 3] = 0ull;
+}
+
+template <int LIM, int RS>
+__global__ void __launch_bounds__(128)
+k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
+{
+    const int lane = threadIdx.x & 31;
+    const Decision dec = decide(ctl, slot, rp);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        publish_decision(ctl, dec, rp, slot, out_buf);
+    }
+    if (dec.noop || dec.neg_dt) {
+        return;
+    }
+    const int ncolw = (g.nx[0] + kStripLanesOut - 1) / kStripLanesOut;
+    const int nstrip = (g.nx[1] + L - 1) / L;
+    const int wg = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (wg >= ncolw * nstrip) {
+        return;
+    }
+    double inv_max = 0.0;
+    int64_t bad_cell = -1;
+    strip_work<LIM, RS>(g, in.q, out.q, in.plane, in.pitch, dec.dt, wg % ncolw, wg / ncolw, L, inv_max, bad_cell);
     // warp max of 1/dt -> one atomic per warp
-    bool nan_seen = isnan(inv_max);
+    const bool nan_seen = isnan(inv_max);
     double m = nan_seen ? 0.0 : inv_max;
     m = warp_max_d(m);
     const unsigned nanv = __ballot_sync(0xffffffffu, nan_seen);
@@ -329,7 +369,7 @@ k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             atomicMax(&ctl->inv_dt_bits[(slot + 1) % 3], 0x7ff8000000000000ull);
         }
     }
-    if (bad) {
+    if (bad_cell >= 0) {
         atomicMin(&ctl->bad_cell, (unsigned long long)bad_cell);
         ctl->err = 4;
         ctl->errflag[(slot + 1) & 1] = 1;

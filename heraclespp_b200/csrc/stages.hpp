@@ -47,6 +47,10 @@ void integrate(const GridDev& g, const double* var, double* partials, double* ou
 
 namespace fused {
 
+// Output columns of one warp strip of the 2-D mixed kernel (32 lanes less a
+// 2-cell halo on each side).
+constexpr int kStripLanesOut = 28;
+
 // State buffers of the fused path: nvar planes, each n2*n1*pitch doubles with
 // the x0 row padded to `pitch` (a multiple of 16 doubles).
 struct StateDev {
@@ -84,6 +88,40 @@ void unpack_state(const GridDev& g, const StateDev& st, double* rho, double* rho
 void conservation_sums(const GridDev& g, const StateDev& st, double* partials, double* out_dev, cudaStream_t s);
 
 } // namespace fused
+
+namespace ensemble {
+
+// One problem of the batch: its grid, its two state buffers, its control
+// block, dt log and its range of work items (warp strips).
+struct Prob {
+    GridDev g;
+    double* q[2];
+    int64_t plane;
+    int pitch;
+    int ncolw, nstrip;
+    int item0;
+    StepCtl* ctl;
+    double* dt_log;
+    int dt_cap;
+};
+
+struct Params {
+    double cfl;
+    int nsteps;
+    int step0;   // global step index of the first step (slots and buffers)
+    int L;       // strip rows
+    int nitems;
+    int nprob;
+    int fixed_dt;
+    const double* dts; // [nprob][dts_stride], indexed by iteration
+    int dts_stride;
+};
+
+int max_blocks_per_sm(int lim, int rs);
+cudaError_t launch(int lim, int rs, int grid, const Prob* probs, const int* item_prob, const Params& ep,
+                   unsigned int* barrier, int* status, cudaStream_t s);
+
+} // namespace ensemble
 
 namespace adjoint {
 

@@ -242,7 +242,7 @@ int hcl_get_stream(const hcl_handle* h, void** stream);
  * grids, uniform gravity, HLL/HLLC, every limiter.  Branches (limiter sign
  * tests, wave-speed min/max, HLLC switches) are differentiated along the
  * branch the forward evaluation took.  No reference counterpart: the
- * reference has no adjoint (BASELINE north_star asks for one). */
+ * reference has no adjoint. */
 typedef struct hcl_adjoint_params {
     int nsteps;
     const double* dts;        /* host, nsteps values; NULL: CFL dt of this forward run (recorded) */
@@ -264,6 +264,50 @@ int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p);
 int hcl_adjoint_backward(hcl_handle* h, const double* lam_final, double* grad, int memory);
 /* The dt of each step of the last hcl_adjoint_forward (host array of nsteps). */
 int hcl_adjoint_dts(const hcl_handle* h, double* dts, int max_count, int* count);
+
+/* ---- batched ensemble of independent 2-D problems --------------------------- */
+/* Many independent domains (uneven grids) stepped together by one persistent
+ * cooperative kernel: warp strips of every problem are the work items, each
+ * problem keeps its own CFL dt, and a bounded grid barrier (HCL_ERR_TIMEOUT
+ * instead of a hang) separates steps.  Every problem must be 2-D, uniform
+ * Cartesian, uniform gravity, FP32-mixed, and share one limiter and Riemann
+ * solver.  No reference counterpart: the reference runs one domain per
+ * executable. */
+typedef struct hcl_ensemble hcl_ensemble;
+
+typedef struct hcl_ensemble_params {
+    int nsteps;               /* steps every problem takes */
+    double cfl;
+    int checkpoint_every;     /* > 0: store checkpoints for hcl_ensemble_adjoint */
+    int strip_rows;           /* 0: autotune among 32/64/128 */
+    int blocks_per_sm;        /* 0: autotune */
+    int use_graph;            /* 1: capture the persistent launch in a CUDA graph and replay it */
+    int adjoint_precision;    /* HCL_FP64 or HCL_FP32_MIXED reverse sweep for hcl_ensemble_adjoint */
+} hcl_ensemble_params;
+
+typedef struct hcl_ensemble_result {
+    int status;               /* HCL_OK, HCL_ERR_INVALID_STATE, HCL_ERR_TIMEOUT */
+    int strip_rows;           /* schedule used */
+    int blocks_per_sm;
+    int grid;                 /* CTAs of the persistent launch */
+    int launches;             /* persistent launches issued (1 per checkpoint segment) */
+    int graph;                /* 1 when replayed from a CUDA graph */
+    int64_t cells;            /* interior cells over all problems */
+} hcl_ensemble_result;
+
+/* Creates one handle per configuration (hcl_create) plus the batch. */
+int hcl_ensemble_create(const hcl_config* cfgs, int nprob, hcl_ensemble** out);
+int hcl_ensemble_destroy(hcl_ensemble* e);
+/* Handle of problem p (set its state, read results, per-problem queries). */
+int hcl_ensemble_handle(hcl_ensemble* e, int p, hcl_handle** h);
+int hcl_ensemble_stream(const hcl_ensemble* e, void** stream);
+/* Advances every problem by nsteps (synchronises at the end). */
+int hcl_ensemble_run(hcl_ensemble* e, const hcl_ensemble_params* p, hcl_ensemble_result* r);
+/* Reverse pass of the last run (which needs checkpoint_every > 0): for every
+ * problem p, lam_final[p] = dJ/dU_p^N and grads[p] receives dJ/dU_p^0 (same
+ * buffer layout as hcl_adjoint_backward).  The problems' sweeps run
+ * concurrently on their own streams. */
+int hcl_ensemble_adjoint(hcl_ensemble* e, const double* const* lam_final, double* const* grads, int memory);
 
 /* ---- .ini front end (host only) ------------------------------------------ */
 /* Compile-time choices of the reference (CMake Heraclespp_NDIM, _GEOM,

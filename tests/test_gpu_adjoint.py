@@ -19,10 +19,30 @@ pytestmark = pytest.mark.gpu
 KW = dict(gamma=5.0 / 3.0, limiter="VanLeer", riemann="HLLC", bc=["Periodic"] * 4)
 
 
-def problem(n, nsteps, precision="fp64"):
+def smooth_background(grid, prim, amp=0.02, seed=11):
+    """Adds smooth seeded Fourier modes to rho and P.  The plain Gresho vortex
+    is exactly uniform for r > 0.4; there every limited slope sits on the
+    limiter's kink (phi(R, L) is homogeneous of degree one at R = L = 0), so a
+    central difference sees a directional derivative that no branch-following
+    derivative has.  The modulation removes the flat region."""
+    rng = np.random.default_rng(seed)
+    s3, (X, Y, Z), _ = grid.interior()
+    rho, u, P = (a.copy() for a in prim)
+    for _ in range(3):
+        kx, ky = rng.integers(1, 3, size=2)
+        ph = rng.uniform(0, 2 * np.pi, size=2)
+        m = np.sin(2 * np.pi * kx * X + ph[0]) * np.sin(2 * np.pi * ky * Y + ph[1])
+        rho[s3] = rho[s3] * (1 + amp * m)
+        P[s3] = P[s3] * (1 + amp * np.roll(m, 3, axis=-1))
+    return rho, u, P
+
+
+def problem(n, nsteps, precision="fp64", smooth=True):
     o = Oracle(2, [n, n], **KW)
     grid = setups.Grid.from_domain(o)
     prim = setups.gresho_vortex(grid)
+    if smooth:
+        prim = smooth_background(grid, prim)
     rho, rhou, E, _ = o.init_from_prim(*prim)
     U0 = np.concatenate([rho[None], rhou, E[None]])  # (4, 1, n+4, n+4)
     d = Domain(2, [n, n], precision=precision, **KW)
@@ -71,14 +91,15 @@ def test_adjoint_matches_finite_differences(n, nsteps, k, ndir):
     for _ in range(ndir):
         v = np.zeros_like(U0)
         v[:, :, ng:-ng, ng:-ng] = rng.uniform(-1, 1, (4, 1, n, n)) * np.abs(U0[:, :, ng:-ng, ng:-ng])
-        eps = 1e-6
+        eps = 1e-7
         jp = J_of(d, o, U0 + eps * v, dts, target)
         jm = J_of(d, o, U0 - eps * v, dts, target)
         fd = (jp - jm) / (2 * eps)
         ad = float(np.sum(g * v))
         errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
     errs = np.array(errs)
-    # smooth flow: all directions agree to 1e-5 except a few that straddle a
+    print(f"n={n} steps={nsteps}: FD rel err median {np.median(errs):.2e} max {errs.max():.2e}")
+    # smooth flow: the directions agree to 1e-5 except any that straddle a
     # limiter / wave-speed switch (the map is only piecewise smooth)
     assert np.median(errs) < 1e-6, errs
     assert np.mean(errs < 1e-5) >= 0.9, errs

@@ -1,0 +1,101 @@
+"""The .ini front end (hcl_create_from_ini) and the heracles_b200 driver:
+the same input file the reference reads, run on the GPU, checked bitwise
+against the oracle run of the same problem."""
+import struct
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from heraclespp_b200 import setups
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parents[1]
+DRIVER = ROOT / "heraclespp_b200" / "bin" / "heracles_b200"
+
+# inputs/shock_tube.ini of the reference with Nx0_glob = 1024 (Sod, 1024 cells)
+SOD_INI = """
+[Grid]
+Nx0_glob = 1024
+Nx1_glob = 1
+Nx2_glob = 1
+x0min = 0
+x0max = 1
+
+[Run]
+t_end = 0.2
+cfl = 0.4
+
+[Output]
+max_iter = 100000
+time_frequency = 0.1
+prefix = shock_tube
+
+[Hydro]
+reconstruction = Minmod
+riemann_solver = HLLC
+
+[Boundary Condition]
+BC_X0 = NullGradient
+
+[Perfect Gas]
+gamma = 1.4
+
+[Initialisation]
+rho0 = 1
+rho1 = 0.125
+u0 = 0
+u1 = 0
+P0 = 1
+P1 = 0.1
+inter = 0.5
+"""
+
+
+def read_dump(path):
+    b = Path(path).read_bytes()
+    nd, n0, n1, n2 = struct.unpack("4i", b[:16])
+    t = struct.unpack("d", b[16:24])[0]
+    a = np.frombuffer(b[24:], dtype=np.float64)
+    N = n0 * n1 * n2
+    rho = a[:N].reshape(n2, n1, n0)
+    rhou = a[N:N * (1 + nd)].reshape(nd, n2, n1, n0)
+    E = a[N * (1 + nd):N * (2 + nd)].reshape(n2, n1, n0)
+    return nd, t, rho, rhou, E
+
+
+def sod_oracle():
+    o = Oracle(1, [1024], gamma=1.4, limiter="Minmod", riemann="HLLC", bc=["NullGradient"] * 2)
+    prim = setups.shock_tube(setups.Grid.from_domain(o))
+    rho, rhou, E, fx = o.init_from_prim(*prim)
+    t, it, st, _ = o.run(rho, rhou, E, fx, cfl=0.4, t_end=0.2, max_iter=100000, time_frequency=0.1)
+    return t, it, rho, rhou, E
+
+
+def test_driver_runs_reference_ini_bitwise(tmp_path):
+    assert DRIVER.exists(), "driver not built"
+    ini = tmp_path / "shock_tube.ini"
+    ini.write_text(SOD_INI)
+    dump = tmp_path / "out.bin"
+    res = subprocess.run([str(DRIVER), str(ini), "--setup=shock_tube", f"--output={dump}"], capture_output=True,
+                         text=True, timeout=120)
+    assert res.returncode == 0, res.stderr
+    assert "Mean performance:" in res.stdout and "Mcell-updates/s" in res.stdout
+    nd, t, rho, rhou, E = read_dump(dump)
+    t_o, it_o, rho_o, rhou_o, E_o = sod_oracle()
+    assert nd == 1 and t == t_o == 0.2
+    assert f"number of iterations = {it_o}" in res.stdout
+    assert np.array_equal(rho, rho_o) and np.array_equal(rhou, rhou_o) and np.array_equal(E, E_o)
+
+
+def test_driver_rejects_unknown_keys(tmp_path):
+    ini = tmp_path / "bad.ini"
+    ini.write_text(SOD_INI.replace("riemann_solver = HLLC", "riemann_solver = Roe"))
+    res = subprocess.run([str(DRIVER), str(ini)], capture_output=True, text=True, timeout=60)
+    assert res.returncode != 0
+    assert "Invalid riemann solver: Roe." in res.stderr
+    ini.write_text(SOD_INI.replace("gamma = 1.4", "gamma = 1.0"))
+    res = subprocess.run([str(DRIVER), str(ini)], capture_output=True, text=True, timeout=60)
+    assert res.returncode != 0 and "Invalid gamma" in res.stderr
