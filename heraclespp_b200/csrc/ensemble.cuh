@@ -23,27 +23,34 @@ namespace hcl::ensemble {
 
 constexpr long long kSpinLimit = 1ll << 26;
 
+// Returns the same answer to every thread of the CTA (thread 0 decides), so a
+// CTA leaves the step loop as a whole and no warp is left half-exited.
 __device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int target, int* status)
 {
+    __shared__ int go_on;
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         atomicAdd(count, 1u);
         long long spins = 0;
+        int ok = 1;
         while (*(volatile unsigned int*)count < target) {
             if (*(volatile int*)status != 0) {
+                ok = 0;
                 break;
             }
             if (++spins > kSpinLimit) {
                 atomicExch(status, 6); // HCL_ERR_TIMEOUT
+                ok = 0;
                 break;
             }
             __nanosleep(64);
         }
         __threadfence();
+        go_on = ok && *(volatile int*)status == 0;
     }
     __syncthreads();
-    return *(volatile int*)status == 0;
+    return go_on != 0;
 }
 
 template <int LIM, int RS>
