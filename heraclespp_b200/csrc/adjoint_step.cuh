@@ -42,7 +42,7 @@ struct AdjShape {
 };
 
 template <int ND, class R, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1))
+__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1), sizeof(R) == 8 ? 2 : 3)
 k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt)
 {
     using S = Shape<ND, TX, TY, TZ>;

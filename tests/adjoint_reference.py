@@ -8,14 +8,57 @@ periodic ghosts) so the GPU adjoint kernel can be compared to it cell by cell.
 Arrays are [var, j, i] with 2 ghost layers.
 """
 import ctypes as C
+import subprocess
+from pathlib import Path
 
 import numpy as np
 
 NG = 2
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def build_cell_lib(out):
+    """Compiles tests/adjoint_cell_check.cpp (the per-cell forward and reverse
+    functions of adjoint_cell.cuh as host code) into `out` and loads it."""
+    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I", str(ROOT / "heraclespp_b200" / "csrc"),
+                    str(ROOT / "tests" / "adjoint_cell_check.cpp"), "-o", str(out)], check=True)
+    L = C.CDLL(str(out))
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    L.t_riemann_fwd.argtypes = [i, i, d, vp, vp, i, vp]
+    L.t_riemann_rev.argtypes = [i, i, d, vp, vp, i, vp, vp, vp]
+    L.t_flux_fwd.argtypes = [d, vp, i, vp]
+    L.t_flux_rev.argtypes = [d, vp, i, vp, vp]
+    L.t_p2c_fwd.argtypes = [d, vp, vp]
+    L.t_p2c_rev.argtypes = [d, vp, vp, vp]
+    L.t_c2p_fwd.argtypes = [d, vp, vp]
+    L.t_c2p_rev.argtypes = [d, vp, vp, vp]
+    L.t_limiter.argtypes = [i, d, d, C.POINTER(d), C.POINTER(d)]
+    L.t_limiter.restype = d
+    return L
 
 
 def p(a):
     return np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(C.c_void_p)
+
+
+def smooth_state(n, seed=0):
+    """Smooth seeded periodic 2-D conserved state [4, n+4, n+4] (gamma 1.4)."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(n) + 0.5) / n
+    X, Y = np.meshgrid(x, x)
+    rho = 1 + 0.2 * np.sin(2 * np.pi * X + 0.3) * np.cos(2 * np.pi * Y + 0.7) + 0.05 * rng.uniform(-1, 1, (n, n))
+    u = 0.3 * np.sin(2 * np.pi * Y + 0.1) + 0.05 * rng.uniform(-1, 1, (n, n))
+    v = 0.2 * np.cos(2 * np.pi * X + 0.5) + 0.05 * rng.uniform(-1, 1, (n, n))
+    P = 1 + 0.1 * np.cos(2 * np.pi * (X + Y)) + 0.05 * rng.uniform(-1, 1, (n, n))
+    gamma = 1.4
+    U = np.zeros((4, n + 2 * NG, n + 2 * NG))
+    s = (slice(NG, NG + n), slice(NG, NG + n))
+    U[0][s] = rho
+    U[1][s] = rho * u
+    U[2][s] = rho * v
+    U[3][s] = P / (gamma - 1) + 0.5 * rho * (u * u + v * v)
+    Ref.fill_periodic(U)
+    return U
 
 
 class Ref:

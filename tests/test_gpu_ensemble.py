@@ -124,7 +124,11 @@ def test_ensemble_adjoint_matches_single_adjoint(precision):
         g1 = torch.empty_like(lams[p])
         d.adjoint_backward(lams[p], g1, device=True)
         torch.cuda.synchronize()
-        assert torch.equal(grads[p], g1), f"problem {p}"
+        # same forward trajectory and sweep; atomics reorder the sums (FP32
+        # shared-memory accumulators in the mixed sweep)
+        scale = float(torch.max(torch.abs(g1)))
+        tol = 1e-12 if precision == "fp64" else 1e-4
+        assert float(torch.max(torch.abs(grads[p] - g1))) <= tol * scale, f"problem {p}"
         # the objective is not trivial: outflow boundaries let energy leave
         E_grad = grads[p][3, 0, 2:-2, 2:-2]
         dv = lams[p][3, 0, 2:-2, 2:-2]
