@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1871,6 +1872,90 @@ int hcl_ensemble_adjoint(hcl_ensemble* e, const double* const* lam_final, double
     }
     HCL_LAUNCH_CHECK();
     return HCL_OK;
+}
+
+} // extern "C"
+
+// ---- hydro reconstruction with fixed scratch (no allocation) ------------------------
+// hcl_hydro_reconstruction_noalloc keeps the scratch of one call (u_rec, P_rec and
+// fx_rec_old of MUSCLHancockHydroReconstruction) in one fixed device array per
+// device instead of the handle's lazily allocated buffers.
+namespace {
+
+constexpr size_t kNoAllocScratchDoubles = size_t(1) << 22; // 32 MiB
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// Device address of this device's copy of the array, looked up on the first
+// call on each device (the caller has made that device current).
+int noalloc_scratch(int dev, double** out)
+{
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        return fail(HCL_ERR_ARGUMENT, "device %d out of range for the fixed scratch", dev);
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_base[dev]) {
+        void* p = nullptr;
+        const cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (err != cudaSuccess || !p) {
+            return fail(HCL_ERR_CUDA, "cudaGetSymbolAddress of the fixed scratch failed: %s", cudaGetErrorString(err));
+        }
+        g_noalloc_base[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_base[dev];
+    return HCL_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int hcl_hydro_reconstruction_noalloc(hcl_handle* h, int ng_eff, double dt, const double* rho, const double* u,
+                                     const double* P, const double* fx, double* rho_rec, double* rhou_rec,
+                                     double* E_rec, double* fx_rec, void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    HCL_CHECK_NGEFF(h, ng_eff);
+    if (ng_eff > h->g.ng - 1) {
+        return fail(HCL_ERR_CONFIG, "reconstruction needs one ghost layer beyond the range");
+    }
+    if (!rho || !u || !P || !rho_rec || !rhou_rec || !E_rec) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    if (h->g.nfx > 0 && (!fx || !fx_rec)) {
+        return fail(HCL_ERR_ARGUMENT, "nfx > 0 needs fx and fx_rec");
+    }
+    const size_t nd = (size_t)h->g.ndim;
+    const size_t N = (size_t)h->g.N;
+    const size_t n_u = N * 2 * nd * nd, n_p = N * 2 * nd, n_fx = N * 2 * nd * (size_t)h->g.nfx;
+    if (n_u + n_p + n_fx > kNoAllocScratchDoubles) {
+        return fail(HCL_ERR_CONFIG,
+                    "hcl_hydro_reconstruction_noalloc: this grid needs %zu scratch doubles (%zu cells x 2*ndim*(ndim+1+nfx)), "
+                    "the fixed buffer holds %zu; use hcl_hydro_reconstruction",
+                    n_u + n_p + n_fx, N, kNoAllocScratchDoubles);
+    }
+    int prev = -1;
+    HCL_CUDA(cudaGetDevice(&prev));
+    if (prev != h->cfg.device) {
+        HCL_CUDA(cudaSetDevice(h->cfg.device));
+    }
+    double* base = nullptr;
+    int rc = noalloc_scratch(h->cfg.device, &base);
+    if (rc == HCL_OK) {
+        hcl::stage::hydro_reconstruction(h->g, ng_eff, dt, rho, u, P, fx, rho_rec, rhou_rec, E_rec, fx_rec, base,
+                                         base + n_u, h->g.nfx > 0 ? base + n_u + n_p : nullptr, pick(h, stream));
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            rc = fail(HCL_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+        }
+    }
+    if (prev != h->cfg.device) {
+        cudaSetDevice(prev);
+    }
+    return rc;
 }
 
 } // extern "C"

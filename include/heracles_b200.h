@@ -146,6 +146,25 @@ int hcl_face_reconstruction(hcl_handle* h, int ng_eff, const double* var, double
 int hcl_hydro_reconstruction(hcl_handle* h, int ng_eff, double dt, const double* rho, const double* u,
                              const double* P, const double* fx, double* rho_rec, double* rhou_rec, double* E_rec,
                              double* fx_rec, double* u_rec, double* P_rec, void* stream);
+/* hcl_hydro_reconstruction with its scratch (u_rec, P_rec, fx_rec_old) in one
+ * fixed 32 MiB device array per device (2^22 doubles) instead of buffers the
+ * handle allocates on first use: the call itself allocates and frees no
+ * device memory.  No counterpart in the reference (its
+ * MUSCLHancockHydroReconstruction owns Kokkos views allocated at
+ * construction).  For host code whose time loop must not allocate after
+ * set-up: an allocation there can synchronise the whole device, and a caller
+ * that hands all free device memory to its own pool has none to give.
+ * Limit: N * 2*ndim*(ndim + 1 + nfx) <= 2^22 doubles, N the cell count with
+ * ghosts (2-D, nfx = 0: N <= 349525; 3-D: N <= 174762); larger grids get
+ * HCL_ERR_CONFIG.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and switches to the handle's device for it; make
+ * that first call before any stream capture.  Nothing in the scratch needs to
+ * start at zero (each call writes every entry it reads).  The array is shared
+ * by all handles on a device: calls whose work overlaps in time on one device
+ * (different streams, threads or handles) race on it; order them. */
+int hcl_hydro_reconstruction_noalloc(hcl_handle* h, int ng_eff, double dt, const double* rho, const double* u,
+                                     const double* P, const double* fx, double* rho_rec, double* rhou_rec,
+                                     double* E_rec, double* fx_rec, void* stream);
 /* IGodunovScheme::execute (hydro/godunov_scheme.hpp:47-63,77-302) with the
  * Riemann solver chosen at hcl_create (factory_godunov_scheme, :305-321). */
 int hcl_godunov_scheme(hcl_handle* h, int ng_eff, double dt, const double* rho, const double* rhou,
