@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     p.add_argument("--no-ensemble", action="store_true", help="skip the batched ensemble measurement")
+    p.add_argument("--no-rt3d", action="store_true", help="skip the 3-D Rayleigh-Taylor measurement")
     return p.parse_args()
 
 
@@ -209,6 +210,61 @@ def adjoint_cost(torch, nsteps=400, n=512, k=32):
                              d.adjoint_backward(lam)))
         out[prec] = {"forward_ms": fwd, "gradient_ms": adj, "adj_over_fwd": adj / fwd}
         d.close()
+    return out
+
+
+def rt3d_cost(torch, steps=500, nx=(256, 256, 512)):
+    """3-D Rayleigh-Taylor 256x256x512 on [0,0.5]^2 x [0,1], g_z = -0.1,
+    reflecting z walls, periodic x/y, HLL, Minmod: FP32-mixed run with its
+    CFL dts, then the FP64 step with the same dts (device time of both, and
+    the relative L1/Linf density error of mixed against FP64)."""
+    from heraclespp_b200 import Domain, setups
+
+    kw = dict(gamma=1.4, limiter="Minmod", riemann="HLL",
+              bc=["Periodic", "Periodic", "Periodic", "Periodic", "Reflexive", "Reflexive"],
+              g=(0.0, 0.0, -0.1), xmax=(0.5, 0.5, 1.0))
+    cells = nx[0] * nx[1] * nx[2]
+    out = {"config": f"rayleigh_taylor_3d_{nx[0]}x{nx[1]}x{nx[2]}_minmod_hll_{steps}steps", "cells": cells,
+           "bytes_per_cell": 80}
+    dm = Domain(3, list(nx), precision="fp32_mixed", **kw)
+    prim = setups.rayleigh_taylor_3d(setups.Grid.from_domain(dm))
+    dm.set_state_from_prim(*prim)
+    dm.run(cfl=0.4, nsteps=3)  # warm-up (tuning, graphs)
+    dm.set_state_from_prim(*prim)
+    stream = torch.cuda.ExternalStream(dm.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    dm.run(cfl=0.4, nsteps=steps)
+    e1.record(stream)
+    e1.synchronize()
+    t_mixed = e0.elapsed_time(e1) * 1e-3
+    dts = dm.dt_log()[:steps]
+    rho_m = dm.get_state()[0]
+    dm.close()
+    d64 = Domain(3, list(nx), precision="fp64", **kw)
+    d64.set_state_from_prim(*prim)
+    d64.run(nsteps=3, dts=dts[:3])
+    d64.set_state_from_prim(*prim)
+    stream = torch.cuda.ExternalStream(d64.stream_handle())
+    torch.cuda.synchronize()
+    e0.record(stream)
+    d64.run(nsteps=steps, dts=dts)
+    e1.record(stream)
+    e1.synchronize()
+    t_64 = e0.elapsed_time(e1) * 1e-3
+    rho_64 = d64.get_state()[0]
+    d64.close()
+    ng = 2
+    a = rho_m[ng:-ng, ng:-ng, ng:-ng]
+    b = rho_64[ng:-ng, ng:-ng, ng:-ng]
+    out["fp32_mixed"] = {"mcups": steps * cells / t_mixed * 1e-6, "ms_per_step": t_mixed / steps * 1e3,
+                         "achieved_gbs": 80 * cells / (t_mixed / steps) * 1e-9}
+    out["fp64"] = {"mcups": steps * cells / t_64 * 1e-6, "ms_per_step": t_64 / steps * 1e3,
+                   "achieved_gbs": 80 * cells / (t_64 / steps) * 1e-9}
+    out["speedup_mixed_vs_fp64"] = t_64 / t_mixed
+    out["rel_l1_rho_mixed_vs_fp64"] = float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
+    out["rel_linf_rho_mixed_vs_fp64"] = float(np.max(np.abs(a - b) / np.abs(b)))
     return out
 
 
@@ -429,6 +485,8 @@ def run_ours(args):
         line["adjoint"] = adjoint_cost(torch)
     if rank == 0 and not args.no_ensemble:
         line["ensemble"] = ensemble_cost(torch)
+    if rank == 0 and not args.no_rt3d:
+        line["rt3d"] = rt3d_cost(torch)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.cpu_budget)
     d.close()

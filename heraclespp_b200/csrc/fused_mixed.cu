@@ -11,10 +11,11 @@ namespace hcl::fused {
 
 // Schedules selectable at run time for 2-D (the autotuner picks one):
 // 0-2 shared-memory tiles 16x16, 32x8, 32x16; 3-5 warp strips of 32, 64,
-// 128 rows (uniform Cartesian grids only).
+// 128 rows; 6 warp strips whose height fits one wave of resident warps
+// (uniform Cartesian grids only for 3-6).
 int mixed_shape_count(int ndim)
 {
-    return ndim == 2 ? 6 : 1;
+    return ndim == 2 ? 7 : 1;
 }
 
 bool mixed_shape_valid(const GridDev& g, int shape)
@@ -40,7 +41,8 @@ void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepC
         break;
     case 2:
         if (shape >= 3 && strip2d_eligible(g)) {
-            step_strip2d(g, in, out, ctl, rp, slot, out_buf, shape == 3 ? 32 : (shape == 4 ? 64 : 128), s);
+            step_strip2d(g, in, out, ctl, rp, slot, out_buf, shape == 3 ? 32 : (shape == 4 ? 64 : (shape == 5 ? 128 : 0)),
+                         s);
         } else if (shape == 1) {
             FusedLauncher<2, false, 32, 8, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
         } else if (shape == 2) {

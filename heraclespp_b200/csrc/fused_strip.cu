@@ -2,6 +2,8 @@
 // limiter x Riemann solver pair (same flags as fused_mixed.cu).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "fused_strip2d.cuh"
 #include "stages.hpp"
 
@@ -14,14 +16,36 @@ bool strip2d_eligible(const GridDev& g)
 
 namespace {
 
+// Resident CTAs of one strip kernel on the whole device (queried once).
+template <int LIM, int RS>
+int resident_blocks()
+{
+    static int cached = 0;
+    if (cached == 0) {
+        int per_sm = 0, nsm = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip2d<LIM, RS>, 128, 0);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cached = per_sm > 0 && nsm > 0 ? per_sm * nsm : 148;
+    }
+    return cached;
+}
+
 template <int LIM, int RS>
 void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp, int slot,
                int out_buf, int L, cudaStream_t s)
 {
     const int ncolw = (g.nx[0] + kStripLanesOut - 1) / kStripLanesOut;
+    const int resident = resident_blocks<LIM, RS>();
+    if (L <= 0) {
+        // fitted strips: as many strips per column as one wave of resident
+        // warps holds, so no warp waits for a second wave
+        const int per_col = std::max(1, resident * 4 / ncolw);
+        L = std::max(8, (g.nx[1] + per_col - 1) / per_col);
+    }
     const int nstrip = (g.nx[1] + L - 1) / L;
     const int warps = ncolw * nstrip;
-    const int blocks = (warps + 3) / 4;
+    const int blocks = std::min((warps + 3) / 4, resident);
     k_strip2d<LIM, RS><<<blocks, 128, 0, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
 }
 

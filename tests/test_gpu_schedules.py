@@ -16,7 +16,7 @@ CASES_2D = {
 }
 
 
-@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("name", list(CASES_2D))
 def test_mixed_schedule_matches_oracle(name, schedule):
     o, d, (rho0, u0, P0) = make_pair(name, "fp32_mixed")
