@@ -28,13 +28,6 @@
 #include "physics_fast.cuh"
 #include "stages.hpp"
 
-#ifndef HCL_STRIP_PREFETCH2
-#define HCL_STRIP_PREFETCH2 0
-#endif
-#ifndef HCL_STRIP_UNROLL
-#define HCL_STRIP_UNROLL 1
-#endif
-
 namespace hcl::fused {
 
 template <int LIM>
@@ -186,9 +179,6 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     float hxL[4], hxR[4], hyT[4];
     double Glo[4];
     double qPre[4];
-#if HCL_STRIP_PREFETCH2
-    double qPre2[4];
-#endif
     {
         double q[4];
         float wA[4], hyB[4];
@@ -201,9 +191,6 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         load_row(r0 + 1, q);
         strip_prim(gm1, q, wD);
         load_row(r0 + 2, qPre);
-#if HCL_STRIP_PREFETCH2
-        load_row(r0 + 3, qPre2);
-#endif
         float t0[4], t1[4], t2[4], tT[4];
         strip_hancock<LIM>(c, wA, wB, wC, t0, t1, t2, tT); // row r0-1: keep its top face
         strip_hancock<LIM>(c, wB, wC, wD, hxL, hxR, hyB, hyT); // row r0
@@ -215,8 +202,6 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         }
     }
     // window: wC = P[r], wD = P[r+1]; qPre = U[r+2] (in flight)
-    constexpr int kUnroll = HCL_STRIP_UNROLL;
-#pragma unroll kUnroll
     for (int r = r0; r < r1; ++r) {
         // FP64 state of row r for its update, loaded now so that its latency
         // hides behind this row's Hancock and Riemann work
@@ -230,15 +215,7 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         }
         float wN[4];
         strip_prim(gm1, qPre, wN);
-#if HCL_STRIP_PREFETCH2
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            qPre[v] = qPre2[v];
-        }
-        load_row(r + 4, qPre2); // prefetch two rows ahead
-#else
         load_row(r + 3, qPre); // prefetch for the next row
-#endif
         // Hancock of row r+1
         float nxL[4], nxR[4], nyB[4], nyT[4];
         strip_hancock<LIM>(c, wC, wD, wN, nxL, nxR, nyB, nyT);
@@ -366,12 +343,8 @@ __device__ __forceinline__ void publish_decision(StepCtl* ctl, const Decision& d
     ctl->inv_dt_bits[(slot + 2) % 3] = 0ull;
 }
 
-#ifndef HCL_STRIP_MIN_BLOCKS
-#define HCL_STRIP_MIN_BLOCKS 5
-#endif
-
 template <int LIM, int RS>
-__global__ void __launch_bounds__(128, HCL_STRIP_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, 5)
 k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
 {
     const int lane = threadIdx.x & 31;
