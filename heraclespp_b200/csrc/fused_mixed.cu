@@ -11,16 +11,20 @@ namespace hcl::fused {
 
 // Schedules selectable at run time for 2-D (the autotuner picks one):
 // 0-2 shared-memory tiles 16x16, 32x8, 32x16; 3-5 warp strips of 32, 64,
-// 128 rows; 6 warp strips whose height fits one wave of resident warps
-// (uniform Cartesian grids only for 3-6).
+// 128 rows; 6 warp strips whose height fits one wave of resident warps;
+// 7 and 8 paired-column warp strips (fitted height, 32 rows).  3-8 need a
+// uniform Cartesian grid, 7-8 an even ghost width.
 int mixed_shape_count(int ndim)
 {
-    return ndim == 2 ? 7 : 1;
+    return ndim == 2 ? 9 : 1;
 }
 
 bool mixed_shape_valid(const GridDev& g, int shape)
 {
-    return shape < 3 || strip2d_eligible(g);
+    if (shape < 3) {
+        return true;
+    }
+    return shape < 7 ? strip2d_eligible(g) : strip2d_pair_eligible(g);
 }
 
 void configure_mixed()
@@ -40,7 +44,9 @@ void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepC
         FusedLauncher<1, false, 256, 1, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
         break;
     case 2:
-        if (shape >= 3 && strip2d_eligible(g)) {
+        if (shape >= 7 && strip2d_pair_eligible(g)) {
+            step_strip2d_pair(g, in, out, ctl, rp, slot, out_buf, shape == 7 ? 0 : 32, s);
+        } else if (shape >= 3 && strip2d_eligible(g)) {
             step_strip2d(g, in, out, ctl, rp, slot, out_buf, shape == 3 ? 32 : (shape == 4 ? 64 : (shape == 5 ? 128 : 0)),
                          s);
         } else if (shape == 1) {

@@ -5,6 +5,7 @@
 #include <algorithm>
 
 #include "fused_strip2d.cuh"
+#include "fused_strip2d_pair.cuh"
 #include "stages.hpp"
 
 namespace hcl::fused {
@@ -12,6 +13,13 @@ namespace hcl::fused {
 bool strip2d_eligible(const GridDev& g)
 {
     return g.ndim == 2 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM;
+}
+
+// The paired schedule loads and stores column pairs as 16-byte vectors: the
+// first column of a pair is even, which needs an even ghost width.
+bool strip2d_pair_eligible(const GridDev& g)
+{
+    return strip2d_eligible(g) && g.ng % 2 == 0;
 }
 
 namespace {
@@ -62,7 +70,70 @@ void launch_l(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl
     }
 }
 
+template <int LIM, int RS>
+int resident_blocks_pair()
+{
+    static int cached = 0;
+    if (cached == 0) {
+        int per_sm = 0, nsm = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip2d_pair<LIM, RS>, 128, 0);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cached = per_sm > 0 && nsm > 0 ? per_sm * nsm : 148;
+    }
+    return cached;
+}
+
+template <int LIM, int RS>
+void launch_pair_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                    int slot, int out_buf, int L, cudaStream_t s)
+{
+    const int ncolw = (g.nx[0] + kPairLanesOut - 1) / kPairLanesOut;
+    const int resident = resident_blocks_pair<LIM, RS>();
+    if (L <= 0) {
+        const int per_col = std::max(1, resident * 4 / ncolw);
+        L = std::max(8, (g.nx[1] + per_col - 1) / per_col);
+    }
+    const int nstrip = (g.nx[1] + L - 1) / L;
+    const int warps = ncolw * nstrip;
+    const int blocks = std::min((warps + 3) / 4, resident);
+    k_strip2d_pair<LIM, RS><<<blocks, 128, 0, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
+}
+
+template <int LIM>
+void launch_pair_l(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                   int slot, int out_buf, int L, cudaStream_t s)
+{
+    if (g.riemann == RS_HLL) {
+        launch_pair_lr<LIM, RS_HLL>(g, in, out, ctl, rp, slot, out_buf, L, s);
+    } else if (g.riemann == RS_HLLC) {
+        launch_pair_lr<LIM, RS_HLLC>(g, in, out, ctl, rp, slot, out_buf, L, s);
+    } else {
+        launch_pair_lr<LIM, RS_SPLITTING>(g, in, out, ctl, rp, slot, out_buf, L, s);
+    }
+}
+
 } // namespace
+
+void step_strip2d_pair(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                       int slot, int out_buf, int L, cudaStream_t s)
+{
+    switch (g.limiter) {
+    case LIM_CONSTANT:
+        launch_pair_l<LIM_CONSTANT>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        break;
+    case LIM_VANLEER:
+        launch_pair_l<LIM_VANLEER>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        break;
+    case LIM_MINMOD:
+        launch_pair_l<LIM_MINMOD>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        break;
+    default:
+        launch_pair_l<LIM_VANALBADA>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        break;
+    }
+    ++g_launches;
+}
 
 void step_strip2d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                   int slot, int out_buf, int L, cudaStream_t s)
