@@ -271,20 +271,29 @@ def rt3d_cost(torch, steps=500, nx=(256, 256, 512)):
 ENSEMBLE_SIDES = (128, 256, 512, 1024)
 
 
-def ensemble_cost(torch, nprob=96, nsteps=300, k=20, seed=2024):
+def ensemble_cost(torch, nprob=96, nsteps=300, k=20, seed=2024, rank=0, world=1):
     """96 independent 2-D four-quadrant Riemann problems (sides drawn from
     {128, 256, 512, 1024}, seeded), outflow, Minmod, HLLC, FP32-mixed,
     300 steps: one persistent graph-replayed launch against looping the
     single-problem step (each problem's own hcl_run), then the adjoint of
-    the sum of the final total energies.  Wall-clock of synchronous calls."""
+    the sum of the final total energies.  Wall-clock of synchronous calls.
+    With world > 1 the problems are sharded over the ranks (cost-balanced),
+    times are the maximum over ranks and the objective is summed."""
     from heraclespp_b200 import Domain, Ensemble, setups
+    from heraclespp_b200.sharding import partition, problem_cost, torch_reducers, total_energy
 
     rng = np.random.default_rng(seed)
     sides = [(int(rng.choice(ENSEMBLE_SIDES)), int(rng.choice(ENSEMBLE_SIDES))) for _ in range(nprob)]
     cells = sum(a * b for a, b in sides)
+    mine = partition([problem_cost(s, nsteps) for s in sides], world)[rank]
+    if world > 1:
+        rsum, rmax = torch_reducers(device="cuda")
+    else:
+        rsum = rmax = (lambda x: x)  # noqa: E731
+    my_sides = [sides[p] for p in mine]
     kw = dict(gamma=1.4, limiter="Minmod", riemann="HLLC", bc=["NullGradient"] * 4)
-    ens = Ensemble([dict(nx=list(s), **kw) for s in sides])
-    prims = [setups.four_quadrant(setups.Grid.from_domain(d), seed=1000 + p) for p, d in enumerate(ens.domains)]
+    ens = Ensemble([dict(nx=list(s), **kw) for s in my_sides])
+    prims = [setups.four_quadrant(setups.Grid.from_domain(d), seed=1000 + p) for p, d in zip(mine, ens.domains)]
 
     def reset(doms):
         for d, prim in zip(doms, prims):
@@ -295,20 +304,22 @@ def ensemble_cost(torch, nprob=96, nsteps=300, k=20, seed=2024):
         t0 = time.perf_counter()
         out = fn()
         torch.cuda.synchronize()
-        return time.perf_counter() - t0, out
+        return rmax(time.perf_counter() - t0), out
 
     reset(ens.domains)
     ens.run(nsteps)  # autotune, capture
     reset(ens.domains)
     t_ens, r = wall(lambda: ens.run(nsteps))
+    energy = rsum(sum(total_energy(d) for d in ens.domains))
     out = {"config": f"{nprob} four-quadrant problems, sides from {list(ENSEMBLE_SIDES)} (seed {seed}), "
                      f"{cells} cells, {nsteps} steps, Minmod, HLLC, outflow, fp32_mixed",
-           "cells": cells,
+           "cells": cells, "ranks": world, "problems_on_rank0": len(mine),
+           "final_total_energy": energy,
            "ensemble": {"ms": t_ens * 1e3, "mcups": cells * nsteps / t_ens * 1e-6, "strip_rows": r.strip_rows,
                         "blocks_per_sm": r.blocks_per_sm, "grid": r.grid, "launches": r.launches,
                         "graph": bool(r.graph)}}
     # looping the single-problem step (each problem graph-replays its own steps)
-    doms = [Domain(2, list(s), precision="fp32_mixed", **kw) for s in sides]
+    doms = [Domain(2, list(s), precision="fp32_mixed", **kw) for s in my_sides]
     reset(doms)
     for d in doms:
         d.run(cfl=0.4, nsteps=nsteps)  # autotune, capture
@@ -326,6 +337,7 @@ def ensemble_cost(torch, nprob=96, nsteps=300, k=20, seed=2024):
         lam[3, :, 2:-2, 2:-2] = dv[:, 2:-2, 2:-2]
         lams.append(lam)
     grads = [torch.empty_like(x) for x in lams]
+    torch.cuda.synchronize()
     for prec in ("fp64", "fp32_mixed"):
         reset(ens.domains)
         ens.run(nsteps, checkpoint_every=k, adjoint_precision=prec)
@@ -483,8 +495,10 @@ def run_ours(args):
     }
     if rank == 0 and not args.no_adjoint:
         line["adjoint"] = adjoint_cost(torch)
-    if rank == 0 and not args.no_ensemble:
-        line["ensemble"] = ensemble_cost(torch)
+    if not args.no_ensemble:
+        ens = ensemble_cost(torch, rank=rank, world=world)
+        if rank == 0:
+            line["ensemble"] = ens
     if rank == 0 and not args.no_rt3d:
         line["rt3d"] = rt3d_cost(torch)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
