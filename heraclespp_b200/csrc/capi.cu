@@ -144,6 +144,12 @@ struct hcl_handle {
     int adj_prec = 0;
     int adj_ready = 0;
     int adj_ddts_cap = 0;
+    // second stream of the reverse pass: recomputes segment s-1 while the
+    // main stream sweeps segment s back; events order the two segment buffers
+    cudaStream_t adj_stream = nullptr;
+    cudaEvent_t adj_ev_start = nullptr;
+    cudaEvent_t adj_ev_rec[2] = {nullptr, nullptr};
+    cudaEvent_t adj_ev_rev[2] = {nullptr, nullptr};
 };
 
 static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double* grad, int memory);
@@ -187,6 +193,14 @@ void free_handle(hcl_handle* h)
     cudaFree(h->adj_lam);
     cudaFree(h->adj_ddts);
     cudaFree(h->adj_ctl);
+    for (cudaEvent_t ev : {h->adj_ev_start, h->adj_ev_rec[0], h->adj_ev_rec[1], h->adj_ev_rev[0], h->adj_ev_rev[1]}) {
+        if (ev) {
+            cudaEventDestroy(ev);
+        }
+    }
+    if (h->adj_stream) {
+        cudaStreamDestroy(h->adj_stream);
+    }
     if (h->stream) {
         cudaStreamDestroy(h->stream);
     }
@@ -1385,14 +1399,23 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
     const int k = h->adj_k;
     const size_t sz = (size_t)h->st[0].plane * (nd + 2);
     int rc;
-    if (h->adj_cap_seg < k + 1) {
+    // two segment buffers of k+1 states: the recompute of one overlaps the sweep of the other
+    if (h->adj_cap_seg < 2 * (k + 1)) {
         cudaFree(h->adj_seg);
         h->adj_seg = nullptr;
         h->adj_cap_seg = 0;
-        if ((rc = dalloc(&h->adj_seg, sz * (size_t)(k + 1)))) {
+        if ((rc = dalloc(&h->adj_seg, sz * (size_t)(2 * (k + 1))))) {
             return rc;
         }
-        h->adj_cap_seg = k + 1;
+        h->adj_cap_seg = 2 * (k + 1);
+    }
+    if (!h->adj_stream) {
+        HCL_CUDA(cudaStreamCreateWithFlags(&h->adj_stream, cudaStreamNonBlocking));
+        HCL_CUDA(cudaEventCreateWithFlags(&h->adj_ev_start, cudaEventDisableTiming));
+        for (int b = 0; b < 2; ++b) {
+            HCL_CUDA(cudaEventCreateWithFlags(&h->adj_ev_rec[b], cudaEventDisableTiming));
+            HCL_CUDA(cudaEventCreateWithFlags(&h->adj_ev_rev[b], cudaEventDisableTiming));
+        }
     }
     if (!h->adj_lam && (rc = dalloc(&h->adj_lam, sz * 2))) {
         return rc;
@@ -1430,30 +1453,60 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
     rp.fixed_dt = 1;
     rp.dts = h->adj_ddts;
     const bool fp64_sweep = h->adj_prec == HCL_FP64;
-    int cur = 0;
-    for (int sg = h->adj_nck - 1; sg >= 0; --sg) {
+    cudaStream_t a = h->adj_stream;
+    // recompute U^{first} .. U^{first+len-1} of segment sg into buffer sg & 1 (stream a)
+    auto recompute = [&](int sg) -> int {
+        const int b = sg & 1;
+        const size_t base = (size_t)b * (k + 1);
         const int first = sg * k;
         const int len = std::min(k, N - first);
-        // recompute U^{first} .. U^{first+len-1} into the segment buffer
-        HCL_CUDA(cudaMemcpyAsync(h->adj_seg, h->adj_ckpt + sz * sg, sizeof(double) * sz, cudaMemcpyDeviceToDevice, s));
-        hcl::fused::prologue(g, state_at(h->adj_seg, 0), h->adj_ctl, 0.0, first, s);
+        // the buffer was last read by the sweep of segment sg + 2
+        HCL_CUDA(cudaStreamWaitEvent(a, h->adj_ev_rev[b], 0));
+        HCL_CUDA(cudaMemcpyAsync(h->adj_seg + sz * base, h->adj_ckpt + sz * sg, sizeof(double) * sz,
+                                 cudaMemcpyDeviceToDevice, a));
+        hcl::fused::prologue(g, state_at(h->adj_seg, base), h->adj_ctl, 0.0, first, a);
         for (int j = 0; j + 1 < len; ++j) {
             if (h->cfg.precision == HCL_FP64) {
-                hcl::fused::step_exact(g, state_at(h->adj_seg, j), state_at(h->adj_seg, j + 1), h->adj_ctl, rp, j % 6,
-                                       1, s);
+                hcl::fused::step_exact(g, state_at(h->adj_seg, base + j), state_at(h->adj_seg, base + j + 1),
+                                       h->adj_ctl, rp, j % 6, 1, a);
             } else {
-                hcl::fused::step_mixed(g, state_at(h->adj_seg, j), state_at(h->adj_seg, j + 1), h->adj_ctl, rp, j % 6,
-                                       1, h->mixed_shape < 0 ? 0 : h->mixed_shape, s);
+                hcl::fused::step_mixed(g, state_at(h->adj_seg, base + j), state_at(h->adj_seg, base + j + 1),
+                                       h->adj_ctl, rp, j % 6, 1, h->mixed_shape < 0 ? 0 : h->mixed_shape, a);
             }
         }
+        HCL_CUDA(cudaEventRecord(h->adj_ev_rec[b], a));
+        return HCL_OK;
+    };
+    // the dts, λ^N and its fold are on stream s: stream a starts after them
+    HCL_CUDA(cudaEventRecord(h->adj_ev_start, s));
+    HCL_CUDA(cudaStreamWaitEvent(a, h->adj_ev_start, 0));
+    // no sweep has read either buffer yet
+    for (int b = 0; b < 2; ++b) {
+        HCL_CUDA(cudaEventRecord(h->adj_ev_rev[b], s));
+    }
+    if ((rc = recompute(h->adj_nck - 1))) {
+        return rc;
+    }
+    int cur = 0;
+    for (int sg = h->adj_nck - 1; sg >= 0; --sg) {
+        if (sg > 0 && (rc = recompute(sg - 1))) {
+            return rc;
+        }
+        const int b = sg & 1;
+        const size_t base = (size_t)b * (k + 1);
+        const int first = sg * k;
+        const int len = std::min(k, N - first);
+        HCL_CUDA(cudaStreamWaitEvent(s, h->adj_ev_rec[b], 0));
         // backward through the segment
         for (int j = len - 1; j >= 0; --j) {
             const int n = first + j;
             HCL_CUDA(cudaMemsetAsync(lam[cur ^ 1].q, 0, sizeof(double) * sz, s));
-            hcl::adjoint::step(g, state_at(h->adj_seg, j), lam[cur], lam[cur ^ 1], h->adj_dts[n], fp64_sweep, s);
+            hcl::adjoint::step(g, state_at(h->adj_seg, base + j), lam[cur], lam[cur ^ 1], h->adj_dts[n], fp64_sweep,
+                               s);
             hcl::adjoint::fold(g, lam[cur ^ 1], s);
             cur ^= 1;
         }
+        HCL_CUDA(cudaEventRecord(h->adj_ev_rev[b], s));
     }
     HCL_LAUNCH_CHECK();
     // the gradient lives on the interior cells; ghost entries are zero
