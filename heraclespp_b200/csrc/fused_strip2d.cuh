@@ -6,13 +6,14 @@
 //  * a warp owns 28 output columns x L output rows.  Lane l holds column
 //    c0 - 2 + l, so x-neighbours (slopes, the left state of an x-face, the
 //    right flux of a cell) come from warp shuffles; lanes 2..29 write output;
-//  * the warp marches up its rows with a register window: at row r it turns
-//    the prefetched state row r+2 into primitives (FP64 internal-energy
-//    recovery) and issues the load of row r+3, builds the Hancock face states
-//    of row r+1, solves the y-face r+1/2 and the x-faces of row r, and updates
-//    row r in FP64.  Every primitive, Hancock state and face flux is computed
-//    once per lane (plus a 4-row start-up and the 4 halo lanes), with no
-//    shared memory and no barriers;
+//  * the warp marches up its rows with a register window: at row r it issues
+//    the copy of FP64 row r+4 into its shared-memory ring (cp.async), turns
+//    row r+2 into primitives (FP64 internal-energy recovery), builds the
+//    Hancock face states of row r+1, solves the y-face r+1/2 and the x-faces
+//    of row r, and updates row r in FP64.  Every primitive, Hancock state and
+//    face flux is computed once per lane (plus a 4-row start-up and the 4
+//    halo lanes), with no barriers (a lane reads only the ring entries it
+//    copied);
 //  * ghost images, the internal-energy check and the CFL max of the new
 //    state are done in the same pass.
 // strip_work() is the per-strip body shared by the single-domain kernel and
@@ -165,12 +166,25 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     const double dgy = dt * g.g[1];
     const double gm1 = g.gamma_m1;
 
-    auto load_row = [&](int r, double q[4]) {
+    // The FP64 rows stream through a per-warp ring of 8 row slots in shared
+    // memory (one 8-byte cp.async per lane and variable; a lane only reads
+    // what it copied, so no barrier is needed).  Rows are issued 4 ahead.
+    __shared__ __align__(16) double s_ring[4][8][4][32];
+    double(*ring)[4][32] = s_ring[(threadIdx.x >> 5) & 3];
+    auto stage_row = [&](int r) {
         const int rc = min(max(r, 0), n1 - 1);
         const int64_t o = (int64_t)rc * pitch + colc;
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            q[v] = __ldg(qin + o + plane * v);
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(&ring[r & 7][v][lane]);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(qin + o + plane * v) : "memory");
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    auto ring_row = [&](int r, double q[4]) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            q[v] = ring[r & 7][v][lane];
         }
     };
 
@@ -178,19 +192,21 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     float wB[4], wC[4], wD[4];
     float hxL[4], hxR[4], hyT[4];
     double Glo[4];
-    double qPre[4];
     {
         double q[4];
         float wA[4], hyB[4];
-        load_row(r0 - 2, q);
+        for (int rr = r0 - 2; rr <= r0 + 3; ++rr) {
+            stage_row(rr);
+        }
+        asm volatile("cp.async.wait_group 2;\n" ::: "memory"); // rows r0-2 .. r0+1 landed
+        ring_row(r0 - 2, q);
         strip_prim(gm1, q, wA);
-        load_row(r0 - 1, q);
+        ring_row(r0 - 1, q);
         strip_prim(gm1, q, wB);
-        load_row(r0, q);
+        ring_row(r0, q);
         strip_prim(gm1, q, wC);
-        load_row(r0 + 1, q);
+        ring_row(r0 + 1, q);
         strip_prim(gm1, q, wD);
-        load_row(r0 + 2, qPre);
         float t0[4], t1[4], t2[4], tT[4];
         strip_hancock<LIM>(c, wA, wB, wC, t0, t1, t2, tT); // row r0-1: keep its top face
         strip_hancock<LIM>(c, wB, wC, wD, hxL, hxR, hyB, hyT); // row r0
@@ -201,21 +217,18 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             Glo[v] = (double)G[v];
         }
     }
-    // window: wC = P[r], wD = P[r+1]; qPre = U[r+2] (in flight)
+    // window: wC = P[r], wD = P[r+1]; ring rows r+3, r+4 in flight
     for (int r = r0; r < r1; ++r) {
-        // FP64 state of row r for its update, loaded now so that its latency
-        // hides behind this row's Hancock and Riemann work
         double q[4];
-        {
-            const int64_t oq = (int64_t)r * pitch + colc;
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                q[v] = __ldg(qin + oq + plane * v);
-            }
-        }
         float wN[4];
-        strip_prim(gm1, qPre, wN);
-        load_row(r + 3, qPre); // prefetch for the next row
+        stage_row(r + 4);
+        asm volatile("cp.async.wait_group 2;\n" ::: "memory"); // rows up to r+2 landed
+        ring_row(r, q);
+        {
+            double qn2[4];
+            ring_row(r + 2, qn2);
+            strip_prim(gm1, qn2, wN);
+        }
         // Hancock of row r+1
         float nxL[4], nxR[4], nyB[4], nyT[4];
         strip_hancock<LIM>(c, wC, wD, wN, nxL, nxR, nyB, nyT);
@@ -304,6 +317,7 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             Glo[v] = Ghi[v];
         }
     }
+    asm volatile("cp.async.wait_all;\n" ::: "memory"); // the ring is reused by the next strip
     (void)wB;
 }
 
