@@ -1231,7 +1231,7 @@ int hcl_set_schedule(hcl_handle* h, int schedule, int* used)
         return fail(HCL_ERR_ARGUMENT, "schedule %d out of range", schedule);
     }
     if (schedule >= 0 && !hcl::fused::mixed_shape_valid(h->g, schedule)) {
-        return fail(HCL_ERR_CONFIG, "schedule %d needs a uniform Cartesian 2-D grid", schedule);
+        return fail(HCL_ERR_CONFIG, "schedule %d needs a uniform Cartesian grid (and an even ghost width for 7-8)", schedule);
     }
     h->mixed_shape = schedule < 0 ? -1 : schedule;
     if (used) {

@@ -14,13 +14,17 @@ namespace hcl::fused {
 // 128 rows; 6 warp strips whose height fits one wave of resident warps;
 // 7 and 8 paired-column warp strips (fitted height, 32 rows).  3-8 need a
 // uniform Cartesian grid, 7-8 an even ghost width.
+// 3-D: 0 shared-memory tiles 8x8x4; 1 column march (uniform Cartesian grids).
 int mixed_shape_count(int ndim)
 {
-    return ndim == 2 ? 9 : 1;
+    return ndim == 2 ? 9 : (ndim == 3 ? 2 : 1);
 }
 
 bool mixed_shape_valid(const GridDev& g, int shape)
 {
+    if (g.ndim == 3) {
+        return shape == 0 || (shape == 1 && strip3d_eligible(g));
+    }
     if (shape < 3) {
         return true;
     }
@@ -58,7 +62,11 @@ void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepC
         }
         break;
     default:
-        FusedLauncher<3, false, 8, 8, 4>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        if (shape == 1 && strip3d_eligible(g)) {
+            step_strip3d(g, in, out, ctl, rp, slot, out_buf, 0, s);
+        } else {
+            FusedLauncher<3, false, 8, 8, 4>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        }
         break;
     }
 }

@@ -54,6 +54,7 @@ struct StripCtx {
     fast::Eos eos;
     float cthx, cthy; // (dt/2)/dx, (dt/2)/dy
     float dgx, dgy;   // (dt/2) g
+    bool gravity;     // any g component non-zero (the terms vanish exactly otherwise)
 };
 
 // FP64 state -> FP32 primitives, internal energy recovered in FP64 (the
@@ -126,9 +127,15 @@ __device__ __forceinline__ void strip_hancock(const StripCtx& c, const float wd[
         // gravity on the face state (extrapolation_reconstruction.hpp:306-312)
         const float r0 = u[0], m0 = u[1], m1 = u[2];
         u[0] = r0 + inc[0];
-        u[1] = fmaf(c.dgx, r0, m0 + inc[1]);
-        u[2] = fmaf(c.dgy, r0, m1 + inc[2]);
-        u[3] = fmaf(c.dgx, m0, fmaf(c.dgy, m1, u[3] + inc[3]));
+        if (c.gravity) {
+            u[1] = fmaf(c.dgx, r0, m0 + inc[1]);
+            u[2] = fmaf(c.dgy, r0, m1 + inc[2]);
+            u[3] = fmaf(c.dgx, m0, fmaf(c.dgy, m1, u[3] + inc[3]));
+        } else {
+            u[1] = m0 + inc[1];
+            u[2] = m1 + inc[2];
+            u[3] = u[3] + inc[3];
+        }
     }
 }
 
@@ -160,6 +167,7 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     c.cthy = (float)(0.5 * dt * g.inv_dx[1]);
     c.dgx = (float)(0.5 * dt * g.g[0]);
     c.dgy = (float)(0.5 * dt * g.g[1]);
+    c.gravity = g.g[0] != 0.0 || g.g[1] != 0.0;
     const double cx = dt * g.inv_dx[0];
     const double cy = dt * g.inv_dx[1];
     const double dgx = dt * g.g[0];
@@ -261,9 +269,11 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             for (int v = 0; v < 4; ++v) {
                 qn[v] = q[v] + fma(cx, Fld[v] - Frd[v], cy * (Glo[v] - Ghi[v]));
             }
-            qn[1] = fma(dgx, q[0], qn[1]);
-            qn[2] = fma(dgy, q[0], qn[2]);
-            qn[3] = fma(dgx, q[1], fma(dgy, q[2], qn[3]));
+            if (c.gravity) {
+                qn[1] = fma(dgx, q[0], qn[1]);
+                qn[2] = fma(dgy, q[0], qn[2]);
+                qn[3] = fma(dgx, q[1], fma(dgy, q[2], qn[3]));
+            }
             // health check (main.cpp:397-425) and CFL (time_step.hpp:55-77) of the new state
             double rr = (double)__fdividef(1.f, (float)qn[0]);
             rr = rr * (2.0 - qn[0] * rr);

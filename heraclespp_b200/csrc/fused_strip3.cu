@@ -1,0 +1,86 @@
+// fused_strip3.cu -- instantiations and launcher of the 3-D column-march
+// mixed step for every limiter x Riemann solver pair (same flags as
+// fused_mixed.cu).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "fused_strip3d.cuh"
+#include "stages.hpp"
+
+namespace hcl::fused {
+
+bool strip3d_eligible(const GridDev& g)
+{
+    return g.ndim == 3 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM && g.ng >= 2;
+}
+
+namespace {
+
+template <int LIM, int RS>
+void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp, int slot,
+               int out_buf, int L, cudaStream_t s)
+{
+    static int resident = 0;
+    if (resident == 0) {
+        cudaFuncSetAttribute(k_strip3d<LIM, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S3Shared));
+        int per_sm = 0, nsm = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip3d<LIM, RS>, kS3Threads, sizeof(S3Shared));
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        resident = std::max(1, per_sm) * (nsm > 0 ? nsm : 148);
+    }
+    const int ncol = ((g.nx[0] + 27) / 28) * ((g.nx[1] + 11) / 12);
+    if (L <= 0) {
+        // plane count per CTA that minimises waves x (planes + 2 start-up planes)
+        long best = -1;
+        for (int nzc = 1; nzc <= std::max(1, g.nx[2] / 4); ++nzc) {
+            const int Lc = (g.nx[2] + nzc - 1) / nzc;
+            const long waves = ((long)ncol * nzc + resident - 1) / resident;
+            const long cost = waves * (Lc + 2);
+            if (best < 0 || cost < best) {
+                best = cost;
+                L = Lc;
+            }
+        }
+    }
+    const int nzc = (g.nx[2] + L - 1) / L;
+    k_strip3d<LIM, RS><<<ncol * nzc, kS3Threads, sizeof(S3Shared), s>>>(g, in, out, ctl, rp, slot, out_buf, L);
+}
+
+template <int LIM>
+void launch_l(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp, int slot,
+              int out_buf, int L, cudaStream_t s)
+{
+    if (g.riemann == RS_HLL) {
+        launch_lr<LIM, RS_HLL>(g, in, out, ctl, rp, slot, out_buf, L, s);
+    } else if (g.riemann == RS_HLLC) {
+        launch_lr<LIM, RS_HLLC>(g, in, out, ctl, rp, slot, out_buf, L, s);
+    } else {
+        launch_lr<LIM, RS_SPLITTING>(g, in, out, ctl, rp, slot, out_buf, L, s);
+    }
+}
+
+} // namespace
+
+void step_strip3d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                  int slot, int out_buf, int L, cudaStream_t s)
+{
+    switch (g.limiter) {
+    case LIM_CONSTANT:
+        launch_l<LIM_CONSTANT>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        break;
+    case LIM_VANLEER:
+        launch_l<LIM_VANLEER>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        break;
+    case LIM_MINMOD:
+        launch_l<LIM_MINMOD>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        break;
+    default:
+        launch_l<LIM_VANALBADA>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        break;
+    }
+    ++g_launches;
+}
+
+} // namespace hcl::fused

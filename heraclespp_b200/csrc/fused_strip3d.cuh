@@ -1,0 +1,387 @@
+// fused_strip3d.cuh -- the FP32-mixed 3-D fused step as a column march
+// (uniform Cartesian grids, uniform gravity).
+//
+// Same mathematics and precision split as k_fused_step<3, false, ...>; a
+// different schedule.  A CTA of 16 warps owns a block of 28 x 12 output
+// columns (x, y) and marches it along z over L planes:
+//  * lane l of warp w holds the column (c0 - 2 + l, j0 - 2 + w); x-neighbours
+//    come from warp shuffles, y-neighbours from the neighbouring warps through
+//    shared memory, z-neighbours from a register window;
+//  * at step z the CTA turns plane z+2 into primitives (FP64 internal-energy
+//    recovery), builds the Hancock face states of plane z+1, solves the
+//    x-faces of plane z+1, the z-face z+1/2 and the y-faces of plane z, and
+//    updates plane z in FP64 with the ghost images, the health check and the
+//    CFL contribution.  One CTA barrier per plane orders the shared planes.
+// Lanes 2..29 and warps 2..13 write; the others are the stencil halo.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fused_step.cuh"
+#include "fused_strip2d.cuh"
+#include "hcl_device.cuh"
+#include "physics_fast.cuh"
+#include "stages.hpp"
+
+namespace hcl::fused {
+
+constexpr int kS3Warps = 16;
+constexpr int kS3Threads = 32 * kS3Warps;
+
+namespace s3 {
+
+struct Ctx {
+    fast::Eos eos;
+    float cth[3]; // (dt/2)/dx_d
+    float dg[3];  // (dt/2) g_d
+    bool gravity;
+};
+
+// FP64 state -> FP32 primitives (rho, u, v, w, P); internal energy in FP64
+__device__ __forceinline__ void prim(double gm1, const double q[5], float w[5])
+{
+    double r = (double)__fdividef(1.f, (float)q[0]);
+    r = r * (2.0 - q[0] * r);
+    const double u = q[1] * r;
+    const double v = q[2] * r;
+    const double x = q[3] * r;
+    const double mu = fma(q[1], u, fma(q[2], v, q[3] * x));
+    w[0] = (float)q[0];
+    w[1] = (float)u;
+    w[2] = (float)v;
+    w[3] = (float)x;
+    w[4] = (float)(gm1 * fma(-0.5, mu, q[4]));
+}
+
+// conservative state and flux along l of a face primitive state
+__device__ __forceinline__ void cons_and_flux(const fast::Eos& e, const float w[5], int l, float U[5], float F[5])
+{
+    const float m0 = w[0] * w[1];
+    const float m1 = w[0] * w[2];
+    const float m2 = w[0] * w[3];
+    const float Et = fmaf(0.5f, fmaf(m0, w[1], fmaf(m1, w[2], m2 * w[3])), w[4] * e.inv_gm1);
+    U[0] = w[0];
+    U[1] = m0;
+    U[2] = m1;
+    U[3] = m2;
+    U[4] = Et;
+    const float ml = l == 0 ? m0 : (l == 1 ? m1 : m2);
+    const float ul = w[1 + l];
+    F[0] = ml;
+    F[1] = ml * w[1];
+    F[2] = ml * w[2];
+    F[3] = ml * w[3];
+    F[1 + l] += w[4];
+    F[4] = ul * (Et + w[4]);
+}
+
+// Hancock face states of one cell: minus/plus faces along x, y, z
+// (extrapolation_reconstruction.hpp:65-143, gravity :306-312).  wyd/wyu are
+// the y-neighbours, wzd/wzu the z-neighbours; x-neighbours come by shuffle.
+template <int LIM>
+__device__ __forceinline__ void hancock(const Ctx& c, const float wc[5], const float wyd[5], const float wyu[5],
+                                        const float wzd[5], const float wzu[5], float hm[3][5], float hp[3][5])
+{
+    float fm[3][5], fp[3][5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        const float wl = __shfl_up_sync(0xffffffffu, wc[v], 1);
+        const float wr = __shfl_down_sync(0xffffffffu, wc[v], 1);
+        const float sx = 0.5f * lim_fast<LIM>(wr - wc[v], wc[v] - wl);
+        fm[0][v] = wc[v] - sx;
+        fp[0][v] = wc[v] + sx;
+        const float sy = 0.5f * lim_fast<LIM>(wyu[v] - wc[v], wc[v] - wyd[v]);
+        fm[1][v] = wc[v] - sy;
+        fp[1][v] = wc[v] + sy;
+        const float sz = 0.5f * lim_fast<LIM>(wzu[v] - wc[v], wc[v] - wzd[v]);
+        fm[2][v] = wc[v] - sz;
+        fp[2][v] = wc[v] + sz;
+    }
+    float inc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        float Fm[5], Fp[5];
+        cons_and_flux(c.eos, fm[d], d, hm[d], Fm);
+        cons_and_flux(c.eos, fp[d], d, hp[d], Fp);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            inc[v] = fmaf(c.cth[d], Fm[v] - Fp[v], inc[v]);
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            float* u = s == 0 ? hm[d] : hp[d];
+            const float r0 = u[0], m0 = u[1], m1 = u[2], m2 = u[3];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                u[v] += inc[v];
+            }
+            if (c.gravity) {
+                u[1] = fmaf(c.dg[0], r0, u[1]);
+                u[2] = fmaf(c.dg[1], r0, u[2]);
+                u[3] = fmaf(c.dg[2], r0, u[3]);
+                u[4] = fmaf(c.dg[0], m0, fmaf(c.dg[1], m1, fmaf(c.dg[2], m2, u[4])));
+            }
+        }
+    }
+}
+
+} // namespace s3
+
+// Shared planes of one CTA: primitives of the current Hancock plane, the
+// y-face states of the last two Hancock planes and the y-face fluxes.
+struct S3Shared {
+    float prim[2][kS3Warps][5][32];
+    float yface[2][kS3Warps][2][5][32]; // [.][w][0: bottom (minus), 1: top (plus)]
+    float gflux[2][kS3Warps][5][32];    // flux of the y-face above row w
+};
+
+template <int LIM, int RS>
+__global__ void __launch_bounds__(kS3Threads, 1)
+k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
+{
+    extern __shared__ __align__(16) unsigned char s3_raw[];
+    S3Shared& sh = *reinterpret_cast<S3Shared*>(s3_raw);
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const Decision dec = decide(ctl, slot, rp);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        publish_decision(ctl, dec, rp, slot, out_buf);
+    }
+    if (dec.noop || dec.neg_dt) {
+        return;
+    }
+    const double dt = dec.dt;
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const int ncx = (g.nx[0] + 27) / 28, ncy = (g.nx[1] + 11) / 12;
+    int b = blockIdx.x;
+    const int bx = b % ncx;
+    b /= ncx;
+    const int by = b % ncy;
+    const int bz = b / ncy;
+    const int col = g.ng + 28 * bx - 2 + lane;
+    const int row = g.ng + 12 * by - 2 + w;
+    const int colc = min(col, n0 - 1);
+    const int rowc = min(row, n1 - 1);
+    const bool out_cell = lane >= 2 && lane < 30 && w >= 2 && w < 14 && col < g.ng + g.nx[0] &&
+                          row < g.ng + g.nx[1];
+    const int z0 = g.ng + L * bz;
+    const int z1 = min(z0 + L, g.ng + g.nx[2]);
+    const int64_t pitch = in.pitch;
+    const int64_t plane = in.plane;
+    const double* __restrict__ qin = in.q;
+    double* __restrict__ qout = out.q;
+
+    s3::Ctx c;
+    c.eos = fast::Eos{(float)g.gamma, (float)g.gamma_m1, (float)(1.0 / g.gamma_m1)};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        c.cth[d] = (float)(0.5 * dt * g.inv_dx[d]);
+        c.dg[d] = (float)(0.5 * dt * g.g[d]);
+    }
+    c.gravity = g.g[0] != 0.0 || g.g[1] != 0.0 || g.g[2] != 0.0;
+    const double gm1 = g.gamma_m1;
+
+    auto load = [&](int z, double q[5]) {
+        const int zc = min(max(z, 0), n2 - 1);
+        const int64_t o = ((int64_t)zc * n1 + rowc) * pitch + colc;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            q[v] = __ldg(qin + o + plane * v);
+        }
+    };
+    auto put_prim = [&](int z, const float p[5]) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            sh.prim[z & 1][w][v][lane] = p[v];
+        }
+    };
+    const int wd = max(w - 1, 0), wu = min(w + 1, kS3Warps - 1);
+
+    // window: wC = P[z], wD = P[z+1]; qN = U[z+2] in flight
+    float wC[5], wD[5];
+    float hzU[5];      // z-plus face state of plane z (for the z-face z+1/2)
+    double dFx[5];     // x-flux difference (left - right face) of plane z, exact in FP64
+    float Gzlo[5];     // z-face flux z-1/2
+    double qN[5];
+    {
+        double q[5];
+        load(z0 - 2, q);
+        s3::prim(gm1, q, wC);
+        load(z0 - 1, q);
+        s3::prim(gm1, q, wD);
+        put_prim(z0 - 1, wD);
+        load(z0, qN);
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        hzU[v] = Gzlo[v] = 0.f;
+        dFx[v] = 0.0;
+    }
+    double inv_max = 0.0;
+    int64_t bad_cell = -1;
+    const double cxyz[3] = {dt * g.inv_dx[0], dt * g.inv_dx[1], dt * g.inv_dx[2]};
+    const double Dg[3] = {dt * g.g[0], dt * g.g[1], dt * g.g[2]};
+    __syncthreads();
+
+    for (int z = z0 - 2; z < z1; ++z) {
+        // 1. primitives of plane z+2
+        float wN[5];
+        s3::prim(gm1, qN, wN);
+        put_prim(z + 2, wN);
+        load(z + 3, qN);
+        // 2. Hancock of plane z+1 (y-neighbours' primitives of plane z+1 were shared last step)
+        float wyd[5], wyu[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            wyd[v] = sh.prim[(z + 1) & 1][wd][v][lane];
+            wyu[v] = sh.prim[(z + 1) & 1][wu][v][lane];
+        }
+        float hm[3][5], hp[3][5];
+        s3::hancock<LIM>(c, wD, wyd, wyu, wC, wN, hm, hp);
+        // 3. x-faces of plane z+1: left face at this lane, right face from lane+1
+        double dFxN[5];
+        {
+            float uL[5], Fl[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                uL[v] = __shfl_up_sync(0xffffffffu, hp[0][v], 1);
+            }
+            fast::riemann<3>(c.eos, RS, uL, hm[0], 0, Fl);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                dFxN[v] = (double)Fl[v] - (double)__shfl_down_sync(0xffffffffu, Fl[v], 1);
+            }
+        }
+        // 4. z-face z+1/2
+        float Gzhi[5];
+        fast::riemann<3>(c.eos, RS, hzU, hm[2], 2, Gzhi);
+        // 5. y-face states of plane z+1 for the neighbours
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            sh.yface[(z + 1) & 1][w][0][v][lane] = hm[1][v];
+            sh.yface[(z + 1) & 1][w][1][v][lane] = hp[1][v];
+        }
+        // 6. y-face above this row, plane z
+        const bool upd = z >= z0;
+        if (upd) {
+            float yL[5], yR[5], G[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                yL[v] = sh.yface[z & 1][w][1][v][lane];
+                yR[v] = sh.yface[z & 1][wu][0][v][lane];
+            }
+            fast::riemann<3>(c.eos, RS, yL, yR, 1, G);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                sh.gflux[z & 1][w][v][lane] = G[v];
+            }
+        }
+        __syncthreads();
+        // 7. update of plane z
+        if (upd && out_cell) {
+            double q[5], qn[5];
+            const int64_t oo = ((int64_t)z * n1 + row) * pitch + col;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                q[v] = __ldg(qin + oo + plane * v);
+            }
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                const double gb = (double)sh.gflux[z & 1][wd][v][lane];
+                const double gt = (double)sh.gflux[z & 1][w][v][lane];
+                qn[v] = q[v] + fma(cxyz[0], dFx[v],
+                                   fma(cxyz[1], gb - gt, cxyz[2] * ((double)Gzlo[v] - (double)Gzhi[v])));
+            }
+            if (c.gravity) {
+                qn[1] = fma(Dg[0], q[0], qn[1]);
+                qn[2] = fma(Dg[1], q[0], qn[2]);
+                qn[3] = fma(Dg[2], q[0], qn[3]);
+                qn[4] = fma(Dg[0], q[1], fma(Dg[1], q[2], fma(Dg[2], q[3], qn[4])));
+            }
+            double rr = (double)__fdividef(1.f, (float)qn[0]);
+            rr = rr * (2.0 - qn[0] * rr);
+            const double u = qn[1] * rr, vv = qn[2] * rr, ww = qn[3] * rr;
+            const double evol = fma(-0.5, fma(qn[1], u, fma(qn[2], vv, qn[3] * ww)), qn[4]);
+            const double c2 = g.gamma * gm1 * evol * rr;
+            double y = (double)rsqrtf((float)c2);
+            y = y * (1.5 - 0.5 * c2 * y * y);
+            const double snd = c2 * y;
+            const double cell = fma(fabs(u) + snd, g.inv_dx[0],
+                                    fma(fabs(vv) + snd, g.inv_dx[1], (fabs(ww) + snd) * g.inv_dx[2]));
+            inv_max = cell > inv_max ? cell : (isnan(cell) ? cell : inv_max);
+            if (!(evol >= 0.0) && bad_cell < 0) {
+                bad_cell = lidx(g, col, row, z);
+            }
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                qout[oo + plane * v] = qn[v];
+            }
+            // ghost images of border cells (boundary_distribute.hpp:42-76)
+            const int idx[3] = {col, row, z};
+            bool border = false;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                border |= !(idx[d] >= 2 * g.ng && idx[d] < g.n[d] - 2 * g.ng);
+            }
+            if (border) {
+                int pos[3][9], flp[3][9], cnt[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    pos[d][0] = idx[d];
+                    flp[d][0] = 0;
+                    cnt[d] = 1 + ghost_images(idx[d], g.n[d], g.ng, g.bc[2 * d], g.bc[2 * d + 1], &pos[d][1],
+                                              &flp[d][1]);
+                }
+                for (int a2 = 0; a2 < cnt[2]; ++a2) {
+                    for (int a1 = 0; a1 < cnt[1]; ++a1) {
+                        for (int a0 = 0; a0 < cnt[0]; ++a0) {
+                            if (a0 == 0 && a1 == 0 && a2 == 0) {
+                                continue;
+                            }
+                            const int64_t og = ((int64_t)pos[2][a2] * n1 + pos[1][a1]) * pitch + pos[0][a0];
+                            qout[og] = qn[0];
+                            qout[og + plane] = flp[0][a0] ? -qn[1] : qn[1];
+                            qout[og + 2 * plane] = flp[1][a1] ? -qn[2] : qn[2];
+                            qout[og + 3 * plane] = flp[2][a2] ? -qn[3] : qn[3];
+                            qout[og + 4 * plane] = qn[4];
+                        }
+                    }
+                }
+            }
+        }
+        // slide the window
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            wC[v] = wD[v];
+            wD[v] = wN[v];
+            hzU[v] = hp[2][v];
+            dFx[v] = dFxN[v];
+            Gzlo[v] = Gzhi[v];
+        }
+    }
+
+    // warp max of 1/dt -> one atomic per warp
+    const bool nan_seen = isnan(inv_max);
+    double m = nan_seen ? 0.0 : inv_max;
+    m = warp_max_d(m);
+    const unsigned nanv = __ballot_sync(0xffffffffu, nan_seen);
+    if (lane == 0) {
+        atomicMax(&ctl->inv_dt_bits[(slot + 1) % 3], dbl_bits(m));
+        if (nanv) {
+            atomicMax(&ctl->inv_dt_bits[(slot + 1) % 3], 0x7ff8000000000000ull);
+        }
+    }
+    if (bad_cell >= 0) {
+        atomicMin(&ctl->bad_cell, (unsigned long long)bad_cell);
+        ctl->err = 4;
+        ctl->errflag[(slot + 1) & 1] = 1;
+        ctl->final_buf = out_buf;
+    }
+}
+
+} // namespace hcl::fused

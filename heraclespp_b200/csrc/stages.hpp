@@ -79,6 +79,11 @@ bool strip2d_eligible(const GridDev& g);
 bool strip2d_pair_eligible(const GridDev& g);
 void step_strip2d_pair(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                        int slot, int out_buf, int L, cudaStream_t s);
+// 3-D column march (uniform Cartesian grids, uniform gravity); L <= 0 fits
+// the plane count per CTA to the resident CTAs.
+bool strip3d_eligible(const GridDev& g);
+void step_strip3d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                  int slot, int out_buf, int L, cudaStream_t s);
 void step_strip2d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                   int slot, int out_buf, int L, cudaStream_t s);
 void configure_exact();

@@ -26,6 +26,14 @@ CASES = {
     "rt_3d": (3, [16, 16, 32], dict(gamma=1.4, limiter="Minmod", riemann="HLL",
                                     bc=["Periodic", "Periodic", "Periodic", "Periodic", "Reflexive", "Reflexive"],
                                     g=(0.0, 0.0, -0.1), xmax=(0.5, 0.5, 1.0)), "rayleigh_taylor3d", {}),
+    "rt_3d_ragged": (3, [30, 14, 21], dict(gamma=1.4, limiter="Minmod", riemann="HLL",
+                                           bc=["Periodic", "Periodic", "Periodic", "Periodic", "Reflexive",
+                                               "Reflexive"], g=(0.0, 0.0, -0.1), xmax=(0.5, 0.5, 1.0)),
+                     "rayleigh_taylor3d", {}),
+    "rt_3d_hllc": (3, [29, 13, 16], dict(gamma=1.4, limiter="VanLeer", riemann="HLLC",
+                                         bc=["NullGradient", "NullGradient", "Periodic", "Periodic", "Reflexive",
+                                             "Reflexive"], g=(0.02, 0.0, -0.1), xmax=(0.5, 0.5, 1.0)),
+                   "rayleigh_taylor3d", {}),
     "sph_1d_pointmass": (1, [96], dict(gamma=1.4, limiter="VanLeer", riemann="HLLC", geometry="Spherical",
                                        bc=["Reflexive", "NullGradient"], gravity="Point_mass", central_mass=1e8,
                                        xmin=(0.2, 0.0, 0.0), xmax=(1.2, 1.0, 1.0)), "shock_tube", {"inter": 0.7}),

@@ -97,7 +97,8 @@ def test_stage_entry_points_bitwise(name):
 
 
 NSTEPS = {"sod_1d": 200, "sod_1d_odd": 60, "advection_1d": 100, "kh_2d": 60, "kh_2d_ragged": 40, "quad_2d": 40,
-          "gresho_2d_lowmach": 30, "rt_3d": 12, "sph_1d_pointmass": 50, "sph_2d": 25, "sph_3d": 8}
+          "gresho_2d_lowmach": 30, "rt_3d": 12, "rt_3d_ragged": 10, "rt_3d_hllc": 10, "sph_1d_pointmass": 50,
+          "sph_2d": 25, "sph_3d": 8}
 
 
 @pytest.mark.parametrize("name", ALL)
