@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     p.add_argument("--no-ensemble", action="store_true", help="skip the batched ensemble measurement")
     p.add_argument("--no-rt3d", action="store_true", help="skip the 3-D Rayleigh-Taylor measurement")
+    p.add_argument("--rt3d-steps", type=int, default=500, help="steps of the 3-D Rayleigh-Taylor measurement")
     return p.parse_args()
 
 
@@ -500,7 +501,7 @@ def run_ours(args):
         if rank == 0:
             line["ensemble"] = ens
     if rank == 0 and not args.no_rt3d:
-        line["rt3d"] = rt3d_cost(torch)
+        line["rt3d"] = rt3d_cost(torch, steps=args.rt3d_steps)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.cpu_budget)
     d.close()
