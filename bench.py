@@ -328,8 +328,6 @@ def ensemble_cost(torch, nprob=96, nsteps=300, k=20, seed=2024, rank=0, world=1)
     t_loop, _ = wall(lambda: [d.run(cfl=0.4, nsteps=nsteps) for d in doms])
     out["loop"] = {"ms": t_loop * 1e3, "mcups": cells * nsteps / t_loop * 1e-6}
     out["ensemble_over_loop"] = t_loop / t_ens
-    for d in doms:
-        d.close()
     # adjoint of J = sum_p sum_cells E dV
     lams = []
     for d in ens.domains:
@@ -349,6 +347,21 @@ def ensemble_cost(torch, nprob=96, nsteps=300, k=20, seed=2024, rank=0, world=1)
         out[f"adjoint_{prec}"] = {"forward_ckpt_ms": t_f * 1e3, "backward_ms": t_b * 1e3,
                                   "adj_over_fwd": (t_f + t_b) / t_ens, "checkpoint_every": k}
     ens.close()
+    # looping the single-problem adjoint (FP32 sweep) over the same problems
+    def loop_adjoint():
+        for d, lam, gr in zip(doms, lams, grads):
+            d.adjoint_forward(nsteps, cfl=0.4, checkpoint_every=k, precision="fp32_mixed")
+            d.adjoint_backward(lam, gr, device=True)
+
+    reset(doms)
+    loop_adjoint()  # allocate
+    reset(doms)
+    t_la, _ = wall(loop_adjoint)
+    out["loop_adjoint_fp32_mixed_ms"] = t_la * 1e3
+    ens_adj = out["adjoint_fp32_mixed"]
+    out["adjoint_ensemble_over_loop"] = t_la * 1e3 / (ens_adj["forward_ckpt_ms"] + ens_adj["backward_ms"])
+    for d in doms:
+        d.close()
     return out
 
 

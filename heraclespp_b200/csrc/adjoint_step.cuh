@@ -41,14 +41,17 @@ struct AdjShape {
     }
 };
 
+// The reverse sweep of one tile (index `tile` in x-fastest tile order) by the
+// whole CTA; smem_raw holds AdjShape::smem() bytes.  It starts with a CTA
+// barrier, so a CTA may run several tiles back to back.
 template <int ND, class R, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1), sizeof(R) == 8 ? 2 : 3)
-k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt)
+__device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U, const StateDev& lam_out,
+                                             const StateDev& lam_in, double dt, int tile, unsigned char* smem_raw)
 {
     using S = Shape<ND, TX, TY, TZ>;
     constexpr int NV = S::NV;
     constexpr int NT = S::TVOL;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __syncthreads(); // the previous tile of this CTA is done with the shared arrays
     double* sl = reinterpret_cast<double*>(smem_raw);       // lambda' [NV][NP] (FP64)
     R* sw = reinterpret_cast<R*>(sl + NV * S::NP);          // primitives [NV][NP]
     R* swb = sw + NV * S::NP;                               // primitive adjoints [NV][NP]
@@ -70,7 +73,7 @@ k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double 
     ntile[1] = (g.nx[1] + S::T1 - 1) / S::T1;
     int tc[3];
     {
-        int b = blockIdx.x;
+        int b = tile;
         tc[0] = b % ntile[0];
         b /= ntile[0];
         tc[1] = b % ntile[1];
@@ -456,14 +459,22 @@ k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double 
     }
 }
 
+template <int ND, class R, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1), sizeof(R) == 8 ? 2 : 3)
+k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    adjoint_tile<ND, R, TX, TY, TZ>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw);
+}
+
 // Transpose of the boundary fill: every interior cell gathers the adjoints of
-// its ghost images (sign-flipped momentum for Reflexive faces).
+// its ghost images (sign-flipped momentum for Reflexive faces).  Cells
+// first, first + stride, ... of the interior.
 template <int ND>
-__global__ void k_fold_ghosts(GridDev g, StateDev lam)
+__device__ __forceinline__ void fold_cells(const GridDev& g, const StateDev& lam, int64_t first, int64_t stride)
 {
     const int64_t count = (int64_t)g.nx[0] * g.nx[1] * g.nx[2];
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < count;
-         idx += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t idx = first; idx < count; idx += stride) {
         const int ii = (int)(idx % g.nx[0]);
         const int64_t r = idx / g.nx[0];
         const int jj = (int)(r % g.nx[1]);
@@ -510,6 +521,12 @@ __global__ void k_fold_ghosts(GridDev g, StateDev lam)
             lam.q[oc + lam.plane * v] = acc[v];
         }
     }
+}
+
+template <int ND>
+__global__ void k_fold_ghosts(GridDev g, StateDev lam)
+{
+    fold_cells<ND>(g, lam, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
 }
 
 } // namespace hcl::adjoint

@@ -1533,6 +1533,11 @@ struct hcl_ensemble {
     int L = 0, bps = 0; // tuned schedule
     int64_t cells = 0;
     std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs; // (nsteps, step0, L, bps)
+    // batched reverse pass: problem tables, tile work list, dts of all problems
+    hcl::ensemble::AdjProb* d_adjprobs = nullptr;
+    hcl::ensemble::Prob* d_rec_probs = nullptr;
+    int* d_tiles = nullptr;
+    double* d_adj_dts = nullptr;
 };
 
 namespace {
@@ -1547,6 +1552,10 @@ void free_ensemble(hcl_ensemble* e)
     }
     cudaFree(e->d_probs);
     cudaFree(e->d_probs_tune);
+    cudaFree(e->d_adjprobs);
+    cudaFree(e->d_rec_probs);
+    cudaFree(e->d_tiles);
+    cudaFree(e->d_adj_dts);
     cudaFree(e->d_items);
     cudaFree(e->d_barrier);
     cudaFree(e->d_status);
@@ -1911,19 +1920,197 @@ int hcl_ensemble_run(hcl_ensemble* e, const hcl_ensemble_params* p, hcl_ensemble
 
 int hcl_ensemble_adjoint(hcl_ensemble* e, const double* const* lam_final, double* const* grads, int memory)
 {
+    using hcl::ensemble::AdjProb;
+    using hcl::ensemble::Prob;
     if (!e || !lam_final || !grads) {
         return fail(HCL_ERR_ARGUMENT, "null argument");
     }
-    for (size_t q = 0; q < e->h.size(); ++q) {
-        int rc = adjoint_backward_impl(e->h[q], lam_final[q], grads[q], memory);
-        if (rc) {
-            return rc;
+    const size_t np = e->h.size();
+    hcl_handle* h0 = e->h[0];
+    const int N = (int)h0->adj_dts.size();
+    const int k = h0->adj_k;
+    const int nck = h0->adj_nck;
+    for (hcl_handle* h : e->h) {
+        if (!h->adj_ready || (int)h->adj_dts.size() != N || h->adj_k != k || N <= 0) {
+            return fail(HCL_ERR_CONFIG, "run the ensemble with checkpoint_every > 0 before its adjoint");
         }
     }
-    for (hcl_handle* h : e->h) {
-        HCL_CUDA(cudaStreamSynchronize(h->stream));
+    const bool fp64 = h0->adj_prec == HCL_FP64;
+    HCL_CUDA(cudaSetDevice(h0->cfg.device));
+    cudaStream_t s = e->stream;
+    int rc;
+    // per-problem buffers and tables
+    std::vector<AdjProb> ap(np);
+    std::vector<Prob> rec = e->probs;
+    std::vector<int> tiles;
+    std::vector<double> dts_all(np * (size_t)N);
+    for (size_t q = 0; q < np; ++q) {
+        hcl_handle* h = e->h[q];
+        const GridDev& g = h->g;
+        const size_t sz = (size_t)h->st[0].plane * (g.ndim + 2);
+        if (h->adj_cap_seg < k + 1) {
+            cudaFree(h->adj_seg);
+            h->adj_seg = nullptr;
+            h->adj_cap_seg = 0;
+            if ((rc = dalloc(&h->adj_seg, sz * (size_t)(2 * (k + 1))))) {
+                return rc;
+            }
+            h->adj_cap_seg = 2 * (k + 1);
+        }
+        if (!h->adj_lam && (rc = dalloc(&h->adj_lam, sz * 2))) {
+            return rc;
+        }
+        if (!h->adj_ctl && (rc = dalloc(&h->adj_ctl, 1))) {
+            return rc;
+        }
+        AdjProb& A = ap[q];
+        std::memset(&A, 0, sizeof(A));
+        A.g = g;
+        A.seg0 = h->st[0];
+        A.seg0.q = h->adj_seg;
+        A.sz = (int64_t)sz;
+        A.lam[0] = h->st[0];
+        A.lam[0].q = h->adj_lam;
+        A.lam[1] = h->st[0];
+        A.lam[1].q = h->adj_lam + sz;
+        A.ckpt = h->adj_ckpt;
+        A.ctl = h->adj_ctl;
+        A.tile0 = (int)tiles.size();
+        const int nt = ((g.nx[0] + hcl::ensemble::kRevTile - 1) / hcl::ensemble::kRevTile) *
+                       ((g.nx[1] + hcl::ensemble::kRevTile - 1) / hcl::ensemble::kRevTile);
+        tiles.insert(tiles.end(), (size_t)nt, (int)q);
+        rec[q].q[0] = h->adj_seg;
+        rec[q].q[1] = nullptr;
+        rec[q].seg_stride = (int64_t)sz;
+        rec[q].ctl = h->adj_ctl;
+        rec[q].dt_log = nullptr;
+        rec[q].dt_cap = 0;
+        std::copy(h->adj_dts.begin(), h->adj_dts.end(), dts_all.begin() + q * (size_t)N);
     }
+    cudaFree(e->d_adjprobs);
+    cudaFree(e->d_rec_probs);
+    cudaFree(e->d_tiles);
+    cudaFree(e->d_adj_dts);
+    e->d_adjprobs = nullptr;
+    e->d_rec_probs = nullptr;
+    e->d_tiles = nullptr;
+    e->d_adj_dts = nullptr;
+    if ((rc = dalloc(&e->d_adjprobs, np)) || (rc = dalloc(&e->d_rec_probs, np)) ||
+        (rc = dalloc(&e->d_tiles, tiles.size())) || (rc = dalloc(&e->d_adj_dts, dts_all.size()))) {
+        return rc;
+    }
+    for (size_t q = 0; q < np; ++q) {
+        ap[q].dts = e->d_adj_dts + q * (size_t)N;
+    }
+    HCL_CUDA(cudaMemcpyAsync(e->d_adj_dts, dts_all.data(), sizeof(double) * dts_all.size(), cudaMemcpyHostToDevice, s));
+    HCL_CUDA(cudaMemcpyAsync(e->d_adjprobs, ap.data(), sizeof(AdjProb) * np, cudaMemcpyHostToDevice, s));
+    HCL_CUDA(cudaMemcpyAsync(e->d_rec_probs, rec.data(), sizeof(Prob) * np, cudaMemcpyHostToDevice, s));
+    HCL_CUDA(cudaMemcpyAsync(e->d_tiles, tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, s));
+    // lambda^N, folded onto the interior
+    const cudaMemcpyKind kin = memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (size_t q = 0; q < np; ++q) {
+        const GridDev& g = e->h[q]->g;
+        const int nd = g.ndim;
+        HCL_CUDA(cudaMemsetAsync(ap[q].lam[0].q, 0, sizeof(double) * ap[q].sz * 2, s));
+        hcl::fused::pack_state(g, ap[q].lam[0], lam_final[q], lam_final[q] + g.N, lam_final[q] + g.N * (nd + 1), kin,
+                               s);
+        hcl::adjoint::fold(g, ap[q].lam[0], s);
+    }
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h0->cfg.device);
+    const int rev_bps = hcl::ensemble::reverse_blocks_per_sm(fp64);
+    if (rev_bps <= 0) {
+        return fail(HCL_ERR_CUDA, "the batched reverse kernel cannot be resident");
+    }
+    if (e->L == 0 || e->items_L != e->L) {
+        return fail(HCL_ERR_CONFIG, "run the ensemble before its adjoint");
+    }
+    hcl::ensemble::Params ep;
+    std::memset(&ep, 0, sizeof(ep));
+    ep.cfl = 0.4;
+    ep.step0 = 0;
+    ep.L = e->L;
+    ep.nitems = e->nitems;
+    ep.nprob = (int)np;
+    ep.fixed_dt = 1;
+    ep.dts = e->d_adj_dts;
+    ep.dts_stride = N;
+    ep.seg_mode = 1;
+    HCL_CUDA(cudaMemsetAsync(e->d_status, 0, sizeof(int), s));
+    // the segment loop (2 persistent launches per checkpoint segment) is
+    // captured in a CUDA graph and replayed; it is rebuilt for every call
+    // because the tables it reads are reallocated above
+    int cur = 0;
+    auto issue = [&]() -> cudaError_t {
+        cudaError_t err = cudaSuccess;
+        for (int sg = nck - 1; sg >= 0 && err == cudaSuccess; --sg) {
+            const int first = sg * k;
+            const int len = std::min(k, N - first);
+            hcl::ensemble::seg_init(e->d_adjprobs, (int)np, sg, first, s);
+            if (len > 1) {
+                ep.nsteps = len - 1;
+                err = cudaMemsetAsync(e->d_barrier, 0, sizeof(unsigned int), s);
+                if (err == cudaSuccess) {
+                    err = hcl::ensemble::launch(e->lim, e->rs, e->bps * nsm, e->d_rec_probs, e->d_items, ep,
+                                                e->d_barrier, e->d_status, s);
+                }
+            }
+            hcl::ensemble::AdjParams prm;
+            prm.nprob = (int)np;
+            prm.ntiles = (int)tiles.size();
+            prm.first = first;
+            prm.len = len;
+            prm.cur = cur;
+            if (err == cudaSuccess) {
+                err = cudaMemsetAsync(e->d_barrier, 0, sizeof(unsigned int), s);
+            }
+            if (err == cudaSuccess) {
+                err = hcl::ensemble::reverse(fp64, rev_bps * nsm, e->d_adjprobs, e->d_tiles, prm, e->d_barrier,
+                                             e->d_status, s);
+            }
+            cur ^= len & 1;
+        }
+        return err;
+    };
+    {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        HCL_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t err = issue();
+        const cudaError_t err2 = cudaStreamEndCapture(s, &graph);
+        bool replayed = false;
+        if (err == cudaSuccess && err2 == cudaSuccess && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+            replayed = cudaGraphLaunch(exec, s) == cudaSuccess;
+        }
+        if (graph) {
+            cudaGraphDestroy(graph);
+        }
+        if (exec) {
+            cudaGraphExecDestroy(exec); // a launched graph may be destroyed; its work completes
+        }
+        cudaGetLastError();
+        if (!replayed) {
+            cur = 0;
+            HCL_CUDA(issue());
+        }
+    }
+    const cudaMemcpyKind kout = memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    for (size_t q = 0; q < np; ++q) {
+        const GridDev& g = e->h[q]->g;
+        const int nd = g.ndim;
+        hcl::adjoint::zero_ghosts(g, ap[q].lam[cur], s);
+        hcl::fused::unpack_state(g, ap[q].lam[cur], grads[q], grads[q] + g.N, grads[q] + g.N * (nd + 1), kout, s);
+    }
+    int status = 0;
+    HCL_CUDA(cudaMemcpyAsync(&status, e->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HCL_CUDA(cudaStreamSynchronize(s));
     HCL_LAUNCH_CHECK();
+    if (status == HCL_ERR_TIMEOUT) {
+        return fail(HCL_ERR_TIMEOUT, "ensemble adjoint grid barrier timed out");
+    }
+    if (status != 0) {
+        return fail(HCL_ERR_INVALID_STATE, "invalid state in the ensemble adjoint's recomputation");
+    }
     return HCL_OK;
 }
 

@@ -88,8 +88,10 @@ k_ensemble(const Prob* __restrict__ probs, const int* __restrict__ item_prob, Pa
             const int local = w - P.item0;
             double inv_max = 0.0;
             int64_t bad_cell = -1;
-            fused::strip_work<LIM, RS>(P.g, P.q[gs & 1], P.q[(gs + 1) & 1], P.plane, P.pitch, dt, local % P.ncolw,
-                                       local / P.ncolw, ep.L, inv_max, bad_cell);
+            const double* qin = ep.seg_mode ? P.q[0] + (int64_t)s * P.seg_stride : P.q[gs & 1];
+            double* qout = ep.seg_mode ? P.q[0] + (int64_t)(s + 1) * P.seg_stride : P.q[(gs + 1) & 1];
+            fused::strip_work<LIM, RS>(P.g, qin, qout, P.plane, P.pitch, dt, local % P.ncolw, local / P.ncolw, ep.L,
+                                       inv_max, bad_cell);
             const bool nan_seen = isnan(inv_max);
             double m = nan_seen ? 0.0 : inv_max;
             m = fused::warp_max_d(m);

@@ -115,6 +115,7 @@ struct Prob {
     StepCtl* ctl;
     double* dt_log;
     int dt_cap;
+    int64_t seg_stride; // segment mode: state s at q[0] + s * seg_stride
 };
 
 struct Params {
@@ -127,7 +128,36 @@ struct Params {
     int fixed_dt;
     const double* dts; // [nprob][dts_stride], indexed by iteration
     int dts_stride;
+    int seg_mode;      // 1: step s reads state s and writes state s+1 of each segment buffer
 };
+
+// Reverse pass of a batch: one problem's segment states, adjoint buffers,
+// checkpoints and dts.
+struct AdjProb {
+    GridDev g;
+    fused::StateDev seg0;  // segment state 0; state j at seg0.q + j * sz
+    int64_t sz;            // doubles per state buffer
+    fused::StateDev lam[2];
+    const double* ckpt;    // checkpoints, sz apart
+    StepCtl* ctl;          // control block of the recomputation
+    const double* dts;     // dts of the forward run
+    int tile0;             // first work item of this problem
+};
+
+struct AdjParams {
+    int nprob;
+    int ntiles;  // work items (16x16 tiles) over all problems
+    int first;   // step index of the segment's first state
+    int len;     // steps in the segment
+    int cur;     // lam[cur] holds the adjoint of the segment's last output state
+};
+
+int reverse_blocks_per_sm(bool fp64);
+// adjoint-tile size (16x16) of the batched reverse kernel
+constexpr int kRevTile = 16;
+void seg_init(const AdjProb* probs, int nprob, int sg, int first, cudaStream_t s);
+cudaError_t reverse(bool fp64, int grid, const AdjProb* probs, const int* tile_prob, const AdjParams& ap,
+                    unsigned int* barrier, int* status, cudaStream_t s);
 
 int max_blocks_per_sm(int lim, int rs);
 cudaError_t launch(int lim, int rs, int grid, const Prob* probs, const int* item_prob, const Params& ep,
