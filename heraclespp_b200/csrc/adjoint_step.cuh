@@ -44,13 +44,12 @@ struct AdjShape {
 // The reverse sweep of one tile (index `tile` in x-fastest tile order) by the
 // whole CTA; smem_raw holds AdjShape::smem() bytes.  It starts with a CTA
 // barrier, so a CTA may run several tiles back to back.
-template <int ND, class R, int TX, int TY, int TZ>
+template <int ND, class R, int TX, int TY, int TZ, int NT>
 __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U, const StateDev& lam_out,
                                              const StateDev& lam_in, double dt, int tile, unsigned char* smem_raw)
 {
     using S = Shape<ND, TX, TY, TZ>;
     constexpr int NV = S::NV;
-    constexpr int NT = S::TVOL;
     __syncthreads(); // the previous tile of this CTA is done with the shared arrays
     double* sl = reinterpret_cast<double*>(smem_raw);       // lambda' [NV][NP] (FP64)
     R* sw = reinterpret_cast<R*>(sl + NV * S::NP);          // primitives [NV][NP]
@@ -459,12 +458,19 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
     }
 }
 
-template <int ND, class R, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1), sizeof(R) == 8 ? 2 : 3)
+// NT threads per CTA (any count: every phase strides over its items by NT)
+template <class R, int NT>
+constexpr int adj_min_blocks()
+{
+    return sizeof(R) == 8 ? (NT <= 256 ? 2 : 1) : (NT <= 256 ? 3 : (NT <= 384 ? 2 : 1));
+}
+
+template <int ND, class R, int TX, int TY, int TZ, int NT>
+__global__ void __launch_bounds__(NT, adj_min_blocks<R, NT>())
 k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    adjoint_tile<ND, R, TX, TY, TZ>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw);
+    adjoint_tile<ND, R, TX, TY, TZ, NT>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw);
 }
 
 // Transpose of the boundary fill: every interior cell gathers the adjoints of

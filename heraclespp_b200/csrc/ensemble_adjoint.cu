@@ -88,8 +88,8 @@ k_ens_reverse(const AdjProb* __restrict__ probs, const int* __restrict__ tile_pr
             }
             fused::StateDev U = P.seg0;
             U.q += P.sz * j;
-            adjoint::adjoint_tile<2, R, kRevTile, kRevTile, 1>(sg, U, P.lam[cur], P.lam[cur ^ 1], P.dts[n],
-                                                               item - P.tile0, smem_raw);
+            adjoint::adjoint_tile<2, R, kRevTile, kRevTile, 1, kRevTile * kRevTile>(
+                sg, U, P.lam[cur], P.lam[cur ^ 1], P.dts[n], item - P.tile0, smem_raw);
         }
         if (!grid_barrier(barrier, (++phase) * gridDim.x, status)) {
             return;
