@@ -43,7 +43,8 @@ def _ptr(t):
 
 def make_config(ndim, nx, *, nghost=2, nfx=0, geometry="Cartesian", gamma=5.0 / 3.0, mmw=1.0, limiter="VanLeer",
                 riemann="HLL", bc=("Periodic",) * 6, gravity="Uniform", g=(0.0, 0.0, 0.0), central_mass=1.0,
-                xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0), nodes=None, precision="fp64", device=0):
+                xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0), nodes=None, precision="fp64", device=0,
+                pressure_fix=False, eps_pf=1e-6):
     """hcl_config from the reference's plugin keys; returns (config, node arrays kept alive)."""
     L = lib()
     cfg = Config()
@@ -69,6 +70,8 @@ def make_config(ndim, nx, *, nghost=2, nfx=0, geometry="Cartesian", gamma=5.0 / 
     cfg.central_mass = float(central_mass)
     cfg.precision = _key(PRECISION, precision, "precision")
     cfg.device = int(device)
+    cfg.pressure_fix = 1 if pressure_fix else 0
+    cfg.eps_pf = float(eps_pf)
     _nodes = None
     if nodes is not None:
         _nodes = [np.ascontiguousarray(x, dtype=np.float64) for x in nodes]
@@ -83,11 +86,12 @@ class Domain:
     def __init__(self, ndim, nx, *, nghost=2, nfx=0, geometry="Cartesian", gamma=5.0 / 3.0, mmw=1.0,
                  limiter="VanLeer", riemann="HLL", bc=("Periodic",) * 6, gravity="Uniform", g=(0.0, 0.0, 0.0),
                  central_mass=1.0, xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0), nodes=None, precision="fp64",
-                 device=0):
+                 device=0, pressure_fix=False, eps_pf=1e-6):
         cfg, self._nodes = make_config(ndim, nx, nghost=nghost, nfx=nfx, geometry=geometry, gamma=gamma, mmw=mmw,
                                        limiter=limiter, riemann=riemann, bc=bc, gravity=gravity, g=g,
                                        central_mass=central_mass, xmin=xmin, xmax=xmax, nodes=nodes,
-                                       precision=precision, device=device)
+                                       precision=precision, device=device, pressure_fix=pressure_fix,
+                                       eps_pf=eps_pf)
         h = C.c_void_p()
         check(lib().hcl_create(C.byref(cfg), C.byref(h)))
         self._owned = True
@@ -169,6 +173,11 @@ class Domain:
                                        _ptr(rho_rec), _ptr(rhou_rec), _ptr(E_rec), _ptr(fx_rec), _ptr(rho_new),
                                        _ptr(rhou_new), _ptr(E_new), _ptr(fx_new), stream))
 
+    def pressure_fix(self, dt, eps, rho, rhou, E, rho_rec, rhou_rec, E_rec, rho_new, rhou_new, E_new, stream=None):
+        check(lib().hcl_pressure_fix(self.h, float(dt), float(eps), _ptr(rho), _ptr(rhou), _ptr(E), _ptr(rho_rec),
+                                     _ptr(rhou_rec), _ptr(E_rec), _ptr(rho_new), _ptr(rhou_new), _ptr(E_new),
+                                     stream))
+
     def boundary_conditions(self, rho, rhou, E, fx=None, stream=None):
         check(lib().hcl_boundary_conditions(self.h, _ptr(rho), _ptr(rhou), _ptr(E), _ptr(fx), stream))
 
@@ -191,18 +200,23 @@ class Domain:
     def set_state(self, rho, rhou, E, fx=None, device=False):
         if not device:
             rho, rhou, E = (np.ascontiguousarray(a, dtype=np.float64) for a in (rho, rhou, E))
+            if fx is not None:
+                fx = np.ascontiguousarray(fx, dtype=np.float64)
         check(lib().hcl_set_state(self.h, _ptr(rho), _ptr(rhou), _ptr(E), _ptr(fx), 1 if device else 0))
 
-    def get_state(self, out=None, device=False):
+    def get_state(self, out=None, device=False, fx=None):
+        """(rho, rhou, E); with nfx > 0, fx (an array of nfx planes) is filled too."""
         if out is None:
             out = (self.zeros(), self.zeros(self.ndim), self.zeros())
         rho, rhou, E = out
-        check(lib().hcl_get_state(self.h, _ptr(rho), _ptr(rhou), _ptr(E), None, 1 if device else 0))
+        check(lib().hcl_get_state(self.h, _ptr(rho), _ptr(rhou), _ptr(E), _ptr(fx), 1 if device else 0))
         return out
 
-    def set_state_from_prim(self, rho, u, P):
+    def set_state_from_prim(self, rho, u, P, fx=None):
         rho, u, P = (np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, P))
-        check(lib().hcl_set_state_from_prim(self.h, _ptr(rho), _ptr(u), _ptr(P), None))
+        if fx is not None:
+            fx = np.ascontiguousarray(fx, dtype=np.float64)
+        check(lib().hcl_set_state_from_prim(self.h, _ptr(rho), _ptr(u), _ptr(P), _ptr(fx)))
 
     def reset_clock(self, t_ini=0.0):
         check(lib().hcl_reset_clock(self.h, float(t_ini)))

@@ -36,7 +36,7 @@ EXPORTS = [
     "hcl_conservation_sums", "hcl_kernel_launch_count", "hcl_get_stream", "hcl_get_interior",
     "hcl_adjoint_forward", "hcl_adjoint_backward", "hcl_adjoint_dts", "hcl_set_schedule",
     "hcl_ensemble_create", "hcl_ensemble_destroy", "hcl_ensemble_handle", "hcl_ensemble_stream",
-    "hcl_ensemble_run", "hcl_ensemble_adjoint",
+    "hcl_ensemble_run", "hcl_ensemble_adjoint", "hcl_pressure_fix",
 ]
 
 
@@ -70,6 +70,8 @@ class Config(C.Structure):
         ("nodes", C.c_void_p * 3),
         ("precision", C.c_int),
         ("device", C.c_int),
+        ("pressure_fix", C.c_int),
+        ("eps_pf", C.c_double),
     ]
 
 
@@ -164,6 +166,7 @@ def lib():
     L.hcl_hydro_reconstruction.argtypes = [H, i, d] + [vp] * 11
     L.hcl_godunov_scheme.argtypes = [H, i, d] + [vp] * 13
     L.hcl_boundary_conditions.argtypes = [H, vp, vp, vp, vp, vp]
+    L.hcl_pressure_fix.argtypes = [H, d, d] + [vp] * 10
     L.hcl_time_step.argtypes = [H, i, vp, vp, vp, C.POINTER(d), vp]
     L.hcl_minimum_internal_energy.argtypes = [H, vp, vp, vp, C.POINTER(d), vp]
     L.hcl_integrate.argtypes = [H, vp, C.POINTER(d), vp]

@@ -144,6 +144,17 @@ struct hcl_handle {
     int adj_prec = 0;
     int adj_ready = 0;
     int adj_ddts_cap = 0;
+    // reference-layout state of the stage-composed loop (passive scalars or
+    // pressure fix): one allocation, carved by stage_buffers()
+    double* sl_mem = nullptr;
+    double *sl_rho = nullptr, *sl_rhou = nullptr, *sl_E = nullptr, *sl_fx = nullptr, *sl_u = nullptr, *sl_P = nullptr;
+    double *sl_rho_rec = nullptr, *sl_rhou_rec = nullptr, *sl_E_rec = nullptr, *sl_fx_rec = nullptr;
+    double *sl_rho_new = nullptr, *sl_rhou_new = nullptr, *sl_E_new = nullptr, *sl_fx_new = nullptr;
+    double sl_t = 0.0;
+    int sl_iter = 0;
+    int sl_toid = -1, sl_ioid = -1;
+    int sl_status = 0;
+    std::vector<double> sl_dts;
     // second stream of the reverse pass: recomputes segment s-1 while the
     // main stream sweeps segment s back; events order the two segment buffers
     cudaStream_t adj_stream = nullptr;
@@ -193,6 +204,7 @@ void free_handle(hcl_handle* h)
     cudaFree(h->adj_lam);
     cudaFree(h->adj_ddts);
     cudaFree(h->adj_ctl);
+    cudaFree(h->sl_mem);
     for (cudaEvent_t ev : {h->adj_ev_start, h->adj_ev_rec[0], h->adj_ev_rec[1], h->adj_ev_rev[0], h->adj_ev_rev[1]}) {
         if (ev) {
             cudaEventDestroy(ev);
@@ -331,6 +343,9 @@ int validate(const hcl_config* c)
 {
     if (!c) {
         return fail(HCL_ERR_ARGUMENT, "null config");
+    }
+    if (c->pressure_fix && !(c->eps_pf > 0)) {
+        return fail(HCL_ERR_CONFIG, "eps_pf must be > 0 with the pressure fix");
     }
     if (c->ndim < 1 || c->ndim > 3) {
         return fail(HCL_ERR_CONFIG, "ndim must be 1, 2 or 3 (got %d)", c->ndim);
@@ -523,6 +538,42 @@ int get_graph(hcl_handle* h, const RunParamsDev& rp, int k, cudaGraphExec_t* out
     return HCL_OK;
 }
 
+// Handles whose time loop is composed of the FP64 stage entry points: passive
+// scalars and the pressure fix are not carried by the fused kernels.
+bool stage_mode(const hcl_handle* h)
+{
+    return h->cfg.nfx > 0 || h->cfg.pressure_fix != 0;
+}
+
+// The reference-layout arrays of the stage-composed loop (main.cpp:187-205).
+int stage_buffers(hcl_handle* h)
+{
+    if (h->sl_mem) {
+        return HCL_OK;
+    }
+    const size_t N = (size_t)h->g.N, nd = (size_t)h->g.ndim, nf = (size_t)std::max(h->g.nfx, 1);
+    const size_t sizes[14] = {N, N * nd, N, N * nf, N * nd, N, N * 2 * nd, N * 2 * nd * nd, N * 2 * nd,
+                              N * 2 * nd * nf, N, N * nd, N, N * nf};
+    size_t total = 0;
+    for (size_t v : sizes) {
+        total += v;
+    }
+    int rc = dalloc(&h->sl_mem, total);
+    if (rc) {
+        return rc;
+    }
+    HCL_CUDA(cudaMemset(h->sl_mem, 0, sizeof(double) * total));
+    double** ptrs[14] = {&h->sl_rho,     &h->sl_rhou,     &h->sl_E,       &h->sl_fx,        &h->sl_u,
+                         &h->sl_P,       &h->sl_rho_rec,  &h->sl_rhou_rec, &h->sl_E_rec,   &h->sl_fx_rec,
+                         &h->sl_rho_new, &h->sl_rhou_new, &h->sl_E_new,   &h->sl_fx_new};
+    double* q = h->sl_mem;
+    for (int i = 0; i < 14; ++i) {
+        *ptrs[i] = q;
+        q += sizes[i];
+    }
+    return HCL_OK;
+}
+
 // Normalises the fused state after a finished run so that it sits in buffer 0
 // with a fresh control block (t and iteration carried over).
 int restart_clock(hcl_handle* h, double t, int iter)
@@ -596,6 +647,8 @@ void hcl_config_default(hcl_config* c)
     }
     c->precision = HCL_FP64;
     c->device = 0;
+    c->pressure_fix = 0;
+    c->eps_pf = 0.000001;
 }
 
 int hcl_create(const hcl_config* cfg, hcl_handle** out)
@@ -893,6 +946,20 @@ int hcl_godunov_scheme(hcl_handle* h, int ng_eff, double dt, const double* rho, 
     return HCL_OK;
 }
 
+int hcl_pressure_fix(hcl_handle* h, double dt, double eps, const double* rho, const double* rhou, const double* E,
+                     const double* rho_rec, const double* rhou_rec, const double* E_rec, const double* rho_new,
+                     const double* rhou_new, double* E_new, void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!rho || !rhou || !E || !rho_rec || !rhou_rec || !E_rec || !rho_new || !rhou_new || !E_new) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    hcl::stage::pressure_fix(h->g, dt, eps, rho, rhou, E, rho_rec, rhou_rec, E_rec, rho_new, rhou_new, E_new,
+                             pick(h, stream));
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
 int hcl_boundary_conditions(hcl_handle* h, double* rho, double* rhou, double* E, double* fx, void* stream)
 {
     HCL_CHECK_HANDLE(h);
@@ -970,11 +1037,33 @@ int hcl_set_state(hcl_handle* h, const double* rho, const double* rhou, const do
     if (!rho || !rhou || !E) {
         return fail(HCL_ERR_ARGUMENT, "null array");
     }
-    if (h->g.nfx > 0) {
-        return fail(HCL_ERR_CONFIG, "the fused path does not carry passive scalars (nfx > 0); use the stage entry points");
+    const cudaMemcpyKind kind = memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (stage_mode(h)) {
+        int rc = stage_buffers(h);
+        if (rc) {
+            return rc;
+        }
+        const size_t N = (size_t)h->g.N, nd = (size_t)h->g.ndim;
+        cudaStream_t s = h->stream;
+        HCL_CUDA(cudaMemcpyAsync(h->sl_rho, rho, sizeof(double) * N, kind, s));
+        HCL_CUDA(cudaMemcpyAsync(h->sl_rhou, rhou, sizeof(double) * N * nd, kind, s));
+        HCL_CUDA(cudaMemcpyAsync(h->sl_E, E, sizeof(double) * N, kind, s));
+        if (h->g.nfx > 0) {
+            if (fx) {
+                HCL_CUDA(cudaMemcpyAsync(h->sl_fx, fx, sizeof(double) * N * h->g.nfx, kind, s));
+            } else {
+                HCL_CUDA(cudaMemsetAsync(h->sl_fx, 0, sizeof(double) * N * h->g.nfx, s));
+            }
+        }
+        // main.cpp:311
+        if ((rc = hcl_conv_cons_to_prim(h, h->g.ng, h->sl_rho, h->sl_rhou, h->sl_E, h->sl_u, h->sl_P, s))) {
+            return rc;
+        }
+        HCL_CUDA(cudaStreamSynchronize(s));
+        h->state_valid = 1;
+        return hcl_reset_clock(h, 0.0);
     }
     (void)fx;
-    const cudaMemcpyKind kind = memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     hcl::fused::pack_state(h->g, h->st[0], rho, rhou, E, kind, h->stream);
     HCL_CUDA(cudaGetLastError());
     h->cur = 0;
@@ -988,11 +1077,23 @@ int hcl_get_state(hcl_handle* h, double* rho, double* rhou, double* E, double* f
     if (!rho || !rhou || !E) {
         return fail(HCL_ERR_ARGUMENT, "null array");
     }
-    (void)fx;
     if (!h->state_valid) {
         return fail(HCL_ERR_CONFIG, "no state set");
     }
     const cudaMemcpyKind kind = memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (stage_mode(h)) {
+        const size_t N = (size_t)h->g.N, nd = (size_t)h->g.ndim;
+        cudaStream_t s = h->stream;
+        HCL_CUDA(cudaMemcpyAsync(rho, h->sl_rho, sizeof(double) * N, kind, s));
+        HCL_CUDA(cudaMemcpyAsync(rhou, h->sl_rhou, sizeof(double) * N * nd, kind, s));
+        HCL_CUDA(cudaMemcpyAsync(E, h->sl_E, sizeof(double) * N, kind, s));
+        if (fx && h->g.nfx > 0) {
+            HCL_CUDA(cudaMemcpyAsync(fx, h->sl_fx, sizeof(double) * N * h->g.nfx, kind, s));
+        }
+        HCL_CUDA(cudaStreamSynchronize(s));
+        return HCL_OK;
+    }
+    (void)fx;
     hcl::fused::unpack_state(h->g, h->st[h->cur], rho, rhou, E, kind, h->stream);
     HCL_CUDA(cudaGetLastError());
     HCL_CUDA(cudaStreamSynchronize(h->stream));
@@ -1005,14 +1106,38 @@ int hcl_set_state_from_prim(hcl_handle* h, const double* rho, const double* u, c
     if (!rho || !u || !P) {
         return fail(HCL_ERR_ARGUMENT, "null array");
     }
-    if (h->g.nfx > 0) {
-        return fail(HCL_ERR_CONFIG, "the fused path does not carry passive scalars (nfx > 0)");
-    }
-    (void)fx;
     const int nd = h->g.ndim;
     const size_t N = (size_t)h->g.N;
-    double *d_rho = nullptr, *d_u = nullptr, *d_P = nullptr, *d_m = nullptr, *d_E = nullptr;
     int rc;
+    if (stage_mode(h)) {
+        // main.cpp:305-311 on the reference-layout arrays
+        if ((rc = stage_buffers(h))) {
+            return rc;
+        }
+        cudaStream_t s = h->stream;
+        HCL_CUDA(cudaMemcpyAsync(h->sl_rho, rho, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+        HCL_CUDA(cudaMemcpyAsync(h->sl_u, u, sizeof(double) * N * nd, cudaMemcpyHostToDevice, s));
+        HCL_CUDA(cudaMemcpyAsync(h->sl_P, P, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+        HCL_CUDA(cudaMemsetAsync(h->sl_rhou, 0, sizeof(double) * N * nd, s));
+        HCL_CUDA(cudaMemsetAsync(h->sl_E, 0, sizeof(double) * N, s));
+        if (h->g.nfx > 0) {
+            if (fx) {
+                HCL_CUDA(cudaMemcpyAsync(h->sl_fx, fx, sizeof(double) * N * h->g.nfx, cudaMemcpyHostToDevice, s));
+            } else {
+                HCL_CUDA(cudaMemsetAsync(h->sl_fx, 0, sizeof(double) * N * h->g.nfx, s));
+            }
+        }
+        if ((rc = hcl_conv_prim_to_cons(h, 0, h->sl_rho, h->sl_u, h->sl_P, h->sl_rhou, h->sl_E, s)) ||
+            (rc = hcl_boundary_conditions(h, h->sl_rho, h->sl_rhou, h->sl_E, h->g.nfx > 0 ? h->sl_fx : nullptr, s)) ||
+            (rc = hcl_conv_cons_to_prim(h, h->g.ng, h->sl_rho, h->sl_rhou, h->sl_E, h->sl_u, h->sl_P, s))) {
+            return rc;
+        }
+        HCL_CUDA(cudaStreamSynchronize(s));
+        h->state_valid = 1;
+        return hcl_reset_clock(h, 0.0);
+    }
+    (void)fx;
+    double *d_rho = nullptr, *d_u = nullptr, *d_P = nullptr, *d_m = nullptr, *d_E = nullptr;
     if ((rc = dalloc(&d_rho, N)) || (rc = dalloc(&d_u, N * nd)) || (rc = dalloc(&d_P, N)) ||
         (rc = dalloc(&d_m, N * nd)) || (rc = dalloc(&d_E, N))) {
         cudaFree(d_rho);
@@ -1052,7 +1177,137 @@ int hcl_reset_clock(hcl_handle* h, double t_ini)
     if (!h->state_valid) {
         return fail(HCL_ERR_CONFIG, "no state set");
     }
+    if (stage_mode(h)) {
+        h->sl_t = t_ini;
+        h->sl_iter = 0;
+        h->sl_toid = h->sl_ioid = -1;
+        h->sl_status = 0;
+        h->sl_dts.clear();
+        return HCL_OK;
+    }
     return restart_clock(h, t_ini, 0);
+}
+
+// The reference time loop (main.cpp:354-531) composed of the FP64 stage entry
+// points on the reference-layout arrays: dt and the health check are read back
+// each step, as the reference does.
+static int run_stage_loop(hcl_handle* h, const hcl_run_params* p, hcl_run_result* r)
+{
+    if (h->sl_status) {
+        return fail(HCL_ERR_INVALID_STATE, "the state is invalid; set a new state");
+    }
+    if (p->fixed_dt && (!p->dts || p->nsteps <= 0)) {
+        return fail(HCL_ERR_ARGUMENT, "fixed_dt needs dts and nsteps > 0");
+    }
+    cudaStream_t s = h->stream;
+    const int ng = h->g.ng;
+    const bool pf = h->cfg.pressure_fix != 0;
+    const bool has_fx = h->g.nfx > 0;
+    int rc;
+    int done = 0;
+    int status = 0;
+    bool finished = false;
+    double last_dt = 0.0;
+    while (p->nsteps <= 0 || done < p->nsteps) {
+        double dt;
+        if (p->fixed_dt) {
+            dt = p->dts[done];
+        } else {
+            double dt_inv = 0.0;
+            if ((rc = hcl_time_step(h, ng, h->sl_rho, h->sl_u, h->sl_P, &dt_inv, s))) {
+                return rc;
+            }
+            dt = p->cfl * dt_inv; // main.cpp:355
+        }
+        bool should_exit = false;
+        if (p->iter_frequency > 0) { // main.cpp:358-364
+            const int next_output = (h->sl_ioid + 1) * p->iter_frequency;
+            if ((h->sl_iter + 1) >= next_output) {
+                ++h->sl_ioid;
+            }
+        }
+        if (p->time_frequency > 0) { // main.cpp:365-375
+            const double next_output = p->time_first_output + ((h->sl_toid + 1) * p->time_frequency);
+            if ((h->sl_t + dt) >= next_output) {
+                dt = next_output - h->sl_t;
+                if (dt <= 0) {
+                    status = HCL_ERR_NEGATIVE_DT;
+                    break;
+                }
+                ++h->sl_toid;
+            }
+        }
+        if ((h->sl_t + dt) >= p->t_end) { // main.cpp:377-381
+            dt = p->t_end - h->sl_t;
+            should_exit = true;
+        }
+        if ((h->sl_iter + 1) >= p->max_iter) { // main.cpp:382-385
+            should_exit = true;
+        }
+        double min_evol = 0.0; // main.cpp:397-425
+        if ((rc = hcl_minimum_internal_energy(h, h->sl_rho, h->sl_rhou, h->sl_E, &min_evol, s))) {
+            return rc;
+        }
+        if (std::isnan(min_evol) || min_evol < 0) {
+            status = HCL_ERR_INVALID_STATE;
+            break;
+        }
+        h->sl_dts.push_back(dt);
+        double* const fxp = has_fx ? h->sl_fx : nullptr; // the buffers swap every step
+        // main.cpp:427-479
+        if ((rc = hcl_hydro_reconstruction(h, 1, dt / 2, h->sl_rho, h->sl_u, h->sl_P, fxp, h->sl_rho_rec,
+                                           h->sl_rhou_rec, h->sl_E_rec, fxp ? h->sl_fx_rec : nullptr, nullptr,
+                                           nullptr, s)) ||
+            (rc = hcl_godunov_scheme(h, 0, dt, h->sl_rho, h->sl_rhou, h->sl_E, fxp, h->sl_rho_rec, h->sl_rhou_rec,
+                                     h->sl_E_rec, fxp ? h->sl_fx_rec : nullptr, h->sl_rho_new, h->sl_rhou_new,
+                                     h->sl_E_new, fxp ? h->sl_fx_new : nullptr, s))) {
+            return rc;
+        }
+        if (pf && (rc = hcl_pressure_fix(h, dt, h->cfg.eps_pf, h->sl_rho, h->sl_rhou, h->sl_E, h->sl_rho_rec,
+                                         h->sl_rhou_rec, h->sl_E_rec, h->sl_rho_new, h->sl_rhou_new, h->sl_E_new,
+                                         s))) {
+            return rc;
+        }
+        if ((rc = hcl_boundary_conditions(h, h->sl_rho_new, h->sl_rhou_new, h->sl_E_new,
+                                          fxp ? h->sl_fx_new : nullptr, s))) {
+            return rc;
+        }
+        // main.cpp:481-484: the new state becomes the current one
+        std::swap(h->sl_rho, h->sl_rho_new);
+        std::swap(h->sl_rhou, h->sl_rhou_new);
+        std::swap(h->sl_E, h->sl_E_new);
+        std::swap(h->sl_fx, h->sl_fx_new);
+        if ((rc = hcl_conv_cons_to_prim(h, ng, h->sl_rho, h->sl_rhou, h->sl_E, h->sl_u, h->sl_P, s))) {
+            return rc;
+        }
+        h->sl_t += dt; // main.cpp:530-531
+        ++h->sl_iter;
+        ++done;
+        last_dt = dt;
+        if (should_exit) {
+            finished = true;
+            break;
+        }
+    }
+    HCL_CUDA(cudaStreamSynchronize(s));
+    HCL_LAUNCH_CHECK();
+    if (r) {
+        r->t = h->sl_t;
+        r->iter = h->sl_iter;
+        r->status = status;
+        r->bad_cell = -1;
+        r->finished = finished ? 1 : 0;
+        r->last_dt = last_dt;
+    }
+    if (status == HCL_ERR_INVALID_STATE) {
+        h->sl_status = status;
+        return fail(HCL_ERR_INVALID_STATE, "detected invalid volumic internal energy");
+    }
+    if (status == HCL_ERR_NEGATIVE_DT) {
+        h->sl_status = status;
+        return fail(HCL_ERR_NEGATIVE_DT, "Error: the time step is negative");
+    }
+    return HCL_OK;
 }
 
 int hcl_run(hcl_handle* h, const hcl_run_params* p, hcl_run_result* r)
@@ -1063,6 +1318,9 @@ int hcl_run(hcl_handle* h, const hcl_run_params* p, hcl_run_result* r)
     }
     if (!h->state_valid) {
         return fail(HCL_ERR_CONFIG, "no state set");
+    }
+    if (stage_mode(h)) {
+        return run_stage_loop(h, p, r);
     }
     int rc;
     StepCtl ctl;
@@ -1190,6 +1448,9 @@ int hcl_run(hcl_handle* h, const hcl_run_params* p, hcl_run_result* r)
 int hcl_step_fixed_dt(hcl_handle* h, double dt, void* stream)
 {
     HCL_CHECK_HANDLE(h);
+    if (stage_mode(h)) {
+        return fail(HCL_ERR_CONFIG, "hcl_step_fixed_dt runs the fused step (no passive scalars, no pressure fix)");
+    }
     if (!h->state_valid) {
         return fail(HCL_ERR_CONFIG, "no state set");
     }
@@ -1243,6 +1504,16 @@ int hcl_set_schedule(hcl_handle* h, int schedule, int* used)
 int hcl_get_dt_log(hcl_handle* h, double* dts, int max_count, int* count)
 {
     HCL_CHECK_HANDLE(h);
+    if (stage_mode(h)) {
+        const int n = std::min(max_count, (int)h->sl_dts.size());
+        if (n > 0 && dts) {
+            std::memcpy(dts, h->sl_dts.data(), sizeof(double) * n);
+        }
+        if (count) {
+            *count = n;
+        }
+        return HCL_OK;
+    }
     StepCtl ctl;
     int rc = read_ctl(h, &ctl);
     if (rc) {
@@ -1267,6 +1538,17 @@ int hcl_conservation_sums(hcl_handle* h, double* out)
     if (!h->state_valid) {
         return fail(HCL_ERR_CONFIG, "no state set");
     }
+    if (stage_mode(h)) {
+        const int nd = h->g.ndim;
+        int rc = hcl_integrate(h, h->sl_rho, &out[0], h->stream);
+        for (int d = 0; d < nd && rc == HCL_OK; ++d) {
+            rc = hcl_integrate(h, h->sl_rhou + h->g.N * d, &out[1 + d], h->stream);
+        }
+        if (rc == HCL_OK) {
+            rc = hcl_integrate(h, h->sl_E, &out[1 + nd], h->stream);
+        }
+        return rc;
+    }
     hcl::fused::conservation_sums(h->g, h->st[h->cur], h->red_partials, h->red_out, h->stream);
     HCL_LAUNCH_CHECK();
     HCL_CUDA(cudaMemcpyAsync(out, h->red_out, sizeof(double) * (h->g.ndim + 2), cudaMemcpyDeviceToHost, h->stream));
@@ -1286,8 +1568,9 @@ int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p)
     }
     const GridDev& g = h->g;
     if (g.geom != HCL_GEOM_CARTESIAN || !g.uniform_cart || g.gravity != HCL_GRAVITY_UNIFORM ||
-        g.riemann == HCL_RIEMANN_LOW_MACH || g.nfx > 0) {
-        return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian uniform grids, uniform gravity, HLL/HLLC, nfx = 0");
+        g.riemann == HCL_RIEMANN_LOW_MACH || g.nfx > 0 || h->cfg.pressure_fix) {
+        return fail(HCL_ERR_CONFIG,
+                    "the adjoint supports Cartesian uniform grids, uniform gravity, HLL/HLLC, nfx = 0, no pressure fix");
     }
     int rc;
     StepCtl ctl;
@@ -1722,7 +2005,7 @@ int hcl_ensemble_create(const hcl_config* cfgs, int nprob, hcl_ensemble** out)
     for (int p = 0; p < nprob; ++p) {
         const hcl_config& c = cfgs[p];
         if (c.ndim != 2 || c.precision != HCL_FP32_MIXED || c.geometry != HCL_GEOM_CARTESIAN ||
-            c.gravity != HCL_GRAVITY_UNIFORM || c.nfx != 0 || c.limiter != cfgs[0].limiter ||
+            c.gravity != HCL_GRAVITY_UNIFORM || c.nfx != 0 || c.pressure_fix != 0 || c.limiter != cfgs[0].limiter ||
             c.riemann != cfgs[0].riemann) {
             return bail(fail(HCL_ERR_CONFIG, "ensemble problem %d: needs 2-D Cartesian FP32-mixed, uniform gravity, "
                                              "and the limiter and Riemann solver of problem 0", p));

@@ -459,6 +459,113 @@ __global__ void k_godunov(GridDev g, Box bx, double dt, const double* __restrict
     }
 }
 
+// pressure_fix.hpp:19-172: where the old internal energy is below eps times
+// the kinetic energy, E_new is rebuilt from a blend of the Godunov increment
+// and a pressure-work estimate from the face velocities (the reference's loop
+// order, including the overwrite of E_new inside the inner loop)
+template <int ND>
+__global__ void k_pressure_fix(GridDev g, Box bx, double dt, double eps, const double* __restrict__ rho,
+                               const double* __restrict__ rhou, const double* __restrict__ E,
+                               const double* __restrict__ rho_rec, const double* __restrict__ rhou_rec,
+                               const double* __restrict__ E_rec, const double* __restrict__ rho_new,
+                               const double* __restrict__ rhou_new, double* __restrict__ E_new)
+{
+    const exact::Eos eos{g.gamma, g.gamma_m1, g.mmw};
+    const int64_t N = g.N;
+    const int64_t S5 = 2 * N;
+    const int64_t S6 = 2 * N * ND;
+    const double eps2 = eps / 10;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < bx.count;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        box_ijk(bx, idx, i, j, k);
+        const int64_t c = lidx(g, i, j, k);
+        double cons[ND + 2], cons_new[ND + 2], prim[ND + 2];
+        cons[0] = rho[c];
+        cons_new[0] = rho_new[c];
+#pragma unroll
+        for (int r = 0; r < ND; ++r) {
+            cons[1 + r] = rhou[c + N * r];
+            cons_new[1 + r] = rhou_new[c + N * r];
+        }
+        cons[1 + ND] = E[c];
+        cons_new[1 + ND] = E_new[c];
+        exact::to_prim<ND>(eos, cons, prim);
+        const double ekin = exact::ek_cons<ND>(cons);
+        const double evol = E[c] - ekin;
+        const double evol_new = E_new[c] - exact::ek_cons<ND>(cons_new);
+        const double de_god = evol_new - evol;
+        if (!(evol < eps * ekin)) {
+            continue;
+        }
+        double En = E[c];
+        double divU = 0;
+        double divUE = 0;
+        double einL = 0;
+        double einR = 0;
+        double alpha = (evol * evol) / (ekin * ekin * eps * eps);
+        if (evol < eps2 * ekin) {
+            alpha = 0;
+        }
+        for (int idim = 0; idim < ND; ++idim) {
+            const int64_t cm = lidx(g, i - (idim == 0), j - (idim == 1), k - (idim == 2));
+            const int64_t cp = lidx(g, i + (idim == 0), j + (idim == 1), k + (idim == 2));
+            for (int ipos = 0; ipos < ND; ++ipos) {
+                double vL[ND + 2], vR[ND + 2], mR[ND + 2], pL[ND + 2], cons_p[ND + 2], cons_m[ND + 2];
+                double primL[ND + 2], primR[ND + 2], prim_mR[ND + 2], prim_pL[ND + 2];
+                vL[0] = rho_rec[c + S5 * idim];
+                vR[0] = rho_rec[c + N + S5 * idim];
+                mR[0] = rho_rec[cm + N + S5 * idim];
+                pL[0] = rho_rec[cp + S5 * idim];
+                cons_p[0] = rho[cp];
+                cons_m[0] = rho[cm];
+#pragma unroll
+                for (int r = 0; r < ND; ++r) {
+                    vL[1 + r] = rhou_rec[c + S5 * idim + S6 * r];
+                    vR[1 + r] = rhou_rec[c + N + S5 * idim + S6 * r];
+                    mR[1 + r] = rhou_rec[cm + N + S5 * idim + S6 * r];
+                    pL[1 + r] = rhou_rec[cp + S5 * idim + S6 * r];
+                    cons_p[1 + r] = rhou[cp + N * r];
+                    cons_m[1 + r] = rhou[cm + N * r];
+                }
+                vL[1 + ND] = E_rec[c + S5 * idim];
+                vR[1 + ND] = E_rec[c + N + S5 * idim];
+                mR[1 + ND] = E_rec[cm + N + S5 * idim];
+                pL[1 + ND] = E_rec[cp + S5 * idim];
+                cons_p[1 + ND] = E[cp];
+                cons_m[1 + ND] = E[cm];
+                exact::to_prim<ND>(eos, vL, primL);
+                exact::to_prim<ND>(eos, vR, primR);
+                exact::to_prim<ND>(eos, mR, prim_mR);
+                exact::to_prim<ND>(eos, pL, prim_pL);
+                const double us = (prim_mR[1 + ipos] + primL[1 + ipos]) / 2;
+                const double us_p = (primR[1 + ipos] + prim_pL[1 + ipos]) / 2;
+                divU += ((us_p * g.ds[cp + N * ipos]) - (us * g.ds[c + N * ipos])) / g.dv[c];
+                if (us_p > 0) {
+                    einR = E[c] - exact::ek_cons<ND>(cons);
+                } else {
+                    einR = E[cp] - exact::ek_cons<ND>(cons_p);
+                }
+                if (us < 0) {
+                    einL = E[c] - exact::ek_cons<ND>(cons);
+                } else {
+                    einL = E[cm] - exact::ek_cons<ND>(cons_m);
+                }
+                divUE += ((us_p * einR * g.ds[cp + N * ipos]) - (us * einL * g.ds[c + N * ipos])) / g.dv[c];
+                const double de_pf = dt * ((-prim[1 + ND] * divU) - divUE);
+                double sum = 0;
+#pragma unroll
+                for (int idr = 0; idr < ND; ++idr) {
+                    sum += cons[1 + idr] * cons[1 + idr] / cons[0];
+                }
+                const double de_tot = (alpha * de_god) + ((1 - alpha) * de_pf);
+                En = evol + de_tot + (1. / 2 * sum);
+            }
+        }
+        E_new[c] = En;
+    }
+}
+
 // godunov_scheme.hpp:294-301 "passive_scalar_Godunov"
 __global__ void k_passive_godunov(GridDev g, Box bx, const double* __restrict__ rho_new, double* __restrict__ fx_new)
 {
@@ -763,6 +870,19 @@ void godunov(const GridDev& g, int ng_eff, double dt, const double* rho, const d
         k_passive_godunov<<<grid_for(bx.count), kThreads, 0, s>>>(g, bx, rho_new, fx_new);
         ++g_launches;
     }
+}
+
+void pressure_fix(const GridDev& g, double dt, double eps, const double* rho, const double* rhou, const double* E,
+                  const double* rho_rec, const double* rhou_rec, const double* E_rec, const double* rho_new,
+                  const double* rhou_new, double* E_new, cudaStream_t s)
+{
+    const Box bx = make_box(g, 0);
+    dispatch_nd(g.ndim, [&](auto ndc) {
+        constexpr int ND = decltype(ndc)::value;
+        k_pressure_fix<ND><<<grid_for(bx.count), kThreads, 0, s>>>(g, bx, dt, eps, rho, rhou, E, rho_rec, rhou_rec,
+                                                                   E_rec, rho_new, rhou_new, E_new);
+    });
+    ++g_launches;
 }
 
 void boundaries(const GridDev& g, double* rho, double* rhou, double* E, double* fx, cudaStream_t s)

@@ -30,6 +30,10 @@ void godunov(const GridDev& g, int ng_eff, double dt, const double* rho, const d
              const double* fx_rec, double* rho_new, double* rhou_new, double* E_new, double* fx_new,
              cudaStream_t s);
 void boundaries(const GridDev& g, double* rho, double* rhou, double* E, double* fx, cudaStream_t s);
+// pressure_fix.hpp:19-172 on no_ghosts: updates E_new in place
+void pressure_fix(const GridDev& g, double dt, double eps, const double* rho, const double* rhou, const double* E,
+                  const double* rho_rec, const double* rhou_rec, const double* E_rec, const double* rho_new,
+                  const double* rhou_new, double* E_new, cudaStream_t s);
 // writes the bits of max_cells(sum_d (|u_d|+c)/dx_d) into *inv_bits (device),
 // which must hold 0 before the call
 void time_step_inv(const GridDev& g, int ng_eff, const double* rho, const double* u, const double* P,

@@ -164,6 +164,8 @@ hcl_config make_config(INIReader const& reader, Param const& param, int ndim, in
     c.xmax[2] = param.x2max;
     c.precision = precision;
     c.device = device;
+    c.pressure_fix = param.pressure_fix == "On" ? 1 : 0; // main.cpp:459
+    c.eps_pf = param.eps_pf;
     if (param.grid_type != "Regular") {
         throw std::runtime_error("Unknown grid type: " + param.grid_type + " (UserDefined grids go through hcl_config::nodes).");
     }

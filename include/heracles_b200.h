@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define HCL_ABI_VERSION 1
+#define HCL_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 enum hcl_status {
@@ -97,6 +97,8 @@ typedef struct hcl_config {
                                  UserDefined grid; NULL selects Regular (grid_type.cpp:151-186) */
     int precision;            /* enum hcl_precision, fused path */
     int device;               /* CUDA device ordinal */
+    int pressure_fix;         /* [Pressure fix] pressure_fix == "On" (main.cpp:459-474) */
+    double eps_pf;            /* [Pressure fix] eps_pf */
 } hcl_config;
 
 typedef struct hcl_handle hcl_handle;
@@ -165,6 +167,13 @@ int hcl_hydro_reconstruction(hcl_handle* h, int ng_eff, double dt, const double*
 int hcl_hydro_reconstruction_noalloc(hcl_handle* h, int ng_eff, double dt, const double* rho, const double* u,
                                      const double* P, const double* fx, double* rho_rec, double* rhou_rec,
                                      double* E_rec, double* fx_rec, void* stream);
+/* pressure_fix (hydro/pressure_fix.hpp:19-172, called at main.cpp:459-474) on
+ * no_ghosts: where the old internal energy is below eps times the kinetic
+ * energy, E_new is rebuilt from a blend of the Godunov increment and a
+ * pressure-work estimate.  Updates E_new in place; FP64, reference order. */
+int hcl_pressure_fix(hcl_handle* h, double dt, double eps, const double* rho, const double* rhou, const double* E,
+                     const double* rho_rec, const double* rhou_rec, const double* E_rec, const double* rho_new,
+                     const double* rhou_new, double* E_new, void* stream);
 /* IGodunovScheme::execute (hydro/godunov_scheme.hpp:47-63,77-302) with the
  * Riemann solver chosen at hcl_create (factory_godunov_scheme, :305-321). */
 int hcl_godunov_scheme(hcl_handle* h, int ng_eff, double dt, const double* rho, const double* rhou,
@@ -226,7 +235,11 @@ typedef struct hcl_run_result {
 /* Runs the reference time loop (main.cpp:354-531) with the fused step kernel,
  * everything on the device: CFL dt reduced inside the step kernel, dt clamps,
  * health check and ghost filling in place; steps are replayed from CUDA graphs.
- * Synchronises at the end (and between graph chunks when nsteps <= 0). */
+ * Synchronises at the end (and between graph chunks when nsteps <= 0).
+ * Handles with passive scalars (nfx > 0) or pressure_fix run the same loop
+ * composed of the FP64 stage entry points (reconstruction, Godunov, pressure
+ * fix, boundaries, cons->prim) in the reference's order, with dt and the
+ * health check read back each step; the state then includes fx. */
 int hcl_run(hcl_handle* h, const hcl_run_params* p, hcl_run_result* r);
 /* One step of the fused kernel with the given dt (no CFL clamp logic, no
  * synchronisation): the building block the adapters use. */

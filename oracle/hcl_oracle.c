@@ -1017,6 +1017,114 @@ static void copy_cell(const or_ctx* c, double* rho, double* rhou, double* E, dou
     }
 }
 
+/* pressure_fix.hpp:19-172 on the no_ghosts range (main.cpp:459-474): where the
+ * old internal energy is below eps times the kinetic energy, E_new is rebuilt
+ * from a blend of the Godunov increment and a pressure-work estimate from the
+ * face velocities.  The loops and the overwrite of E_new inside the inner loop
+ * follow the reference. */
+void or_pressure_fix(const or_ctx* c, double dt, double eps, const double* rho, const double* rhou, const double* E,
+                     const double* rho_rec, const double* rhou_rec, const double* E_rec, const double* rho_new,
+                     const double* rhou_new, double* E_new)
+{
+    int b[3], e[3];
+    cell_range(c, 0, b, e);
+    const long N = or_ncells(c);
+    const int nd = c->ndim;
+    const long S5 = 2 * N;
+    const long S6r = 2 * N * nd;
+    const double* ds = c->ds;
+    const double* dv = c->dv;
+    const double eps2 = eps / 10;
+
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = b[2]; k < e[2]; ++k) {
+        for (int j = b[1]; j < e[1]; ++j) {
+            for (int i = b[0]; i < e[0]; ++i) {
+                const long id = IDX(c, i, j, k);
+                double cons[MAXV], cons_new[MAXV], prim[MAXV];
+                cons[0] = rho[id];
+                cons_new[0] = rho_new[id];
+                for (int r = 0; r < nd; ++r) {
+                    cons[1 + r] = rhou[id + N * r];
+                    cons_new[1 + r] = rhou_new[id + N * r];
+                }
+                cons[1 + nd] = E[id];
+                cons_new[1 + nd] = E_new[id];
+                or_to_prim(c, cons, prim);
+                const double ekin = or_ek_cons(c, cons);
+                const double evol = E[id] - ekin;
+                const double evol_new = E_new[id] - or_ek_cons(c, cons_new);
+                const double de_god = evol_new - evol;
+                if (evol < eps * ekin) {
+                    E_new[id] = E[id];
+                    double divU = 0;
+                    double divUE = 0;
+                    double einL = 0;
+                    double einR = 0;
+                    double alpha = (evol * evol) / (ekin * ekin * eps * eps);
+                    if (evol < eps2 * ekin) {
+                        alpha = 0;
+                    }
+                    for (int idim = 0; idim < nd; ++idim) {
+                        const long idm = IDX(c, i - (idim == 0), j - (idim == 1), k - (idim == 2));
+                        const long idp = IDX(c, i + (idim == 0), j + (idim == 1), k + (idim == 2));
+                        for (int ipos = 0; ipos < nd; ++ipos) {
+                            double vL[MAXV], vR[MAXV], mR[MAXV], pL[MAXV];
+                            double primL[MAXV], primR[MAXV], prim_mR[MAXV], prim_pL[MAXV];
+                            double cons_p[MAXV], cons_m[MAXV];
+                            vL[0] = rho_rec[id + S5 * idim];
+                            vR[0] = rho_rec[id + N + S5 * idim];
+                            mR[0] = rho_rec[idm + N + S5 * idim];
+                            pL[0] = rho_rec[idp + S5 * idim];
+                            cons_p[0] = rho[idp];
+                            cons_m[0] = rho[idm];
+                            for (int r = 0; r < nd; ++r) {
+                                vL[1 + r] = rhou_rec[id + S5 * idim + S6r * r];
+                                vR[1 + r] = rhou_rec[id + N + S5 * idim + S6r * r];
+                                mR[1 + r] = rhou_rec[idm + N + S5 * idim + S6r * r];
+                                pL[1 + r] = rhou_rec[idp + S5 * idim + S6r * r];
+                                cons_p[1 + r] = rhou[idp + N * r];
+                                cons_m[1 + r] = rhou[idm + N * r];
+                            }
+                            vL[1 + nd] = E_rec[id + S5 * idim];
+                            vR[1 + nd] = E_rec[id + N + S5 * idim];
+                            mR[1 + nd] = E_rec[idm + N + S5 * idim];
+                            pL[1 + nd] = E_rec[idp + S5 * idim];
+                            cons_p[1 + nd] = E[idp];
+                            cons_m[1 + nd] = E[idm];
+                            or_to_prim(c, vL, primL);
+                            or_to_prim(c, vR, primR);
+                            or_to_prim(c, mR, prim_mR);
+                            or_to_prim(c, pL, prim_pL);
+                            const double us = (prim_mR[1 + ipos] + primL[1 + ipos]) / 2;
+                            const double us_p = (primR[1 + ipos] + prim_pL[1 + ipos]) / 2;
+                            divU += ((us_p * ds[idp + N * ipos]) - (us * ds[id + N * ipos])) / dv[id];
+                            if (us_p > 0) {
+                                einR = E[id] - or_ek_cons(c, cons);
+                            } else {
+                                einR = E[idp] - or_ek_cons(c, cons_p);
+                            }
+                            if (us < 0) {
+                                einL = E[id] - or_ek_cons(c, cons);
+                            } else {
+                                einL = E[idm] - or_ek_cons(c, cons_m);
+                            }
+                            divUE += ((us_p * einR * ds[idp + N * ipos]) - (us * einL * ds[id + N * ipos])) / dv[id];
+                            const double de_pf = dt * ((-prim[1 + nd] * divU) - divUE);
+                            double sum = 0;
+                            for (int idr = 0; idr < nd; ++idr) {
+                                sum += cons[1 + idr] * cons[1 + idr] / cons[0];
+                            }
+                            const double de_tot = (alpha * de_god) + ((1 - alpha) * de_pf);
+                            E_new[id] = evol + de_tot + (1. / 2 * sum);
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
 void or_boundaries(const or_ctx* c, double* rho, double* rhou, double* E, double* fx)
 {
     const long N = or_ncells(c);
@@ -1266,6 +1374,9 @@ int or_run(const or_ctx* c, double* rho, double* rhou, double* E, double* fx, co
         }
         or_hydro_reconstruction(c, 1, dt / 2, rho, u, P, fx, rho_rec, rhou_rec, E_rec, fx_rec, u_rec, P_rec);
         or_godunov(c, 0, dt, rho, rhou, E, fx, rho_rec, rhou_rec, E_rec, fx_rec, rho_new, rhou_new, E_new, fx_new);
+        if (p->pressure_fix) { /* :459-474 */
+            or_pressure_fix(c, dt, p->eps_pf, rho, rhou, E, rho_rec, rhou_rec, E_rec, rho_new, rhou_new, E_new);
+        }
         or_boundaries(c, rho_new, rhou_new, E_new, fx_new); /* :479 */
         memcpy(rho, rho_new, sizeof(double) * (size_t)N);   /* :481-484 */
         memcpy(rhou, rhou_new, sizeof(double) * (size_t)N * nd);

@@ -123,6 +123,8 @@ typedef struct or_run_params {
     double time_first_output;  /* [Output] time_first_output */
     int fixed_dt;              /* 1: use dts[] instead of the CFL dt (adjoint checks) */
     const double* dts;
+    int pressure_fix;          /* [Pressure fix] pressure_fix == "On" (main.cpp:459) */
+    double eps_pf;             /* [Pressure fix] eps_pf */
 } or_run_params;
 
 typedef struct or_run_result {
@@ -136,6 +138,11 @@ typedef struct or_run_result {
  * (ghost cells included).  If dts_out is non-NULL, the dt of each step is stored. */
 int or_run(const or_ctx* c, double* rho, double* rhou, double* E, double* fx, const or_run_params* p,
            or_run_result* r, double* dts_out);
+
+/* pressure_fix.hpp:19-172 on no_ghosts; updates E_new in place. */
+void or_pressure_fix(const or_ctx* c, double dt, double eps, const double* rho, const double* rhou, const double* E,
+                     const double* rho_rec, const double* rhou_rec, const double* E_rec, const double* rho_new,
+                     const double* rhou_new, double* E_new);
 
 /* Initial state helper: given primitives on the interior, computes the
  * conserved state and fills the ghosts (main.cpp:305-307). */

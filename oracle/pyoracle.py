@@ -64,6 +64,8 @@ class _RunParams(C.Structure):
         ("time_first_output", C.c_double),
         ("fixed_dt", C.c_int),
         ("dts", _dp),
+        ("pressure_fix", C.c_int),
+        ("eps_pf", C.c_double),
     ]
 
 
@@ -133,6 +135,7 @@ def _lib():
         lib.or_hydro_reconstruction.argtypes = [C.POINTER(_Ctx), C.c_int, C.c_double] + [vp] * 10
         lib.or_godunov.argtypes = [C.POINTER(_Ctx), C.c_int, C.c_double] + [vp] * 12
         lib.or_boundaries.argtypes = [C.POINTER(_Ctx), vp, vp, vp, vp]
+        lib.or_pressure_fix.argtypes = [C.POINTER(_Ctx), C.c_double, C.c_double] + [vp] * 9
         lib.or_time_step.argtypes = [C.POINTER(_Ctx), C.c_int, vp, vp, vp]
         lib.or_time_step.restype = C.c_double
         lib.or_min_internal_energy.argtypes = [C.POINTER(_Ctx), vp, vp, vp]
@@ -315,6 +318,12 @@ class Oracle:
                             _p(rhou_rec), _p(E_rec), _p(fx_rec), _p(rho_new), _p(rhou_new), _p(E_new), _p(fx_new))
         return rho_new, rhou_new, E_new, fx_new
 
+    def pressure_fix(self, dt, eps, rho, rhou, E, rho_rec, rhou_rec, E_rec, rho_new, rhou_new, E_new):
+        """Updates E_new in place (pressure_fix.hpp:19-172)."""
+        self.lib.or_pressure_fix(C.byref(self.ctx), dt, eps, _p(rho), _p(rhou), _p(E), _p(rho_rec), _p(rhou_rec),
+                                 _p(E_rec), _p(rho_new), _p(rhou_new), _p(E_new))
+        return E_new
+
     def boundaries(self, rho, rhou, E, fx=None):
         if fx is None:
             fx = self.zeros(max(self.nfx, 1))
@@ -339,7 +348,8 @@ class Oracle:
         return rho, rhou, E, fx
 
     def run(self, rho, rhou, E, fx=None, *, cfl=0.4, t_ini=0.0, t_end=1e30, max_iter=10000, iter_frequency=0,
-            time_frequency=0.0, time_first_output=None, dts=None, record_dts=False):
+            time_frequency=0.0, time_first_output=None, dts=None, record_dts=False, pressure_fix=False,
+            eps_pf=1e-6):
         """Runs main.cpp's time loop in place.  Returns (t, iter, status, dts)."""
         if fx is None:
             fx = self.zeros(max(self.nfx, 1))
@@ -351,6 +361,8 @@ class Oracle:
         p.iter_frequency = iter_frequency
         p.time_frequency = time_frequency
         p.time_first_output = t_ini + time_frequency if time_first_output is None else time_first_output
+        p.pressure_fix = 1 if pressure_fix else 0
+        p.eps_pf = eps_pf
         if dts is not None:
             dts_arr = np.ascontiguousarray(dts, dtype=np.float64)
             p.fixed_dt = 1
