@@ -99,3 +99,28 @@ def test_driver_rejects_unknown_keys(tmp_path):
     ini.write_text(SOD_INI.replace("gamma = 1.4", "gamma = 1.0"))
     res = subprocess.run([str(DRIVER), str(ini)], capture_output=True, text=True, timeout=60)
     assert res.returncode != 0 and "Invalid gamma" in res.stderr
+
+
+def test_driver_runs_stage_loop_for_passive_scalars_and_pressure_fix(tmp_path):
+    """[Passive Scalar] nfx and [Pressure fix] On select the stage-composed
+    loop; the driver's result equals the oracle's main loop bit for bit."""
+    ini = tmp_path / "sod_pf.ini"
+    ini.write_text(SOD_INI + "\n[Passive Scalar]\nnfx = 1\n\n[Pressure fix]\npressure_fix = On\neps_pf = 4\n")
+    dump = tmp_path / "out.bin"
+    res = subprocess.run([str(DRIVER), str(ini), "--setup=shock_tube", f"--output={dump}"], capture_output=True,
+                         text=True, timeout=300)
+    assert res.returncode == 0, res.stderr
+    nd, t, rho, rhou, E = read_dump(dump)
+    o = Oracle(1, [1024], nfx=1, gamma=1.4, limiter="Minmod", riemann="HLLC", bc=["NullGradient"] * 2)
+    prim = setups.shock_tube(setups.Grid.from_domain(o))
+    r, m, e, fx = o.init_from_prim(*prim)
+    r2, m2, e2, fx2 = (a.copy() for a in (r, m, e, fx))
+    t_o, it_o, st_o, _ = o.run(r, m, e, fx, cfl=0.4, t_end=0.2, max_iter=100000, time_frequency=0.1,
+                               pressure_fix=True, eps_pf=4.0)
+    assert st_o == 0 and t == t_o == 0.2
+    assert f"number of iterations = {it_o}" in res.stdout
+    assert np.array_equal(rho, r) and np.array_equal(rhou, m) and np.array_equal(E, e)
+    # the fix acts on this flow (eps_pf = 4: the post-shock and rarefaction
+    # cells have internal energy below 4x their kinetic energy)
+    o.run(r2, m2, e2, fx2, cfl=0.4, t_end=0.2, max_iter=100000, time_frequency=0.1)
+    assert not np.array_equal(e2, e)
