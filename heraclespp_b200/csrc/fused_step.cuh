@@ -189,6 +189,127 @@ __device__ __forceinline__ int ghost_images(int l, int n, int ng, int bcl, int b
     return cnt;
 }
 
+// The same images as a mask over the 2*ng ghost slots of a dimension (slot
+// k < ng: cell k; slot k >= ng: cell n - 2ng + k): bit k is set when slot k
+// takes its value from cell l, bit 16 + k when that image has its normal
+// momentum negated (Nghost <= 4, so 2*ng <= 8 slots).
+__device__ __forceinline__ unsigned ghost_mask(int l, int n, int ng, int bcl, int bcr)
+{
+    if (l >= 2 * ng && l < n - 2 * ng) {
+        return 0u;
+    }
+    unsigned m = 0u;
+    for (int k = 0; k < 2 * ng; ++k) {
+        const int p = k < ng ? k : n - 2 * ng + k;
+        int f;
+        if (bc_source(p, n, ng, bcl, bcr, &f) == l) {
+            m |= (1u << k) | ((unsigned)f << (16 + k));
+        }
+    }
+    return m;
+}
+
+__device__ __forceinline__ int ghost_slot(int k, int n, int ng)
+{
+    return k < ng ? k : n - 2 * ng + k;
+}
+
+// Writes a 2-D cell's new state to its ghost images: every (x image or the
+// cell's own column) x (y image or its own row) pair except the cell itself.
+// xm, ym: ghost_mask of the column and the row.
+__device__ __forceinline__ void store_images_2d(double* __restrict__ q, int64_t plane, int pitch, int n0, int n1,
+                                                int ng, int col, int r, unsigned xm, unsigned ym, const double qn[4])
+{
+    unsigned yb = ym & 0xffffu;
+    int py = r, fy = 0;
+    bool self_y = true;
+    for (;;) {
+        unsigned xb = xm & 0xffffu;
+        int px = col, fx = 0;
+        bool self_x = true;
+        for (;;) {
+            if (!(self_x && self_y)) {
+                const int64_t og = (int64_t)py * pitch + px;
+                q[og] = qn[0];
+                q[og + plane] = fx ? -qn[1] : qn[1];
+                q[og + 2 * plane] = fy ? -qn[2] : qn[2];
+                q[og + 3 * plane] = qn[3];
+            }
+            if (xb == 0u) {
+                break;
+            }
+            const int k = __ffs(xb) - 1;
+            xb &= xb - 1u;
+            px = ghost_slot(k, n0, ng);
+            fx = (xm >> (16 + k)) & 1u;
+            self_x = false;
+        }
+        if (yb == 0u) {
+            break;
+        }
+        const int k = __ffs(yb) - 1;
+        yb &= yb - 1u;
+        py = ghost_slot(k, n1, ng);
+        fy = (ym >> (16 + k)) & 1u;
+        self_y = false;
+    }
+}
+
+// 3-D form: every (x image or own column) x (y image or own row) x (z image
+// or own plane) triple except the cell itself.
+__device__ __forceinline__ void store_images_3d(double* __restrict__ q, int64_t plane, int pitch, int n0, int n1,
+                                                int n2, int ng, int col, int row, int z, unsigned xm, unsigned ym,
+                                                unsigned zm, const double qn[5])
+{
+    unsigned zb = zm & 0xffffu;
+    int pz = z, fz = 0;
+    bool self_z = true;
+    for (;;) {
+        unsigned yb = ym & 0xffffu;
+        int py = row, fy = 0;
+        bool self_y = true;
+        for (;;) {
+            unsigned xb = xm & 0xffffu;
+            int px = col, fx = 0;
+            bool self_x = true;
+            for (;;) {
+                if (!(self_x && self_y && self_z)) {
+                    const int64_t og = ((int64_t)pz * n1 + py) * pitch + px;
+                    q[og] = qn[0];
+                    q[og + plane] = fx ? -qn[1] : qn[1];
+                    q[og + 2 * plane] = fy ? -qn[2] : qn[2];
+                    q[og + 3 * plane] = fz ? -qn[3] : qn[3];
+                    q[og + 4 * plane] = qn[4];
+                }
+                if (xb == 0u) {
+                    break;
+                }
+                const int k = __ffs(xb) - 1;
+                xb &= xb - 1u;
+                px = ghost_slot(k, n0, ng);
+                fx = (xm >> (16 + k)) & 1u;
+                self_x = false;
+            }
+            if (yb == 0u) {
+                break;
+            }
+            const int k = __ffs(yb) - 1;
+            yb &= yb - 1u;
+            py = ghost_slot(k, n1, ng);
+            fy = (ym >> (16 + k)) & 1u;
+            self_y = false;
+        }
+        if (zb == 0u) {
+            break;
+        }
+        const int k = __ffs(zb) - 1;
+        zb &= zb - 1u;
+        pz = ghost_slot(k, n2, ng);
+        fz = (zm >> (16 + k)) & 1u;
+        self_z = false;
+    }
+}
+
 // ---------------------------------------------------------------------------
 template <int ND, bool EXACT, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1))

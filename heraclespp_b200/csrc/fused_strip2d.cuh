@@ -160,6 +160,7 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     const bool out_lane = lane >= 2 && lane < 2 + kStripLanesOut && col < g.ng + g.nx[0];
     const int r0 = g.ng + L * sy;
     const int r1 = min(r0 + L, g.ng + g.nx[1]);
+    const unsigned xm = out_lane ? ghost_mask(col, n0, g.ng, g.bc[0], g.bc[1]) : 0u;
 
     StripCtx c;
     c.eos = fast::Eos{(float)g.gamma, (float)g.gamma_m1, (float)(1.0 / g.gamma_m1)};
@@ -293,27 +294,9 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             for (int v = 0; v < 4; ++v) {
                 qout[oo + plane * v] = qn[v];
             }
-            // ghost images of border cells (boundary_distribute.hpp:42-76)
-            if (!(col >= 2 * g.ng && col < n0 - 2 * g.ng && r >= 2 * g.ng && r < n1 - 2 * g.ng)) {
-                int px[9], fx[9], py[9], fy[9];
-                px[0] = col;
-                fx[0] = 0;
-                py[0] = r;
-                fy[0] = 0;
-                const int cxn = 1 + ghost_images(col, n0, g.ng, g.bc[0], g.bc[1], &px[1], &fx[1]);
-                const int cyn = 1 + ghost_images(r, n1, g.ng, g.bc[2], g.bc[3], &py[1], &fy[1]);
-                for (int b = 0; b < cyn; ++b) {
-                    for (int a = 0; a < cxn; ++a) {
-                        if (a == 0 && b == 0) {
-                            continue;
-                        }
-                        const int64_t og = (int64_t)py[b] * pitch + px[a];
-                        qout[og] = qn[0];
-                        qout[og + plane] = fx[a] ? -qn[1] : qn[1];
-                        qout[og + 2 * plane] = fy[b] ? -qn[2] : qn[2];
-                        qout[og + 3 * plane] = qn[3];
-                    }
-                }
+            const unsigned ym = (r < 2 * g.ng || r >= n1 - 2 * g.ng) ? ghost_mask(r, n1, g.ng, g.bc[2], g.bc[3]) : 0u;
+            if ((xm | ym) != 0u) {
+                store_images_2d(qout, plane, pitch, n0, n1, g.ng, col, r, xm, ym, qn);
             }
         }
         // slide the window
@@ -368,7 +351,7 @@ __device__ __forceinline__ void publish_decision(StepCtl* ctl, const Decision& d
 }
 
 template <int LIM, int RS>
-__global__ void __launch_bounds__(128, 5)
+__global__ void __launch_bounds__(128, 4)
 k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
 {
     const int lane = threadIdx.x & 31;

@@ -324,25 +324,9 @@ __device__ __forceinline__ void pair_update_cell(const GridDev& g, double* __res
         }
     }
     if (!(col >= 2 * g.ng && col < n0 - 2 * g.ng && r >= 2 * g.ng && r < n1 - 2 * g.ng)) {
-        int px[9], fx[9], py[9], fy[9];
-        px[0] = col;
-        fx[0] = 0;
-        py[0] = r;
-        fy[0] = 0;
-        const int cxn = 1 + ghost_images(col, n0, g.ng, g.bc[0], g.bc[1], &px[1], &fx[1]);
-        const int cyn = 1 + ghost_images(r, n1, g.ng, g.bc[2], g.bc[3], &py[1], &fy[1]);
-        for (int b = 0; b < cyn; ++b) {
-            for (int a = 0; a < cxn; ++a) {
-                if (a == 0 && b == 0) {
-                    continue;
-                }
-                const int64_t og = (int64_t)py[b] * pitch + px[a];
-                qout[og] = qn[0];
-                qout[og + plane] = fx[a] ? -qn[1] : qn[1];
-                qout[og + 2 * plane] = fy[b] ? -qn[2] : qn[2];
-                qout[og + 3 * plane] = qn[3];
-            }
-        }
+        const unsigned xm = ghost_mask(col, n0, g.ng, g.bc[0], g.bc[1]);
+        const unsigned ym = ghost_mask(r, n1, g.ng, g.bc[2], g.bc[3]);
+        store_images_2d(qout, plane, pitch, n0, n1, g.ng, col, r, xm, ym, qn);
     }
 }
 

@@ -169,6 +169,10 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     const int rowc = min(row, n1 - 1);
     const bool out_cell = lane >= 2 && lane < 30 && w >= 2 && w < 14 && col < g.ng + g.nx[0] &&
                           row < g.ng + g.nx[1];
+    // this column's x and y images (ghost_mask), fixed over the march
+    const unsigned xm = out_cell ? ghost_mask(col, n0, g.ng, g.bc[0], g.bc[1]) : 0u;
+    const unsigned ym = out_cell ? ghost_mask(row, n1, g.ng, g.bc[2], g.bc[3]) : 0u;
+    const unsigned xym = xm | ym;
     const int z0 = g.ng + L * bz;
     const int z1 = min(z0 + L, g.ng + g.nx[2]);
     const int64_t pitch = in.pitch;
@@ -322,36 +326,11 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
                 qout[oo + plane * v] = qn[v];
             }
             // ghost images of border cells (boundary_distribute.hpp:42-76)
-            const int idx[3] = {col, row, z};
-            bool border = false;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                border |= !(idx[d] >= 2 * g.ng && idx[d] < g.n[d] - 2 * g.ng);
-            }
-            if (border) {
-                int pos[3][9], flp[3][9], cnt[3];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    pos[d][0] = idx[d];
-                    flp[d][0] = 0;
-                    cnt[d] = 1 + ghost_images(idx[d], g.n[d], g.ng, g.bc[2 * d], g.bc[2 * d + 1], &pos[d][1],
-                                              &flp[d][1]);
-                }
-                for (int a2 = 0; a2 < cnt[2]; ++a2) {
-                    for (int a1 = 0; a1 < cnt[1]; ++a1) {
-                        for (int a0 = 0; a0 < cnt[0]; ++a0) {
-                            if (a0 == 0 && a1 == 0 && a2 == 0) {
-                                continue;
-                            }
-                            const int64_t og = ((int64_t)pos[2][a2] * n1 + pos[1][a1]) * pitch + pos[0][a0];
-                            qout[og] = qn[0];
-                            qout[og + plane] = flp[0][a0] ? -qn[1] : qn[1];
-                            qout[og + 2 * plane] = flp[1][a1] ? -qn[2] : qn[2];
-                            qout[og + 3 * plane] = flp[2][a2] ? -qn[3] : qn[3];
-                            qout[og + 4 * plane] = qn[4];
-                        }
-                    }
-                }
+            const unsigned zm = (z < 2 * g.ng || z >= g.n[2] - 2 * g.ng)
+                                    ? ghost_mask(z, g.n[2], g.ng, g.bc[4], g.bc[5])
+                                    : 0u;
+            if ((xym | zm) != 0u) {
+                store_images_3d(qout, plane, pitch, n0, n1, g.n[2], g.ng, col, row, z, xm, ym, zm, qn);
             }
         }
         // slide the window
