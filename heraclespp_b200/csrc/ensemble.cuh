@@ -61,6 +61,8 @@ k_ensemble(const Prob* __restrict__ probs, const int* __restrict__ item_prob, Pa
     const int lane = threadIdx.x & 31;
     const int warps_total = gridDim.x * (blockDim.x >> 5);
     const int wid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    __shared__ __align__(16) double s_ring[4][fused::kStripRingDoubles];
+    const fused::StripRing ring = reinterpret_cast<fused::StripRing>(s_ring[(threadIdx.x >> 5) & 3]);
     for (int s = 0; s < ep.nsteps; ++s) {
         const int gs = ep.step0 + s;
         // per-problem bookkeeping: t, iteration, dt log, clear the slot two ahead
@@ -91,7 +93,7 @@ k_ensemble(const Prob* __restrict__ probs, const int* __restrict__ item_prob, Pa
             const double* qin = ep.seg_mode ? P.q[0] + (int64_t)s * P.seg_stride : P.q[gs & 1];
             double* qout = ep.seg_mode ? P.q[0] + (int64_t)(s + 1) * P.seg_stride : P.q[(gs + 1) & 1];
             fused::strip_work<LIM, RS>(P.g, qin, qout, P.plane, P.pitch, dt, local % P.ncolw, local / P.ncolw, ep.L,
-                                       inv_max, bad_cell);
+                                       inv_max, bad_cell, ring);
             const bool nan_seen = isnan(inv_max);
             double m = nan_seen ? 0.0 : inv_max;
             m = fused::warp_max_d(m);

@@ -12,12 +12,13 @@ namespace hcl::fused {
 // Schedules selectable at run time for 2-D (the autotuner picks one):
 // 0-2 shared-memory tiles 16x16, 32x8, 32x16; 3-5 warp strips of 32, 64,
 // 128 rows; 6 warp strips whose height fits one wave of resident warps;
-// 7 and 8 paired-column warp strips (fitted height, 32 rows).  3-8 need a
-// uniform Cartesian grid, 7-8 an even ghost width.
+// 7 and 8 paired-column warp strips (fitted height, 32 rows); 9 fitted warp
+// strips in CTAs of 16 warps that march in step.  3-9 need a uniform
+// Cartesian grid, 7-8 an even ghost width.
 // 3-D: 0 shared-memory tiles 8x8x4; 1 column march (uniform Cartesian grids).
 int mixed_shape_count(int ndim)
 {
-    return ndim == 2 ? 9 : (ndim == 3 ? 2 : 1);
+    return ndim == 2 ? 10 : (ndim == 3 ? 2 : 1);
 }
 
 bool mixed_shape_valid(const GridDev& g, int shape)
@@ -28,7 +29,7 @@ bool mixed_shape_valid(const GridDev& g, int shape)
     if (shape < 3) {
         return true;
     }
-    return shape < 7 ? strip2d_eligible(g) : strip2d_pair_eligible(g);
+    return (shape < 7 || shape == 9) ? strip2d_eligible(g) : strip2d_pair_eligible(g);
 }
 
 void configure_mixed()
@@ -48,11 +49,13 @@ void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepC
         FusedLauncher<1, false, 256, 1, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
         break;
     case 2:
-        if (shape >= 7 && strip2d_pair_eligible(g)) {
+        if (shape == 9 && strip2d_eligible(g)) {
+            step_strip2d(g, in, out, ctl, rp, slot, out_buf, 0, true, s);
+        } else if (shape >= 7 && shape < 9 && strip2d_pair_eligible(g)) {
             step_strip2d_pair(g, in, out, ctl, rp, slot, out_buf, shape == 7 ? 0 : 32, s);
         } else if (shape >= 3 && strip2d_eligible(g)) {
             step_strip2d(g, in, out, ctl, rp, slot, out_buf, shape == 3 ? 32 : (shape == 4 ? 64 : (shape == 5 ? 128 : 0)),
-                         s);
+                         false, s);
         } else if (shape == 1) {
             FusedLauncher<2, false, 32, 8, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
         } else if (shape == 2) {

@@ -39,34 +39,59 @@ int resident_blocks()
     return cached;
 }
 
+constexpr int kSyncSmem = kStripSyncWarps * kStripRingDoubles * (int)sizeof(double);
+
+// Resident CTAs of the in-step strip kernel (one per SM), queried once.
+template <int LIM, int RS>
+int resident_blocks_sync()
+{
+    static int cached = 0;
+    if (cached == 0) {
+        int per_sm = 0, nsm = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaFuncSetAttribute(k_strip2d_sync<LIM, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSyncSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip2d_sync<LIM, RS>, 32 * kStripSyncWarps,
+                                                      kSyncSmem);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cached = per_sm > 0 && nsm > 0 ? per_sm * nsm : 148;
+    }
+    return cached;
+}
+
+// sync: CTAs of 16 warps marching in step (k_strip2d_sync); otherwise CTAs
+// of 4 independent warps (k_strip2d).  L <= 0: strips fitted so that one wave
+// of resident warps covers the grid (no warp waits for a second wave).
 template <int LIM, int RS>
 void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp, int slot,
-               int out_buf, int L, cudaStream_t s)
+               int out_buf, int L, bool sync, cudaStream_t s)
 {
     const int ncolw = (g.nx[0] + kStripLanesOut - 1) / kStripLanesOut;
-    const int resident = resident_blocks<LIM, RS>();
+    const int wpb = sync ? kStripSyncWarps : 4;
+    const int resident = sync ? resident_blocks_sync<LIM, RS>() : resident_blocks<LIM, RS>();
     if (L <= 0) {
-        // fitted strips: as many strips per column as one wave of resident
-        // warps holds, so no warp waits for a second wave
-        const int per_col = std::max(1, resident * 4 / ncolw);
+        const int per_col = std::max(1, resident * wpb / ncolw);
         L = std::max(8, (g.nx[1] + per_col - 1) / per_col);
     }
     const int nstrip = (g.nx[1] + L - 1) / L;
     const int warps = ncolw * nstrip;
-    const int blocks = std::min((warps + 3) / 4, resident);
-    k_strip2d<LIM, RS><<<blocks, 128, 0, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
+    const int blocks = std::min((warps + wpb - 1) / wpb, resident);
+    if (sync) {
+        k_strip2d_sync<LIM, RS><<<blocks, 32 * kStripSyncWarps, kSyncSmem, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
+    } else {
+        k_strip2d<LIM, RS><<<blocks, 128, 0, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
+    }
 }
 
 template <int LIM>
 void launch_l(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp, int slot,
-              int out_buf, int L, cudaStream_t s)
+              int out_buf, int L, bool sync, cudaStream_t s)
 {
     if (g.riemann == RS_HLL) {
-        launch_lr<LIM, RS_HLL>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        launch_lr<LIM, RS_HLL>(g, in, out, ctl, rp, slot, out_buf, L, sync, s);
     } else if (g.riemann == RS_HLLC) {
-        launch_lr<LIM, RS_HLLC>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        launch_lr<LIM, RS_HLLC>(g, in, out, ctl, rp, slot, out_buf, L, sync, s);
     } else {
-        launch_lr<LIM, RS_SPLITTING>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        launch_lr<LIM, RS_SPLITTING>(g, in, out, ctl, rp, slot, out_buf, L, sync, s);
     }
 }
 
@@ -136,20 +161,20 @@ void step_strip2d_pair(const GridDev& g, const StateDev& in, const StateDev& out
 }
 
 void step_strip2d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
-                  int slot, int out_buf, int L, cudaStream_t s)
+                  int slot, int out_buf, int L, bool sync, cudaStream_t s)
 {
     switch (g.limiter) {
     case LIM_CONSTANT:
-        launch_l<LIM_CONSTANT>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        launch_l<LIM_CONSTANT>(g, in, out, ctl, rp, slot, out_buf, L, sync, s);
         break;
     case LIM_VANLEER:
-        launch_l<LIM_VANLEER>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        launch_l<LIM_VANLEER>(g, in, out, ctl, rp, slot, out_buf, L, sync, s);
         break;
     case LIM_MINMOD:
-        launch_l<LIM_MINMOD>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        launch_l<LIM_MINMOD>(g, in, out, ctl, rp, slot, out_buf, L, sync, s);
         break;
     default:
-        launch_l<LIM_VANALBADA>(g, in, out, ctl, rp, slot, out_buf, L, s);
+        launch_l<LIM_VANALBADA>(g, in, out, ctl, rp, slot, out_buf, L, sync, s);
         break;
     }
     ++g_launches;

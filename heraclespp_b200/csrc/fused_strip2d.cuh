@@ -145,12 +145,20 @@ __device__ __forceinline__ void strip_riemann(const fast::Eos& e, const float* L
     fast::riemann<2>(e, RS, L, R, l, F);
 }
 
+// Shared-memory row ring of one warp: 8 row slots x 4 variables x 32 lanes.
+using StripRing = double (*)[4][32];
+constexpr int kStripRingDoubles = 8 * 4 * 32;
+
 // One strip (28 columns x rows [r0, r1)) of one domain: reads qin, writes qout.
 // Accumulates the CFL max and the first bad cell of the lanes' output cells.
-template <int LIM, int RS>
+// SYNC > 0: the warp takes part in a CTA barrier after every SYNC rows and
+// after row L - 1 of its strip, L barriers' worth of rows whatever the
+// strip's own height (strip_idle() is the same barrier sequence without a
+// strip), so that all warps of a CTA march in step.
+template <int LIM, int RS, int SYNC = 0>
 __device__ __forceinline__ void strip_work(const GridDev& g, const double* __restrict__ qin, double* __restrict__ qout,
                                            int64_t plane, int pitch, double dt, int sx, int sy, int L, double& inv_max,
-                                           int64_t& bad_cell)
+                                           int64_t& bad_cell, StripRing ring)
 {
     const int lane = threadIdx.x & 31;
     const int n0 = g.n[0], n1 = g.n[1];
@@ -161,6 +169,15 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     const int r0 = g.ng + L * sy;
     const int r1 = min(r0 + L, g.ng + g.nx[1]);
     const unsigned xm = out_lane ? ghost_mask(col, n0, g.ng, g.bc[0], g.bc[1]) : 0u;
+    // A column with at most one x image stores it on every row that has no y
+    // image, as one store in step with the other lanes of the warp (which
+    // store their own cell again): no divergent branch on the common border
+    // rows.  Other cases take store_images_2d.
+    const unsigned xbits = xm & 0xffffu;
+    const bool x_single = __popc(xbits) <= 1;
+    const bool x_any = __any_sync(0xffffffffu, xbits != 0u);
+    const int x_img = xbits ? ghost_slot(__ffs(xbits) - 1, n0, g.ng) : col;
+    const bool x_flip = xbits ? ((xm >> (15 + __ffs(xbits))) & 1u) != 0u : false;
 
     StripCtx c;
     c.eos = fast::Eos{(float)g.gamma, (float)g.gamma_m1, (float)(1.0 / g.gamma_m1)};
@@ -175,11 +192,9 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     const double dgy = dt * g.g[1];
     const double gm1 = g.gamma_m1;
 
-    // The FP64 rows stream through a per-warp ring of 8 row slots in shared
+    // The FP64 rows stream through the warp's ring of 8 row slots in shared
     // memory (one 8-byte cp.async per lane and variable; a lane only reads
     // what it copied, so no barrier is needed).  Rows are issued 4 ahead.
-    __shared__ __align__(16) double s_ring[4][8][4][32];
-    double(*ring)[4][32] = s_ring[(threadIdx.x >> 5) & 3];
     auto stage_row = [&](int r) {
         const int rc = min(max(r, 0), n1 - 1);
         const int64_t o = (int64_t)rc * pitch + colc;
@@ -227,7 +242,16 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         }
     }
     // window: wC = P[r], wD = P[r+1]; ring rows r+3, r+4 in flight
-    for (int r = r0; r < r1; ++r) {
+    for (int i = 0; i < (SYNC > 0 ? L : r1 - r0); ++i) {
+        const int r = r0 + i;
+        if constexpr (SYNC > 0) {
+            if (r >= r1) {
+                if (i % SYNC == SYNC - 1 || i == L - 1) {
+                    __syncthreads();
+                }
+                continue;
+            }
+        }
         double q[4];
         float wN[4];
         stage_row(r + 4);
@@ -295,8 +319,16 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
                 qout[oo + plane * v] = qn[v];
             }
             const unsigned ym = (r < 2 * g.ng || r >= n1 - 2 * g.ng) ? ghost_mask(r, n1, g.ng, g.bc[2], g.bc[3]) : 0u;
-            if ((xm | ym) != 0u) {
-                store_images_2d(qout, plane, pitch, n0, n1, g.ng, col, r, xm, ym, qn);
+            if (ym != 0u || !x_single) {
+                if ((xm | ym) != 0u) {
+                    store_images_2d(qout, plane, pitch, n0, n1, g.ng, col, r, xm, ym, qn);
+                }
+            } else if (x_any) {
+                const int64_t og = (int64_t)r * pitch + x_img;
+                qout[og] = qn[0];
+                qout[og + plane] = x_flip ? -qn[1] : qn[1];
+                qout[og + 2 * plane] = qn[2];
+                qout[og + 3 * plane] = qn[3];
             }
         }
         // slide the window
@@ -309,9 +341,25 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             hyT[v] = nyT[v];
             Glo[v] = Ghi[v];
         }
+        if constexpr (SYNC > 0) {
+            if (i % SYNC == SYNC - 1 || i == L - 1) {
+                __syncthreads();
+            }
+        }
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory"); // the ring is reused by the next strip
     (void)wB;
+}
+
+// The barrier sequence of strip_work<..., SYNC> for a warp without a strip.
+template <int SYNC>
+__device__ __forceinline__ void strip_idle(int L)
+{
+    for (int i = 0; i < L; ++i) {
+        if (i % SYNC == SYNC - 1 || i == L - 1) {
+            __syncthreads();
+        }
+    }
 }
 
 // time-loop control of one step, published by one thread (main.cpp:354-385)
@@ -374,10 +422,70 @@ k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     // grid-stride over the strips (the launcher sizes the grid to the
     // resident warps, so a warp usually takes one or two strips)
     const int wstride = gridDim.x * (blockDim.x >> 5);
+    __shared__ __align__(16) double s_ring[4][kStripRingDoubles];
+    const StripRing ring = reinterpret_cast<StripRing>(s_ring[(threadIdx.x >> 5) & 3]);
     for (int w = wg; w < nitems; w += wstride) {
-        strip_work<LIM, RS>(g, in.q, out.q, in.plane, in.pitch, dec.dt, w % ncolw, w / ncolw, L, inv_max, bad_cell);
+        strip_work<LIM, RS>(g, in.q, out.q, in.plane, in.pitch, dec.dt, w % ncolw, w / ncolw, L, inv_max, bad_cell,
+                            ring);
     }
     // warp max of 1/dt -> one atomic per warp
+    const bool nan_seen = isnan(inv_max);
+    double m = nan_seen ? 0.0 : inv_max;
+    m = warp_max_d(m);
+    const unsigned nanv = __ballot_sync(0xffffffffu, nan_seen);
+    if (lane == 0) {
+        atomicMax(&ctl->inv_dt_bits[(slot + 1) % 3], dbl_bits(m));
+        if (nanv) {
+            atomicMax(&ctl->inv_dt_bits[(slot + 1) % 3], 0x7ff8000000000000ull);
+        }
+    }
+    if (bad_cell >= 0) {
+        atomicMin(&ctl->bad_cell, (unsigned long long)bad_cell);
+        ctl->err = 4;
+        ctl->errflag[(slot + 1) & 1] = 1;
+        ctl->final_buf = out_buf;
+    }
+}
+
+// The same step with one CTA of 16 warps per SM whose strips march in step:
+// a CTA barrier every kStripSyncRows rows keeps the 16 strips of an SM at the
+// same height.  Without it the warp schedulers' preference for older warps
+// spreads the finishing times of one SM's strips by up to ~20 %, and the last
+// strips of an SM run with few warps left to hide their latency.
+constexpr int kStripSyncRows = 8;
+constexpr int kStripSyncWarps = 16;
+
+template <int LIM, int RS>
+__global__ void __launch_bounds__(32 * kStripSyncWarps, 1)
+k_strip2d_sync(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
+{
+    extern __shared__ __align__(16) double s_sync_rings[]; // [kStripSyncWarps][kStripRingDoubles]
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const Decision dec = decide(ctl, slot, rp);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        publish_decision(ctl, dec, rp, slot, out_buf);
+    }
+    if (dec.noop || dec.neg_dt) {
+        return;
+    }
+    const int ncolw = (g.nx[0] + kStripLanesOut - 1) / kStripLanesOut;
+    const int nstrip = (g.nx[1] + L - 1) / L;
+    const int nitems = ncolw * nstrip;
+    double inv_max = 0.0;
+    int64_t bad_cell = -1;
+    const StripRing ring = reinterpret_cast<StripRing>(s_sync_rings + warp * kStripRingDoubles);
+    // the CTA takes strips in groups of 16 (one per warp); every warp of the
+    // CTA runs the same loop, so the barrier sequences match
+    for (int base = blockIdx.x * kStripSyncWarps; base < nitems; base += gridDim.x * kStripSyncWarps) {
+        const int w = base + warp;
+        if (w < nitems) {
+            strip_work<LIM, RS, kStripSyncRows>(g, in.q, out.q, in.plane, in.pitch, dec.dt, w % ncolw, w / ncolw, L,
+                                                inv_max, bad_cell, ring);
+        } else {
+            strip_idle<kStripSyncRows>(L);
+        }
+    }
     const bool nan_seen = isnan(inv_max);
     double m = nan_seen ? 0.0 : inv_max;
     m = warp_max_d(m);

@@ -89,7 +89,7 @@ bool strip3d_eligible(const GridDev& g);
 void step_strip3d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                   int slot, int out_buf, int L, cudaStream_t s);
 void step_strip2d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
-                  int slot, int out_buf, int L, cudaStream_t s);
+                  int slot, int out_buf, int L, bool sync, cudaStream_t s);
 void configure_exact();
 void configure_mixed();
 int conservation_partials_doubles(int ndim);
