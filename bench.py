@@ -492,7 +492,7 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32-mixed (f32 fluxes, f64 state)", "data": "synthetic",
         "config": {"workload": WORKLOAD, "cells": CELLS, "precision": "fp32_mixed", "parallelism": "replicas",
                    "l2": "inputs larger than L2 (state 134 MB read + 134 MB written per step)",
-                   "e2e_steps_per_call": chunk},
+                   "e2e_steps_per_call": chunk, "schedule": d.schedule()},
         "fp64": {"value": value64, "ms_per_step": el64_max / args.steps * 1e3, "unit": "Mcell-updates/s"},
         "speedup_mixed_vs_fp64": value / value64,
         "accuracy": {"rel_l1_rho_mixed_vs_fp64": l1, "rel_linf_rho_mixed_vs_fp64": linf,

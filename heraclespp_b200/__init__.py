@@ -287,6 +287,10 @@ class Domain:
         check(lib().hcl_set_schedule(self.h, int(schedule), C.byref(used)))
         return used.value
 
+    def schedule(self):
+        """Schedule of the mixed kernel in use (-1 until the autotuner has run)."""
+        return self.set_schedule(-2)
+
     def interior(self):
         nx = (C.c_int * 3)()
         ng = C.c_int()

@@ -1488,7 +1488,13 @@ int hcl_step_fixed_dt(hcl_handle* h, double dt, void* stream)
 int hcl_set_schedule(hcl_handle* h, int schedule, int* used)
 {
     HCL_CHECK_HANDLE(h);
-    if (schedule >= hcl::fused::mixed_shape_count(h->g.ndim)) {
+    if (schedule == -2) {
+        if (used) {
+            *used = h->mixed_shape;
+        }
+        return HCL_OK;
+    }
+    if (schedule < -1 || schedule >= hcl::fused::mixed_shape_count(h->g.ndim)) {
         return fail(HCL_ERR_ARGUMENT, "schedule %d out of range", schedule);
     }
     if (schedule >= 0 && !hcl::fused::mixed_shape_valid(h->g, schedule)) {

@@ -92,7 +92,7 @@ k_ensemble(const Prob* __restrict__ probs, const int* __restrict__ item_prob, Pa
             int64_t bad_cell = -1;
             const double* qin = ep.seg_mode ? P.q[0] + (int64_t)s * P.seg_stride : P.q[gs & 1];
             double* qout = ep.seg_mode ? P.q[0] + (int64_t)(s + 1) * P.seg_stride : P.q[(gs + 1) & 1];
-            fused::strip_work<LIM, RS>(P.g, qin, qout, P.plane, P.pitch, dt, local % P.ncolw, local / P.ncolw, ep.L,
+            fused::strip_work<LIM, RS, 0, 2>(P.g, qin, qout, P.plane, P.pitch, dt, local % P.ncolw, local / P.ncolw, ep.L,
                                        inv_max, bad_cell, ring);
             const bool nan_seen = isnan(inv_max);
             double m = nan_seen ? 0.0 : inv_max;

@@ -155,7 +155,10 @@ constexpr int kStripRingDoubles = 8 * 4 * 32;
 // after row L - 1 of its strip, L barriers' worth of rows whatever the
 // strip's own height (strip_idle() is the same barrier sequence without a
 // strip), so that all warps of a CTA march in step.
-template <int LIM, int RS, int SYNC = 0>
+// XIMG: border columns with up to XIMG x images (1: Periodic, Reflexive; 2:
+// also NullGradient with two ghost layers) store them without a divergent
+// branch.
+template <int LIM, int RS, int SYNC = 0, int XIMG = 1>
 __device__ __forceinline__ void strip_work(const GridDev& g, const double* __restrict__ qin, double* __restrict__ qout,
                                            int64_t plane, int pitch, double dt, int sx, int sy, int L, double& inv_max,
                                            int64_t& bad_cell, StripRing ring)
@@ -169,14 +172,16 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     const int r0 = g.ng + L * sy;
     const int r1 = min(r0 + L, g.ng + g.nx[1]);
     const unsigned xm = out_lane ? ghost_mask(col, n0, g.ng, g.bc[0], g.bc[1]) : 0u;
-    // A column with at most one x image stores it on every row that has no y
-    // image, as one store in step with the other lanes of the warp (which
-    // store their own cell again): no divergent branch on the common border
-    // rows.  Other cases take store_images_2d.
+    // A column with at most XIMG x images stores them on every row that has
+    // no y image, in step with the other lanes of the warp (which store their
+    // own cell again): no divergent branch on the common border rows.  Other
+    // cases take store_images_2d.
     const unsigned xbits = xm & 0xffffu;
-    const bool x_single = __popc(xbits) <= 1;
-    const bool x_any = __any_sync(0xffffffffu, xbits != 0u);
-    const int x_img = xbits ? ghost_slot(__ffs(xbits) - 1, n0, g.ng) : col;
+    const int x_cnt = __popc(xbits);
+    const bool x_fast = x_cnt <= XIMG;
+    const bool x_any = __any_sync(0xffffffffu, x_cnt != 0);
+    const bool x_two = XIMG > 1 && __any_sync(0xffffffffu, x_cnt == 2);
+    const int x_img = xbits ? ghost_slot(__ffs(xbits) - 1, n0, g.ng) : col; // first image, or the cell
     const bool x_flip = xbits ? ((xm >> (15 + __ffs(xbits))) & 1u) != 0u : false;
 
     StripCtx c;
@@ -319,7 +324,7 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
                 qout[oo + plane * v] = qn[v];
             }
             const unsigned ym = (r < 2 * g.ng || r >= n1 - 2 * g.ng) ? ghost_mask(r, n1, g.ng, g.bc[2], g.bc[3]) : 0u;
-            if (ym != 0u || !x_single) {
+            if (ym != 0u || !x_fast) {
                 if ((xm | ym) != 0u) {
                     store_images_2d(qout, plane, pitch, n0, n1, g.ng, col, r, xm, ym, qn);
                 }
@@ -329,6 +334,17 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
                 qout[og + plane] = x_flip ? -qn[1] : qn[1];
                 qout[og + 2 * plane] = qn[2];
                 qout[og + 3 * plane] = qn[3];
+                if (XIMG > 1 && x_two) {
+                    // the second image, or the first again
+                    const unsigned b2 = xbits & (xbits - 1u);
+                    const int px = b2 ? ghost_slot(__ffs(b2) - 1, n0, g.ng) : x_img;
+                    const bool fl = b2 ? ((xm >> (15 + __ffs(b2))) & 1u) != 0u : x_flip;
+                    const int64_t og2 = (int64_t)r * pitch + px;
+                    qout[og2] = qn[0];
+                    qout[og2 + plane] = fl ? -qn[1] : qn[1];
+                    qout[og2 + 2 * plane] = qn[2];
+                    qout[og2 + 3 * plane] = qn[3];
+                }
             }
         }
         // slide the window

@@ -173,16 +173,6 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     const unsigned xm = out_cell ? ghost_mask(col, n0, g.ng, g.bc[0], g.bc[1]) : 0u;
     const unsigned ym = out_cell ? ghost_mask(row, n1, g.ng, g.bc[2], g.bc[3]) : 0u;
     const unsigned xym = xm | ym;
-    // A column with at most one (x, y) image stores it on every plane that has
-    // no z image, in step with the other lanes of the warp (which store their
-    // own cell again); corner columns and z-border planes take store_images_3d.
-    const unsigned xbits = xm & 0xffffu, ybits = ym & 0xffffu;
-    const bool xy_single = __popc(xbits) + __popc(ybits) <= 1;
-    const bool xy_any = __any_sync(0xffffffffu, (xbits | ybits) != 0u);
-    const int x_img = xbits ? ghost_slot(__ffs(xbits) - 1, n0, g.ng) : col;
-    const int y_img = ybits ? ghost_slot(__ffs(ybits) - 1, n1, g.ng) : row;
-    const bool x_flip = xbits ? ((xm >> (15 + __ffs(xbits))) & 1u) != 0u : false;
-    const bool y_flip = ybits ? ((ym >> (15 + __ffs(ybits))) & 1u) != 0u : false;
     const int z0 = g.ng + L * bz;
     const int z1 = min(z0 + L, g.ng + g.nx[2]);
     const int64_t pitch = in.pitch;
@@ -339,17 +329,8 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             const unsigned zm = (z < 2 * g.ng || z >= g.n[2] - 2 * g.ng)
                                     ? ghost_mask(z, g.n[2], g.ng, g.bc[4], g.bc[5])
                                     : 0u;
-            if (zm != 0u || !xy_single) {
-                if ((xym | zm) != 0u) {
-                    store_images_3d(qout, plane, pitch, n0, n1, g.n[2], g.ng, col, row, z, xm, ym, zm, qn);
-                }
-            } else if (xy_any) {
-                const int64_t og = ((int64_t)z * n1 + y_img) * pitch + x_img;
-                qout[og] = qn[0];
-                qout[og + plane] = x_flip ? -qn[1] : qn[1];
-                qout[og + 2 * plane] = y_flip ? -qn[2] : qn[2];
-                qout[og + 3 * plane] = qn[3];
-                qout[og + 4 * plane] = qn[4];
+            if ((xym | zm) != 0u) {
+                store_images_3d(qout, plane, pitch, n0, n1, g.n[2], g.ng, col, row, z, xm, ym, zm, qn);
             }
         }
         // slide the window

@@ -251,9 +251,14 @@ int hcl_reset_clock(hcl_handle* h, double t_ini);
 int hcl_get_dt_log(hcl_handle* h, double* dts, int max_count, int* count);
 
 /* Schedule of the FP32-mixed fused kernel.  -1 (default): autotuned on the
- * first run.  2-D: 0-2 shared-memory tiles (16x16, 32x8, 32x16), 3-5 warp
- * strips of 32/64/128 rows (uniform Cartesian grids).  Returns the schedule
- * in use through *used (may be NULL). */
+ * first run; -2: leaves the schedule unchanged (query).  2-D: 0-2
+ * shared-memory tiles (16x16, 32x8, 32x16); on uniform Cartesian grids 3-5
+ * warp strips of 32/64/128 rows, 6 warp strips fitted to one wave of
+ * resident warps, 7-8 paired-column warp strips (fitted, 32 rows; even ghost
+ * width), 9 fitted warp strips in 16-warp CTAs that march in step.  3-D: 0
+ * shared-memory tiles, 1 column march (uniform Cartesian grids).  Returns
+ * the schedule in use through *used (may be NULL; -1 before the autotuner
+ * ran). */
 int hcl_set_schedule(hcl_handle* h, int schedule, int* used);
 
 /* Compensated FP64 sums over no_ghosts: out[0] = sum rho dv, out[1..ndim] =
