@@ -50,10 +50,25 @@ __device__ __forceinline__ float lim_fast(float dR, float dL)
     }
 }
 
+// Half the limited slope, lim_fast(dR, dL) / 2: the same value (scaling by a
+// power of two is exact) with the factors 2 and 1/2 of van Leer cancelled.
+template <int LIM>
+__device__ __forceinline__ float half_lim_fast(float dR, float dL)
+{
+    if constexpr (LIM == LIM_VANLEER) {
+        const float prod = dR * dL;
+        return prod > 0.f ? prod * __fdividef(1.f, dR + dL) : 0.f;
+    } else {
+        return 0.5f * lim_fast<LIM>(dR, dL);
+    }
+}
+
 struct StripCtx {
     fast::Eos eos;
     float cthx, cthy; // (dt/2)/dx, (dt/2)/dy
     float dgx, dgy;   // (dt/2) g
+    float kc2;        // gamma (gamma - 1) / 2
+    float idx, idy;   // 1/dx, 1/dy
     bool gravity;     // any g component non-zero (the terms vanish exactly otherwise)
 };
 
@@ -103,10 +118,10 @@ __device__ __forceinline__ void strip_hancock(const StripCtx& c, const float wd[
     for (int v = 0; v < 4; ++v) {
         const float wl = __shfl_up_sync(0xffffffffu, wc[v], 1);
         const float wr = __shfl_down_sync(0xffffffffu, wc[v], 1);
-        const float sx = 0.5f * lim_fast<LIM>(wr - wc[v], wc[v] - wl);
+        const float sx = half_lim_fast<LIM>(wr - wc[v], wc[v] - wl);
         fxL[v] = wc[v] - sx;
         fxR[v] = wc[v] + sx;
-        const float sy = 0.5f * lim_fast<LIM>(wu[v] - wc[v], wc[v] - wd[v]);
+        const float sy = half_lim_fast<LIM>(wu[v] - wc[v], wc[v] - wd[v]);
         fyB[v] = wc[v] - sy;
         fyT[v] = wc[v] + sy;
     }
@@ -190,7 +205,11 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     c.cthy = (float)(0.5 * dt * g.inv_dx[1]);
     c.dgx = (float)(0.5 * dt * g.g[0]);
     c.dgy = (float)(0.5 * dt * g.g[1]);
+    c.kc2 = (float)(0.5 * g.gamma * g.gamma_m1);
+    c.idx = (float)g.inv_dx[0];
+    c.idy = (float)g.inv_dx[1];
     c.gravity = g.g[0] != 0.0 || g.g[1] != 0.0;
+    float inv_f = 0.f; // this strip's CFL max (NaN once a NaN was seen)
     const double cx = dt * g.inv_dx[0];
     const double cy = dt * g.inv_dx[1];
     const double dgx = dt * g.g[0];
@@ -304,20 +323,26 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
                 qn[2] = fma(dgy, q[0], qn[2]);
                 qn[3] = fma(dgx, q[1], fma(dgy, q[2], qn[3]));
             }
-            // health check (main.cpp:397-425) and CFL (time_step.hpp:55-77) of the new state
-            double rr = (double)__fdividef(1.f, (float)qn[0]);
-            rr = rr * (2.0 - qn[0] * rr);
-            const double u = qn[1] * rr;
-            const double vv = qn[2] * rr;
-            const double evol = fma(-0.5, fma(qn[1], u, qn[2] * vv), qn[3]);
-            const double c2 = g.gamma * gm1 * evol * rr;
-            double y = (double)rsqrtf((float)c2);
-            y = y * (1.5 - 0.5 * c2 * y * y);
-            const double snd = c2 * y;
-            const double cell = fma(fabs(u) + snd, g.inv_dx[0], (fabs(vv) + snd) * g.inv_dx[1]);
-            inv_max = cell > inv_max ? cell : (isnan(cell) ? cell : inv_max);
-            if (!(evol >= 0.0) && bad_cell < 0) {
+            // health check (main.cpp:397-425): the new state fails when
+            // evol = E - |m|^2 / (2 rho) is negative or NaN.  Evaluated in FP64
+            // without the division, as the sign of 2 rho evol = 2 rho E - |m|^2
+            // (reversed for rho < 0; rho = 0 gives -inf or NaN: fails).
+            const double tre = (qn[0] + qn[0]) * qn[3];
+            const double mm = fma(qn[1], qn[1], qn[2] * qn[2]);
+            const bool healthy = qn[0] > 0.0 ? tre >= mm : (qn[0] < 0.0 && tre <= mm);
+            if (!healthy && bad_cell < 0) {
                 bad_cell = lidx(g, col, r, 0);
+            }
+            // CFL contribution (time_step.hpp:55-77) in FP32 from the FP64
+            // internal energy: c^2 = gamma (gamma-1) evol / rho
+            //                      = gamma (gamma-1) / 2 * (2 rho E - |m|^2) / rho^2
+            {
+                const float ir = __fdividef(1.f, (float)qn[0]);
+                const float c2 = c.kc2 * (float)(tre - mm) * ir * ir;
+                const float snd = sqrtf(c2);
+                const float cell =
+                    fmaf(fabsf((float)qn[1] * ir) + snd, c.idx, (fabsf((float)qn[2] * ir) + snd) * c.idy);
+                inv_f = cell > inv_f ? cell : (isnan(cell) ? cell : inv_f);
             }
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
@@ -364,6 +389,8 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         }
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory"); // the ring is reused by the next strip
+    const double inv_d = (double)inv_f;
+    inv_max = inv_d > inv_max ? inv_d : (isnan(inv_d) ? inv_d : inv_max);
     (void)wB;
 }
 
