@@ -336,6 +336,10 @@ void build_grid_host(hcl_handle* h)
         }
         g.inv_dx[d] = 1.0 / ref;
     }
+    for (int d = 0; d < 3; ++d) {
+        g.inv_dx_f[d] = (float)g.inv_dx[d];
+    }
+    g.cfl_kc2 = (float)(0.5 * g.gamma * g.gamma_m1);
     g.uniform_cart = uniform;
 }
 

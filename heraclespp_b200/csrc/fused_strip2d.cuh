@@ -67,8 +67,6 @@ struct StripCtx {
     fast::Eos eos;
     float cthx, cthy; // (dt/2)/dx, (dt/2)/dy
     float dgx, dgy;   // (dt/2) g
-    float kc2;        // gamma (gamma - 1) / 2
-    float idx, idy;   // 1/dx, 1/dy
     bool gravity;     // any g component non-zero (the terms vanish exactly otherwise)
 };
 
@@ -205,9 +203,6 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     c.cthy = (float)(0.5 * dt * g.inv_dx[1]);
     c.dgx = (float)(0.5 * dt * g.g[0]);
     c.dgy = (float)(0.5 * dt * g.g[1]);
-    c.kc2 = (float)(0.5 * g.gamma * g.gamma_m1);
-    c.idx = (float)g.inv_dx[0];
-    c.idy = (float)g.inv_dx[1];
     c.gravity = g.g[0] != 0.0 || g.g[1] != 0.0;
     float inv_f = 0.f; // this strip's CFL max (NaN once a NaN was seen)
     const double cx = dt * g.inv_dx[0];
@@ -338,10 +333,10 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             //                      = gamma (gamma-1) / 2 * (2 rho E - |m|^2) / rho^2
             {
                 const float ir = __fdividef(1.f, (float)qn[0]);
-                const float c2 = c.kc2 * (float)(tre - mm) * ir * ir;
+                const float c2 = g.cfl_kc2 * (float)(tre - mm) * ir * ir;
                 const float snd = sqrtf(c2);
                 const float cell =
-                    fmaf(fabsf((float)qn[1] * ir) + snd, c.idx, (fabsf((float)qn[2] * ir) + snd) * c.idy);
+                    fmaf(fabsf((float)qn[1] * ir) + snd, g.inv_dx_f[0], (fabsf((float)qn[2] * ir) + snd) * g.inv_dx_f[1]);
                 inv_f = cell > inv_f ? cell : (isnan(cell) ? cell : inv_f);
             }
 #pragma unroll

@@ -89,13 +89,13 @@ __device__ __forceinline__ void hancock(const Ctx& c, const float wc[5], const f
     for (int v = 0; v < 5; ++v) {
         const float wl = __shfl_up_sync(0xffffffffu, wc[v], 1);
         const float wr = __shfl_down_sync(0xffffffffu, wc[v], 1);
-        const float sx = 0.5f * lim_fast<LIM>(wr - wc[v], wc[v] - wl);
+        const float sx = half_lim_fast<LIM>(wr - wc[v], wc[v] - wl);
         fm[0][v] = wc[v] - sx;
         fp[0][v] = wc[v] + sx;
-        const float sy = 0.5f * lim_fast<LIM>(wyu[v] - wc[v], wc[v] - wyd[v]);
+        const float sy = half_lim_fast<LIM>(wyu[v] - wc[v], wc[v] - wyd[v]);
         fm[1][v] = wc[v] - sy;
         fp[1][v] = wc[v] + sy;
-        const float sz = 0.5f * lim_fast<LIM>(wzu[v] - wc[v], wc[v] - wzd[v]);
+        const float sz = half_lim_fast<LIM>(wzu[v] - wc[v], wc[v] - wzd[v]);
         fm[2][v] = wc[v] - sz;
         fp[2][v] = wc[v] + sz;
     }
@@ -189,6 +189,7 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     }
     c.gravity = g.g[0] != 0.0 || g.g[1] != 0.0 || g.g[2] != 0.0;
     const double gm1 = g.gamma_m1;
+    float inv_f = 0.f; // CFL max of this CTA's cells (NaN once a NaN was seen)
 
     auto load = [&](int z, double q[5]) {
         const int zc = min(max(z, 0), n2 - 1);
@@ -307,19 +308,25 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
                 qn[3] = fma(Dg[2], q[0], qn[3]);
                 qn[4] = fma(Dg[0], q[1], fma(Dg[1], q[2], fma(Dg[2], q[3], qn[4])));
             }
-            double rr = (double)__fdividef(1.f, (float)qn[0]);
-            rr = rr * (2.0 - qn[0] * rr);
-            const double u = qn[1] * rr, vv = qn[2] * rr, ww = qn[3] * rr;
-            const double evol = fma(-0.5, fma(qn[1], u, fma(qn[2], vv, qn[3] * ww)), qn[4]);
-            const double c2 = g.gamma * gm1 * evol * rr;
-            double y = (double)rsqrtf((float)c2);
-            y = y * (1.5 - 0.5 * c2 * y * y);
-            const double snd = c2 * y;
-            const double cell = fma(fabs(u) + snd, g.inv_dx[0],
-                                    fma(fabs(vv) + snd, g.inv_dx[1], (fabs(ww) + snd) * g.inv_dx[2]));
-            inv_max = cell > inv_max ? cell : (isnan(cell) ? cell : inv_max);
-            if (!(evol >= 0.0) && bad_cell < 0) {
+            // health check (main.cpp:397-425) in FP64 without the division:
+            // evol = E - |m|^2 / (2 rho) has the sign of 2 rho E - |m|^2
+            // (reversed for rho < 0; rho = 0 fails)
+            const double tre = (qn[0] + qn[0]) * qn[4];
+            const double mm = fma(qn[1], qn[1], fma(qn[2], qn[2], qn[3] * qn[3]));
+            const bool healthy = qn[0] > 0.0 ? tre >= mm : (qn[0] < 0.0 && tre <= mm);
+            if (!healthy && bad_cell < 0) {
                 bad_cell = lidx(g, col, row, z);
+            }
+            // CFL contribution (time_step.hpp:55-77) in FP32 from the FP64
+            // internal energy: c^2 = gamma (gamma-1) / 2 * (2 rho E - |m|^2) / rho^2
+            {
+                const float ir = __fdividef(1.f, (float)qn[0]);
+                const float c2 = g.cfl_kc2 * (float)(tre - mm) * ir * ir;
+                const float snd = sqrtf(c2);
+                const float cell = fmaf(fabsf((float)qn[1] * ir) + snd, g.inv_dx_f[0],
+                                        fmaf(fabsf((float)qn[2] * ir) + snd, g.inv_dx_f[1],
+                                             (fabsf((float)qn[3] * ir) + snd) * g.inv_dx_f[2]));
+                inv_f = cell > inv_f ? cell : (isnan(cell) ? cell : inv_f);
             }
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
@@ -345,6 +352,7 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     }
 
     // warp max of 1/dt -> one atomic per warp
+    inv_max = (double)inv_f;
     const bool nan_seen = isnan(inv_max);
     double m = nan_seen ? 0.0 : inv_max;
     m = warp_max_d(m);
