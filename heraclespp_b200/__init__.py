@@ -178,6 +178,11 @@ class Domain:
                                      _ptr(rhou_rec), _ptr(E_rec), _ptr(rho_new), _ptr(rhou_new), _ptr(E_new),
                                      stream))
 
+    def internal_mass_gravity(self, rho, g_out=None, stream=None):
+        """make_internal_mass_gravity: the radial gravity table from the device
+        density rho; g_out (device, n0 doubles) receives a copy of it."""
+        check(lib().hcl_internal_mass_gravity(self.h, _ptr(rho), _ptr(g_out), stream))
+
     def boundary_conditions(self, rho, rhou, E, fx=None, stream=None):
         check(lib().hcl_boundary_conditions(self.h, _ptr(rho), _ptr(rhou), _ptr(E), _ptr(fx), stream))
 

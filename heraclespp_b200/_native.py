@@ -23,7 +23,7 @@ LIMITERS = {"Constant": 0, "VanLeer": 1, "Minmod": 2, "VanAlbada": 3}
 RIEMANN = {"HLL": 0, "HLLC": 1, "Low Mach": 2}
 BCS = {"NullGradient": 0, "Periodic": 1, "Reflexive": 2}
 GEOMS = {"Cartesian": 0, "Spherical": 1}
-GRAVITY = {"Uniform": 0, "Point_mass": 1}
+GRAVITY = {"Uniform": 0, "Point_mass": 1, "Internal_mass": 2}
 PRECISION = {"fp64": 0, "fp32_mixed": 1}
 
 # Every entry point declared in include/heracles_b200.h.
@@ -36,7 +36,7 @@ EXPORTS = [
     "hcl_conservation_sums", "hcl_kernel_launch_count", "hcl_get_stream", "hcl_get_interior",
     "hcl_adjoint_forward", "hcl_adjoint_backward", "hcl_adjoint_dts", "hcl_set_schedule",
     "hcl_ensemble_create", "hcl_ensemble_destroy", "hcl_ensemble_handle", "hcl_ensemble_stream",
-    "hcl_ensemble_run", "hcl_ensemble_adjoint", "hcl_pressure_fix",
+    "hcl_ensemble_run", "hcl_ensemble_adjoint", "hcl_pressure_fix", "hcl_internal_mass_gravity",
 ]
 
 
@@ -167,6 +167,7 @@ def lib():
     L.hcl_godunov_scheme.argtypes = [H, i, d] + [vp] * 13
     L.hcl_boundary_conditions.argtypes = [H, vp, vp, vp, vp, vp]
     L.hcl_pressure_fix.argtypes = [H, d, d] + [vp] * 10
+    L.hcl_internal_mass_gravity.argtypes = [H, vp, vp, vp]
     L.hcl_time_step.argtypes = [H, i, vp, vp, vp, C.POINTER(d), vp]
     L.hcl_minimum_internal_energy.argtypes = [H, vp, vp, vp, C.POINTER(d), vp]
     L.hcl_integrate.argtypes = [H, vp, C.POINTER(d), vp]

@@ -103,6 +103,7 @@ struct hcl_handle {
     // device grid arrays
     double *dx_nodes[3] = {}, *ddx[3] = {}, *dxc[3] = {}, *dds = nullptr, *ddv = nullptr, *dgr = nullptr;
     double *dcot = nullptr, *dsin1 = nullptr, *dsinxc1 = nullptr;
+    double* grav_shell = nullptr; // InternalMassGravity: shell means of rho (nx0 + ng)
     // stage-path scratch (MUSCLHancockHydroReconstruction's P_rec/u_rec, fx_rec_old)
     double *u_rec = nullptr, *P_rec = nullptr, *fx_rec_old = nullptr;
     // reductions
@@ -183,6 +184,7 @@ void free_handle(hcl_handle* h)
     cudaFree(h->dds);
     cudaFree(h->ddv);
     cudaFree(h->dgr);
+    cudaFree(h->grav_shell);
     cudaFree(h->dcot);
     cudaFree(h->dsin1);
     cudaFree(h->dsinxc1);
@@ -290,6 +292,8 @@ void build_grid_host(hcl_handle* h)
         for (int i = 0; i < n[0]; ++i) {
             h->hgr[i] = -hcl::kG * c.central_mass / (h->hxc[0][i] * h->hxc[0][i]);
         }
+    } else if (c.gravity == HCL_GRAVITY_INTERNAL_MASS) {
+        h->hgr.assign(n[0], 0.0); // filled from the density (refresh_gravity)
     }
     // spherical trig factors per index (source_terms.hpp:38, :58-59, time_step.hpp:67)
     h->hcot.assign(n[1], 0.0);
@@ -384,7 +388,8 @@ int validate(const hcl_config* c)
     if (c->geometry != HCL_GEOM_CARTESIAN && c->geometry != HCL_GEOM_SPHERICAL) {
         return fail(HCL_ERR_CONFIG, "Unknown geometry id %d", c->geometry);
     }
-    if (c->gravity != HCL_GRAVITY_UNIFORM && c->gravity != HCL_GRAVITY_POINT_MASS) {
+    if (c->gravity != HCL_GRAVITY_UNIFORM && c->gravity != HCL_GRAVITY_POINT_MASS &&
+        c->gravity != HCL_GRAVITY_INTERNAL_MASS) {
         return fail(HCL_ERR_CONFIG, "Unknown gravity id %d", c->gravity);
     }
     if (c->precision != HCL_FP64 && c->precision != HCL_FP32_MIXED) {
@@ -446,6 +451,11 @@ void launch_step(hcl_handle* h, const RunParamsDev& rp, int64_t counter, StepCtl
 {
     const int slot = (int)(counter % 6);
     const int out_buf = in_buf ^ 1;
+    if (h->g.gravity == HCL_GRAVITY_INTERNAL_MASS) {
+        // the radial gravity of the step's input density (main.cpp:309, :528)
+        hcl::stage::internal_mass_gravity(h->g, h->st[in_buf].q, h->st[in_buf].pitch, h->cfg.central_mass,
+                                          h->grav_shell, h->dgr, s);
+    }
     if (h->cfg.precision == HCL_FP64) {
         hcl::fused::step_exact(h->g, h->st[in_buf], h->st[out_buf], ctl, rp, slot, out_buf, s);
     } else {
@@ -709,6 +719,10 @@ int hcl_create(const hcl_config* cfg, hcl_handle** out)
     if ((rc = upload(&h->dds, h->hds)) || (rc = upload(&h->ddv, h->hdv)) || (rc = upload(&h->dgr, h->hgr)) ||
         (rc = upload(&h->dcot, h->hcot)) || (rc = upload(&h->dsin1, h->hsin1)) ||
         (rc = upload(&h->dsinxc1, h->hsinxc1))) {
+        return bail(rc);
+    }
+    if (h->cfg.gravity == HCL_GRAVITY_INTERNAL_MASS &&
+        (rc = dalloc(&h->grav_shell, (size_t)(g.nx[0] + g.ng)))) {
         return bail(rc);
     }
     g.ds = h->dds;
@@ -975,6 +989,24 @@ int hcl_boundary_conditions(hcl_handle* h, double* rho, double* rhou, double* E,
     return HCL_OK;
 }
 
+int hcl_internal_mass_gravity(hcl_handle* h, const double* rho, double* g_out, void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    if (h->g.gravity != HCL_GRAVITY_INTERNAL_MASS) {
+        return fail(HCL_ERR_CONFIG, "the handle was not created with HCL_GRAVITY_INTERNAL_MASS");
+    }
+    if (!rho) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    cudaStream_t s = pick(h, stream);
+    hcl::stage::internal_mass_gravity(h->g, rho, h->g.n[0], h->cfg.central_mass, h->grav_shell, h->dgr, s);
+    if (g_out) {
+        HCL_CUDA(cudaMemcpyAsync(g_out, h->dgr, sizeof(double) * (size_t)h->g.n[0], cudaMemcpyDeviceToDevice, s));
+    }
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
 int hcl_time_step(hcl_handle* h, int ng_eff, const double* rho, const double* u, const double* P, double* dt_out,
                   void* stream)
 {
@@ -1034,6 +1066,20 @@ int hcl_integrate(hcl_handle* h, const double* var, double* out, void* stream)
 }
 
 // ---- handle-owned state ----------------------------------------------------
+// InternalMassGravity handles: the radial gravity table of the current state
+// (main.cpp:309 after the initial state, :528 after every step).
+static int refresh_gravity(hcl_handle* h)
+{
+    if (h->g.gravity != HCL_GRAVITY_INTERNAL_MASS || !h->state_valid) {
+        return HCL_OK;
+    }
+    const double* rho = stage_mode(h) ? h->sl_rho : h->st[h->cur].q;
+    const int pitch = stage_mode(h) ? h->g.n[0] : h->st[h->cur].pitch;
+    hcl::stage::internal_mass_gravity(h->g, rho, pitch, h->cfg.central_mass, h->grav_shell, h->dgr, h->stream);
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
 int hcl_set_state(hcl_handle* h, const double* rho, const double* rhou, const double* E, const double* fx,
                   int memory)
 {
@@ -1065,6 +1111,9 @@ int hcl_set_state(hcl_handle* h, const double* rho, const double* rhou, const do
         }
         HCL_CUDA(cudaStreamSynchronize(s));
         h->state_valid = 1;
+        if ((rc = refresh_gravity(h))) {
+            return rc;
+        }
         return hcl_reset_clock(h, 0.0);
     }
     (void)fx;
@@ -1072,7 +1121,8 @@ int hcl_set_state(hcl_handle* h, const double* rho, const double* rhou, const do
     HCL_CUDA(cudaGetLastError());
     h->cur = 0;
     h->state_valid = 1;
-    return restart_clock(h, 0.0, 0);
+    int rc = refresh_gravity(h);
+    return rc ? rc : restart_clock(h, 0.0, 0);
 }
 
 int hcl_get_state(hcl_handle* h, double* rho, double* rhou, double* E, double* fx, int memory)
@@ -1138,6 +1188,9 @@ int hcl_set_state_from_prim(hcl_handle* h, const double* rho, const double* u, c
         }
         HCL_CUDA(cudaStreamSynchronize(s));
         h->state_valid = 1;
+        if ((rc = refresh_gravity(h))) {
+            return rc;
+        }
         return hcl_reset_clock(h, 0.0);
     }
     (void)fx;
@@ -1172,6 +1225,9 @@ int hcl_set_state_from_prim(hcl_handle* h, const double* rho, const double* u, c
     }
     h->cur = 0;
     h->state_valid = 1;
+    if ((rc = refresh_gravity(h))) {
+        return rc;
+    }
     return restart_clock(h, 0.0, 0);
 }
 
@@ -1283,6 +1339,10 @@ static int run_stage_loop(hcl_handle* h, const hcl_run_params* p, hcl_run_result
         std::swap(h->sl_fx, h->sl_fx_new);
         if ((rc = hcl_conv_cons_to_prim(h, ng, h->sl_rho, h->sl_rhou, h->sl_E, h->sl_u, h->sl_P, s))) {
             return rc;
+        }
+        if (h->g.gravity == HCL_GRAVITY_INTERNAL_MASS) { // main.cpp:528
+            hcl::stage::internal_mass_gravity(h->g, h->sl_rho, h->g.n[0], h->cfg.central_mass, h->grav_shell,
+                                              h->dgr, s);
         }
         h->sl_t += dt; // main.cpp:530-531
         ++h->sl_iter;
@@ -1431,6 +1491,9 @@ int hcl_run(hcl_handle* h, const hcl_run_params* p, hcl_run_result* r)
     const bool stop = ctl.stop[q] || ctl.err;
     h->cur = stop ? ctl.final_buf : q;
     h->stopped = stop ? 1 : 0;
+    if ((rc = refresh_gravity(h))) {
+        return rc;
+    }
     if (r) {
         r->t = ctl.t[q];
         r->iter = ctl.iter[q];
@@ -1486,6 +1549,11 @@ int hcl_step_fixed_dt(hcl_handle* h, double dt, void* stream)
     ++h->counter;
     h->cur = (int)(h->counter & 1);
     HCL_LAUNCH_CHECK();
+    if (h->g.gravity == HCL_GRAVITY_INTERNAL_MASS) {
+        hcl::stage::internal_mass_gravity(h->g, h->st[h->cur].q, h->st[h->cur].pitch, h->cfg.central_mass,
+                                          h->grav_shell, h->dgr, s);
+        HCL_LAUNCH_CHECK();
+    }
     return HCL_OK;
 }
 

@@ -19,7 +19,7 @@ enum : int { LIM_CONSTANT = 0, LIM_VANLEER = 1, LIM_MINMOD = 2, LIM_VANALBADA = 
 enum : int { RS_HLL = 0, RS_HLLC = 1, RS_SPLITTING = 2 };
 enum : int { BC_NULLGRADIENT = 0, BC_PERIODIC = 1, BC_REFLEXIVE = 2 };
 enum : int { GEOM_CARTESIAN = 0, GEOM_SPHERICAL = 1 };
-enum : int { GRAV_UNIFORM = 0, GRAV_POINT_MASS = 1 };
+enum : int { GRAV_UNIFORM = 0, GRAV_POINT_MASS = 1, GRAV_INTERNAL_MASS = 2 };
 
 // Everything a kernel needs to know about the grid and the physics plugins.
 // Passed by value (it lives in the kernel parameter space).
@@ -43,7 +43,7 @@ struct GridDev {
     const double* xc[3];  // n
     const double* ds;     // N*3
     const double* dv;     // N
-    const double* g_r;    // point-mass g(i), n[0]
+    const double* g_r;    // point-mass / internal-mass g(i), n[0]
     // geometry helpers precomputed on the host for spherical runs (per index):
     const double* cot_mid1;   // cos((x1_j+x1_{j+1})/2)/sin(...) per j, source_terms.hpp:38
     const double* sin1;       // sin(x1_j) per node j, source_terms.hpp:58-59
@@ -62,7 +62,7 @@ __host__ __device__ inline int64_t lidx(const GridDev& g, int i, int j, int k)
 // Gravity functor value g(i,j,k,dir) (gravity/gravity.hpp:36-40, :63-70).
 __device__ inline double gravity_at(const GridDev& g, int i, int dir)
 {
-    if (g.gravity == GRAV_POINT_MASS) {
+    if (g.gravity != GRAV_UNIFORM) { // point mass, internal mass: the radial table
         return dir == 0 ? g.g_r[i] : 0.0;
     }
     return g.g[dir];

@@ -785,6 +785,59 @@ void dispatch_nd(int nd, F&& f)
     }
 }
 
+// InternalMassGravity (gravity.cpp:59-128), one CTA: each thread sums the
+// density of one radial shell over the interior (j, k) (j outer, k inner),
+// thread 0 runs the enclosed-mass sum outwards from the central mass, then
+// every thread turns its cells' enclosed mass into g = -G M / xc^2.  rho has
+// rows of `pitch` doubles (n0 for the reference layout); shell: nx0 + ng
+// doubles of scratch; g_r: n0 doubles (the handle's radial table).
+__global__ void k_internal_mass_gravity(GridDev g, const double* __restrict__ rho, int pitch, double central_mass,
+                                        double* __restrict__ shell, double* __restrict__ g_r)
+{
+    const int ng = g.ng;
+    const int nsh = g.nx[0] + ng;
+    const int g1 = g.ndim >= 2 ? ng : 0;
+    const int g2 = g.ndim >= 3 ? ng : 0;
+    for (int i = threadIdx.x; i < nsh; i += blockDim.x) {
+        double sm = 0;
+        double sd = 0;
+        for (int j = 0; j < g.nx[1]; ++j) {
+            for (int k = 0; k < g.nx[2]; ++k) {
+                const int64_t id = lidx(g, i + ng, j + g1, k + g2);
+                const int64_t ir = ((int64_t)(k + g2) * g.n[1] + (j + g1)) * pitch + (i + ng);
+                sm += rho[ir] * g.dv[id];
+                sd += g.dv[id];
+            }
+        }
+        shell[i] = sm / sd;
+    }
+    __syncthreads();
+    const double* x0 = g.x[0];
+    const double* xc = g.xc[0];
+    if (threadIdx.x == 0) {
+        const double vol_s3 = 4 * kPi / 3;
+        for (int i = 0; i < ng; ++i) {
+            g_r[i] = central_mass;
+        }
+        double partial = 0;
+        for (int i = ng; i < g.nx[0] + 2 * ng; ++i) {
+            const int off = i - ng;
+            const double x3 = x0[i] * x0[i] * x0[i];
+            if (i == ng) {
+                partial += central_mass + (vol_s3 * ((xc[i] * xc[i] * xc[i]) - x3) * shell[off]);
+            } else {
+                partial += (vol_s3 * (x3 - (xc[i - 1] * xc[i - 1] * xc[i - 1])) * shell[off - 1]) +
+                           (vol_s3 * ((xc[i] * xc[i] * xc[i]) - x3) * shell[off]);
+            }
+            g_r[i] = partial;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < g.n[0]; i += blockDim.x) {
+        g_r[i] = -kG * g_r[i] / (xc[i] * xc[i]);
+    }
+}
+
 } // namespace
 
 namespace stage {
@@ -882,6 +935,13 @@ void pressure_fix(const GridDev& g, double dt, double eps, const double* rho, co
         k_pressure_fix<ND><<<grid_for(bx.count), kThreads, 0, s>>>(g, bx, dt, eps, rho, rhou, E, rho_rec, rhou_rec,
                                                                    E_rec, rho_new, rhou_new, E_new);
     });
+    ++g_launches;
+}
+
+void internal_mass_gravity(const GridDev& g, const double* rho, int pitch, double central_mass, double* shell,
+                           double* g_r, cudaStream_t s)
+{
+    k_internal_mass_gravity<<<1, 256, 0, s>>>(g, rho, pitch, central_mass, shell, g_r);
     ++g_launches;
 }
 

@@ -30,6 +30,11 @@ void godunov(const GridDev& g, int ng_eff, double dt, const double* rho, const d
              const double* fx_rec, double* rho_new, double* rhou_new, double* E_new, double* fx_new,
              cudaStream_t s);
 void boundaries(const GridDev& g, double* rho, double* rhou, double* E, double* fx, cudaStream_t s);
+// InternalMassGravity (gravity.cpp:59-128): the radial table g_r (n0 doubles)
+// from rho, whose rows are `pitch` doubles apart (n0 for the reference
+// layout, StateDev::pitch for the fused state); shell: nx0 + ng doubles
+void internal_mass_gravity(const GridDev& g, const double* rho, int pitch, double central_mass, double* shell,
+                           double* g_r, cudaStream_t s);
 // pressure_fix.hpp:19-172 on no_ghosts: updates E_new in place
 void pressure_fix(const GridDev& g, double dt, double eps, const double* rho, const double* rhou, const double* E,
                   const double* rho_rec, const double* rhou_rec, const double* E_rec, const double* rho_new,

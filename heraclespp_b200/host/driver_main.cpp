@@ -4,7 +4,7 @@
 // and prints the reference's summary lines (main.cpp:570-583).
 //
 // Options (the reference fixes these at CMake time, CMakeLists.txt:11-79):
-//   --ndim=1|2|3  --geometry=Cartesian|Spherical  --gravity=Uniform|Point_mass
+//   --ndim=1|2|3  --geometry=Cartesian|Spherical  --gravity=Uniform|Point_mass|Internal_mass
 //   --setup=<name>  --precision=fp64|fp32_mixed  --device=N  --output=<file>
 #include <chrono>
 #include <cstdio>
@@ -52,7 +52,9 @@ int main(int argc, char** argv)
     const std::string setup = opt_value(argc, argv, "--setup", "shock_tube");
     const std::string output = opt_value(argc, argv, "--output", "");
     opt.geometry = geom == "Spherical" ? HCL_GEOM_SPHERICAL : HCL_GEOM_CARTESIAN;
-    opt.gravity = grav == "Point_mass" ? HCL_GRAVITY_POINT_MASS : HCL_GRAVITY_UNIFORM;
+    opt.gravity = grav == "Point_mass"      ? HCL_GRAVITY_POINT_MASS
+                  : grav == "Internal_mass" ? HCL_GRAVITY_INTERNAL_MASS
+                                            : HCL_GRAVITY_UNIFORM;
     opt.precision = prec == "fp32_mixed" ? HCL_FP32_MIXED : HCL_FP64;
     opt.device = std::atoi(opt_value(argc, argv, "--device", "0").c_str());
     opt.setup = setup.c_str();

@@ -67,7 +67,11 @@ enum hcl_bc {                  /* boundary_factory.hpp:31-47 */
     HCL_BC_REFLEXIVE = 2
 };
 enum hcl_geometry { HCL_GEOM_CARTESIAN = 0, HCL_GEOM_SPHERICAL = 1 };   /* utils/geom.hpp.in:17-25 */
-enum hcl_gravity { HCL_GRAVITY_UNIFORM = 0, HCL_GRAVITY_POINT_MASS = 1 }; /* main.cpp:73-96 */
+enum hcl_gravity { /* main.cpp:73-96 */
+    HCL_GRAVITY_UNIFORM = 0,
+    HCL_GRAVITY_POINT_MASS = 1,
+    HCL_GRAVITY_INTERNAL_MASS = 2 /* g(r) = -G M(r) / r^2 with M(r) from the density, gravity.cpp:59-128 */
+};
 enum hcl_precision {
     HCL_FP64 = 0,              /* reference arithmetic, bitwise-comparable to the FP64 CPU build */
     HCL_FP32_MIXED = 1         /* FP32 prim/slopes/faces/fluxes, FP64 state, energy recovery, dt, sums */
@@ -91,7 +95,7 @@ typedef struct hcl_config {
     int bc[6];                /* enum hcl_bc, index 2*idim + iface (main.cpp:174-185) */
     int gravity;              /* enum hcl_gravity */
     double g[3];              /* [Gravity] gx0..gx2 (uniform) */
-    double central_mass;      /* [Gravity] M (point mass) */
+    double central_mass;      /* [Gravity] M (point mass; central mass of the internal mass) */
     double xmin[3], xmax[3];  /* [Grid] x{0,1,2}{min,max} for the Regular grid */
     const double* nodes[3];   /* optional host node coordinates (length n_d + 1) for a
                                  UserDefined grid; NULL selects Regular (grid_type.cpp:151-186) */
@@ -184,6 +188,16 @@ int hcl_godunov_scheme(hcl_handle* h, int ng_eff, double dt, const double* rho, 
  * (boundary_distribute.hpp:42-76) + every IBoundaryCondition::execute
  * (boundary.hpp:81-87, boundary.cpp:221-296): fills all ghost cells in place. */
 int hcl_boundary_conditions(hcl_handle* h, double* rho, double* rhou, double* E, double* fx, void* stream);
+/* make_internal_mass_gravity (gravity/gravity.cpp:59-128) for handles created
+ * with HCL_GRAVITY_INTERNAL_MASS: recomputes the handle's radial gravity table
+ * from the density rho (device, with the ghost layers of dimension 0 filled):
+ * shell means of rho over the interior (j, k), the enclosed mass at the cell
+ * centres from the central mass outwards, g(i) = -G M(i) / xc(i)^2.  The
+ * stage entry points that take gravity use the table from then on (the
+ * reference rebuilds its Gravity object the same way, main.cpp:309 and :528).
+ * g_out (device, n0 doubles, may be NULL) receives a copy of the table.
+ * hcl_run and hcl_set_state* keep the table current by themselves. */
+int hcl_internal_mass_gravity(hcl_handle* h, const double* rho, double* g_out, void* stream);
 /* time_step (hydro/time_step.hpp:35-82): writes 1/max_cells(sum_d (|u_d|+c)/dx_d)
  * to *dt_out (host), i.e. the value the reference returns before main
  * multiplies by cfl.  Synchronises the stream. */

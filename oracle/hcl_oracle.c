@@ -24,6 +24,7 @@ static const double KB = 1.380649E-23;
 static const double MP = 1.672649E-27;
 /* units.hpp:179 */
 static const double GRAV_G = 6.6743015E-11;
+static const double OR_PI = 3.141592653589793238462643383279502884; /* Kokkos::numbers::pi */
 /* Kokkos::numbers::pi */
 static const double PI = 3.141592653589793238462643383279502884;
 
@@ -370,8 +371,9 @@ static inline long IDX(const or_ctx* c, int i, int j, int k)
 
 static inline double gravity_at(const or_ctx* c, int i, int dir)
 {
-    /* gravity.hpp:36-40 (uniform) and :63-70 (point mass) */
-    if (c->gravity == OR_GRAV_POINT_MASS) {
+    /* gravity.hpp:36-40 (uniform), :63-70 (point mass) and the same radial
+       table for the internal mass */
+    if (c->gravity != OR_GRAV_UNIFORM) {
         return dir == 0 ? c->g_r[i] : 0;
     }
     return c->g[dir];
@@ -474,7 +476,7 @@ static int ctx_alloc(or_ctx* c, int ndim, const int nx[3], int ng, int nfx, int 
     }
     c->ds = (double*)calloc((size_t)N * 3, sizeof(double));
     c->dv = (double*)calloc((size_t)N, sizeof(double));
-    if (gravity == OR_GRAV_POINT_MASS) {
+    if (gravity != OR_GRAV_UNIFORM) {
         c->g_r = (double*)calloc((size_t)c->n[0], sizeof(double));
     }
     return 0;
@@ -1022,6 +1024,55 @@ static void copy_cell(const or_ctx* c, double* rho, double* rhou, double* E, dou
  * from a blend of the Godunov increment and a pressure-work estimate from the
  * face velocities.  The loops and the overwrite of E_new inside the inner loop
  * follow the reference. */
+void or_internal_mass_gravity(const or_ctx* c, const double* rho)
+{
+    /* gravity.cpp:59-128 on one rank.  Shells: the nx0 interior cells of
+       dimension 0 and the ng ghost cells after them (offset i + ng).  Sums
+       over the interior (j, k), j outer and k inner (Kokkos' default
+       right-most-fastest MDRange order; the reference's threaded reduction
+       may associate differently). */
+    const int ng = c->ng;
+    const int nsh = c->nx[0] + ng;
+    const int g1 = c->ndim >= 2 ? ng : 0;
+    const int g2 = c->ndim >= 3 ? ng : 0;
+    double* rho_mean = (double*)calloc((size_t)nsh, sizeof(double));
+    for (int i = 0; i < nsh; ++i) {
+        double sm = 0;
+        double sd = 0;
+        for (int j = 0; j < c->nx[1]; ++j) {
+            for (int k = 0; k < c->nx[2]; ++k) {
+                const long id = IDX(c, i + ng, j + g1, k + g2);
+                sm += rho[id] * c->dv[id];
+                sd += c->dv[id];
+            }
+        }
+        rho_mean[i] = sm / sd; /* :96-100 */
+    }
+    const double* x0 = c->x[0];
+    const double* xc = c->xc[0];
+    const double vol_s3 = 4 * OR_PI / 3;
+    double* M = c->g_r; /* the enclosed mass first, then g in place */
+    for (int i = 0; i < ng; ++i) {
+        M[i] = c->central_mass; /* :102 */
+    }
+    double partial = 0; /* :104-120, a sequential running sum */
+    for (int i = ng; i < c->nx[0] + 2 * ng; ++i) {
+        const int off = i - ng;
+        const double x3 = x0[i] * x0[i] * x0[i];
+        if (i == ng) {
+            partial += c->central_mass + (vol_s3 * ((xc[i] * xc[i] * xc[i]) - x3) * rho_mean[off]);
+        } else {
+            partial += (vol_s3 * (x3 - (xc[i - 1] * xc[i - 1] * xc[i - 1])) * rho_mean[off - 1])
+                       + (vol_s3 * ((xc[i] * xc[i] * xc[i]) - x3) * rho_mean[off]);
+        }
+        M[i] = partial;
+    }
+    for (int i = 0; i < c->n[0]; ++i) {
+        M[i] = -GRAV_G * M[i] / (xc[i] * xc[i]); /* :122-125 */
+    }
+    free(rho_mean);
+}
+
 void or_pressure_fix(const or_ctx* c, double dt, double eps, const double* rho, const double* rhou, const double* E,
                      const double* rho_rec, const double* rhou_rec, const double* E_rec, const double* rho_new,
                      const double* rhou_new, double* E_new)
@@ -1329,7 +1380,10 @@ int or_run(const or_ctx* c, double* rho, double* rhou, double* E, double* fx, co
         ++iter_output_id;
     }
 
-    /* main.cpp:311 */
+    /* main.cpp:309-311 */
+    if (c->gravity == OR_GRAV_INTERNAL_MASS) {
+        or_internal_mass_gravity(c, rho);
+    }
     or_conv_cons_to_prim(c, c->ng, rho, rhou, E, u, P);
     res->initial_mass = or_integrate(c, rho);
 
@@ -1385,6 +1439,9 @@ int or_run(const or_ctx* c, double* rho, double* rhou, double* E, double* fx, co
             memcpy(fx, fx_new, sizeof(double) * (size_t)N * nfx);
         }
         or_conv_cons_to_prim(c, c->ng, rho, rhou, E, u, P); /* :526 */
+        if (c->gravity == OR_GRAV_INTERNAL_MASS) {
+            or_internal_mass_gravity(c, rho); /* :528 */
+        }
         t += dt;                                             /* :530-531 */
         ++iter;
     }

@@ -31,7 +31,7 @@ enum { OR_LIM_CONSTANT = 0, OR_LIM_VANLEER = 1, OR_LIM_MINMOD = 2, OR_LIM_VANALB
 enum { OR_RS_HLL = 0, OR_RS_HLLC = 1, OR_RS_SPLITTING = 2 };
 enum { OR_BC_NULLGRADIENT = 0, OR_BC_PERIODIC = 1, OR_BC_REFLEXIVE = 2 };
 enum { OR_GEOM_CARTESIAN = 0, OR_GEOM_SPHERICAL = 1 };
-enum { OR_GRAV_UNIFORM = 0, OR_GRAV_POINT_MASS = 1 };
+enum { OR_GRAV_UNIFORM = 0, OR_GRAV_POINT_MASS = 1, OR_GRAV_INTERNAL_MASS = 2 };
 
 /* Everything the reference keeps in Grid, EOS, Gravity and the factories. */
 typedef struct or_ctx {
@@ -54,7 +54,7 @@ typedef struct or_ctx {
     double *xc[3];     /* n[d] */
     double *ds;        /* N*3 */
     double *dv;        /* N */
-    double *g_r;       /* PointMassGravity g(i), n[0] (NULL for uniform) */
+    double *g_r;       /* PointMassGravity / InternalMassGravity g(i), n[0] (NULL for uniform) */
 } or_ctx;
 
 /* ---- grid / context -------------------------------------------------- */
@@ -140,6 +140,10 @@ int or_run(const or_ctx* c, double* rho, double* rhou, double* E, double* fx, co
            or_run_result* r, double* dts_out);
 
 /* pressure_fix.hpp:19-172 on no_ghosts; updates E_new in place. */
+/* InternalMassGravity (gravity.cpp:59-128) on one rank: recomputes c->g_r
+ * from the density rho (shell means over the interior (j, k), enclosed mass at
+ * the cell centres by a running sum from the central mass). */
+void or_internal_mass_gravity(const or_ctx* c, const double* rho);
 void or_pressure_fix(const or_ctx* c, double dt, double eps, const double* rho, const double* rhou, const double* E,
                      const double* rho_rec, const double* rhou_rec, const double* E_rec, const double* rho_new,
                      const double* rhou_new, double* E_new);

@@ -21,7 +21,7 @@ LIMITERS = {"Constant": 0, "VanLeer": 1, "Minmod": 2, "VanAlbada": 3}
 RIEMANN = {"HLL": 0, "HLLC": 1, "Low Mach": 2}
 BCS = {"NullGradient": 0, "Periodic": 1, "Reflexive": 2}
 GEOMS = {"Cartesian": 0, "Spherical": 1}
-GRAVITY = {"Uniform": 0, "Point_mass": 1}
+GRAVITY = {"Uniform": 0, "Point_mass": 1, "Internal_mass": 2}
 
 _dp = C.POINTER(C.c_double)
 
@@ -136,6 +136,7 @@ def _lib():
         lib.or_godunov.argtypes = [C.POINTER(_Ctx), C.c_int, C.c_double] + [vp] * 12
         lib.or_boundaries.argtypes = [C.POINTER(_Ctx), vp, vp, vp, vp]
         lib.or_pressure_fix.argtypes = [C.POINTER(_Ctx), C.c_double, C.c_double] + [vp] * 9
+        lib.or_internal_mass_gravity.argtypes = [C.POINTER(_Ctx), vp]
         lib.or_time_step.argtypes = [C.POINTER(_Ctx), C.c_int, vp, vp, vp]
         lib.or_time_step.restype = C.c_double
         lib.or_min_internal_energy.argtypes = [C.POINTER(_Ctx), vp, vp, vp]
@@ -323,6 +324,17 @@ class Oracle:
         self.lib.or_pressure_fix(C.byref(self.ctx), dt, eps, _p(rho), _p(rhou), _p(E), _p(rho_rec), _p(rhou_rec),
                                  _p(E_rec), _p(rho_new), _p(rhou_new), _p(E_new))
         return E_new
+
+    def internal_mass_gravity(self, rho):
+        """Recomputes the radial gravity table from rho (gravity.cpp:59-128) and
+        returns a copy of it (g along dimension 0 per x0 index, ghosts included)."""
+        self.lib.or_internal_mass_gravity(C.byref(self.ctx), _p(rho))
+        return self.gravity_table()
+
+    def gravity_table(self):
+        """Copy of the radial gravity table g(i) (point-mass and internal-mass gravity)."""
+        n0 = self.ctx.n[0]
+        return np.ctypeslib.as_array(self.ctx.g_r, shape=(n0,)).copy()
 
     def boundaries(self, rho, rhou, E, fx=None):
         if fx is None:

@@ -37,6 +37,15 @@ CASES = {
     "sph_1d_pointmass": (1, [96], dict(gamma=1.4, limiter="VanLeer", riemann="HLLC", geometry="Spherical",
                                        bc=["Reflexive", "NullGradient"], gravity="Point_mass", central_mass=1e8,
                                        xmin=(0.2, 0.0, 0.0), xmax=(1.2, 1.0, 1.0)), "shock_tube", {"inter": 0.7}),
+    "sph_1d_internalmass": (1, [96], dict(gamma=1.4, limiter="VanLeer", riemann="HLLC", geometry="Spherical",
+                                          bc=["Reflexive", "NullGradient"], gravity="Internal_mass",
+                                          central_mass=1e8, xmin=(0.2, 0.0, 0.0), xmax=(1.2, 1.0, 1.0)),
+                            "shock_tube", {"inter": 0.7}),
+    "sph_2d_internalmass": (2, [40, 24], dict(gamma=1.4, limiter="Minmod", riemann="HLLC", geometry="Spherical",
+                                              bc=["Reflexive", "NullGradient", "Reflexive", "Reflexive"],
+                                              gravity="Internal_mass", central_mass=3e7,
+                                              xmin=(0.2, 0.5, 0.0), xmax=(1.0, 2.6, 1.0)),
+                            "shock_tube", {"inter": 0.6}),
     "sph_2d": (2, [40, 24], dict(gamma=1.4, limiter="Minmod", riemann="HLLC", geometry="Spherical",
                                  bc=["Reflexive", "NullGradient", "Reflexive", "Reflexive"],
                                  xmin=(0.2, 0.5, 0.0), xmax=(1.0, 2.6, 1.0)), "shock_tube", {"inter": 0.6}),

@@ -47,6 +47,14 @@ def test_stage_entry_points_bitwise(name):
     nd = o.ndim
     rho, rhou, E, _ = o.init_from_prim(rho0, u0, P0)
     ng = 2
+    if CASES[name][2].get("gravity") == "Internal_mass":
+        # make_internal_mass_gravity from this state: the radial table the
+        # reconstruction and Godunov stages below use
+        g_o = o.internal_mass_gravity(rho)
+        t_g = torch.zeros(g_o.shape, dtype=torch.float64, device="cuda")
+        d.internal_mass_gravity(_dev(rho), t_g)
+        torch.cuda.synchronize()
+        assert np.array_equal(_host(t_g), g_o)
     # cons -> prim on all_ghosts
     u_o, P_o = o.conv_cons_to_prim(ng, rho, rhou, E)
     t_rho, t_rhou, t_E = _dev(rho), _dev(rhou), _dev(E)
@@ -98,7 +106,7 @@ def test_stage_entry_points_bitwise(name):
 
 NSTEPS = {"sod_1d": 200, "sod_1d_odd": 60, "advection_1d": 100, "kh_2d": 60, "kh_2d_ragged": 40, "quad_2d": 40,
           "gresho_2d_lowmach": 30, "rt_3d": 12, "rt_3d_ragged": 10, "rt_3d_hllc": 10, "sph_1d_pointmass": 50,
-          "sph_2d": 25, "sph_3d": 8}
+          "sph_2d": 25, "sph_3d": 8, "sph_1d_internalmass": 50, "sph_2d_internalmass": 25}
 
 
 @pytest.mark.parametrize("name", ALL)
@@ -137,7 +145,7 @@ def test_sod_to_t_end_bitwise():
 
 
 @pytest.mark.parametrize("name,tol", [("kh_2d", 1e-6), ("sod_1d", 2e-6), ("rt_3d", 1e-6), ("quad_2d", 1e-5),
-                                      ("sph_2d", 1e-5)])
+                                      ("sph_2d", 1e-5), ("sph_1d_internalmass", 2e-6)])
 def test_fused_mixed_l1(name, tol):
     """FP32-mixed against the FP64 oracle with the same dt sequence."""
     o, d, (rho0, u0, P0) = make_pair(name, "fp32_mixed")
