@@ -13,7 +13,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._native import (BCS, GEOMS, GRAVITY, LIMITERS, PRECISION, RIEMANN, Config, DomainError, HclError,
+from ._native import (BCS, EOS, GEOMS, GRAVITY, LIMITERS, PRECISION, RIEMANN, Config, DomainError, HclError,
                       RunParams, RunResult, check, lib)
 
 __all__ = ["Domain", "Ensemble", "make_config", "HclError", "DomainError", "lib", "kernel_launch_count"]
@@ -44,7 +44,7 @@ def _ptr(t):
 def make_config(ndim, nx, *, nghost=2, nfx=0, geometry="Cartesian", gamma=5.0 / 3.0, mmw=1.0, limiter="VanLeer",
                 riemann="HLL", bc=("Periodic",) * 6, gravity="Uniform", g=(0.0, 0.0, 0.0), central_mass=1.0,
                 xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0), nodes=None, precision="fp64", device=0,
-                pressure_fix=False, eps_pf=1e-6):
+                pressure_fix=False, eps_pf=1e-6, eos="PerfectGas"):
     """hcl_config from the reference's plugin keys; returns (config, node arrays kept alive)."""
     L = lib()
     cfg = Config()
@@ -72,6 +72,7 @@ def make_config(ndim, nx, *, nghost=2, nfx=0, geometry="Cartesian", gamma=5.0 / 
     cfg.device = int(device)
     cfg.pressure_fix = 1 if pressure_fix else 0
     cfg.eps_pf = float(eps_pf)
+    cfg.eos = _key(EOS, eos, "eos")
     _nodes = None
     if nodes is not None:
         _nodes = [np.ascontiguousarray(x, dtype=np.float64) for x in nodes]
@@ -86,12 +87,12 @@ class Domain:
     def __init__(self, ndim, nx, *, nghost=2, nfx=0, geometry="Cartesian", gamma=5.0 / 3.0, mmw=1.0,
                  limiter="VanLeer", riemann="HLL", bc=("Periodic",) * 6, gravity="Uniform", g=(0.0, 0.0, 0.0),
                  central_mass=1.0, xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0), nodes=None, precision="fp64",
-                 device=0, pressure_fix=False, eps_pf=1e-6):
+                 device=0, pressure_fix=False, eps_pf=1e-6, eos="PerfectGas"):
         cfg, self._nodes = make_config(ndim, nx, nghost=nghost, nfx=nfx, geometry=geometry, gamma=gamma, mmw=mmw,
                                        limiter=limiter, riemann=riemann, bc=bc, gravity=gravity, g=g,
                                        central_mass=central_mass, xmin=xmin, xmax=xmax, nodes=nodes,
                                        precision=precision, device=device, pressure_fix=pressure_fix,
-                                       eps_pf=eps_pf)
+                                       eps_pf=eps_pf, eos=eos)
         h = C.c_void_p()
         check(lib().hcl_create(C.byref(cfg), C.byref(h)))
         self._owned = True

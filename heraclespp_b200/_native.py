@@ -24,6 +24,7 @@ RIEMANN = {"HLL": 0, "HLLC": 1, "Low Mach": 2}
 BCS = {"NullGradient": 0, "Periodic": 1, "Reflexive": 2}
 GEOMS = {"Cartesian": 0, "Spherical": 1}
 GRAVITY = {"Uniform": 0, "Point_mass": 1, "Internal_mass": 2}
+EOS = {"PerfectGas": 0, "RadGas": 1}
 PRECISION = {"fp64": 0, "fp32_mixed": 1}
 
 # Every entry point declared in include/heracles_b200.h.
@@ -72,6 +73,7 @@ class Config(C.Structure):
         ("device", C.c_int),
         ("pressure_fix", C.c_int),
         ("eps_pf", C.c_double),
+        ("eos", C.c_int),
     ]
 
 

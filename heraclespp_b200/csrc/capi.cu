@@ -327,6 +327,7 @@ void build_grid_host(hcl_handle* h)
     g.gamma = c.gamma;
     g.gamma_m1 = c.gamma - 1;
     g.mmw = c.mmw;
+    g.eos = c.eos;
     // uniform Cartesian spacing (to 1e-12 relative) enables the fast forms of
     // the mixed kernel
     int uniform = c.geometry == HCL_GEOM_CARTESIAN;
@@ -394,6 +395,13 @@ int validate(const hcl_config* c)
     }
     if (c->precision != HCL_FP64 && c->precision != HCL_FP32_MIXED) {
         return fail(HCL_ERR_CONFIG, "Unknown precision id %d", c->precision);
+    }
+    if (c->eos != HCL_EOS_PERFECT_GAS && c->eos != HCL_EOS_RAD_GAS) {
+        return fail(HCL_ERR_CONFIG, "Unknown eos id %d", c->eos);
+    }
+    if (c->eos == HCL_EOS_RAD_GAS && c->precision != HCL_FP64) {
+        // the FP32-mixed kernels use the perfect-gas algebra (P = (gamma-1) e)
+        return fail(HCL_ERR_CONFIG, "the RadGas EOS needs precision HCL_FP64");
     }
     if (c->nfx < 0) {
         return fail(HCL_ERR_CONFIG, "nfx must be >= 0");
@@ -663,6 +671,7 @@ void hcl_config_default(hcl_config* c)
     c->device = 0;
     c->pressure_fix = 0;
     c->eps_pf = 0.000001;
+    c->eos = HCL_EOS_PERFECT_GAS;
 }
 
 int hcl_create(const hcl_config* cfg, hcl_handle** out)
@@ -1646,9 +1655,9 @@ int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p)
     }
     const GridDev& g = h->g;
     if (g.geom != HCL_GEOM_CARTESIAN || !g.uniform_cart || g.gravity != HCL_GRAVITY_UNIFORM ||
-        g.riemann == HCL_RIEMANN_LOW_MACH || g.nfx > 0 || h->cfg.pressure_fix) {
-        return fail(HCL_ERR_CONFIG,
-                    "the adjoint supports Cartesian uniform grids, uniform gravity, HLL/HLLC, nfx = 0, no pressure fix");
+        g.riemann == HCL_RIEMANN_LOW_MACH || g.nfx > 0 || h->cfg.pressure_fix || g.eos != HCL_EOS_PERFECT_GAS) {
+        return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian uniform grids, uniform gravity, HLL/HLLC, nfx = 0, "
+                                    "no pressure fix, the perfect-gas EOS");
     }
     int rc;
     StepCtl ctl;

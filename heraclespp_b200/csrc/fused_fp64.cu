@@ -62,7 +62,7 @@ __device__ __forceinline__ double warp_max(double v)
 template <int ND>
 __global__ void k_prologue(GridDev g, StateDev st, StepCtl* ctl)
 {
-    const exact::Eos eos{g.gamma, g.gamma_m1, g.mmw};
+    const exact::Eos eos = exact::eos_of(g);
     double local = 0;
     bool nan_seen = false;
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < g.N; c += (int64_t)gridDim.x * blockDim.x) {

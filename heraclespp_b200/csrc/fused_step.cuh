@@ -385,7 +385,7 @@ k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp
         nvalid[d] = d < ND ? min(tdim, g.nx[d] - t0[d]) : 1;
     }
 
-    const exact::Eos eeos{g.gamma, g.gamma_m1, g.mmw};
+    const exact::Eos eeos = exact::eos_of(g);
     const fast::Eos feos{(float)g.gamma, (float)g.gamma_m1, (float)(1.0 / g.gamma_m1)};
 
     // ---- phase 1: state tile + halo -> primitives --------------------------

@@ -14,12 +14,17 @@ constexpr double kKb = 1.380649E-23;
 constexpr double kMp = 1.672649E-27;
 constexpr double kG = 6.6743015E-11;
 constexpr double kPi = 3.141592653589793238462643383279502884;
+// radiation constant, units.hpp:69-74 (Joule, m, K are 1 there)
+constexpr double kAr = (8 * (kPi * kPi * kPi * kPi * kPi) * (kKb * kKb * kKb * kKb)) /
+                       (15 * (6.62607015E-34 * 6.62607015E-34 * 6.62607015E-34) *
+                        ((2.99792458E8 * 2.99792458E8) * 2.99792458E8));
 
 enum : int { LIM_CONSTANT = 0, LIM_VANLEER = 1, LIM_MINMOD = 2, LIM_VANALBADA = 3 };
 enum : int { RS_HLL = 0, RS_HLLC = 1, RS_SPLITTING = 2 };
 enum : int { BC_NULLGRADIENT = 0, BC_PERIODIC = 1, BC_REFLEXIVE = 2 };
 enum : int { GEOM_CARTESIAN = 0, GEOM_SPHERICAL = 1 };
 enum : int { GRAV_UNIFORM = 0, GRAV_POINT_MASS = 1, GRAV_INTERNAL_MASS = 2 };
+enum : int { EOS_PERFECT_GAS = 0, EOS_RAD_GAS = 1 };
 
 // Everything a kernel needs to know about the grid and the physics plugins.
 // Passed by value (it lives in the kernel parameter space).
@@ -37,6 +42,7 @@ struct GridDev {
     int gravity;
     double g[3];
     double gamma, gamma_m1, mmw;
+    int eos;              // EOS_PERFECT_GAS or EOS_RAD_GAS
     // grid arrays (device)
     const double* x[3];   // nodes (n+1)
     const double* dx[3];  // n

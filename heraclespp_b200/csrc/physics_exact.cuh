@@ -13,7 +13,77 @@ namespace hcl::exact {
 
 struct Eos {
     double gamma, gamma_m1, mmw;
+    int kind; // EOS_PERFECT_GAS or EOS_RAD_GAS
 };
+
+__device__ __forceinline__ Eos eos_of(const GridDev& g)
+{
+    return Eos{g.gamma, g.gamma_m1, g.mmw, g.eos};
+}
+
+// thermodynamics/rad_gas.hpp:47-146: gas plus radiation.  The temperature
+// comes from a Newton iteration (at most 100 steps, stop at |dT| <= 1e-6)
+// started at the larger of the gas-only and radiation-only temperatures.
+namespace rad {
+__device__ __forceinline__ double evol_from_temp(const Eos& e, double rho, double T)
+{
+    const double T4 = T * T * T * T;
+    return (rho * kKb * T / (e.mmw * kMp * e.gamma_m1)) + (kAr * T4);
+}
+__device__ __forceinline__ double pres_from_temp(const Eos& e, double rho, double T)
+{
+    const double T4 = T * T * T * T;
+    return (rho * kKb * T / (e.mmw * kMp)) + (kAr * T4 / 3);
+}
+static __device__ __noinline__ double temp_from_pres(const Eos& e, double rho, double P)
+{
+    const double C1 = rho * kKb / (e.mmw * kMp);
+    const double Tg = P / C1;
+    const double Tr = pow(3 * P / kAr, 1. / 4);
+    double T = Tr > Tg ? Tr : Tg;
+    for (int i = 0; i < 100; ++i) {
+        const double T3 = T * T * T;
+        const double f = (kAr * T3 * T / 3) + (C1 * T) - P;
+        const double df = (4 * kAr * T3 / 3) + C1;
+        const double delta_T = -f / df;
+        T += delta_T;
+        if (fabs(delta_T) <= 1E-6) {
+            break;
+        }
+    }
+    return T;
+}
+static __device__ __noinline__ double temp_from_evol(const Eos& e, double rho, double evol)
+{
+    const double C1 = rho * kKb / (e.mmw * kMp * e.gamma_m1);
+    const double Tg = evol / C1;
+    const double Tr = pow(evol / kAr, 1. / 4);
+    double T = Tr > Tg ? Tr : Tg;
+    for (int i = 0; i < 100; ++i) {
+        const double T3 = T * T * T;
+        const double f = (kAr * T3 * T) + (C1 * T) - evol;
+        const double df = (4 * kAr * T3) + C1;
+        const double delta_T = -f / df;
+        T += delta_T;
+        if (fabs(delta_T) <= 1E-6 || isnan(delta_T)) {
+            break;
+        }
+    }
+    return T;
+}
+static __device__ __noinline__ double sound(const Eos& e, double rho, double P)
+{
+    const double T = temp_from_pres(e, rho, P);
+    const double Pg = rho * kKb * T / (e.mmw * kMp);
+    const double T4 = T * T * T * T;
+    const double Pr = kAr * T4 / 3;
+    const double alpha = Pr / Pg;
+    const double num = (e.gamma / (e.gamma - 1)) + (20 * alpha) + (16 * alpha * alpha);
+    const double den = (1. / (e.gamma - 1)) + (12 * alpha);
+    const double gamma_eff = num / den;
+    return sqrt(gamma_eff * Pg / rho);
+}
+} // namespace rad
 
 // thermodynamics/perfect_gas.hpp:46-83: P <-> e through the temperature.
 __device__ __forceinline__ double temp_from_pres(const Eos& e, double rho, double P)
@@ -34,14 +104,23 @@ __device__ __forceinline__ double temp_from_evol(const Eos& e, double rho, doubl
 }
 __device__ __forceinline__ double evol_from_pres(const Eos& e, double rho, double P)
 {
+    if (e.kind == EOS_RAD_GAS) {
+        return rad::evol_from_temp(e, rho, rad::temp_from_pres(e, rho, P)); // rad_gas.hpp:47-51
+    }
     return evol_from_temp(e, rho, temp_from_pres(e, rho, P));
 }
 __device__ __forceinline__ double pres_from_evol(const Eos& e, double rho, double evol)
 {
+    if (e.kind == EOS_RAD_GAS) {
+        return rad::pres_from_temp(e, rho, rad::temp_from_evol(e, rho, evol)); // rad_gas.hpp:65-69
+    }
     return pres_from_temp(e, rho, temp_from_evol(e, rho, evol));
 }
 __device__ __forceinline__ double sound(const Eos& e, double rho, double P)
 {
+    if (e.kind == EOS_RAD_GAS) {
+        return rad::sound(e, rho, P);
+    }
     return sqrt(e.gamma * P / rho);
 }
 

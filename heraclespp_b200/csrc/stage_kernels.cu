@@ -66,7 +66,7 @@ template <int ND>
 __global__ void k_prim_to_cons(GridDev g, Box bx, const double* __restrict__ rho, const double* __restrict__ u,
                                const double* __restrict__ P, double* __restrict__ rhou, double* __restrict__ E)
 {
-    const exact::Eos eos{g.gamma, g.gamma_m1, g.mmw};
+    const exact::Eos eos = exact::eos_of(g);
     for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < bx.count;
          idx += (int64_t)gridDim.x * blockDim.x) {
         int i, j, k;
@@ -93,7 +93,7 @@ template <int ND>
 __global__ void k_cons_to_prim(GridDev g, Box bx, const double* __restrict__ rho, const double* __restrict__ rhou,
                                const double* __restrict__ E, double* __restrict__ u, double* __restrict__ P)
 {
-    const exact::Eos eos{g.gamma, g.gamma_m1, g.mmw};
+    const exact::Eos eos = exact::eos_of(g);
     for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < bx.count;
          idx += (int64_t)gridDim.x * blockDim.x) {
         int i, j, k;
@@ -147,7 +147,7 @@ __global__ void k_faces_prim_to_cons(GridDev g, Box bx, const double* __restrict
                                      const double* __restrict__ u_rec, const double* __restrict__ P_rec,
                                      double* __restrict__ rhou_rec, double* __restrict__ E_rec)
 {
-    const exact::Eos eos{g.gamma, g.gamma_m1, g.mmw};
+    const exact::Eos eos = exact::eos_of(g);
     const int64_t S5 = 2 * g.N;
     const int64_t S6 = 2 * g.N * ND;
     for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < bx.count;
@@ -184,7 +184,7 @@ __global__ void k_hancock(GridDev g, Box bx, double dt, const double* __restrict
                           const double* __restrict__ P_rec, double* __restrict__ rho_rec, double* __restrict__ rhou_rec,
                           double* __restrict__ E_rec, double* __restrict__ fx_rec, const double* __restrict__ fx_rec_old)
 {
-    const exact::Eos eos{g.gamma, g.gamma_m1, g.mmw};
+    const exact::Eos eos = exact::eos_of(g);
     const int64_t N = g.N;
     const int64_t S5 = 2 * N;
     const int64_t S6 = 2 * N * ND;
@@ -348,7 +348,7 @@ __global__ void k_godunov(GridDev g, Box bx, double dt, const double* __restrict
                           double* __restrict__ rho_new, double* __restrict__ rhou_new, double* __restrict__ E_new,
                           double* __restrict__ fx_new)
 {
-    const exact::Eos eos{g.gamma, g.gamma_m1, g.mmw};
+    const exact::Eos eos = exact::eos_of(g);
     const int64_t N = g.N;
     const int64_t S5 = 2 * N;
     const int64_t S6 = 2 * N * ND;
@@ -470,7 +470,7 @@ __global__ void k_pressure_fix(GridDev g, Box bx, double dt, double eps, const d
                                const double* __restrict__ E_rec, const double* __restrict__ rho_new,
                                const double* __restrict__ rhou_new, double* __restrict__ E_new)
 {
-    const exact::Eos eos{g.gamma, g.gamma_m1, g.mmw};
+    const exact::Eos eos = exact::eos_of(g);
     const int64_t N = g.N;
     const int64_t S5 = 2 * N;
     const int64_t S6 = 2 * N * ND;
@@ -631,7 +631,7 @@ template <int ND>
 __global__ void k_time_step(GridDev g, Box bx, const double* __restrict__ rho, const double* __restrict__ u,
                             const double* __restrict__ P, unsigned long long* inv_bits)
 {
-    const exact::Eos eos{g.gamma, g.gamma_m1, g.mmw};
+    const exact::Eos eos = exact::eos_of(g);
     double local = 0;
     bool has_nan = false;
     for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < bx.count;

@@ -58,6 +58,7 @@ int hcl_create_from_ini(const char* ini_path, const hcl_build_options* opt, hcl_
             ndim = param.Nx_glob_ng[2] > 1 ? 3 : (param.Nx_glob_ng[1] > 1 ? 2 : 1);
         }
         hcl_config cfg = make_config(reader, param, ndim, opt->geometry, opt->gravity, opt->precision, opt->device);
+        cfg.eos = opt->eos;
         int rc = hcl_create(&cfg, &h);
         if (rc) {
             return rc;

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define HCL_ABI_VERSION 2
+#define HCL_ABI_VERSION 3
 
 /* ---- status codes ------------------------------------------------------ */
 enum hcl_status {
@@ -77,6 +77,10 @@ enum hcl_precision {
     HCL_FP32_MIXED = 1         /* FP32 prim/slopes/faces/fluxes, FP64 state, energy recovery, dt, sums */
 };
 enum hcl_memory { HCL_HOST = 0, HCL_DEVICE = 1 };
+enum hcl_eos { /* eos.hpp.in, selected at CMake time in the reference */
+    HCL_EOS_PERFECT_GAS = 0, /* thermodynamics/perfect_gas.hpp */
+    HCL_EOS_RAD_GAS = 1      /* thermodynamics/rad_gas.hpp: gas plus radiation (FP64 precision only) */
+};
 
 /* ---- configuration ------------------------------------------------------ */
 /* Everything Param (utils/param.cpp:14-73), Grid (mesh/grid.cpp:48-76), the
@@ -103,6 +107,7 @@ typedef struct hcl_config {
     int device;               /* CUDA device ordinal */
     int pressure_fix;         /* [Pressure fix] pressure_fix == "On" (main.cpp:459-474) */
     double eps_pf;            /* [Pressure fix] eps_pf */
+    int eos;                  /* enum hcl_eos ([Perfect Gas] gamma and mu serve both) */
 } hcl_config;
 
 typedef struct hcl_handle hcl_handle;
@@ -370,6 +375,7 @@ typedef struct hcl_build_options {
     int precision;            /* enum hcl_precision */
     int device;
     const char* setup;        /* setup plugin name, e.g. "shock_tube" */
+    int eos;                  /* enum hcl_eos */
 } hcl_build_options;
 
 /* Initial primitives of a setup plugin (InitializationSetup::execute,

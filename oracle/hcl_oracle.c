@@ -72,16 +72,109 @@ static inline double temp_from_evol(const or_ctx* c, double rho, double evol)
 {
     return evol * c->mmw * MP * c->gamma_m1 / (rho * KB); /* :74-78 */
 }
+
+/* ------------------------------------------------------------------ */
+/* EOS: thermodynamics/rad_gas.hpp:47-141 (gas plus radiation)          */
+/* ------------------------------------------------------------------ */
+/* units.hpp:69-74 (Joule, m, K are 1 there) */
+#define OR_PI5 (3.141592653589793238462643383279502884 * 3.141592653589793238462643383279502884 * \
+                3.141592653589793238462643383279502884 * 3.141592653589793238462643383279502884 * \
+                3.141592653589793238462643383279502884)
+#define OR_KB4 (1.380649E-23 * 1.380649E-23 * 1.380649E-23 * 1.380649E-23)
+#define OR_HPLANCK3 (6.62607015E-34 * 6.62607015E-34 * 6.62607015E-34)
+#define OR_C3 ((2.99792458E8 * 2.99792458E8) * 2.99792458E8)
+static const double AR = (8 * OR_PI5 * OR_KB4) / (15 * OR_HPLANCK3 * OR_C3); /* radiation constant */
+
+static double rad_evol_from_temp(const or_ctx* c, double rho, double T)
+{
+    const double T4 = T * T * T * T; /* :58-63 */
+    return (rho * KB * T / (c->mmw * MP * c->gamma_m1)) + (AR * T4);
+}
+static double rad_pres_from_temp(const or_ctx* c, double rho, double T)
+{
+    const double T4 = T * T * T * T; /* :71-75 */
+    return (rho * KB * T / (c->mmw * MP)) + (AR * T4 / 3);
+}
+static double rad_temp_from_pres(const or_ctx* c, double rho, double P)
+{
+    /* :77-104: Newton from the larger of the gas-only and radiation-only
+       temperatures, at most 100 steps, stop when |dT| <= 1e-6 */
+    const double C1 = rho * KB / (c->mmw * MP);
+    const double Tg = P / C1;
+    const double Tr = pow(3 * P / AR, 1. / 4);
+    double T = Tr > Tg ? Tr : Tg;
+    for (int i = 0; i < 100; ++i) {
+        const double T3 = T * T * T;
+        const double f = (AR * T3 * T / 3) + (C1 * T) - P;
+        const double df = (4 * AR * T3 / 3) + C1;
+        const double delta_T = -f / df;
+        T += delta_T;
+        if (fabs(delta_T) <= 1E-6) {
+            break;
+        }
+    }
+    return T;
+}
+static double rad_temp_from_evol(const or_ctx* c, double rho, double evol)
+{
+    /* :106-133: as above on evol = rho eint; also stops on a NaN step */
+    const double C1 = rho * KB / (c->mmw * MP * c->gamma_m1);
+    const double Tg = evol / C1;
+    const double Tr = pow(evol / AR, 1. / 4);
+    double T = Tr > Tg ? Tr : Tg;
+    for (int i = 0; i < 100; ++i) {
+        const double T3 = T * T * T;
+        const double f = (AR * T3 * T) + (C1 * T) - evol;
+        const double df = (4 * AR * T3) + C1;
+        const double delta_T = -f / df;
+        T += delta_T;
+        if (fabs(delta_T) <= 1E-6 || isnan(delta_T)) {
+            break;
+        }
+    }
+    return T;
+}
+static double rad_speed_of_sound(const or_ctx* c, double rho, double P)
+{
+    /* :135-146: effective adiabatic index of the gas-radiation mixture */
+    const double T = rad_temp_from_pres(c, rho, P);
+    const double Pg = rho * KB * T / (c->mmw * MP);
+    const double T4 = T * T * T * T;
+    const double Pr = AR * T4 / 3;
+    const double alpha = Pr / Pg;
+    const double num = (c->gamma / (c->gamma - 1)) + (20 * alpha) + (16 * alpha * alpha);
+    const double den = (1. / (c->gamma - 1)) + (12 * alpha);
+    const double gamma_eff = num / den;
+    return sqrt(gamma_eff * Pg / rho);
+}
+
+void or_set_eos(or_ctx* c, int eos)
+{
+    c->eos = eos;
+}
+double or_temperature(const or_ctx* c, double rho, double P)
+{
+    return c->eos == OR_EOS_RAD_GAS ? rad_temp_from_pres(c, rho, P) : temp_from_pres(c, rho, P);
+}
 double or_evol_from_pres(const or_ctx* c, double rho, double P)
 {
+    if (c->eos == OR_EOS_RAD_GAS) {
+        return rad_evol_from_temp(c, rho, rad_temp_from_pres(c, rho, P)); /* rad_gas.hpp:47-51 */
+    }
     return evol_from_temp(c, rho, temp_from_pres(c, rho, P)); /* :46-50 */
 }
 double or_pres_from_evol(const or_ctx* c, double rho, double evol)
 {
+    if (c->eos == OR_EOS_RAD_GAS) {
+        return rad_pres_from_temp(c, rho, rad_temp_from_evol(c, rho, evol)); /* rad_gas.hpp:65-69 */
+    }
     return pres_from_temp(c, rho, temp_from_evol(c, rho, evol)); /* :58-62 */
 }
 double or_speed_of_sound(const or_ctx* c, double rho, double P)
 {
+    if (c->eos == OR_EOS_RAD_GAS) {
+        return rad_speed_of_sound(c, rho, P);
+    }
     return sqrt(c->gamma * P / rho); /* :80-83 */
 }
 int or_eos_valid(double rho, double P)

@@ -32,6 +32,7 @@ enum { OR_RS_HLL = 0, OR_RS_HLLC = 1, OR_RS_SPLITTING = 2 };
 enum { OR_BC_NULLGRADIENT = 0, OR_BC_PERIODIC = 1, OR_BC_REFLEXIVE = 2 };
 enum { OR_GEOM_CARTESIAN = 0, OR_GEOM_SPHERICAL = 1 };
 enum { OR_GRAV_UNIFORM = 0, OR_GRAV_POINT_MASS = 1, OR_GRAV_INTERNAL_MASS = 2 };
+enum { OR_EOS_PERFECT_GAS = 0, OR_EOS_RAD_GAS = 1 };
 
 /* Everything the reference keeps in Grid, EOS, Gravity and the factories. */
 typedef struct or_ctx {
@@ -55,6 +56,7 @@ typedef struct or_ctx {
     double *ds;        /* N*3 */
     double *dv;        /* N */
     double *g_r;       /* PointMassGravity / InternalMassGravity g(i), n[0] (NULL for uniform) */
+    int eos;           /* OR_EOS_PERFECT_GAS or OR_EOS_RAD_GAS (eos.hpp.in) */
 } or_ctx;
 
 /* ---- grid / context -------------------------------------------------- */
@@ -90,6 +92,11 @@ double or_speed_of_sound(const or_ctx* c, double rho, double P);             /* 
 double or_evol_from_pres(const or_ctx* c, double rho, double P);             /* perfect_gas.hpp:46-50 */
 double or_pres_from_evol(const or_ctx* c, double rho, double evol);          /* perfect_gas.hpp:58-62 */
 int or_eos_valid(double rho, double P);                                      /* perfect_gas.hpp:85-89 */
+/* selects the EOS of a context (PerfectGas after or_create); RadGas:
+ * thermodynamics/rad_gas.hpp:47-141 with the constructor checks of
+ * rad_gas.cpp:13-22, which are the PerfectGas ones */
+void or_set_eos(or_ctx* c, int eos);
+double or_temperature(const or_ctx* c, double rho, double P);                /* compute_temp_from_pres */
 
 /* ---- array kernels ---------------------------------------------------- */
 /* ng_eff selects Range::with_ghosts(ng_eff) (range.cpp:367-403). */

@@ -22,6 +22,7 @@ RIEMANN = {"HLL": 0, "HLLC": 1, "Low Mach": 2}
 BCS = {"NullGradient": 0, "Periodic": 1, "Reflexive": 2}
 GEOMS = {"Cartesian": 0, "Spherical": 1}
 GRAVITY = {"Uniform": 0, "Point_mass": 1, "Internal_mass": 2}
+EOS = {"PerfectGas": 0, "RadGas": 1}
 
 _dp = C.POINTER(C.c_double)
 
@@ -50,6 +51,7 @@ class _Ctx(C.Structure):
         ("ds", _dp),
         ("dv", _dp),
         ("g_r", _dp),
+        ("eos", C.c_int),
     ]
 
 
@@ -137,6 +139,9 @@ def _lib():
         lib.or_boundaries.argtypes = [C.POINTER(_Ctx), vp, vp, vp, vp]
         lib.or_pressure_fix.argtypes = [C.POINTER(_Ctx), C.c_double, C.c_double] + [vp] * 9
         lib.or_internal_mass_gravity.argtypes = [C.POINTER(_Ctx), vp]
+        lib.or_set_eos.argtypes = [C.POINTER(_Ctx), C.c_int]
+        lib.or_temperature.argtypes = [C.POINTER(_Ctx), C.c_double, C.c_double]
+        lib.or_temperature.restype = C.c_double
         lib.or_time_step.argtypes = [C.POINTER(_Ctx), C.c_int, vp, vp, vp]
         lib.or_time_step.restype = C.c_double
         lib.or_min_internal_energy.argtypes = [C.POINTER(_Ctx), vp, vp, vp]
@@ -170,7 +175,7 @@ class Oracle:
 
     def __init__(self, ndim, nx, *, ng=2, nfx=0, geom="Cartesian", gamma=1.4, mmw=1.0, limiter="VanLeer",
                  riemann="HLLC", bc=("Periodic",) * 6, gravity="Uniform", g=(0.0, 0.0, 0.0), central_mass=1.0,
-                 xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0), nodes=None):
+                 xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0), nodes=None, eos="PerfectGas"):
         self.lib = _lib()
         self.ctx = _Ctx()
         nx3 = (C.c_int * 3)(*[int(v) for v in (list(nx) + [1, 1, 1])[:3]])
@@ -185,6 +190,7 @@ class Oracle:
             rc = self.lib.or_ctx_init_nodes(*args, *[_p(x) for x in self._nodes])
         if rc != 0:
             raise ValueError("Invalid gamma" if rc == -1 else "Invalid mmw")
+        self.lib.or_set_eos(C.byref(self.ctx), _id(EOS, eos))
         self.ndim = int(ndim)
         self.nfx = int(nfx)
         self.n = tuple(self.ctx.n)
@@ -271,6 +277,9 @@ class Oracle:
 
     def eos_valid(self, rho, P):
         return bool(self.lib.or_eos_valid(rho, P))
+
+    def temperature(self, rho, P):
+        return self.lib.or_temperature(C.byref(self.ctx), rho, P)
 
     # ---- arrays --------------------------------------------------------
     def conv_prim_to_cons(self, ng_eff, rho, u, P):
@@ -409,9 +418,13 @@ class RefCell:
         lib.ref_perfect_gas_check.restype = C.c_int
         lib.ref_eos_valid.argtypes = [d, d]
         lib.ref_eos_valid.restype = C.c_int
-        for name in ("ref_evol_from_pres", "ref_pres_from_evol", "ref_speed_of_sound"):
+        for name in ("ref_evol_from_pres", "ref_pres_from_evol", "ref_speed_of_sound", "ref_rad_evol_from_pres",
+                     "ref_rad_pres_from_evol", "ref_rad_speed_of_sound", "ref_rad_temp_from_pres"):
             getattr(lib, name).argtypes = [d, d, d, d]
             getattr(lib, name).restype = d
+        lib.ref_rad_gas_check.argtypes = [d, d]
+        lib.ref_rad_gas_check.restype = C.c_int
+        lib.ref_rad_riemann.argtypes = [C.c_int, d, d, vp, vp, C.c_int, vp]
         lib.ref_to_prim.argtypes = [d, d, vp, vp]
         lib.ref_to_cons.argtypes = [d, d, vp, vp]
         lib.ref_flux_from_prim.argtypes = [d, d, vp, C.c_int, vp]
@@ -460,10 +473,11 @@ class RefCell:
         self.lib.ref_flux_from_cons(gamma, mmw, _p(np.ascontiguousarray(cons, dtype=np.float64)), locdim, _p(out))
         return out
 
-    def riemann(self, solver, gamma, mmw, consL, consR, locdim):
+    def riemann(self, solver, gamma, mmw, consL, consR, locdim, eos="PerfectGas"):
         out = self._vec()
-        self.lib.ref_riemann(_id(RIEMANN, solver), gamma, mmw, _p(np.ascontiguousarray(consL, dtype=np.float64)),
-                             _p(np.ascontiguousarray(consR, dtype=np.float64)), locdim, _p(out))
+        fn = self.lib.ref_rad_riemann if eos == "RadGas" else self.lib.ref_riemann
+        fn(_id(RIEMANN, solver), gamma, mmw, _p(np.ascontiguousarray(consL, dtype=np.float64)),
+           _p(np.ascontiguousarray(consR, dtype=np.float64)), locdim, _p(out))
         return out
 
     def slope(self, limiter, diffR, diffL):

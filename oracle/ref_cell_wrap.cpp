@@ -2,7 +2,8 @@
 // per-cell physics headers, compiled from where they lie in the reference
 // tree (hydro/euler_equations.hpp, hydro/riemann_solver.hpp,
 // hydro/slope_limiters.hpp, hydro/source_terms.hpp,
-// thermodynamics/perfect_gas.hpp + perfect_gas.cpp).
+// thermodynamics/perfect_gas.hpp + perfect_gas.cpp,
+// thermodynamics/rad_gas.hpp + rad_gas.cpp).
 //
 // TEST INFRASTRUCTURE ONLY: built into oracle/_ref/ by oracle/Makefile and
 // used by tests to check the C restatement in hcl_oracle.c bit for bit.
@@ -11,6 +12,7 @@
 
 #include <euler_equations.hpp>
 #include <perfect_gas.hpp>
+#include <rad_gas.hpp>
 #include <riemann_solver.hpp>
 #include <slope_limiters.hpp>
 #include <source_terms.hpp>
@@ -22,6 +24,7 @@ using hclpp::EulerFlux;
 using hclpp::EulerPrim;
 using hclpp::ndim;
 using hclpp::thermodynamics::PerfectGas;
+using hclpp::thermodynamics::RadGas;
 
 EulerCons load_cons(double const* v)
 {
@@ -61,6 +64,30 @@ void store(S const& s, double* v)
     } else {
         v[1 + ndim] = s.P;
     }
+}
+
+} // namespace
+
+namespace {
+
+template <class Eos>
+void riemann_with(int solver, Eos const& eos, double const* consL, double const* consR, int locdim, double* flux)
+{
+    EulerCons const L = load_cons(consL);
+    EulerCons const R = load_cons(consR);
+    EulerFlux f;
+    if (solver == 0) {
+        f = hclpp::HLL()(L, R, locdim, eos);
+    } else if (solver == 1) {
+        f = hclpp::HLLC()(L, R, locdim, eos);
+    } else {
+        f = hclpp::Splitting()(L, R, locdim, eos);
+    }
+    flux[0] = f.rho;
+    for (int d = 0; d < ndim; ++d) {
+        flux[1 + d] = f.rhou[d];
+    }
+    flux[1 + ndim] = f.E;
 }
 
 } // namespace
@@ -142,6 +169,45 @@ double ref_ek_prim(double const* prim)
 double ref_ek_cons(double const* cons)
 {
     return hclpp::compute_ek(load_cons(cons));
+}
+
+// 0 = valid, 1 = std::domain_error from the RadGas constructor
+int ref_rad_gas_check(double gamma, double mmw)
+{
+    try {
+        RadGas const eos(gamma, mmw);
+        (void)eos;
+    } catch (std::domain_error const&) {
+        return 1;
+    }
+    return 0;
+}
+
+double ref_rad_evol_from_pres(double gamma, double mmw, double rho, double P)
+{
+    return RadGas(gamma, mmw).compute_evol_from_pres(rho, P);
+}
+
+double ref_rad_pres_from_evol(double gamma, double mmw, double rho, double evol)
+{
+    return RadGas(gamma, mmw).compute_pres_from_evol(rho, evol);
+}
+
+double ref_rad_speed_of_sound(double gamma, double mmw, double rho, double P)
+{
+    return RadGas(gamma, mmw).compute_speed_of_sound(rho, P);
+}
+
+double ref_rad_temp_from_pres(double gamma, double mmw, double rho, double P)
+{
+    return RadGas(gamma, mmw).compute_temp_from_pres(rho, P);
+}
+
+// the Riemann solvers with the RadGas EOS
+void ref_rad_riemann(int solver, double gamma, double mmw, double const* consL, double const* consR, int locdim,
+                     double* flux)
+{
+    riemann_with(solver, RadGas(gamma, mmw), consL, consR, locdim, flux);
 }
 
 // solver: 0 HLL, 1 HLLC, 2 Splitting ("Low Mach")

@@ -11,6 +11,7 @@ using std::fmax;
 using std::fmin;
 using std::isfinite;
 using std::isnan;
+using std::pow;
 using std::sin;
 using std::sqrt;
 } // namespace Kokkos
