@@ -181,15 +181,18 @@ def adjoint_cost(torch, nsteps=400, n=512, k=32):
     from heraclespp_b200 import Domain, setups
 
     kw = dict(gamma=5.0 / 3.0, limiter="VanLeer", riemann="HLLC", bc=["Periodic"] * 4)
-    out = {"config": f"gresho_vortex_2d_{n}x{n}_{nsteps}steps_checkpoint{k}"}
+    out = {"config": f"gresho_vortex_2d_{n}x{n}_{nsteps}steps_checkpoint{k}", "buffers": "device"}
     for prec in ("fp64", "fp32_mixed"):
         d = Domain(2, [n, n], precision=prec, **kw)
         prim = setups.gresho_vortex(setups.Grid.from_domain(d))
         d.set_state_from_prim(*prim)
         d.run(cfl=0.4, nsteps=nsteps)
         dts = d.dt_log()[:nsteps]
-        lam = np.zeros((4,) + d.shape3)
+        # the final adjoint and the gradient stay on the device, as the state
+        # does in the forward run it is compared with
+        lam = torch.zeros((4,) + d.shape3, dtype=torch.float64, device="cuda")
         lam[0] = 1.0
+        grad = torch.zeros_like(lam)
         stream = torch.cuda.ExternalStream(d.stream_handle())
 
         def timed(fn):
@@ -208,7 +211,7 @@ def adjoint_cost(torch, nsteps=400, n=512, k=32):
         fwd = timed(lambda: d.run(nsteps=nsteps, dts=dts))
         d.set_state_from_prim(*prim)
         adj = timed(lambda: (d.adjoint_forward(nsteps, dts=dts, precision=prec, checkpoint_every=k),
-                             d.adjoint_backward(lam)))
+                             d.adjoint_backward(lam, grad, device=True)))
         out[prec] = {"forward_ms": fwd, "gradient_ms": adj, "adj_over_fwd": adj / fwd}
         d.close()
     return out

@@ -2,6 +2,8 @@
 // reverse sweeps; the stored state and the adjoint state are FP64).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "adjoint_step.cuh"
 #include "stages.hpp"
 
@@ -112,6 +114,28 @@ void zero_ghosts(const GridDev& g, const StateDev& lam, cudaStream_t s)
         k_zero_ghosts<2><<<blocks, 256, 0, s>>>(g, lam);
     } else {
         k_zero_ghosts<3><<<blocks, 256, 0, s>>>(g, lam);
+    }
+    ++g_launches;
+}
+
+void fold_zero(const GridDev& g, const StateDev& lam, double* zero, int64_t zero_count, cudaStream_t s)
+{
+    const int64_t count = (int64_t)g.nx[0] * g.nx[1] * g.nx[2];
+    if (count > (int64_t)0xffffffffll) { // beyond the kernel's 32-bit cell index
+        cudaMemsetAsync(zero, 0, sizeof(double) * (size_t)zero_count, s);
+        fold(g, lam, s);
+        return;
+    }
+    int blocks = (int)((std::max(count, zero_count / 2) + 255) / 256);
+    if (blocks > 148 * 8) {
+        blocks = 148 * 8;
+    }
+    if (g.ndim == 1) {
+        k_fold_ghosts_zero<1><<<blocks, 256, 0, s>>>(g, lam, zero, zero_count);
+    } else if (g.ndim == 2) {
+        k_fold_ghosts_zero<2><<<blocks, 256, 0, s>>>(g, lam, zero, zero_count);
+    } else {
+        k_fold_ghosts_zero<3><<<blocks, 256, 0, s>>>(g, lam, zero, zero_count);
     }
     ++g_launches;
 }

@@ -1870,10 +1870,11 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
         // backward through the segment
         for (int j = len - 1; j >= 0; --j) {
             const int n = first + j;
-            HCL_CUDA(cudaMemsetAsync(lam[cur ^ 1].q, 0, sizeof(double) * sz, s));
+            // lam[cur ^ 1] holds zeros here: from the initial clear, then from the
+            // previous step's fold_zero, which cleared the adjoint it had just read
             hcl::adjoint::step(g, state_at(h->adj_seg, base + j), lam[cur], lam[cur ^ 1], h->adj_dts[n], fp64_sweep,
                                s);
-            hcl::adjoint::fold(g, lam[cur ^ 1], s);
+            hcl::adjoint::fold_zero(g, lam[cur ^ 1], lam[cur].q, (int64_t)sz, s);
             cur ^= 1;
         }
         HCL_CUDA(cudaEventRecord(h->adj_ev_rev[b], s));

@@ -311,7 +311,10 @@ __device__ __forceinline__ void store_images_3d(double* __restrict__ q, int64_t 
 }
 
 // ---------------------------------------------------------------------------
-template <int ND, bool EXACT, int TX, int TY, int TZ>
+// EOSK: the EOS as a compile-time constant (EOS_PERFECT_GAS or EOS_RAD_GAS;
+// the FP32-mixed variant is perfect gas only), so that the FP64 physics
+// carries no run-time EOS branch.
+template <int ND, bool EXACT, int TX, int TY, int TZ, int EOSK = EOS_PERFECT_GAS>
 __global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1))
 k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf)
 {
@@ -385,7 +388,7 @@ k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp
         nvalid[d] = d < ND ? min(tdim, g.nx[d] - t0[d]) : 1;
     }
 
-    const exact::Eos eeos = exact::eos_of(g);
+    const exact::Eos eeos{g.gamma, g.gamma_m1, g.mmw, EOSK};
     const fast::Eos feos{(float)g.gamma, (float)g.gamma_m1, (float)(1.0 / g.gamma_m1)};
 
     // ---- phase 1: state tile + halo -> primitives --------------------------
@@ -1053,6 +1056,10 @@ struct FusedLauncher {
     static void configure()
     {
         cudaFuncSetAttribute(k_fused_step<ND, EXACT, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
+        if constexpr (EXACT) {
+            cudaFuncSetAttribute(k_fused_step<ND, EXACT, TX, TY, TZ, EOS_RAD_GAS>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
+        }
     }
     static void launch(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                        int slot, int out_buf, cudaStream_t s)
@@ -1062,7 +1069,12 @@ struct FusedLauncher {
         const int nt1 = (g.nx[1] + S::T1 - 1) / S::T1;
         const int nt2 = (g.nx[2] + S::T2 - 1) / S::T2;
         const int blocks = nt0 * nt1 * nt2;
-        k_fused_step<ND, EXACT, TX, TY, TZ><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot, out_buf);
+        if (EXACT && g.eos == EOS_RAD_GAS) {
+            k_fused_step<ND, EXACT, TX, TY, TZ, EOS_RAD_GAS><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot,
+                                                                                        out_buf);
+        } else {
+            k_fused_step<ND, EXACT, TX, TY, TZ><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot, out_buf);
+        }
         ++g_launches;
     }
 };

@@ -183,6 +183,8 @@ void step(const GridDev& g, const fused::StateDev& U, const fused::StateDev& lam
           double dt, bool fp64, cudaStream_t s);
 // Transpose of the boundary fill, in place on interior cells.
 void fold(const GridDev& g, const fused::StateDev& lam, cudaStream_t s);
+// fold of lam, and zero_count doubles of `zero` set to 0 in the same launch
+void fold_zero(const GridDev& g, const fused::StateDev& lam, double* zero, int64_t zero_count, cudaStream_t s);
 void zero_ghosts(const GridDev& g, const fused::StateDev& lam, cudaStream_t s);
 
 } // namespace adjoint
