@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     p.add_argument("--no-ensemble", action="store_true", help="skip the batched ensemble measurement")
+    p.add_argument("--no-stage-loop", action="store_true",
+                   help="skip the passive-scalar (stage-composed loop) measurement")
     p.add_argument("--no-rt3d", action="store_true", help="skip the 3-D Rayleigh-Taylor measurement")
     p.add_argument("--rt3d-steps", type=int, default=500, help="steps of the 3-D Rayleigh-Taylor measurement")
     return p.parse_args()
@@ -214,6 +216,33 @@ def adjoint_cost(torch, nsteps=400, n=512, k=32):
                              d.adjoint_backward(lam, grad, device=True)))
         out[prec] = {"forward_ms": fwd, "gradient_ms": adj, "adj_over_fwd": adj / fwd}
         d.close()
+    return out
+
+
+def stage_loop_cost(torch, steps=20):
+    """KH 2048^2 FP64 with one passive scalar: hcl_run composes the step of the
+    FP64 stage entry points (the reference's per-stage kernels, dt and health
+    readbacks each step); device time per step against the fused FP64 step."""
+    from heraclespp_b200 import Domain, setups
+
+    kw = dict(gamma=1.4, limiter="VanLeer", riemann="HLLC", bc=["Periodic"] * 4)
+    out = {"config": f"kelvin_helmholtz_2d_{NX}x{NX}_fp64_nfx1_{steps}steps"}
+    for name, nfx in (("stage_loop_nfx1", 1), ("fused_nfx0", 0)):
+        d = Domain(2, [NX, NX], nfx=nfx, precision="fp64", **kw)
+        prim = setups.kelvin_helmholtz(setups.Grid.from_domain(d))
+        d.set_state_from_prim(*prim)
+        d.run(cfl=0.4, nsteps=2)
+        stream = torch.cuda.ExternalStream(d.stream_handle())
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        d.run(cfl=0.4, nsteps=steps)
+        e1.record(stream)
+        e1.synchronize()
+        out[name] = {"ms_per_step": e0.elapsed_time(e1) / steps}
+        d.close()
+    out["stage_over_fused"] = out["stage_loop_nfx1"]["ms_per_step"] / out["fused_nfx0"]["ms_per_step"]
     return out
 
 
@@ -518,6 +547,8 @@ def run_ours(args):
             line["ensemble"] = ens
     if rank == 0 and not args.no_rt3d:
         line["rt3d"] = rt3d_cost(torch, steps=args.rt3d_steps)
+    if rank == 0 and not args.no_stage_loop:
+        line["stage_loop"] = stage_loop_cost(torch)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.cpu_budget)
     d.close()
