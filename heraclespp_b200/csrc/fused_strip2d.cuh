@@ -485,12 +485,15 @@ k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     }
 }
 
-// The same step with one CTA of 16 warps per SM whose strips march in step:
-// a CTA barrier every kStripSyncRows rows keeps the 16 strips of an SM at the
-// same height.  Without it the warp schedulers' preference for older warps
-// spreads the finishing times of one SM's strips by up to ~20 %, and the last
-// strips of an SM run with few warps left to hide their latency.
-constexpr int kStripSyncRows = 8;
+// The same step with one CTA of 16 warps per SM (fitted strips, one wave).
+// With four CTAs of 4 warps per SM the strips of one SM finish up to ~20 %
+// apart, in the order the CTAs were launched, and the last strips run with
+// few warps left to hide their latency; the warps of one CTA finish closer
+// together.  A CTA barrier every kStripSyncRows rows can hold the 16 strips
+// at one height; measured on KH 2048^2 (step time for 2/4/8/16/32/64 rows:
+// 113.2/111.3/108.5/107.2/106.7/106.5 us) frequent barriers cost more than
+// they even out, so the interval is a strip's usual height.
+constexpr int kStripSyncRows = 64;
 constexpr int kStripSyncWarps = 16;
 
 template <int LIM, int RS>
