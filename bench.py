@@ -349,7 +349,8 @@ def ensemble_cost(torch, nprob=96, nsteps=300, k=20, seed=2024, rank=0, world=1)
            "cells": cells, "ranks": world, "problems_on_rank0": len(mine),
            "final_total_energy": energy,
            "ensemble": {"ms": t_ens * 1e3, "mcups": cells * nsteps / t_ens * 1e-6, "strip_rows": r.strip_rows,
-                        "blocks_per_sm": r.blocks_per_sm, "grid": r.grid, "launches": r.launches,
+                        "blocks_per_sm": r.blocks_per_sm, "warps_per_cta": r.warps_per_cta, "grid": r.grid,
+                        "launches": r.launches,
                         "graph": bool(r.graph)}}
     # looping the single-problem step (each problem graph-replays its own steps)
     doms = [Domain(2, list(s), precision="fp32_mixed", **kw) for s in my_sides]

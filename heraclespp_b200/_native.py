@@ -111,6 +111,7 @@ class EnsembleParams(C.Structure):
         ("blocks_per_sm", C.c_int),
         ("use_graph", C.c_int),
         ("adjoint_precision", C.c_int),
+        ("warps_per_cta", C.c_int),
     ]
 
 
@@ -123,6 +124,7 @@ class EnsembleResult(C.Structure):
         ("launches", C.c_int),
         ("graph", C.c_int),
         ("cells", C.c_int64),
+        ("warps_per_cta", C.c_int),
     ]
 
 

@@ -1901,9 +1901,9 @@ struct hcl_ensemble {
     int* d_status = nullptr;
     cudaStream_t stream = nullptr;
     int lim = 0, rs = 0;
-    int L = 0, bps = 0; // tuned schedule
+    int L = 0, bps = 0, nw = 4; // tuned schedule: strip rows, CTAs per SM, warps per CTA
     int64_t cells = 0;
-    std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs; // (nsteps, step0, L, bps)
+    std::map<std::tuple<int, int, int, int, int>, cudaGraphExec_t> graphs; // (nsteps, step0, L, bps, nw)
     // batched reverse pass: problem tables, tile work list, dts of all problems
     hcl::ensemble::AdjProb* d_adjprobs = nullptr;
     hcl::ensemble::Prob* d_rec_probs = nullptr;
@@ -1974,7 +1974,7 @@ int ensemble_build_items(hcl_ensemble* e, int L)
     return HCL_OK;
 }
 
-int ensemble_launch(hcl_ensemble* e, const hcl::ensemble::Prob* probs, int nsteps, int step0, int L, int bps,
+int ensemble_launch(hcl_ensemble* e, const hcl::ensemble::Prob* probs, int nsteps, int step0, int L, int bps, int nw,
                     int use_graph, double cfl, int* graphed)
 {
     int nsm = 0;
@@ -1994,13 +1994,14 @@ int ensemble_launch(hcl_ensemble* e, const hcl::ensemble::Prob* probs, int nstep
             err = cudaMemsetAsync(e->d_status, 0, sizeof(int), e->stream);
         }
         if (err == cudaSuccess) {
-            err = hcl::ensemble::launch(e->lim, e->rs, grid, probs, e->d_items, ep, e->d_barrier, e->d_status, e->stream);
+            err = hcl::ensemble::launch(e->lim, e->rs, nw, grid, probs, e->d_items, ep, e->d_barrier, e->d_status,
+                                        e->stream);
         }
         return err;
     };
     *graphed = 0;
     if (use_graph && probs == e->d_probs) {
-        const auto key = std::make_tuple(nsteps, step0, L, bps);
+        const auto key = std::make_tuple(nsteps, step0, L, bps, nw);
         auto it = e->graphs.find(key);
         if (it == e->graphs.end()) {
             cudaGraph_t graph;
@@ -2026,12 +2027,15 @@ int ensemble_launch(hcl_ensemble* e, const hcl::ensemble::Prob* probs, int nstep
     return HCL_OK;
 }
 
-// Picks (strip rows, CTAs per SM) by timing one step of every candidate on the
-// tuning control blocks (reads buffer 0, writes buffer 1; the state is kept).
+// Picks (strip rows, CTAs per SM, warps per CTA) by timing one step of every
+// candidate on the tuning control blocks (reads buffer 0, writes buffer 1;
+// the state is kept).  Candidates: CTAs of 4 warps at the resident maximum
+// per SM and the two counts below it; one CTA of 16 warps per SM.
 int ensemble_autotune(hcl_ensemble* e, double cfl)
 {
-    const int maxb = hcl::ensemble::max_blocks_per_sm(e->lim, e->rs);
-    if (maxb <= 0) {
+    const int maxb4 = hcl::ensemble::max_blocks_per_sm(e->lim, e->rs, 4);
+    const int maxb16 = hcl::ensemble::max_blocks_per_sm(e->lim, e->rs, 16);
+    if (maxb4 <= 0) {
         return fail(HCL_ERR_CUDA, "ensemble kernel cannot be resident");
     }
     cudaEvent_t e0, e1;
@@ -2044,7 +2048,15 @@ int ensemble_autotune(hcl_ensemble* e, double cfl)
         if (rc) {
             return rc;
         }
-        for (int bps = maxb; bps >= 1 && bps >= maxb - 2; --bps) {
+        std::vector<std::pair<int, int>> cands; // (bps, nw)
+        for (int bps = maxb4; bps >= 1 && bps >= maxb4 - 2; --bps) {
+            cands.emplace_back(bps, 4);
+        }
+        if (maxb16 >= 1) {
+            cands.emplace_back(1, 16);
+        }
+        for (const auto& cand : cands) {
+            const int bps = cand.first, nw = cand.second;
             float tot = 0;
             for (int r = 0; r < 3; ++r) {
                 for (hcl_handle* h : e->h) {
@@ -2052,7 +2064,7 @@ int ensemble_autotune(hcl_ensemble* e, double cfl)
                 }
                 int graphed = 0;
                 HCL_CUDA(cudaEventRecord(e0, e->stream));
-                if ((rc = ensemble_launch(e, e->d_probs_tune, 1, 0, L, bps, 0, cfl, &graphed))) {
+                if ((rc = ensemble_launch(e, e->d_probs_tune, 1, 0, L, bps, nw, 0, cfl, &graphed))) {
                     return rc;
                 }
                 HCL_CUDA(cudaEventRecord(e1, e->stream));
@@ -2067,6 +2079,7 @@ int ensemble_autotune(hcl_ensemble* e, double cfl)
                 best = tot;
                 e->L = L;
                 e->bps = bps;
+                e->nw = nw;
             }
         }
     }
@@ -2197,14 +2210,19 @@ int hcl_ensemble_run(hcl_ensemble* e, const hcl_ensemble_params* p, hcl_ensemble
     if (p->strip_rows != 0 && p->strip_rows != 32 && p->strip_rows != 64 && p->strip_rows != 128) {
         return fail(HCL_ERR_ARGUMENT, "strip_rows must be 0 (autotune), 32, 64 or 128");
     }
-    const int maxb = hcl::ensemble::max_blocks_per_sm(e->lim, e->rs);
+    if (p->warps_per_cta != 0 && p->warps_per_cta != 4 && p->warps_per_cta != 16) {
+        return fail(HCL_ERR_ARGUMENT, "warps_per_cta must be 0 (autotune), 4 or 16");
+    }
+    const int nw_req = p->warps_per_cta > 0 ? p->warps_per_cta : 4;
+    const int maxb = hcl::ensemble::max_blocks_per_sm(e->lim, e->rs, nw_req);
     if (p->blocks_per_sm < 0 || p->blocks_per_sm > maxb) {
         return fail(HCL_ERR_ARGUMENT, "blocks_per_sm must be in [0, %d] for a co-resident launch", maxb);
     }
     e->items_L = 0; // the table carries the dt logs: rebuild it
-    if (p->strip_rows > 0 || p->blocks_per_sm > 0) {
+    if (p->strip_rows > 0 || p->blocks_per_sm > 0 || p->warps_per_cta > 0) {
         e->L = p->strip_rows > 0 ? p->strip_rows : 64;
-        e->bps = p->blocks_per_sm > 0 ? p->blocks_per_sm : hcl::ensemble::max_blocks_per_sm(e->lim, e->rs);
+        e->nw = nw_req;
+        e->bps = p->blocks_per_sm > 0 ? p->blocks_per_sm : maxb;
     } else if (e->L == 0) {
         if ((rc = ensemble_autotune(e, p->cfl))) {
             return rc;
@@ -2241,7 +2259,7 @@ int hcl_ensemble_run(hcl_ensemble* e, const hcl_ensemble_params* p, hcl_ensemble
             }
         }
         int graphed = 0;
-        if ((rc = ensemble_launch(e, e->d_probs, len, done, e->L, e->bps, p->use_graph, p->cfl, &graphed))) {
+        if ((rc = ensemble_launch(e, e->d_probs, len, done, e->L, e->bps, e->nw, p->use_graph, p->cfl, &graphed))) {
             return rc;
         }
         graphed_all &= graphed;
@@ -2273,6 +2291,7 @@ int hcl_ensemble_run(hcl_ensemble* e, const hcl_ensemble_params* p, hcl_ensemble
         r->status = status;
         r->strip_rows = e->L;
         r->blocks_per_sm = e->bps;
+        r->warps_per_cta = e->nw;
         int nsm = 0;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->h[0]->cfg.device);
         r->grid = e->bps * nsm;
@@ -2422,7 +2441,7 @@ int hcl_ensemble_adjoint(hcl_ensemble* e, const double* const* lam_final, double
                 ep.nsteps = len - 1;
                 err = cudaMemsetAsync(e->d_barrier, 0, sizeof(unsigned int), s);
                 if (err == cudaSuccess) {
-                    err = hcl::ensemble::launch(e->lim, e->rs, e->bps * nsm, e->d_rec_probs, e->d_items, ep,
+                    err = hcl::ensemble::launch(e->lim, e->rs, e->nw, e->bps * nsm, e->d_rec_probs, e->d_items, ep,
                                                 e->d_barrier, e->d_status, s);
                 }
             }

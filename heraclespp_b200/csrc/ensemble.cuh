@@ -53,16 +53,19 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int t
     return go_on != 0;
 }
 
-template <int LIM, int RS>
-__global__ void __launch_bounds__(128)
+// NW warps per CTA (4 or 16); each warp's row ring lives in dynamic shared
+// memory (NW x kStripRingDoubles doubles).
+template <int LIM, int RS, int NW>
+__global__ void __launch_bounds__(32 * NW, NW == 16 ? 1 : 4)
 k_ensemble(const Prob* __restrict__ probs, const int* __restrict__ item_prob, Params ep, unsigned int* barrier,
            int* status)
 {
+    extern __shared__ __align__(16) double s_ens_ring[];
     const int lane = threadIdx.x & 31;
     const int warps_total = gridDim.x * (blockDim.x >> 5);
     const int wid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    __shared__ __align__(16) double s_ring[4][fused::kStripRingDoubles];
-    const fused::StripRing ring = reinterpret_cast<fused::StripRing>(s_ring[(threadIdx.x >> 5) & 3]);
+    const fused::StripRing ring =
+        reinterpret_cast<fused::StripRing>(s_ens_ring + (threadIdx.x >> 5) * fused::kStripRingDoubles);
     for (int s = 0; s < ep.nsteps; ++s) {
         const int gs = ep.step0 + s;
         // per-problem bookkeeping: t, iteration, dt log, clear the slot two ahead

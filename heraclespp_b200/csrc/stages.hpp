@@ -168,8 +168,8 @@ void seg_init(const AdjProb* probs, int nprob, int sg, int first, cudaStream_t s
 cudaError_t reverse(bool fp64, int grid, const AdjProb* probs, const int* tile_prob, const AdjParams& ap,
                     unsigned int* barrier, int* status, cudaStream_t s);
 
-int max_blocks_per_sm(int lim, int rs);
-cudaError_t launch(int lim, int rs, int grid, const Prob* probs, const int* item_prob, const Params& ep,
+int max_blocks_per_sm(int lim, int rs, int nw);
+cudaError_t launch(int lim, int rs, int nw, int grid, const Prob* probs, const int* item_prob, const Params& ep,
                    unsigned int* barrier, int* status, cudaStream_t s);
 
 } // namespace ensemble

@@ -339,6 +339,7 @@ typedef struct hcl_ensemble_params {
     int blocks_per_sm;        /* 0: autotune */
     int use_graph;            /* 1: capture the persistent launch in a CUDA graph and replay it */
     int adjoint_precision;    /* HCL_FP64 or HCL_FP32_MIXED reverse sweep for hcl_ensemble_adjoint */
+    int warps_per_cta;        /* 0: autotune; 4 or 16 warps per CTA of the persistent launch */
 } hcl_ensemble_params;
 
 typedef struct hcl_ensemble_result {
@@ -349,6 +350,7 @@ typedef struct hcl_ensemble_result {
     int launches;             /* persistent launches issued (1 per checkpoint segment) */
     int graph;                /* 1 when replayed from a CUDA graph */
     int64_t cells;            /* interior cells over all problems */
+    int warps_per_cta;
 } hcl_ensemble_result;
 
 /* Creates one handle per configuration (hcl_create) plus the batch. */

@@ -42,12 +42,13 @@ def make_ensemble(sides=SIDES):
     return ens
 
 
-@pytest.mark.parametrize("strip_rows,use_graph", [(64, False), (32, True), (128, True)])
-def test_ensemble_matches_single_problem_kernel(strip_rows, use_graph):
+@pytest.mark.parametrize("strip_rows,use_graph,nw", [(64, False, 4), (32, True, 4), (128, True, 4), (64, True, 16),
+                                                     (32, False, 16)])
+def test_ensemble_matches_single_problem_kernel(strip_rows, use_graph, nw):
     n = 24
     ens = make_ensemble()
-    r = ens.run(n, strip_rows=strip_rows, use_graph=use_graph)
-    assert r.status == 0 and r.strip_rows == strip_rows and r.launches == 1
+    r = ens.run(n, strip_rows=strip_rows, use_graph=use_graph, warps_per_cta=nw)
+    assert r.status == 0 and r.strip_rows == strip_rows and r.launches == 1 and r.warps_per_cta == nw
     assert r.graph == (1 if use_graph else 0)
     assert r.cells == sum(a * b for a, b in SIDES)
     for p, (nx, d_e) in enumerate(zip(SIDES, ens.domains)):
@@ -65,6 +66,7 @@ def test_ensemble_autotune_and_continue_with_run():
     ens = make_ensemble()
     r = ens.run(10)
     assert r.strip_rows in (32, 64, 128) and r.blocks_per_sm >= 1 and r.grid >= r.blocks_per_sm
+    assert r.warps_per_cta in (4, 16)
     for p, (nx, d_e) in enumerate(zip(SIDES, ens.domains)):
         res = d_e.run(nsteps=14)
         assert res.iter == 24
@@ -90,6 +92,8 @@ def test_ensemble_rejects_bad_configs():
     ens = make_ensemble(SIDES[:2])
     with pytest.raises(HclError):
         ens.run(4, strip_rows=48)
+    with pytest.raises(HclError):
+        ens.run(4, warps_per_cta=8)
     ens.close()
 
 
