@@ -260,7 +260,10 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             Glo[v] = (double)G[v];
         }
     }
-    // window: wC = P[r], wD = P[r+1]; ring rows r+3, r+4 in flight
+    // window: wC = P[r], wD = P[r+1]; ring rows r+3, r+4 in flight.  Two rows
+    // per iteration turn the window slide into register renaming (KH 2048^2:
+    // 106.5 -> 102.7 us per step; four rows per iteration are slower).
+#pragma unroll 2
     for (int i = 0; i < (SYNC > 0 ? L : r1 - r0); ++i) {
         const int r = r0 + i;
         if constexpr (SYNC > 0) {
