@@ -560,11 +560,20 @@ int get_graph(hcl_handle* h, const RunParamsDev& rp, int k, cudaGraphExec_t* out
     return HCL_OK;
 }
 
-// Handles whose time loop is composed of the FP64 stage entry points: passive
-// scalars and the pressure fix are not carried by the fused kernels.
+// Handles whose time loop is composed of the FP64 stage entry points: the
+// pressure fix, and passive scalars too many for the fused tile's shared
+// memory, are not carried by the fused kernels.
 bool stage_mode(const hcl_handle* h)
 {
-    return h->cfg.nfx > 0 || h->cfg.pressure_fix != 0;
+    if (h->cfg.pressure_fix != 0) {
+        return true;
+    }
+    if (h->cfg.nfx == 0) {
+        return false;
+    }
+    const size_t bytes = h->cfg.precision == HCL_FP32_MIXED ? hcl::fused::mixed_smem_bytes(h->g, 0)
+                                                             : hcl::fused::exact_smem_bytes(h->g);
+    return bytes + hcl::fused::kFusedStaticSmemMargin > (size_t)hcl::fused::smem_optin();
 }
 
 // The reference-layout arrays of the stage-composed loop (main.cpp:187-205).
@@ -601,7 +610,7 @@ int stage_buffers(hcl_handle* h)
 int restart_clock(hcl_handle* h, double t, int iter)
 {
     if (h->cur != 0) {
-        const size_t bytes = sizeof(double) * (size_t)h->st[0].plane * (h->g.ndim + 2);
+        const size_t bytes = sizeof(double) * (size_t)h->st[0].plane * (h->g.ndim + 2 + h->g.nfx);
         HCL_CUDA(cudaMemcpyAsync(h->st[0].q, h->st[1].q, bytes, cudaMemcpyDeviceToDevice, h->stream));
         h->cur = 0;
     }
@@ -749,14 +758,15 @@ int hcl_create(const hcl_config* cfg, hcl_handle** out)
         (rc = dalloc(&h->red_out, 16))) {
         return bail(rc);
     }
-    // fused state: nv planes of n2*n1*pitch doubles, pitch a multiple of 16
+    // fused state: nv + nfx planes of n2*n1*pitch doubles, pitch a multiple of 16
     const int pitch = (g.n[0] + 15) / 16 * 16;
     const int64_t plane = (int64_t)pitch * g.n[1] * g.n[2];
+    const size_t nplanes = (size_t)(nv + g.nfx);
     for (int b = 0; b < 2; ++b) {
-        if ((rc = dalloc(&h->state_mem[b], (size_t)plane * nv))) {
+        if ((rc = dalloc(&h->state_mem[b], (size_t)plane * nplanes))) {
             return bail(rc);
         }
-        HCL_CUDA(cudaMemset(h->state_mem[b], 0, sizeof(double) * (size_t)plane * nv));
+        HCL_CUDA(cudaMemset(h->state_mem[b], 0, sizeof(double) * (size_t)plane * nplanes));
         h->st[b].q = h->state_mem[b];
         h->st[b].plane = plane;
         h->st[b].pitch = pitch;
@@ -1125,8 +1135,8 @@ int hcl_set_state(hcl_handle* h, const double* rho, const double* rhou, const do
         }
         return hcl_reset_clock(h, 0.0);
     }
-    (void)fx;
     hcl::fused::pack_state(h->g, h->st[0], rho, rhou, E, kind, h->stream);
+    hcl::fused::pack_fx(h->g, h->st[0], fx, kind, h->stream);
     HCL_CUDA(cudaGetLastError());
     h->cur = 0;
     h->state_valid = 1;
@@ -1156,8 +1166,10 @@ int hcl_get_state(hcl_handle* h, double* rho, double* rhou, double* E, double* f
         HCL_CUDA(cudaStreamSynchronize(s));
         return HCL_OK;
     }
-    (void)fx;
     hcl::fused::unpack_state(h->g, h->st[h->cur], rho, rhou, E, kind, h->stream);
+    if (fx) {
+        hcl::fused::unpack_fx(h->g, h->st[h->cur], fx, kind, h->stream);
+    }
     HCL_CUDA(cudaGetLastError());
     HCL_CUDA(cudaStreamSynchronize(h->stream));
     return HCL_OK;
@@ -1202,15 +1214,16 @@ int hcl_set_state_from_prim(hcl_handle* h, const double* rho, const double* u, c
         }
         return hcl_reset_clock(h, 0.0);
     }
-    (void)fx;
-    double *d_rho = nullptr, *d_u = nullptr, *d_P = nullptr, *d_m = nullptr, *d_E = nullptr;
+    const size_t nf = (size_t)h->g.nfx;
+    double *d_rho = nullptr, *d_u = nullptr, *d_P = nullptr, *d_m = nullptr, *d_E = nullptr, *d_fx = nullptr;
     if ((rc = dalloc(&d_rho, N)) || (rc = dalloc(&d_u, N * nd)) || (rc = dalloc(&d_P, N)) ||
-        (rc = dalloc(&d_m, N * nd)) || (rc = dalloc(&d_E, N))) {
+        (rc = dalloc(&d_m, N * nd)) || (rc = dalloc(&d_E, N)) || (nf > 0 && (rc = dalloc(&d_fx, N * nf)))) {
         cudaFree(d_rho);
         cudaFree(d_u);
         cudaFree(d_P);
         cudaFree(d_m);
         cudaFree(d_E);
+        cudaFree(d_fx);
         return rc;
     }
     cudaStream_t s = h->stream;
@@ -1219,16 +1232,25 @@ int hcl_set_state_from_prim(hcl_handle* h, const double* rho, const double* u, c
     cudaMemcpyAsync(d_P, P, sizeof(double) * N, cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(d_m, 0, sizeof(double) * N * nd, s);
     cudaMemsetAsync(d_E, 0, sizeof(double) * N, s);
+    if (nf > 0) {
+        if (fx) {
+            cudaMemcpyAsync(d_fx, fx, sizeof(double) * N * nf, cudaMemcpyHostToDevice, s);
+        } else {
+            cudaMemsetAsync(d_fx, 0, sizeof(double) * N * nf, s);
+        }
+    }
     // main.cpp:305-307: conv_prim_to_cons(no_ghosts) then the boundaries
     hcl::stage::conv_prim_to_cons(h->g, 0, d_rho, d_u, d_P, d_m, d_E, s);
-    hcl::stage::boundaries(h->g, d_rho, d_m, d_E, nullptr, s);
+    hcl::stage::boundaries(h->g, d_rho, d_m, d_E, d_fx, s);
     hcl::fused::pack_state(h->g, h->st[0], d_rho, d_m, d_E, cudaMemcpyDeviceToDevice, s);
+    hcl::fused::pack_fx(h->g, h->st[0], d_fx, cudaMemcpyDeviceToDevice, s);
     cudaError_t e = cudaStreamSynchronize(s);
     cudaFree(d_rho);
     cudaFree(d_u);
     cudaFree(d_P);
     cudaFree(d_m);
     cudaFree(d_E);
+    cudaFree(d_fx);
     if (e != cudaSuccess) {
         return fail(HCL_ERR_CUDA, "initial state: %s", cudaGetErrorString(e));
     }

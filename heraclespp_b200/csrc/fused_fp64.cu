@@ -28,6 +28,29 @@ void step_exact(const GridDev& g, const StateDev& in, const StateDev& out, StepC
     }
 }
 
+size_t exact_smem_bytes(const GridDev& g)
+{
+    switch (g.ndim) {
+    case 1:
+        return FusedLauncher<1, true, 128, 1, 1>::smem(g.nfx);
+    case 2:
+        return FusedLauncher<2, true, 16, 16, 1>::smem(g.nfx);
+    default:
+        return FusedLauncher<3, true, 8, 4, 4>::smem(g.nfx);
+    }
+}
+
+int smem_optin()
+{
+    static int bytes = [] {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        return v;
+    }();
+    return bytes;
+}
+
 void configure_exact()
 {
     FusedLauncher<1, true, 128, 1, 1>::configure();
@@ -278,6 +301,31 @@ void unpack_state(const GridDev& g, const StateDev& st, double* rho, double* rho
         cudaMemcpy2DAsync(rhou + g.N * d, w, st.q + st.plane * (1 + d), dp, w, rows, kind, s);
     }
     cudaMemcpy2DAsync(E, w, st.q + st.plane * (1 + g.ndim), dp, w, rows, kind, s);
+}
+
+void pack_fx(const GridDev& g, const StateDev& st, const double* fx, cudaMemcpyKind kind, cudaStream_t s)
+{
+    const size_t w = sizeof(double) * (size_t)g.n[0];
+    const size_t rows = (size_t)g.n[1] * g.n[2];
+    const size_t dp = sizeof(double) * (size_t)st.pitch;
+    for (int f = 0; f < g.nfx; ++f) {
+        double* dst = st.q + st.plane * (g.ndim + 2 + f);
+        if (fx) {
+            cudaMemcpy2DAsync(dst, dp, fx + g.N * f, w, w, rows, kind, s);
+        } else {
+            cudaMemsetAsync(dst, 0, sizeof(double) * (size_t)st.plane, s);
+        }
+    }
+}
+
+void unpack_fx(const GridDev& g, const StateDev& st, double* fx, cudaMemcpyKind kind, cudaStream_t s)
+{
+    const size_t w = sizeof(double) * (size_t)g.n[0];
+    const size_t rows = (size_t)g.n[1] * g.n[2];
+    const size_t dp = sizeof(double) * (size_t)st.pitch;
+    for (int f = 0; f < g.nfx; ++f) {
+        cudaMemcpy2DAsync(fx + g.N * f, w, st.q + st.plane * (g.ndim + 2 + f), dp, w, rows, kind, s);
+    }
 }
 
 } // namespace hcl::fused

@@ -21,8 +21,26 @@ int mixed_shape_count(int ndim)
     return ndim == 2 ? 10 : (ndim == 3 ? 2 : 1);
 }
 
+size_t mixed_smem_bytes(const GridDev& g, int shape)
+{
+    switch (g.ndim) {
+    case 1:
+        return FusedLauncher<1, false, 256, 1, 1>::smem(g.nfx);
+    case 2:
+        return shape == 1 ? FusedLauncher<2, false, 32, 8, 1>::smem(g.nfx)
+                          : (shape == 2 ? FusedLauncher<2, false, 32, 16, 1>::smem(g.nfx)
+                                        : FusedLauncher<2, false, 16, 16, 1>::smem(g.nfx));
+    default:
+        return FusedLauncher<3, false, 8, 8, 4>::smem(g.nfx);
+    }
+}
+
 bool mixed_shape_valid(const GridDev& g, int shape)
 {
+    if (g.nfx > 0) {
+        // passive scalars ride in the shared-memory tiles only
+        return (g.ndim == 2 ? shape < 3 : shape == 0) && mixed_smem_bytes(g, shape) + kFusedStaticSmemMargin <= (size_t)smem_optin();
+    }
     if (g.ndim == 3) {
         return shape == 0 || (shape == 1 && strip3d_eligible(g));
     }

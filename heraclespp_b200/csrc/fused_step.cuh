@@ -27,6 +27,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <type_traits>
 
@@ -326,6 +327,10 @@ k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp
     R* sp = reinterpret_cast<R*>(smem_raw);     // [NV][NP] primitives
     R* sa = sp + NV * S::NP;                    // faces: per d [2][NV][A_d]
     R* sf = sa + S::A_TOTAL;                    // fluxes: per d [NV][F_d]
+    R* sx = sf + S::F_TOTAL;                    // passive scalars: [nfx][NP] primitives, then
+                                                // face values per d [2][nfx][A_d]
+    const int nfx = g.nfx;
+    auto sxa = [&](int d) { return sx + nfx * (S::NP + 2 * (S::Aoff(d) / (2 * NV))); };
 
     const int tid = threadIdx.x;
     const Decision dec = decide(ctl, slot, rp);
@@ -425,6 +430,9 @@ k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp
                 sp[(1 + d) * S::NP + p] = (float)u;
             }
             sp[(1 + ND) * S::NP + p] = (float)(g.gamma_m1 * fma(-0.5, mu, q[1 + ND]));
+        }
+        for (int f = 0; f < nfx; ++f) {
+            sx[f * S::NP + p] = (R)__ldg(in.q + o + in.plane * (NV + f));
         }
     }
     __syncthreads();
@@ -558,12 +566,15 @@ k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp
                 ds_p[idim] = g.ds[cp + g.N * idim];
             }
         }
+        R mflux[2][ND]; // mass fluxes of the face states before the update (passive scalars)
 #pragma unroll
         for (int idim = 0; idim < ND; ++idim) {
             R fL[NV], fR[NV];
             if constexpr (EXACT) {
                 exact::flux_prim<ND>(eeos, fp[0][idim], idim, fL);
                 exact::flux_prim<ND>(eeos, fp[1][idim], idim, fR);
+                mflux[0][idim] = fL[0];
+                mflux[1][idim] = fR[0];
                 const double dtodv = dth / dv_c;
                 const double dsc = ds_c[idim];
                 const double dsp = ds_p[idim];
@@ -622,6 +633,8 @@ k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp
             } else {
                 fast::flux_prim<ND>(feos, fp[0][idim], idim, fL);
                 fast::flux_prim<ND>(feos, fp[1][idim], idim, fR);
+                mflux[0][idim] = fL[0];
+                mflux[1][idim] = fR[0];
                 float inc[NV];
                 float dtodv = 0.f;
                 float dsc = 1.f, dsp = 1.f;
@@ -682,6 +695,78 @@ k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp
                         fc[s][ipos][1 + idim] = fmaf(dg, rho_old, fc[s][ipos][1 + idim]);
                         fc[s][ipos][1 + ND] = fmaf(dg, rhou_old, fc[s][ipos][1 + ND]);
                     }
+                }
+            }
+        }
+        // passive scalars: face values with the same limited slopes
+        // (hydro_reconstruction.hpp:105-109), made conservative with the face
+        // density before the predictor, advanced by the predictor's mass
+        // fluxes (extrapolation_reconstruction.hpp:315-337) and turned back
+        // into fractions with the predicted face density (:459-469)
+        for (int f = 0; f < nfx; ++f) {
+            const R* xs = sx + f * S::NP;
+            R xf[2][ND];
+#pragma unroll
+            for (int idim = 0; idim < ND; ++idim) {
+                const R vc = xs[lc];
+                const R vp = xs[lc + lstride[idim]];
+                const R vm = xs[lc - lstride[idim]];
+                if constexpr (EXACT) {
+                    const double dl = g.dx[idim][gcc[idim]];
+                    const double dl_m = g.dx[idim][gcc[idim] - 1];
+                    const double dl_p = g.dx[idim][gcc[idim] + 1];
+                    const double slope = exact::slope(g.limiter, (vp - vc) / ((dl + dl_p) / 2), (vc - vm) / ((dl_m + dl) / 2));
+                    xf[0][idim] = vc - ((dl / 2) * slope);
+                    xf[1][idim] = vc + ((dl / 2) * slope);
+                } else if (g.uniform_cart) {
+                    const float sl = 0.5f * fast::limited(g.limiter, vp - vc, vc - vm);
+                    xf[0][idim] = vc - sl;
+                    xf[1][idim] = vc + sl;
+                } else {
+                    const float fdl = (float)g.dx[idim][gcc[idim]];
+                    const float hR = 2.f * fast::rcp(fdl + (float)g.dx[idim][gcc[idim] + 1]);
+                    const float hL = 2.f * fast::rcp((float)g.dx[idim][gcc[idim] - 1] + fdl);
+                    const float sl = 0.5f * fdl * fast::limited(g.limiter, (vp - vc) * hR, (vc - vm) * hL);
+                    xf[0][idim] = vc - sl;
+                    xf[1][idim] = vc + sl;
+                }
+            }
+            R xc[2][ND];
+#pragma unroll
+            for (int ipos = 0; ipos < ND; ++ipos) {
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    xc[s][ipos] = xf[s][ipos] * fp[s][ipos][0];
+                }
+            }
+#pragma unroll
+            for (int idim = 0; idim < ND; ++idim) {
+                const R ffL = xf[0][idim] * mflux[0][idim];
+                const R ffR = xf[1][idim] * mflux[1][idim];
+                R inc;
+                if constexpr (EXACT) {
+                    inc = (dth / dv_c) * ((ffL * ds_c[idim]) - (ffR * ds_p[idim]));
+                } else if (g.uniform_cart) {
+                    inc = (float)(dth * g.inv_dx[idim]) * (ffL - ffR);
+                } else {
+                    inc = (float)(dth / dv_c) * (ffL * (float)ds_c[idim] - ffR * (float)ds_p[idim]);
+                }
+#pragma unroll
+                for (int ipos = 0; ipos < ND; ++ipos) {
+                    xc[0][ipos] += inc;
+                    xc[1][ipos] += inc;
+                }
+            }
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+                if (own >= 0 && own != d) {
+                    continue;
+                }
+                const int a = (x[0] + (d == 0)) + S::Adim(d, 0) * ((x[1] + (d == 1)) + S::Adim(d, 1) * (x[2] + (d == 2)));
+                R* xb = sxa(d);
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    xb[(s * nfx + f) * S::Asize(d) + a] = xc[s][d] / fc[s][d][0];
                 }
             }
         }
@@ -1019,6 +1104,74 @@ k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp
                 }
             }
         }
+
+        // passive scalars (godunov_scheme.hpp:118-123, :262-301): fx rho plus
+        // the upwind face values times the Riemann mass fluxes, divided by the
+        // new density and clamped to [0, 1]; ghost images copy the value
+        if (nfx > 0) {
+            double dv_c = 1.0, ds_c[ND], ds_p[ND];
+            if (EXACT || !g.uniform_cart) {
+                if (g.geom == GEOM_CARTESIAN) {
+                    const double dxs[3] = {g.dx[0][gi], g.dx[1][gj], g.dx[2][gk]};
+                    dv_c = dxs[0] * dxs[1] * dxs[2];
+#pragma unroll
+                    for (int idim = 0; idim < ND; ++idim) {
+                        double a[3] = {dxs[0], dxs[1], dxs[2]};
+                        a[idim] = 1;
+                        ds_c[idim] = a[0] * a[1] * a[2];
+                        ds_p[idim] = ds_c[idim];
+                    }
+                } else {
+                    dv_c = g.dv[cgl];
+#pragma unroll
+                    for (int idim = 0; idim < ND; ++idim) {
+                        ds_c[idim] = g.ds[cgl + g.N * idim];
+                        ds_p[idim] = g.ds[lidx(g, gi + (idim == 0), gj + (idim == 1), gk + (idim == 2)) + g.N * idim];
+                    }
+                }
+            }
+            const int xs3[3] = {x0, x1, x2};
+            for (int f = 0; f < nfx; ++f) {
+                double xn = in.q[so + in.plane * (NV + f)] * q[0];
+                double xacc = 0.0;
+#pragma unroll
+                for (int idim = 0; idim < ND; ++idim) {
+                    const int fidx = xs3[0] + S::Fdim(idim, 0) * (xs3[1] + S::Fdim(idim, 1) * xs3[2]);
+                    const int fstep = idim == 0 ? 1 : (idim == 1 ? S::Fdim(idim, 0) : S::Fdim(idim, 0) * S::Fdim(idim, 1));
+                    const R* fb = sf + S::Foff(idim);
+                    const R FL = fb[fidx];
+                    const R FR = fb[fidx + fstep];
+                    const int a = (xs3[0] + (idim == 0)) +
+                                  S::Adim(idim, 0) * ((xs3[1] + (idim == 1)) + S::Adim(idim, 1) * (xs3[2] + (idim == 2)));
+                    const int astep = idim == 0 ? 1 : (idim == 1 ? S::Adim(idim, 0) : S::Adim(idim, 0) * S::Adim(idim, 1));
+                    const R* side0 = sxa(idim) + f * S::Asize(idim);
+                    const R* side1 = sxa(idim) + (nfx + f) * S::Asize(idim);
+                    const R xL = FL < 0 ? side0[a] : side1[a - astep];
+                    const R xR = FR < 0 ? side0[a + astep] : side1[a];
+                    if constexpr (EXACT) {
+                        const double ffL = xL * FL;
+                        const double ffR = xR * FR;
+                        xn += (dt / dv_c) * ((ffL * ds_c[idim]) - (ffR * ds_p[idim]));
+                    } else if (g.uniform_cart) {
+                        xacc = fma(dt * g.inv_dx[idim], (double)xL * FL - (double)xR * FR, xacc);
+                    } else {
+                        xacc = fma(dt / dv_c, (double)xL * FL * ds_c[idim] - (double)xR * FR * ds_p[idim], xacc);
+                    }
+                }
+                if constexpr (!EXACT) {
+                    xn += xacc;
+                }
+                double v = xn / qn[0];
+                v = v < 0. ? 0. : (v > 1. ? 1. : v);
+                for (int a2 = 0; a2 < cnt[2]; ++a2) {
+                    for (int a1 = 0; a1 < cnt[1]; ++a1) {
+                        for (int a0 = 0; a0 < cnt[0]; ++a0) {
+                            out.q[sidx(out, g.n[1], pos[0][a0], pos[1][a1], pos[2][a2]) + out.plane * (NV + f)] = v;
+                        }
+                    }
+                }
+            }
+        }
     }
     // CTA max of 1/dt -> one atomic
     __shared__ double red[32];
@@ -1046,25 +1199,39 @@ template <int ND, bool EXACT, int TX, int TY, int TZ>
 struct FusedLauncher {
     using S = Shape<ND, TX, TY, TZ>;
     using R = std::conditional_t<EXACT, double, float>;
-    static size_t smem()
+    // dynamic shared memory of a launch with nfx passive scalars
+    static size_t smem(int nfx = 0)
     {
-        return smem_bytes_for<R>(S::NP, S::A_TOTAL, S::F_TOTAL, S::NV);
+        return smem_bytes_for<R>(S::NP, S::A_TOTAL, S::F_TOTAL, S::NV) +
+               sizeof(R) * (size_t)nfx * (S::NP + 2 * (S::A_TOTAL / (2 * S::NV)));
     }
     static int threads() { return S::TVOL; }
-    // Opts the kernel into its dynamic shared memory size; called once per
-    // process before any launch (never during stream capture).
+    // Opts the kernel into the device's largest dynamic shared memory per
+    // block (launches without passive scalars use smem(0) and keep their
+    // occupancy); called once per process before any launch (never during
+    // stream capture).
     static void configure()
     {
-        cudaFuncSetAttribute(k_fused_step<ND, EXACT, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
+        set_max_dynamic(reinterpret_cast<const void*>(k_fused_step<ND, EXACT, TX, TY, TZ>));
         if constexpr (EXACT) {
-            cudaFuncSetAttribute(k_fused_step<ND, EXACT, TX, TY, TZ, EOS_RAD_GAS>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
+            set_max_dynamic(reinterpret_cast<const void*>(k_fused_step<ND, EXACT, TX, TY, TZ, EOS_RAD_GAS>));
         }
+    }
+    // the per-block opt-in limit less the kernel's static shared memory
+    static void set_max_dynamic(const void* fn)
+    {
+        int dev = 0, optin = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        cudaFuncAttributes fa{};
+        cudaFuncGetAttributes(&fa, fn);
+        const int bytes = std::max(optin - (int)fa.sharedSizeBytes, (int)smem());
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     }
     static void launch(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                        int slot, int out_buf, cudaStream_t s)
     {
-        const size_t sm = smem();
+        const size_t sm = smem(g.nfx);
         const int nt0 = (g.nx[0] + S::T0 - 1) / S::T0;
         const int nt1 = (g.nx[1] + S::T1 - 1) / S::T1;
         const int nt2 = (g.nx[2] + S::T2 - 1) / S::T2;

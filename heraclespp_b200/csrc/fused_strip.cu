@@ -12,7 +12,7 @@ namespace hcl::fused {
 
 bool strip2d_eligible(const GridDev& g)
 {
-    return g.ndim == 2 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM;
+    return g.ndim == 2 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM && g.nfx == 0;
 }
 
 // The paired schedule loads and stores column pairs as 16-byte vectors: the

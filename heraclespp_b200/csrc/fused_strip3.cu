@@ -12,7 +12,8 @@ namespace hcl::fused {
 
 bool strip3d_eligible(const GridDev& g)
 {
-    return g.ndim == 3 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM && g.ng >= 2;
+    return g.ndim == 3 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM && g.ng >= 2 &&
+           g.nfx == 0;
 }
 
 namespace {

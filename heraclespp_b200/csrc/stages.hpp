@@ -83,6 +83,13 @@ void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepC
                 int slot, int out_buf, int shape, cudaStream_t s);
 int mixed_shape_count(int ndim);
 bool mixed_shape_valid(const GridDev& g, int shape);
+// Dynamic shared memory of the fused tile kernels for g (g.nfx passive
+// scalars included), and the device's opt-in limit per block.
+size_t mixed_smem_bytes(const GridDev& g, int shape);
+size_t exact_smem_bytes(const GridDev& g);
+int smem_optin();
+// room left in the opt-in limit for the tile kernels' static shared memory
+constexpr size_t kFusedStaticSmemMargin = 1024;
 bool strip2d_eligible(const GridDev& g);
 // Paired schedule: two columns per lane in packed FP32 pairs (ng even).
 bool strip2d_pair_eligible(const GridDev& g);
@@ -104,6 +111,10 @@ void pack_state(const GridDev& g, const StateDev& st, const double* rho, const d
                 cudaMemcpyKind kind, cudaStream_t s);
 void unpack_state(const GridDev& g, const StateDev& st, double* rho, double* rhou, double* E, cudaMemcpyKind kind,
                   cudaStream_t s);
+// The g.nfx passive-scalar planes (after the ndim + 2 hydro planes); a null
+// fx packs zeros.
+void pack_fx(const GridDev& g, const StateDev& st, const double* fx, cudaMemcpyKind kind, cudaStream_t s);
+void unpack_fx(const GridDev& g, const StateDev& st, double* fx, cudaMemcpyKind kind, cudaStream_t s);
 
 // Compensated conservation sums of the fused state: out[0..ndim+1].
 void conservation_sums(const GridDev& g, const StateDev& st, double* partials, double* out_dev, cudaStream_t s);

@@ -37,9 +37,9 @@ def test_table_from_random_density_bitwise(ndim, nx, bc, xmin, xmax):
 
 
 def test_stage_loop_with_internal_mass_bitwise():
-    """A passive scalar selects the stage-composed loop: the table is rebuilt
-    from the density after every step (main.cpp:528) and the run equals the
-    oracle's main loop."""
+    """With a passive scalar (carried by the fused tile kernel) the table is
+    still rebuilt from the density before every step (main.cpp:528) and the
+    run equals the oracle's main loop."""
     kw = dict(gamma=1.4, limiter="VanLeer", riemann="HLLC", bc=["Reflexive", "NullGradient"],
               gravity="Internal_mass", central_mass=1e8, xmin=(0.2, 0, 0), xmax=(1.2, 1, 1))
     o = Oracle(1, [96], nfx=1, geom="Spherical", **kw)

@@ -1,7 +1,8 @@
 """Passive scalars and the pressure fix: the hcl_pressure_fix stage entry
-point against the oracle's restatement of pressure_fix.hpp, and the
-stage-composed time loop (hcl_run on handles with nfx > 0 or the pressure fix
-on) against the oracle's main loop, bit for bit."""
+point against the oracle's restatement of pressure_fix.hpp, and hcl_run
+against the oracle's main loop, bit for bit: handles with the pressure fix on
+run the stage-composed time loop, handles with passive scalars alone the
+fused tile kernel."""
 import numpy as np
 import pytest
 
