@@ -228,17 +228,16 @@ def stage_loop_cost(torch, steps=20):
     """KH 2048^2 with one passive scalar: the fused tile kernel carrying the
     scalar (FP64 and FP32-mixed) against the fused FP64 step without it and
     against hcl_run composed of the FP64 stage entry points (the reference's
-    per-stage kernels, dt and health readbacks each step; selected here by the
-    pressure fix with eps_pf = 1e-300, whose condition evol < eps_pf ekin never
-    holds on this flow).  Device time per step."""
+    per-stage kernels, dt and health readbacks each step; hcl_set_stage_loop).
+    Device time per step."""
     from heraclespp_b200 import Domain, setups
 
     kw = dict(gamma=1.4, limiter="VanLeer", riemann="HLLC", bc=["Periodic"] * 4)
     out = {"config": f"kelvin_helmholtz_2d_{NX}x{NX}_nfx1_{steps}steps"}
     runs = (("stage_loop_nfx1_fp64", 1, "fp64", True), ("fused_nfx1_fp64", 1, "fp64", False),
             ("fused_nfx1_fp32_mixed", 1, "fp32_mixed", False), ("fused_nfx0_fp64", 0, "fp64", False))
-    for name, nfx, prec, pf in runs:
-        d = Domain(2, [NX, NX], nfx=nfx, precision=prec, pressure_fix=pf, eps_pf=1e-300, **kw)
+    for name, nfx, prec, staged in runs:
+        d = Domain(2, [NX, NX], nfx=nfx, precision=prec, stage_loop=staged, **kw)
         grid = setups.Grid.from_domain(d)
         prim = setups.kelvin_helmholtz(grid)
         fx = None

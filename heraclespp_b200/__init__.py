@@ -87,7 +87,7 @@ class Domain:
     def __init__(self, ndim, nx, *, nghost=2, nfx=0, geometry="Cartesian", gamma=5.0 / 3.0, mmw=1.0,
                  limiter="VanLeer", riemann="HLL", bc=("Periodic",) * 6, gravity="Uniform", g=(0.0, 0.0, 0.0),
                  central_mass=1.0, xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0), nodes=None, precision="fp64",
-                 device=0, pressure_fix=False, eps_pf=1e-6, eos="PerfectGas"):
+                 device=0, pressure_fix=False, eps_pf=1e-6, eos="PerfectGas", stage_loop=False):
         cfg, self._nodes = make_config(ndim, nx, nghost=nghost, nfx=nfx, geometry=geometry, gamma=gamma, mmw=mmw,
                                        limiter=limiter, riemann=riemann, bc=bc, gravity=gravity, g=g,
                                        central_mass=central_mass, xmin=xmin, xmax=xmax, nodes=nodes,
@@ -97,6 +97,8 @@ class Domain:
         check(lib().hcl_create(C.byref(cfg), C.byref(h)))
         self._owned = True
         self._attach(h, cfg)
+        if stage_loop:
+            check(lib().hcl_set_stage_loop(h, 1))
 
     @classmethod
     def _view(cls, h, cfg):

@@ -38,6 +38,7 @@ EXPORTS = [
     "hcl_adjoint_forward", "hcl_adjoint_backward", "hcl_adjoint_dts", "hcl_set_schedule",
     "hcl_ensemble_create", "hcl_ensemble_destroy", "hcl_ensemble_handle", "hcl_ensemble_stream",
     "hcl_ensemble_run", "hcl_ensemble_adjoint", "hcl_pressure_fix", "hcl_internal_mass_gravity",
+    "hcl_set_stage_loop",
 ]
 
 
@@ -190,6 +191,7 @@ def lib():
     L.hcl_adjoint_backward.argtypes = [H, vp, vp, i]
     L.hcl_adjoint_dts.argtypes = [H, vp, i, C.POINTER(i)]
     L.hcl_set_schedule.argtypes = [H, i, C.POINTER(i)]
+    L.hcl_set_stage_loop.argtypes = [H, i]
     L.hcl_ensemble_create.argtypes = [C.POINTER(Config), i, C.POINTER(vp)]
     L.hcl_ensemble_destroy.argtypes = [vp]
     L.hcl_ensemble_handle.argtypes = [vp, i, C.POINTER(H)]

@@ -123,6 +123,7 @@ struct hcl_handle {
     int iter_base = 0;
     int stopped = 0;
     int mixed_shape = -1;  // autotuned tile shape of the mixed 2-D kernel
+    int force_stage = 0;   // hcl_set_stage_loop
     // dt log
     double* dt_log = nullptr;
     int dt_log_cap = 0;
@@ -328,6 +329,8 @@ void build_grid_host(hcl_handle* h)
     g.gamma_m1 = c.gamma - 1;
     g.mmw = c.mmw;
     g.eos = c.eos;
+    g.pressure_fix = c.pressure_fix;
+    g.eps_pf = c.eps_pf;
     // uniform Cartesian spacing (to 1e-12 relative) enables the fast forms of
     // the mixed kernel
     int uniform = c.geometry == HCL_GEOM_CARTESIAN;
@@ -561,11 +564,11 @@ int get_graph(hcl_handle* h, const RunParamsDev& rp, int k, cudaGraphExec_t* out
 }
 
 // Handles whose time loop is composed of the FP64 stage entry points: the
-// pressure fix, and passive scalars too many for the fused tile's shared
-// memory, are not carried by the fused kernels.
+// FP32-mixed kernels carry no pressure fix, and passive scalars too many for
+// the fused tile's shared memory are not carried at all.
 bool stage_mode(const hcl_handle* h)
 {
-    if (h->cfg.pressure_fix != 0) {
+    if (h->force_stage || (h->cfg.pressure_fix != 0 && h->cfg.precision == HCL_FP32_MIXED)) {
         return true;
     }
     if (h->cfg.nfx == 0) {
@@ -1585,6 +1588,16 @@ int hcl_step_fixed_dt(hcl_handle* h, double dt, void* stream)
                                           h->grav_shell, h->dgr, s);
         HCL_LAUNCH_CHECK();
     }
+    return HCL_OK;
+}
+
+int hcl_set_stage_loop(hcl_handle* h, int on)
+{
+    HCL_CHECK_HANDLE(h);
+    if (h->state_valid) {
+        return fail(HCL_ERR_CONFIG, "hcl_set_stage_loop: select the time loop before the state is set");
+    }
+    h->force_stage = on != 0;
     return HCL_OK;
 }
 

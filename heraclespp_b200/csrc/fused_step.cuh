@@ -825,6 +825,89 @@ k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp
     __syncthreads();
 
     // ---- phase 4: Godunov update, ghost images, health, CFL -----------------
+    // pressure_fix.hpp:19-172 on one interior cell (FP64): q the old state,
+    // qn the Godunov update, whose energy it may replace.  The face states are
+    // the predicted ones in shared memory, the neighbours' old states come
+    // from global memory; expression order as in the reference (the energy is
+    // overwritten in the inner loop and the last value stays).
+    auto pressure_fix_cell = [&](int x0, int x1, int x2, int gi, int gj, int gk, int64_t cgl, const double* q,
+                                 double* qn) {
+        const double ekin = exact::ek_cons<ND>(q);
+        const double evol = q[1 + ND] - ekin;
+        const double eps = g.eps_pf;
+        if (!(evol < eps * ekin)) {
+            return;
+        }
+        double prim[NV];
+        exact::to_prim<ND>(eeos, q, prim);
+        const double de_god = (qn[1 + ND] - exact::ek_cons<ND>(qn)) - evol;
+        const double eps2 = eps / 10;
+        double alpha = (evol * evol) / (ekin * ekin * eps * eps);
+        if (evol < eps2 * ekin) {
+            alpha = 0;
+        }
+        double sum = 0;
+#pragma unroll
+        for (int idr = 0; idr < ND; ++idr) {
+            sum += q[1 + idr] * q[1 + idr] / q[0];
+        }
+        double divU = 0, divUE = 0, einL = 0, einR = 0;
+        double En = q[1 + ND];
+        const int xs3[3] = {x0, x1, x2};
+#pragma unroll
+        for (int idim = 0; idim < ND; ++idim) {
+            const int di = idim == 0, dj = idim == 1, dk = idim == 2;
+            const int64_t cp = lidx(g, gi + di, gj + dj, gk + dk);
+            const int64_t om = sidx(in, g.n[1], gi - di, gj - dj, gk - dk);
+            const int64_t op = sidx(in, g.n[1], gi + di, gj + dj, gk + dk);
+            double qm[NV], qp[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                qm[v] = in.q[om + in.plane * v];
+                qp[v] = in.q[op + in.plane * v];
+            }
+            const R* ab = sa + S::Aoff(idim);
+            const int a = (xs3[0] + di) + S::Adim(idim, 0) * ((xs3[1] + dj) + S::Adim(idim, 1) * (xs3[2] + dk));
+            const int astep = idim == 0 ? 1 : (idim == 1 ? S::Adim(idim, 0) : S::Adim(idim, 0) * S::Adim(idim, 1));
+            double vL[NV], vR[NV], mR[NV], pL[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                vL[v] = ab[v * S::Asize(idim) + a];
+                vR[v] = ab[(NV + v) * S::Asize(idim) + a];
+                mR[v] = ab[(NV + v) * S::Asize(idim) + a - astep];
+                pL[v] = ab[v * S::Asize(idim) + a + astep];
+            }
+            double primL[NV], primR[NV], prim_mR[NV], prim_pL[NV];
+            exact::to_prim<ND>(eeos, vL, primL);
+            exact::to_prim<ND>(eeos, vR, primR);
+            exact::to_prim<ND>(eeos, mR, prim_mR);
+            exact::to_prim<ND>(eeos, pL, prim_pL);
+            const double dv = g.dv[cgl];
+#pragma unroll
+            for (int ipos = 0; ipos < ND; ++ipos) {
+                const double us = (prim_mR[1 + ipos] + primL[1 + ipos]) / 2;
+                const double us_p = (primR[1 + ipos] + prim_pL[1 + ipos]) / 2;
+                const double dsp = g.ds[cp + g.N * ipos];
+                const double dsc = g.ds[cgl + g.N * ipos];
+                divU += ((us_p * dsp) - (us * dsc)) / dv;
+                if (us_p > 0) {
+                    einR = q[1 + ND] - exact::ek_cons<ND>(q);
+                } else {
+                    einR = qp[1 + ND] - exact::ek_cons<ND>(qp);
+                }
+                if (us < 0) {
+                    einL = q[1 + ND] - exact::ek_cons<ND>(q);
+                } else {
+                    einL = qm[1 + ND] - exact::ek_cons<ND>(qm);
+                }
+                divUE += ((us_p * einR * dsp) - (us * einL * dsc)) / dv;
+                const double de_pf = dt * ((-prim[1 + ND] * divU) - divUE);
+                const double de_tot = (alpha * de_god) + ((1 - alpha) * de_pf);
+                En = evol + de_tot + (1. / 2 * sum);
+            }
+        }
+        qn[1 + ND] = En;
+    };
     double inv_local = 0.0;
     for (int c = tid; c < S::TVOL; c += NT) {
         const int x0 = c % S::T0;
@@ -1011,6 +1094,12 @@ k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 qn[v] = q[v] + acc[v];
+            }
+        }
+
+        if constexpr (EXACT) {
+            if (g.pressure_fix) {
+                pressure_fix_cell(x0, x1, x2, gi, gj, gk, cgl, q, qn);
             }
         }
 

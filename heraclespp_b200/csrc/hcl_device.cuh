@@ -43,6 +43,8 @@ struct GridDev {
     double g[3];
     double gamma, gamma_m1, mmw;
     int eos;              // EOS_PERFECT_GAS or EOS_RAD_GAS
+    int pressure_fix;     // [Pressure fix] On (the FP64 fused step applies it)
+    double eps_pf;
     // grid arrays (device)
     const double* x[3];   // nodes (n+1)
     const double* dx[3];  // n

@@ -282,6 +282,15 @@ int hcl_get_dt_log(hcl_handle* h, double* dts, int max_count, int* count);
  * ran). */
 int hcl_set_schedule(hcl_handle* h, int schedule, int* used);
 
+/* Selects the time loop of hcl_run: 0 (default) the fused loop wherever the
+ * fused kernels carry the handle's features, 1 the loop composed of the FP64
+ * stage entry points in the reference's order (main.cpp:354-531, one kernel
+ * per Kokkos kernel, dt and the health check read back each step).  Both
+ * give the same FP64 results; the staged loop is the reference's own
+ * structure, for stage-wise comparisons.  Call before the first state is
+ * set (HCL_ERR_CONFIG afterwards). */
+int hcl_set_stage_loop(hcl_handle* h, int on);
+
 /* Compensated FP64 sums over no_ghosts: out[0] = sum rho dv, out[1..ndim] =
  * sum rhou_d dv, out[ndim+1] = sum E dv.  Deterministic. */
 int hcl_conservation_sums(hcl_handle* h, double* out);

@@ -101,9 +101,10 @@ def test_driver_rejects_unknown_keys(tmp_path):
     assert res.returncode != 0 and "Invalid gamma" in res.stderr
 
 
-def test_driver_runs_stage_loop_for_passive_scalars_and_pressure_fix(tmp_path):
-    """[Passive Scalar] nfx and [Pressure fix] On select the stage-composed
-    loop; the driver's result equals the oracle's main loop bit for bit."""
+def test_driver_runs_passive_scalars_and_pressure_fix(tmp_path):
+    """[Passive Scalar] nfx and [Pressure fix] On (both carried by the fused
+    FP64 tile kernel): the driver's result equals the oracle's main loop bit
+    for bit."""
     ini = tmp_path / "sod_pf.ini"
     ini.write_text(SOD_INI + "\n[Passive Scalar]\nnfx = 1\n\n[Pressure fix]\npressure_fix = On\neps_pf = 4\n")
     dump = tmp_path / "out.bin"

@@ -1,8 +1,8 @@
 """Passive scalars and the pressure fix: the hcl_pressure_fix stage entry
 point against the oracle's restatement of pressure_fix.hpp, and hcl_run
-against the oracle's main loop, bit for bit: handles with the pressure fix on
-run the stage-composed time loop, handles with passive scalars alone the
-fused tile kernel."""
+against the oracle's main loop, bit for bit, both as the fused FP64 tile
+kernel (which carries the scalars and the pressure fix) and as the loop
+composed of the stage entry points (hcl_set_stage_loop)."""
 import numpy as np
 import pytest
 
@@ -80,12 +80,13 @@ STAGE_CASES = [
 ]
 
 
+@pytest.mark.parametrize("staged", [True, False], ids=["stage_loop", "fused"])
 @pytest.mark.parametrize("ndim,nx,nfx,pf,eps,steps,fails", STAGE_CASES)
-def test_stage_loop_matches_oracle_bitwise(ndim, nx, nfx, pf, eps, steps, fails):
+def test_stage_loop_matches_oracle_bitwise(ndim, nx, nfx, pf, eps, steps, fails, staged):
     bc = ["NullGradient", "Reflexive"] if ndim == 1 else ["NullGradient", "Periodic", "Reflexive", "Reflexive"]
     kw = dict(gamma=1.4, limiter="Minmod", riemann="HLLC", bc=bc)
     o = Oracle(ndim, nx, nfx=nfx, **kw)
-    d = Domain(ndim, nx, nfx=nfx, pressure_fix=pf, eps_pf=eps, **kw)
+    d = Domain(ndim, nx, nfx=nfx, pressure_fix=pf, eps_pf=eps, stage_loop=staged, **kw)
     rho, rhou, E, fx = o.init_from_prim(*smooth_low_energy(o, -3))
     if nfx:
         grid = setups.Grid.from_domain(o)
