@@ -458,11 +458,14 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
     }
 }
 
-// NT threads per CTA (any count: every phase strides over its items by NT)
+// NT threads per CTA (any count: every phase strides over its items by NT).
+// The FP32 sweep runs three CTAs per SM (56 registers, a few spilled): the
+// tile's phases wait at barriers and the third CTA fills those waits
+// (Gresho 512^2 backward pass 25.4 -> 23.8 ms).
 template <class R, int NT>
 constexpr int adj_min_blocks()
 {
-    return sizeof(R) == 8 ? (NT <= 256 ? 2 : 1) : (NT <= 256 ? 3 : (NT <= 384 ? 2 : 1));
+    return sizeof(R) == 8 ? (NT <= 256 ? 2 : 1) : (NT <= 256 ? 3 : (NT <= 384 ? 3 : 1));
 }
 
 template <int ND, class R, int TX, int TY, int TZ, int NT>

@@ -315,8 +315,11 @@ __device__ __forceinline__ void store_images_3d(double* __restrict__ q, int64_t 
 // EOSK: the EOS as a compile-time constant (EOS_PERFECT_GAS or EOS_RAD_GAS;
 // the FP32-mixed variant is perfect gas only), so that the FP64 physics
 // carries no run-time EOS branch.
+// The 2-D FP64 tile asks for three CTAs per SM (80 registers, some spilled):
+// its phases wait at barriers, and a third CTA fills those waits (KH 2048^2:
+// 1.19 -> 1.02 ms per step; 16x8 tiles at five CTAs per SM: 1.15 ms).
 template <int ND, bool EXACT, int TX, int TY, int TZ, int EOSK = EOS_PERFECT_GAS>
-__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1))
+__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1), (EXACT && ND == 2) ? 3 : 1)
 k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf)
 {
     using S = Shape<ND, TX, TY, TZ>;
