@@ -57,6 +57,16 @@ def parse():
     return p.parse_args()
 
 
+# HBM3e of an HGX B200 (7.7 TB/s nominal), beside the measured copy peak
+HBM_SPEC_GBS = 7700.0
+# Algorithmic HBM bytes per cell and step of one gradient (forward with
+# checkpoints, recomputation, reverse sweep): the forward step reads and writes
+# the 32-byte state (64 B), the recomputation repeats it (64 B), the reverse
+# step reads the state and the incoming adjoint and writes the outgoing one
+# (96 B); the checkpoints add 64 B per cell every k steps.
+ADJ_BYTES_PER_CELL_STEP = 64 + 64 + 96
+
+
 def kh_domain(precision):
     from heraclespp_b200 import Domain, setups
 
@@ -219,7 +229,10 @@ def adjoint_cost(torch, nsteps=400, n=512, k=32):
         gradient()  # warm: checkpoint and segment buffers, the second stream
         d.set_state_from_prim(*prim)
         adj = timed(gradient)
-        out[prec] = {"forward_ms": fwd, "gradient_ms": adj, "adj_over_fwd": adj / fwd}
+        cells = n * n
+        algo = cells * (nsteps * ADJ_BYTES_PER_CELL_STEP + (nsteps // k) * 64)
+        out[prec] = {"forward_ms": fwd, "gradient_ms": adj, "adj_over_fwd": adj / fwd,
+                     "gradient_algorithmic_gb": algo * 1e-9, "gradient_achieved_gbs": algo / (adj * 1e-3) * 1e-9}
         d.close()
     return out
 
@@ -551,6 +564,7 @@ def run_ours(args):
                      "steps_compared": int(len(dts))},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic,
+                     "peak_spec": HBM_SPEC_GBS, "frac_of_spec": achieved / HBM_SPEC_GBS,
                      "peak_source": f"{peaks_kind} (MEASURED_PEAKS.json hbm_gbs)" if peaks_kind == "measured"
                      else "fallback 6.65 TB/s",
                      "bytes_per_cell": BYTES_PER_CELL, "cells_per_launch": CELLS},
