@@ -12,6 +12,13 @@
 
 namespace hcl::fused {
 
+namespace {
+bool big_tile_3d_fits(const GridDev& g)
+{
+    return FusedLauncher<3, true, 8, 8, 4>::smem(g.nfx) + kFusedStaticSmemMargin <= (size_t)smem_optin();
+}
+} // namespace
+
 void step_exact(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                 int slot, int out_buf, cudaStream_t s)
 {
@@ -23,7 +30,13 @@ void step_exact(const GridDev& g, const StateDev& in, const StateDev& out, StepC
         FusedLauncher<2, true, 16, 16, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
         break;
     default:
-        FusedLauncher<3, true, 8, 4, 4>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        // 8x8x4 tiles (less halo than 8x4x4: RT 256^2 x 512 39.9 -> 33.9 ms per
+        // step) unless the passive scalars need the smaller tile's shared memory
+        if (big_tile_3d_fits(g)) {
+            FusedLauncher<3, true, 8, 8, 4>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        } else {
+            FusedLauncher<3, true, 8, 4, 4>::launch(g, in, out, ctl, rp, slot, out_buf, s);
+        }
         break;
     }
 }
@@ -36,7 +49,8 @@ size_t exact_smem_bytes(const GridDev& g)
     case 2:
         return FusedLauncher<2, true, 16, 16, 1>::smem(g.nfx);
     default:
-        return FusedLauncher<3, true, 8, 4, 4>::smem(g.nfx);
+        return big_tile_3d_fits(g) ? FusedLauncher<3, true, 8, 8, 4>::smem(g.nfx)
+                                   : FusedLauncher<3, true, 8, 4, 4>::smem(g.nfx);
     }
 }
 
@@ -56,6 +70,7 @@ void configure_exact()
     FusedLauncher<1, true, 128, 1, 1>::configure();
     FusedLauncher<2, true, 16, 16, 1>::configure();
     FusedLauncher<3, true, 8, 4, 4>::configure();
+    FusedLauncher<3, true, 8, 8, 4>::configure();
 }
 
 namespace {
