@@ -131,3 +131,40 @@ def test_fused_passive_scalars_mixed_close_to_fp64(ndim, nx, nfx, bc, extra, ste
     for f in range(nfx):
         assert rel(fx_d[f], fx[f]) < 1e-5
     assert fx_d.min() >= 0.0 and fx_d.max() <= 1.0
+
+
+def _other_physics_cases():
+    from cases import CASES as PARITY_CASES
+    out = []
+    for name in ("sph_2d", "sph_3d", "sph_2d_internalmass"):
+        ndim, nx, kw, setup, skw = PARITY_CASES[name]
+        out.append((name, ndim, nx, kw, skw))
+    rad = dict(gamma=5.0 / 3.0, mmw=0.6, limiter="Minmod", riemann="HLLC", eos="RadGas")
+    out.append(("radgas_2d", 2, [40, 32], dict(rad, bc=["NullGradient"] * 4),
+                dict(rho0=1.0, rho1=0.125, P0=1e13, P1=1e11)))
+    return out
+
+
+@pytest.mark.parametrize("name,ndim,nx,kw,skw", _other_physics_cases(), ids=lambda v: v if isinstance(v, str) else "")
+def test_fused_passive_scalars_other_physics_bitwise(name, ndim, nx, kw, skw):
+    """Spherical geometry (with the geometric sources and the internal-mass
+    gravity) and the RadGas EOS with two passive scalars: FP64 fused loop
+    against the oracle's main loop, bit for bit."""
+    from cases import oracle_kwargs
+    nfx = 2
+    o = Oracle(ndim, nx, nfx=nfx, **oracle_kwargs(kw))
+    d = Domain(ndim, nx, nfx=nfx, **kw)
+    rho, rhou, E, fx = o.init_from_prim(*setups.shock_tube(setups.Grid.from_domain(o), **skw))
+    scalar_fields(o, fx, nfx)
+    o.boundaries(rho, rhou, E, fx)
+    d.set_state(rho, rhou, E, fx=fx)
+    steps = 25
+    t_o, it_o, st_o, dts_o = o.run(rho, rhou, E, fx, cfl=0.4, max_iter=steps, record_dts=True)
+    assert st_o == 0 and it_o == steps
+    r = d.run(cfl=0.4, max_iter=steps)
+    assert r.iter == it_o and r.t == t_o
+    assert np.array_equal(d.dt_log(), dts_o)
+    fx_d = np.zeros_like(fx)
+    r_d, m_d, E_d = d.get_state(fx=fx_d)
+    assert np.array_equal(r_d, rho) and np.array_equal(m_d, rhou) and np.array_equal(E_d, E)
+    assert np.array_equal(fx_d, fx)
