@@ -19,6 +19,12 @@ std::atomic<int64_t> g_launches{0};
 namespace {
 
 constexpr int kThreads = 256;
+// The two heaviest stage kernels (Hancock predictor, Godunov update: long FP64
+// dependency chains in the reference's order, 130-140 registers unbounded)
+// ask for three CTAs per SM; the extra warps hide the chains' latency (KH
+// 2048^2 FP64 stage-composed step with one passive scalar 3.81 -> 2.61 ms,
+// two CTAs per SM 2.68 ms; the same bits).
+constexpr int kHeavyMinBlocks = 3;
 
 struct Box {
     int b[3];
@@ -180,7 +186,7 @@ __global__ void k_faces_prim_to_cons(GridDev g, Box bx, const double* __restrict
 
 // extrapolation_reconstruction.hpp:90-325 "Hancock_extrapolation"
 template <int ND>
-__global__ void k_hancock(GridDev g, Box bx, double dt, const double* __restrict__ u_rec,
+__global__ void __launch_bounds__(kThreads, kHeavyMinBlocks) k_hancock(GridDev g, Box bx, double dt, const double* __restrict__ u_rec,
                           const double* __restrict__ P_rec, double* __restrict__ rho_rec, double* __restrict__ rhou_rec,
                           double* __restrict__ E_rec, double* __restrict__ fx_rec, const double* __restrict__ fx_rec_old)
 {
@@ -341,7 +347,7 @@ __global__ void k_passive_extrap(GridDev g, Box bx, const double* __restrict__ r
 
 // godunov_scheme.hpp:110-292 "Riemann_based_Godunov_scheme"
 template <int ND>
-__global__ void k_godunov(GridDev g, Box bx, double dt, const double* __restrict__ rho, const double* __restrict__ rhou,
+__global__ void __launch_bounds__(kThreads, kHeavyMinBlocks) k_godunov(GridDev g, Box bx, double dt, const double* __restrict__ rho, const double* __restrict__ rhou,
                           const double* __restrict__ E, const double* __restrict__ fx,
                           const double* __restrict__ rho_rec, const double* __restrict__ rhou_rec,
                           const double* __restrict__ E_rec, const double* __restrict__ fx_rec,
