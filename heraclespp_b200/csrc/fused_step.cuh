@@ -315,11 +315,21 @@ __device__ __forceinline__ void store_images_3d(double* __restrict__ q, int64_t 
 // EOSK: the EOS as a compile-time constant (EOS_PERFECT_GAS or EOS_RAD_GAS;
 // the FP32-mixed variant is perfect gas only), so that the FP64 physics
 // carries no run-time EOS branch.
-// The 2-D FP64 tile asks for three CTAs per SM (80 registers, some spilled):
-// its phases wait at barriers, and a third CTA fills those waits (KH 2048^2:
-// 1.19 -> 1.02 ms per step; 16x8 tiles at five CTAs per SM: 1.15 ms).
+// Occupancy: the tiles' phases wait at barriers and on dependency chains, and
+// more resident CTAs fill those waits.  The 2-D FP64 tile asks for three CTAs
+// per SM (80 registers, some spilled; KH 2048^2: 1.19 -> 1.02 ms per step,
+// 16x8 tiles at five CTAs per SM: 1.15 ms), the 256-thread FP32-mixed 2-D
+// tiles for three (KH 2048^2 with a passive scalar: 0.55 -> 0.42 ms) and the
+// FP32-mixed 3-D tile for two (RT 256^2 x 512 with a passive scalar: 14.3 ->
+// 9.1 ms).
+template <int ND, bool EXACT, int TX, int TY, int TZ>
+constexpr int fused_min_blocks()
+{
+    return ND == 2 ? ((EXACT || TX * TY == 256) ? 3 : 1) : ((!EXACT && ND == 3) ? 2 : 1);
+}
+
 template <int ND, bool EXACT, int TX, int TY, int TZ, int EOSK = EOS_PERFECT_GAS>
-__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1), (EXACT && ND == 2) ? 3 : 1)
+__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1), fused_min_blocks<ND, EXACT, TX, TY, TZ>())
 k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf)
 {
     using S = Shape<ND, TX, TY, TZ>;
