@@ -316,21 +316,23 @@ __device__ __forceinline__ void store_images_3d(double* __restrict__ q, int64_t 
 // the FP32-mixed variant is perfect gas only), so that the FP64 physics
 // carries no run-time EOS branch.
 // Occupancy: the tiles' phases wait at barriers and on dependency chains, and
-// more resident CTAs fill those waits.  The 2-D FP64 tile asks for three CTAs
-// per SM (80 registers, some spilled; KH 2048^2: 1.19 -> 1.02 ms per step,
-// 16x8 tiles at five CTAs per SM: 1.15 ms), the 256-thread FP32-mixed 2-D
-// tiles for three (KH 2048^2 with a passive scalar: 0.55 -> 0.42 ms) and the
-// FP32-mixed 3-D tile for two (RT 256^2 x 512 with a passive scalar: 14.3 ->
-// 9.1 ms).
+// more resident CTAs fill those waits.  Where the shared memory of a launch
+// leaves room for them (no passive scalars), the 2-D FP64 tile runs three CTAs
+// per SM (80 registers, some spilled; KH 2048^2: 1.19 -> 1.02 ms per step;
+// 16x8 tiles at five CTAs per SM: 1.15 ms).  The other tiles (0 here) keep
+// the compiler's register choice, which already gives the FP32-mixed 2-D
+// 256-thread tiles three CTAs per SM and the 3-D tile two (asking for a
+// minimum of one block instead lets it take more registers: RT 256^2 x 512
+// with a passive scalar 8.8 -> 14.3 ms).
 template <int ND, bool EXACT, int TX, int TY, int TZ>
 constexpr int fused_min_blocks()
 {
-    return ND == 2 ? ((EXACT || TX * TY == 256) ? 3 : 1) : ((!EXACT && ND == 3) ? 2 : 1);
+    return (EXACT && ND == 2) ? 3 : 0;
 }
 
-template <int ND, bool EXACT, int TX, int TY, int TZ, int EOSK = EOS_PERFECT_GAS>
-__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1), fused_min_blocks<ND, EXACT, TX, TY, TZ>())
-k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf)
+template <int ND, bool EXACT, int TX, int TY, int TZ, int EOSK>
+__device__ __forceinline__ void fused_step_body(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl,
+                                                const RunParamsDev& rp, int slot, int out_buf)
 {
     using S = Shape<ND, TX, TY, TZ>;
     using R = std::conditional_t<EXACT, double, float>;
@@ -1297,6 +1299,22 @@ k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp
     }
 }
 
+template <int ND, bool EXACT, int TX, int TY, int TZ, int EOSK = EOS_PERFECT_GAS>
+__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1))
+k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf)
+{
+    fused_step_body<ND, EXACT, TX, TY, TZ, EOSK>(g, in, out, ctl, rp, slot, out_buf);
+}
+
+// the same step with the occupancy bound above (instantiated where it is > 0)
+template <int ND, bool EXACT, int TX, int TY, int TZ, int EOSK = EOS_PERFECT_GAS>
+__global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1),
+                                  fused_min_blocks<ND, EXACT, TX, TY, TZ>() > 0 ? fused_min_blocks<ND, EXACT, TX, TY, TZ>() : 1)
+k_fused_step_occ(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf)
+{
+    fused_step_body<ND, EXACT, TX, TY, TZ, EOSK>(g, in, out, ctl, rp, slot, out_buf);
+}
+
 template <int ND, bool EXACT, int TX, int TY, int TZ>
 struct FusedLauncher {
     using S = Shape<ND, TX, TY, TZ>;
@@ -1312,12 +1330,34 @@ struct FusedLauncher {
     // block (launches without passive scalars use smem(0) and keep their
     // occupancy); called once per process before any launch (never during
     // stream capture).
+    static constexpr int kMinBlocks = fused_min_blocks<ND, EXACT, TX, TY, TZ>();
     static void configure()
     {
         set_max_dynamic(reinterpret_cast<const void*>(k_fused_step<ND, EXACT, TX, TY, TZ>));
         if constexpr (EXACT) {
             set_max_dynamic(reinterpret_cast<const void*>(k_fused_step<ND, EXACT, TX, TY, TZ, EOS_RAD_GAS>));
         }
+        if constexpr (kMinBlocks > 0) {
+            set_max_dynamic(reinterpret_cast<const void*>(k_fused_step_occ<ND, EXACT, TX, TY, TZ>));
+            if constexpr (EXACT) {
+                set_max_dynamic(reinterpret_cast<const void*>(k_fused_step_occ<ND, EXACT, TX, TY, TZ, EOS_RAD_GAS>));
+            }
+        }
+    }
+    // the occupancy-bounded kernel pays off when that many CTAs fit the SM's
+    // shared memory (1 KB reserved per CTA, 256 B static)
+    static bool use_occ(int nfx)
+    {
+        if constexpr (kMinBlocks > 0) {
+            static const int per_sm = [] {
+                int dev = 0, v = 0;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+                return v;
+            }();
+            return (size_t)kMinBlocks * (smem(nfx) + 1024 + 256) <= (size_t)per_sm;
+        }
+        return false;
     }
     // the per-block opt-in limit less the kernel's static shared memory
     static void set_max_dynamic(const void* fn)
@@ -1338,9 +1378,17 @@ struct FusedLauncher {
         const int nt1 = (g.nx[1] + S::T1 - 1) / S::T1;
         const int nt2 = (g.nx[2] + S::T2 - 1) / S::T2;
         const int blocks = nt0 * nt1 * nt2;
+        const bool occ = use_occ(g.nfx);
         if (EXACT && g.eos == EOS_RAD_GAS) {
-            k_fused_step<ND, EXACT, TX, TY, TZ, EOS_RAD_GAS><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot,
-                                                                                        out_buf);
+            if (occ) {
+                k_fused_step_occ<ND, EXACT, TX, TY, TZ, EOS_RAD_GAS><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp,
+                                                                                            slot, out_buf);
+            } else {
+                k_fused_step<ND, EXACT, TX, TY, TZ, EOS_RAD_GAS><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot,
+                                                                                            out_buf);
+            }
+        } else if (occ) {
+            k_fused_step_occ<ND, EXACT, TX, TY, TZ><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot, out_buf);
         } else {
             k_fused_step<ND, EXACT, TX, TY, TZ><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot, out_buf);
         }
