@@ -38,7 +38,11 @@ size_t mixed_smem_bytes(const GridDev& g, int shape)
 bool mixed_shape_valid(const GridDev& g, int shape)
 {
     if (g.nfx > 0) {
-        // passive scalars ride in the shared-memory tiles only
+        // passive scalars ride in the shared-memory tiles and, one of them,
+        // in the 4-warp strips
+        if (g.ndim == 2 && shape >= 3 && shape <= 6) {
+            return strip2d_fx_eligible(g);
+        }
         return (g.ndim == 2 ? shape < 3 : shape == 0) && mixed_smem_bytes(g, shape) + kFusedStaticSmemMargin <= (size_t)smem_optin();
     }
     if (g.ndim == 3) {
@@ -71,7 +75,7 @@ void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepC
             step_strip2d(g, in, out, ctl, rp, slot, out_buf, 0, true, s);
         } else if (shape >= 7 && shape < 9 && strip2d_pair_eligible(g)) {
             step_strip2d_pair(g, in, out, ctl, rp, slot, out_buf, shape == 7 ? 0 : 32, s);
-        } else if (shape >= 3 && strip2d_eligible(g)) {
+        } else if (shape >= 3 && (strip2d_eligible(g) || (shape <= 6 && strip2d_fx_eligible(g)))) {
             step_strip2d(g, in, out, ctl, rp, slot, out_buf, shape == 3 ? 32 : (shape == 4 ? 64 : (shape == 5 ? 128 : 0)),
                          false, s);
         } else if (shape == 1) {

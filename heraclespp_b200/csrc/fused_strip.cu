@@ -15,6 +15,12 @@ bool strip2d_eligible(const GridDev& g)
     return g.ndim == 2 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM && g.nfx == 0;
 }
 
+// Strips with one passive scalar (schedules 3-6 only).
+bool strip2d_fx_eligible(const GridDev& g)
+{
+    return g.ndim == 2 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM && g.nfx == 1;
+}
+
 // The paired schedule loads and stores column pairs as 16-byte vectors: the
 // first column of a pair is even, which needs an even ghost width.
 bool strip2d_pair_eligible(const GridDev& g)
@@ -33,6 +39,20 @@ int resident_blocks()
         int per_sm = 0, nsm = 0, dev = 0;
         cudaGetDevice(&dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip2d<LIM, RS>, 128, 0);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cached = per_sm > 0 && nsm > 0 ? per_sm * nsm : 148;
+    }
+    return cached;
+}
+
+template <int LIM, int RS>
+int resident_blocks_fx()
+{
+    static int cached = 0;
+    if (cached == 0) {
+        int per_sm = 0, nsm = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip2d_fx<LIM, RS>, 128, 0);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cached = per_sm > 0 && nsm > 0 ? per_sm * nsm : 148;
     }
@@ -66,8 +86,11 @@ void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCt
                int out_buf, int L, bool sync, cudaStream_t s)
 {
     const int ncolw = (g.nx[0] + kStripLanesOut - 1) / kStripLanesOut;
+    const bool fx = g.nfx == 1;
+    sync = sync && !fx;
     const int wpb = sync ? kStripSyncWarps : 4;
-    const int resident = sync ? resident_blocks_sync<LIM, RS>() : resident_blocks<LIM, RS>();
+    const int resident = sync ? resident_blocks_sync<LIM, RS>()
+                              : (fx ? resident_blocks_fx<LIM, RS>() : resident_blocks<LIM, RS>());
     if (L <= 0) {
         const int per_col = std::max(1, resident * wpb / ncolw);
         L = std::max(8, (g.nx[1] + per_col - 1) / per_col);
@@ -77,6 +100,8 @@ void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCt
     const int blocks = std::min((warps + wpb - 1) / wpb, resident);
     if (sync) {
         k_strip2d_sync<LIM, RS><<<blocks, 32 * kStripSyncWarps, kSyncSmem, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
+    } else if (fx) {
+        k_strip2d_fx<LIM, RS><<<blocks, 128, 0, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
     } else {
         k_strip2d<LIM, RS><<<blocks, 128, 0, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
     }

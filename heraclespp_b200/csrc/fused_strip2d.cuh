@@ -106,10 +106,16 @@ __device__ __forceinline__ void cons_and_flux(const fast::Eos& e, const float w[
     F[3] = ul * (Et + w[3]);
 }
 
-// Hancock face states of one cell: x-left, x-right, y-bottom, y-top (conservative)
-template <int LIM>
+// Hancock face states of one cell: x-left, x-right, y-bottom, y-top (conservative).
+// NFX = 1: also the passive scalar's face values xo[4] (same order, fractions)
+// from its primitives xw = {row below, this row, row above}: limited slopes,
+// times the face density before the predictor, plus the predictor's
+// increment from the face states' mass fluxes, divided by the predicted face
+// density (extrapolation_reconstruction.hpp:315-337, :459-469).
+template <int LIM, int NFX = 0>
 __device__ __forceinline__ void strip_hancock(const StripCtx& c, const float wd[4], const float wc[4], const float wu[4],
-                                              float hxL[4], float hxR[4], float hyB[4], float hyT[4])
+                                              float hxL[4], float hxR[4], float hyB[4], float hyT[4],
+                                              const float* xw = nullptr, float* xo = nullptr)
 {
     float fxL[4], fxR[4], fyB[4], fyT[4];
 #pragma unroll
@@ -150,6 +156,19 @@ __device__ __forceinline__ void strip_hancock(const StripCtx& c, const float wd[
             u[3] = u[3] + inc[3];
         }
     }
+    if constexpr (NFX > 0) {
+        const float xl = __shfl_up_sync(0xffffffffu, xw[1], 1);
+        const float xr = __shfl_down_sync(0xffffffffu, xw[1], 1);
+        const float sx = half_lim_fast<LIM>(xr - xw[1], xw[1] - xl);
+        const float sy = half_lim_fast<LIM>(xw[2] - xw[1], xw[1] - xw[0]);
+        const float pf[4] = {xw[1] - sx, xw[1] + sx, xw[1] - sy, xw[1] + sy};
+        const float xinc = fmaf(c.cthx, pf[0] * FxL[0] - pf[1] * FxR[0], c.cthy * (pf[2] * FyB[0] - pf[3] * FyT[0]));
+        const float rho_pre[4] = {fxL[0], fxR[0], fyB[0], fyT[0]};
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            xo[f] = __fdividef(fmaf(pf[f], rho_pre[f], xinc), outs[f][0]);
+        }
+    }
 }
 
 template <int RS>
@@ -159,8 +178,46 @@ __device__ __forceinline__ void strip_riemann(const fast::Eos& e, const float* L
 }
 
 // Shared-memory row ring of one warp: 8 row slots x 4 variables x 32 lanes.
-using StripRing = double (*)[4][32];
+// Ghost images of one scalar plane q (no sign flips): the loop of
+// store_images_2d for a single value.
+__device__ __forceinline__ void store_images_2d_scalar(double* __restrict__ q, int pitch, int n0, int n1, int ng, int col,
+                                                       int r, unsigned xm, unsigned ym, double v)
+{
+    unsigned yb = ym & 0xffffu;
+    int py = r;
+    bool self_y = true;
+    for (;;) {
+        unsigned xb = xm & 0xffffu;
+        int px = col;
+        bool self_x = true;
+        for (;;) {
+            if (!(self_x && self_y)) {
+                q[(int64_t)py * pitch + px] = v;
+            }
+            if (xb == 0u) {
+                break;
+            }
+            const int k = __ffs(xb) - 1;
+            xb &= xb - 1u;
+            px = ghost_slot(k, n0, ng);
+            self_x = false;
+        }
+        if (yb == 0u) {
+            break;
+        }
+        const int k = __ffs(yb) - 1;
+        yb &= yb - 1u;
+        py = ghost_slot(k, n1, ng);
+        self_y = false;
+    }
+}
+
+// With a passive scalar the ring holds 5 variables.
+template <int NVR>
+using StripRingN = double (*)[NVR][32];
+using StripRing = StripRingN<4>;
 constexpr int kStripRingDoubles = 8 * 4 * 32;
+constexpr int kStripRingDoublesFx = 8 * 5 * 32;
 
 // One strip (28 columns x rows [r0, r1)) of one domain: reads qin, writes qout.
 // Accumulates the CFL max and the first bad cell of the lanes' output cells.
@@ -171,10 +228,14 @@ constexpr int kStripRingDoubles = 8 * 4 * 32;
 // XIMG: border columns with up to XIMG x images (1: Periodic, Reflexive; 2:
 // also NullGradient with two ghost layers) store them without a divergent
 // branch.
-template <int LIM, int RS, int SYNC = 0, int XIMG = 1>
+// NFX = 1: one passive scalar (state plane 4) rides along: face values from
+// strip_hancock, upwind fluxes from the Riemann mass fluxes
+// (godunov_scheme.hpp:262-301), the update in FP64 divided by the new density
+// and clamped to [0, 1], stored with the same ghost images.
+template <int LIM, int RS, int SYNC = 0, int XIMG = 1, int NFX = 0>
 __device__ __forceinline__ void strip_work(const GridDev& g, const double* __restrict__ qin, double* __restrict__ qout,
                                            int64_t plane, int pitch, double dt, int sx, int sy, int L, double& inv_max,
-                                           int64_t& bad_cell, StripRing ring)
+                                           int64_t& bad_cell, StripRingN<4 + NFX> ring)
 {
     const int lane = threadIdx.x & 31;
     const int n0 = g.n[0], n1 = g.n[1];
@@ -218,15 +279,15 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         const int rc = min(max(r, 0), n1 - 1);
         const int64_t o = (int64_t)rc * pitch + colc;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
+        for (int v = 0; v < 4 + NFX; ++v) {
             const unsigned dst = (unsigned)__cvta_generic_to_shared(&ring[r & 7][v][lane]);
             asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(qin + o + plane * v) : "memory");
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
-    auto ring_row = [&](int r, double q[4]) {
+    auto ring_row = [&](int r, double* q) {
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
+        for (int v = 0; v < 4 + NFX; ++v) {
             q[v] = ring[r & 7][v][lane];
         }
     };
@@ -235,29 +296,53 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     float wB[4], wC[4], wD[4];
     float hxL[4], hxR[4], hyT[4];
     double Glo[4];
+    // passive scalar: primitives of rows r, r+1; face values of row r (x-left,
+    // x-right, y-top); upwind flux of the y-face r-1/2
+    float xC = 0.f, xD = 0.f, xoL = 0.f, xoR = 0.f, xoT = 0.f, gx_lo = 0.f;
     {
-        double q[4];
+        double q[4 + NFX];
         float wA[4], hyB[4];
+        float xA = 0.f, xB = 0.f;
         for (int rr = r0 - 2; rr <= r0 + 3; ++rr) {
             stage_row(rr);
         }
         asm volatile("cp.async.wait_group 2;\n" ::: "memory"); // rows r0-2 .. r0+1 landed
         ring_row(r0 - 2, q);
         strip_prim(gm1, q, wA);
+        if constexpr (NFX > 0) {
+            xA = (float)q[4];
+        }
         ring_row(r0 - 1, q);
         strip_prim(gm1, q, wB);
+        if constexpr (NFX > 0) {
+            xB = (float)q[4];
+        }
         ring_row(r0, q);
         strip_prim(gm1, q, wC);
+        if constexpr (NFX > 0) {
+            xC = (float)q[4];
+        }
         ring_row(r0 + 1, q);
         strip_prim(gm1, q, wD);
+        if constexpr (NFX > 0) {
+            xD = (float)q[4];
+        }
         float t0[4], t1[4], t2[4], tT[4];
-        strip_hancock<LIM>(c, wA, wB, wC, t0, t1, t2, tT); // row r0-1: keep its top face
-        strip_hancock<LIM>(c, wB, wC, wD, hxL, hxR, hyB, hyT); // row r0
+        const float xw0[3] = {xA, xB, xC}, xw1[3] = {xB, xC, xD};
+        float xo0[4], xo1[4];
+        strip_hancock<LIM, NFX>(c, wA, wB, wC, t0, t1, t2, tT, xw0, xo0); // row r0-1: keep its top face
+        strip_hancock<LIM, NFX>(c, wB, wC, wD, hxL, hxR, hyB, hyT, xw1, xo1); // row r0
         float G[4];
         strip_riemann<RS>(c.eos, tT, hyB, 1, G);
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             Glo[v] = (double)G[v];
+        }
+        if constexpr (NFX > 0) {
+            gx_lo = (G[0] < 0.f ? xo1[2] : xo0[3]) * G[0];
+            xoL = xo1[0];
+            xoR = xo1[1];
+            xoT = xo1[3];
         }
     }
     // window: wC = P[r], wD = P[r+1]; ring rows r+3, r+4 in flight.  Two rows
@@ -274,19 +359,25 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
                 continue;
             }
         }
-        double q[4];
+        double q[4 + NFX];
         float wN[4];
+        float xN = 0.f;
         stage_row(r + 4);
         asm volatile("cp.async.wait_group 2;\n" ::: "memory"); // rows up to r+2 landed
         ring_row(r, q);
         {
-            double qn2[4];
+            double qn2[4 + NFX];
             ring_row(r + 2, qn2);
             strip_prim(gm1, qn2, wN);
+            if constexpr (NFX > 0) {
+                xN = (float)qn2[4];
+            }
         }
         // Hancock of row r+1
         float nxL[4], nxR[4], nyB[4], nyT[4];
-        strip_hancock<LIM>(c, wC, wD, wN, nxL, nxR, nyB, nyT);
+        const float xw[3] = {xC, xD, xN};
+        float nxo[4];
+        strip_hancock<LIM, NFX>(c, wC, wD, wN, nxL, nxR, nyB, nyT, xw, nxo);
         // y-face r+1/2
         float G[4];
         strip_riemann<RS>(c.eos, hyT, nyB, 1, G);
@@ -294,6 +385,11 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             Ghi[v] = (double)G[v];
+        }
+        float gx_hi = 0.f;
+        if constexpr (NFX > 0) {
+            // the upper cell's bottom face when the mass flows down, else the lower cell's top face
+            gx_hi = (G[0] < 0.f ? nxo[2] : xoT) * G[0];
         }
         // x-faces of row r: left face at this lane, right face from lane+1
         float uL[4], Fl[4];
@@ -307,6 +403,13 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         for (int v = 0; v < 4; ++v) {
             Fld[v] = (double)Fl[v];
             Frd[v] = __shfl_down_sync(0xffffffffu, Fld[v], 1);
+        }
+        float fx_l = 0.f, fx_r = 0.f;
+        if constexpr (NFX > 0) {
+            // left face: this cell's left value when the mass flows left, else the left cell's right value
+            const float up_left = __shfl_up_sync(0xffffffffu, xoR, 1);
+            fx_l = (Fl[0] < 0.f ? xoL : up_left) * Fl[0];
+            fx_r = __shfl_down_sync(0xffffffffu, fx_l, 1);
         }
         if (out_lane) {
             // Godunov update of row r in FP64 (godunov_scheme.hpp:159-163, 258-260)
@@ -346,10 +449,20 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             for (int v = 0; v < 4; ++v) {
                 qout[oo + plane * v] = qn[v];
             }
+            double xnew = 0.0;
+            if constexpr (NFX > 0) {
+                const double xn = fma(q[4], q[0], fma(cx, (double)fx_l - (double)fx_r, cy * ((double)gx_lo - (double)gx_hi)));
+                xnew = xn / qn[0];
+                xnew = xnew < 0. ? 0. : (xnew > 1. ? 1. : xnew);
+                qout[oo + plane * 4] = xnew;
+            }
             const unsigned ym = (r < 2 * g.ng || r >= n1 - 2 * g.ng) ? ghost_mask(r, n1, g.ng, g.bc[2], g.bc[3]) : 0u;
             if (ym != 0u || !x_fast) {
                 if ((xm | ym) != 0u) {
                     store_images_2d(qout, plane, pitch, n0, n1, g.ng, col, r, xm, ym, qn);
+                    if constexpr (NFX > 0) {
+                        store_images_2d_scalar(qout + plane * 4, pitch, n0, n1, g.ng, col, r, xm, ym, xnew);
+                    }
                 }
             } else if (x_any) {
                 const int64_t og = (int64_t)r * pitch + x_img;
@@ -357,6 +470,9 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
                 qout[og + plane] = x_flip ? -qn[1] : qn[1];
                 qout[og + 2 * plane] = qn[2];
                 qout[og + 3 * plane] = qn[3];
+                if constexpr (NFX > 0) {
+                    qout[og + 4 * plane] = xnew;
+                }
                 if (XIMG > 1 && x_two) {
                     // the second image, or the first again
                     const unsigned b2 = xbits & (xbits - 1u);
@@ -367,6 +483,9 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
                     qout[og2 + plane] = fl ? -qn[1] : qn[1];
                     qout[og2 + 2 * plane] = qn[2];
                     qout[og2 + 3 * plane] = qn[3];
+                    if constexpr (NFX > 0) {
+                        qout[og2 + 4 * plane] = xnew;
+                    }
                 }
             }
         }
@@ -379,6 +498,14 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             hxR[v] = nxR[v];
             hyT[v] = nyT[v];
             Glo[v] = Ghi[v];
+        }
+        if constexpr (NFX > 0) {
+            xC = xD;
+            xD = xN;
+            xoL = nxo[0];
+            xoR = nxo[1];
+            xoT = nxo[3];
+            gx_lo = gx_hi;
         }
         if constexpr (SYNC > 0) {
             if (i % SYNC == SYNC - 1 || i == L - 1) {
@@ -468,6 +595,57 @@ k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     for (int w = wg; w < nitems; w += wstride) {
         strip_work<LIM, RS>(g, in.q, out.q, in.plane, in.pitch, dec.dt, w % ncolw, w / ncolw, L, inv_max, bad_cell,
                             ring);
+    }
+    // warp max of 1/dt -> one atomic per warp
+    const bool nan_seen = isnan(inv_max);
+    double m = nan_seen ? 0.0 : inv_max;
+    m = warp_max_d(m);
+    const unsigned nanv = __ballot_sync(0xffffffffu, nan_seen);
+    if (lane == 0) {
+        atomicMax(&ctl->inv_dt_bits[(slot + 1) % 3], dbl_bits(m));
+        if (nanv) {
+            atomicMax(&ctl->inv_dt_bits[(slot + 1) % 3], 0x7ff8000000000000ull);
+        }
+    }
+    if (bad_cell >= 0) {
+        atomicMin(&ctl->bad_cell, (unsigned long long)bad_cell);
+        ctl->err = 4;
+        ctl->errflag[(slot + 1) & 1] = 1;
+        ctl->final_buf = out_buf;
+    }
+}
+
+// k_strip2d with one passive scalar (5-variable rings; three CTAs of 4 warps
+// per SM leave 170 registers for the extra window).
+template <int LIM, int RS>
+__global__ void __launch_bounds__(128, 3)
+k_strip2d_fx(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
+{
+    const int lane = threadIdx.x & 31;
+    const Decision dec = decide(ctl, slot, rp);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        publish_decision(ctl, dec, rp, slot, out_buf);
+    }
+    if (dec.noop || dec.neg_dt) {
+        return;
+    }
+    const int ncolw = (g.nx[0] + kStripLanesOut - 1) / kStripLanesOut;
+    const int nstrip = (g.nx[1] + L - 1) / L;
+    const int nitems = ncolw * nstrip;
+    const int wg = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (wg >= nitems) {
+        return;
+    }
+    double inv_max = 0.0;
+    int64_t bad_cell = -1;
+    // grid-stride over the strips (the launcher sizes the grid to the
+    // resident warps, so a warp usually takes one or two strips)
+    const int wstride = gridDim.x * (blockDim.x >> 5);
+    __shared__ __align__(16) double s_ring[4][kStripRingDoublesFx];
+    const StripRingN<5> ring = reinterpret_cast<StripRingN<5>>(s_ring[(threadIdx.x >> 5) & 3]);
+    for (int w = wg; w < nitems; w += wstride) {
+        strip_work<LIM, RS, 0, 1, 1>(g, in.q, out.q, in.plane, in.pitch, dec.dt, w % ncolw, w / ncolw, L, inv_max,
+                                     bad_cell, ring);
     }
     // warp max of 1/dt -> one atomic per warp
     const bool nan_seen = isnan(inv_max);

@@ -91,6 +91,8 @@ int smem_optin();
 // room left in the opt-in limit for the tile kernels' static shared memory
 constexpr size_t kFusedStaticSmemMargin = 1024;
 bool strip2d_eligible(const GridDev& g);
+// 4-warp strips (schedules 3-6) with one passive scalar.
+bool strip2d_fx_eligible(const GridDev& g);
 // Paired schedule: two columns per lane in packed FP32 pairs (ng even).
 bool strip2d_pair_eligible(const GridDev& g);
 void step_strip2d_pair(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
