@@ -16,7 +16,8 @@
 //    copied);
 //  * ghost images, the internal-energy check and the CFL max of the new
 //    state are done in the same pass.
-// strip_work() is the per-strip body shared by the single-domain kernel and
+// strip_work() is the per-strip body shared by the single-domain kernels
+// (k_strip2d, k_strip2d_sync, and k_strip2d_fx with one passive scalar) and
 // the persistent ensemble kernel.
 #pragma once
 

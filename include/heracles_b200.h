@@ -277,9 +277,10 @@ int hcl_get_dt_log(hcl_handle* h, double* dts, int max_count, int* count);
  * warp strips of 32/64/128 rows, 6 warp strips fitted to one wave of
  * resident warps, 7-8 paired-column warp strips (fitted, 32 rows; even ghost
  * width), 9 fitted warp strips in 16-warp CTAs that march in step.  3-D: 0
- * shared-memory tiles, 1 column march (uniform Cartesian grids).  Returns
- * the schedule in use through *used (may be NULL; -1 before the autotuner
- * ran). */
+ * shared-memory tiles, 1 column march (uniform Cartesian grids).  With
+ * passive scalars only the tiles qualify, and for one scalar in 2-D also
+ * 3-6.  Returns the schedule in use through *used (may be NULL; -1 before
+ * the autotuner ran). */
 int hcl_set_schedule(hcl_handle* h, int schedule, int* used);
 
 /* Selects the time loop of hcl_run: 0 (default) the fused loop wherever the
