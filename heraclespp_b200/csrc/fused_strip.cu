@@ -52,7 +52,7 @@ int resident_blocks_fx()
     if (cached == 0) {
         int per_sm = 0, nsm = 0, dev = 0;
         cudaGetDevice(&dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip2d_fx<LIM, RS>, 128, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip2d<LIM, RS, 1>, 128, 0);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cached = per_sm > 0 && nsm > 0 ? per_sm * nsm : 148;
     }
@@ -101,7 +101,7 @@ void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCt
     if (sync) {
         k_strip2d_sync<LIM, RS><<<blocks, 32 * kStripSyncWarps, kSyncSmem, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
     } else if (fx) {
-        k_strip2d_fx<LIM, RS><<<blocks, 128, 0, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
+        k_strip2d<LIM, RS, 1><<<blocks, 128, 0, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
     } else {
         k_strip2d<LIM, RS><<<blocks, 128, 0, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
     }

@@ -17,8 +17,8 @@
 //  * ghost images, the internal-energy check and the CFL max of the new
 //    state are done in the same pass.
 // strip_work() is the per-strip body shared by the single-domain kernels
-// (k_strip2d, k_strip2d_sync, and k_strip2d_fx with one passive scalar) and
-// the persistent ensemble kernel.
+// (k_strip2d, also with one passive scalar, and k_strip2d_sync) and the
+// persistent ensemble kernel.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -218,7 +218,6 @@ template <int NVR>
 using StripRingN = double (*)[NVR][32];
 using StripRing = StripRingN<4>;
 constexpr int kStripRingDoubles = 8 * 4 * 32;
-constexpr int kStripRingDoublesFx = 8 * 5 * 32;
 
 // One strip (28 columns x rows [r0, r1)) of one domain: reads qin, writes qout.
 // Accumulates the CFL max and the first bad cell of the lanes' output cells.
@@ -567,8 +566,10 @@ __device__ __forceinline__ void publish_decision(StepCtl* ctl, const Decision& d
     ctl->inv_dt_bits[(slot + 2) % 3] = 0ull;
 }
 
-template <int LIM, int RS>
-__global__ void __launch_bounds__(128, 4)
+// NFX = 1: one passive scalar (5-variable rings; three CTAs of 4 warps per SM
+// leave 170 registers for its window).
+template <int LIM, int RS, int NFX = 0>
+__global__ void __launch_bounds__(128, NFX > 0 ? 3 : 4)
 k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
 {
     const int lane = threadIdx.x & 31;
@@ -591,62 +592,11 @@ k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     // grid-stride over the strips (the launcher sizes the grid to the
     // resident warps, so a warp usually takes one or two strips)
     const int wstride = gridDim.x * (blockDim.x >> 5);
-    __shared__ __align__(16) double s_ring[4][kStripRingDoubles];
-    const StripRing ring = reinterpret_cast<StripRing>(s_ring[(threadIdx.x >> 5) & 3]);
+    __shared__ __align__(16) double s_ring[4][8 * (4 + NFX) * 32];
+    const StripRingN<4 + NFX> ring = reinterpret_cast<StripRingN<4 + NFX>>(s_ring[(threadIdx.x >> 5) & 3]);
     for (int w = wg; w < nitems; w += wstride) {
-        strip_work<LIM, RS>(g, in.q, out.q, in.plane, in.pitch, dec.dt, w % ncolw, w / ncolw, L, inv_max, bad_cell,
-                            ring);
-    }
-    // warp max of 1/dt -> one atomic per warp
-    const bool nan_seen = isnan(inv_max);
-    double m = nan_seen ? 0.0 : inv_max;
-    m = warp_max_d(m);
-    const unsigned nanv = __ballot_sync(0xffffffffu, nan_seen);
-    if (lane == 0) {
-        atomicMax(&ctl->inv_dt_bits[(slot + 1) % 3], dbl_bits(m));
-        if (nanv) {
-            atomicMax(&ctl->inv_dt_bits[(slot + 1) % 3], 0x7ff8000000000000ull);
-        }
-    }
-    if (bad_cell >= 0) {
-        atomicMin(&ctl->bad_cell, (unsigned long long)bad_cell);
-        ctl->err = 4;
-        ctl->errflag[(slot + 1) & 1] = 1;
-        ctl->final_buf = out_buf;
-    }
-}
-
-// k_strip2d with one passive scalar (5-variable rings; three CTAs of 4 warps
-// per SM leave 170 registers for the extra window).
-template <int LIM, int RS>
-__global__ void __launch_bounds__(128, 3)
-k_strip2d_fx(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
-{
-    const int lane = threadIdx.x & 31;
-    const Decision dec = decide(ctl, slot, rp);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        publish_decision(ctl, dec, rp, slot, out_buf);
-    }
-    if (dec.noop || dec.neg_dt) {
-        return;
-    }
-    const int ncolw = (g.nx[0] + kStripLanesOut - 1) / kStripLanesOut;
-    const int nstrip = (g.nx[1] + L - 1) / L;
-    const int nitems = ncolw * nstrip;
-    const int wg = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (wg >= nitems) {
-        return;
-    }
-    double inv_max = 0.0;
-    int64_t bad_cell = -1;
-    // grid-stride over the strips (the launcher sizes the grid to the
-    // resident warps, so a warp usually takes one or two strips)
-    const int wstride = gridDim.x * (blockDim.x >> 5);
-    __shared__ __align__(16) double s_ring[4][kStripRingDoublesFx];
-    const StripRingN<5> ring = reinterpret_cast<StripRingN<5>>(s_ring[(threadIdx.x >> 5) & 3]);
-    for (int w = wg; w < nitems; w += wstride) {
-        strip_work<LIM, RS, 0, 1, 1>(g, in.q, out.q, in.plane, in.pitch, dec.dt, w % ncolw, w / ncolw, L, inv_max,
-                                     bad_cell, ring);
+        strip_work<LIM, RS, 0, 1, NFX>(g, in.q, out.q, in.plane, in.pitch, dec.dt, w % ncolw, w / ncolw, L, inv_max,
+                                       bad_cell, ring);
     }
     // warp max of 1/dt -> one atomic per warp
     const bool nan_seen = isnan(inv_max);
