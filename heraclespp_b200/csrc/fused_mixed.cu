@@ -44,6 +44,9 @@ bool mixed_shape_valid(const GridDev& g, int shape)
         if (g.ndim == 2 && shape >= 3 && shape <= 6) {
             return strip2d_fx_eligible(g);
         }
+        if (g.ndim == 3 && shape == 1) {
+            return strip3d_fx_eligible(g);
+        }
         return (g.ndim == 2 ? shape < 3 : shape == 0) && mixed_smem_bytes(g, shape) + kFusedStaticSmemMargin <= (size_t)smem_optin();
     }
     if (g.ndim == 3) {
@@ -88,7 +91,7 @@ void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepC
         }
         break;
     default:
-        if (shape == 1 && strip3d_eligible(g)) {
+        if (shape == 1 && (strip3d_eligible(g) || strip3d_fx_eligible(g))) {
             step_strip3d(g, in, out, ctl, rp, slot, out_buf, 0, s);
         } else {
             FusedLauncher<3, false, 8, 8, 4>::launch(g, in, out, ctl, rp, slot, out_buf, s);

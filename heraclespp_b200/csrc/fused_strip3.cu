@@ -10,6 +10,12 @@
 
 namespace hcl::fused {
 
+bool strip3d_fx_eligible(const GridDev& g)
+{
+    return g.ndim == 3 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM && g.ng >= 2 &&
+           g.nfx == 1;
+}
+
 bool strip3d_eligible(const GridDev& g)
 {
     return g.ndim == 3 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM && g.ng >= 2 &&
@@ -18,16 +24,17 @@ bool strip3d_eligible(const GridDev& g)
 
 namespace {
 
-template <int LIM, int RS>
-void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp, int slot,
-               int out_buf, int L, cudaStream_t s)
+template <int LIM, int RS, int NFX>
+void launch_lrf(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                int slot, int out_buf, int L, cudaStream_t s)
 {
+    constexpr int kSmem = (int)sizeof(S3SharedT<NFX>);
     static int resident = 0;
     if (resident == 0) {
-        cudaFuncSetAttribute(k_strip3d<LIM, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(S3Shared));
+        cudaFuncSetAttribute(k_strip3d<LIM, RS, NFX>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
         int per_sm = 0, nsm = 0, dev = 0;
         cudaGetDevice(&dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip3d<LIM, RS>, kS3Threads, sizeof(S3Shared));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip3d<LIM, RS, NFX>, kS3Threads, kSmem);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         resident = std::max(1, per_sm) * (nsm > 0 ? nsm : 148);
     }
@@ -46,7 +53,18 @@ void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCt
         }
     }
     const int nzc = (g.nx[2] + L - 1) / L;
-    k_strip3d<LIM, RS><<<ncol * nzc, kS3Threads, sizeof(S3Shared), s>>>(g, in, out, ctl, rp, slot, out_buf, L);
+    k_strip3d<LIM, RS, NFX><<<ncol * nzc, kS3Threads, kSmem, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
+}
+
+template <int LIM, int RS>
+void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp, int slot,
+               int out_buf, int L, cudaStream_t s)
+{
+    if (g.nfx == 1) {
+        launch_lrf<LIM, RS, 1>(g, in, out, ctl, rp, slot, out_buf, L, s);
+    } else {
+        launch_lrf<LIM, RS, 0>(g, in, out, ctl, rp, slot, out_buf, L, s);
+    }
 }
 
 template <int LIM>

@@ -80,9 +80,15 @@ __device__ __forceinline__ void cons_and_flux(const fast::Eos& e, const float w[
 // Hancock face states of one cell: minus/plus faces along x, y, z
 // (extrapolation_reconstruction.hpp:65-143, gravity :306-312).  wyd/wyu are
 // the y-neighbours, wzd/wzu the z-neighbours; x-neighbours come by shuffle.
-template <int LIM>
+// NFX = 1: also the passive scalar's face values xo[0..2] (minus faces x, y,
+// z) and xo[3..5] (plus faces) from its primitives xw = {centre, y-, y+, z-,
+// z+}: limited slopes, times the face density before the predictor, plus the
+// predictor's increment from the face states' mass fluxes, divided by the
+// predicted face density (extrapolation_reconstruction.hpp:315-337, :459-469).
+template <int LIM, int NFX = 0>
 __device__ __forceinline__ void hancock(const Ctx& c, const float wc[5], const float wyd[5], const float wyu[5],
-                                        const float wzd[5], const float wzu[5], float hm[3][5], float hp[3][5])
+                                        const float wzd[5], const float wzu[5], float hm[3][5], float hp[3][5],
+                                        const float* xw = nullptr, float* xo = nullptr)
 {
     float fm[3][5], fp[3][5];
 #pragma unroll
@@ -100,11 +106,14 @@ __device__ __forceinline__ void hancock(const Ctx& c, const float wc[5], const f
         fp[2][v] = wc[v] + sz;
     }
     float inc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    float mfm[3], mfp[3]; // mass fluxes of the face states before the update
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         float Fm[5], Fp[5];
         cons_and_flux(c.eos, fm[d], d, hm[d], Fm);
         cons_and_flux(c.eos, fp[d], d, hp[d], Fp);
+        mfm[d] = Fm[0];
+        mfp[d] = Fp[0];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
             inc[v] = fmaf(c.cth[d], Fm[v] - Fp[v], inc[v]);
@@ -128,6 +137,22 @@ __device__ __forceinline__ void hancock(const Ctx& c, const float wc[5], const f
             }
         }
     }
+    if constexpr (NFX > 0) {
+        const float xl = __shfl_up_sync(0xffffffffu, xw[0], 1);
+        const float xr = __shfl_down_sync(0xffffffffu, xw[0], 1);
+        const float s[3] = {half_lim_fast<LIM>(xr - xw[0], xw[0] - xl), half_lim_fast<LIM>(xw[2] - xw[0], xw[0] - xw[1]),
+                            half_lim_fast<LIM>(xw[4] - xw[0], xw[0] - xw[3])};
+        float xinc = 0.f;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            xinc = fmaf(c.cth[d], (xw[0] - s[d]) * mfm[d] - (xw[0] + s[d]) * mfp[d], xinc);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            xo[d] = __fdividef(fmaf(xw[0] - s[d], fm[d][0], xinc), hm[d][0]);
+            xo[3 + d] = __fdividef(fmaf(xw[0] + s[d], fp[d][0], xinc), hp[d][0]);
+        }
+    }
 }
 
 } // namespace s3
@@ -139,13 +164,77 @@ struct S3Shared {
     float yface[2][kS3Warps][2][5][32]; // [.][w][0: bottom (minus), 1: top (plus)]
     float gflux[2][kS3Warps][5][32];    // flux of the y-face above row w
 };
+// the same for one passive scalar
+struct S3SharedFx {
+    float xprim[2][kS3Warps][32];
+    float xyface[2][kS3Warps][2][32];
+    float xgflux[2][kS3Warps][32];
+};
+template <int NFX>
+struct S3SharedT : S3Shared {
+};
+template <>
+struct S3SharedT<1> : S3Shared {
+    S3SharedFx fx;
+};
 
-template <int LIM, int RS>
+// Ghost images of one scalar plane q (no sign flips): the loops of
+// store_images_3d for a single value.
+__device__ __forceinline__ void store_images_3d_scalar(double* __restrict__ q, int64_t pitch, int n0, int n1, int n2,
+                                                       int ng, int col, int row, int z, unsigned xm, unsigned ym,
+                                                       unsigned zm, double v)
+{
+    unsigned zb = zm & 0xffffu;
+    int pz = z;
+    bool self_z = true;
+    for (;;) {
+        unsigned yb = ym & 0xffffu;
+        int py = row;
+        bool self_y = true;
+        for (;;) {
+            unsigned xb = xm & 0xffffu;
+            int px = col;
+            bool self_x = true;
+            for (;;) {
+                if (!(self_x && self_y && self_z)) {
+                    q[((int64_t)pz * n1 + py) * pitch + px] = v;
+                }
+                if (xb == 0u) {
+                    break;
+                }
+                const int k = __ffs(xb) - 1;
+                xb &= xb - 1u;
+                px = ghost_slot(k, n0, ng);
+                self_x = false;
+            }
+            if (yb == 0u) {
+                break;
+            }
+            const int k = __ffs(yb) - 1;
+            yb &= yb - 1u;
+            py = ghost_slot(k, n1, ng);
+            self_y = false;
+        }
+        if (zb == 0u) {
+            break;
+        }
+        const int k = __ffs(zb) - 1;
+        zb &= zb - 1u;
+        pz = ghost_slot(k, n2, ng);
+        self_z = false;
+    }
+}
+
+// NFX = 1: one passive scalar (state plane 5) rides along: face values from
+// hancock, upwind fluxes from the Riemann mass fluxes (godunov_scheme.hpp:
+// 262-301), the update in FP64 divided by the new density and clamped to
+// [0, 1], stored with the same ghost images.
+template <int LIM, int RS, int NFX = 0>
 __global__ void __launch_bounds__(kS3Threads, 1)
 k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
 {
     extern __shared__ __align__(16) unsigned char s3_raw[];
-    S3Shared& sh = *reinterpret_cast<S3Shared*>(s3_raw);
+    S3SharedT<NFX>& sh = *reinterpret_cast<S3SharedT<NFX>*>(s3_raw);
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     const Decision dec = decide(ctl, slot, rp);
@@ -191,11 +280,11 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     const double gm1 = g.gamma_m1;
     float inv_f = 0.f; // CFL max of this CTA's cells (NaN once a NaN was seen)
 
-    auto load = [&](int z, double q[5]) {
+    auto load = [&](int z, double* q) {
         const int zc = min(max(z, 0), n2 - 1);
         const int64_t o = ((int64_t)zc * n1 + rowc) * pitch + colc;
 #pragma unroll
-        for (int v = 0; v < 5; ++v) {
+        for (int v = 0; v < 5 + NFX; ++v) {
             q[v] = __ldg(qin + o + plane * v);
         }
     };
@@ -212,14 +301,25 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     float hzU[5];      // z-plus face state of plane z (for the z-face z+1/2)
     double dFx[5];     // x-flux difference (left - right face) of plane z, exact in FP64
     float Gzlo[5];     // z-face flux z-1/2
-    double qN[5];
+    double qN[5 + NFX];
+    // passive scalar: primitives of planes z, z+1; z-plus face value of plane
+    // z; x-flux difference of plane z; upwind flux of the z-face z-1/2
+    float xC = 0.f, xD = 0.f, xzU = 0.f, gzx_lo = 0.f;
+    double dxx = 0.0;
     {
-        double q[5];
+        double q[5 + NFX];
         load(z0 - 2, q);
         s3::prim(gm1, q, wC);
+        if constexpr (NFX > 0) {
+            xC = (float)q[5];
+        }
         load(z0 - 1, q);
         s3::prim(gm1, q, wD);
         put_prim(z0 - 1, wD);
+        if constexpr (NFX > 0) {
+            xD = (float)q[5];
+            sh.fx.xprim[(z0 - 1) & 1][w][lane] = xD;
+        }
         load(z0, qN);
     }
 #pragma unroll
@@ -241,6 +341,11 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
         float wN[5];
         s3::prim(gm1, qN, wN);
         put_prim(z + 2, wN);
+        float xN = 0.f;
+        if constexpr (NFX > 0) {
+            xN = (float)qN[5];
+            sh.fx.xprim[(z + 2) & 1][w][lane] = xN;
+        }
         load(z + 3, qN);
         // 2. Hancock of plane z+1 (y-neighbours' primitives of plane z+1 were shared last step)
         float wyd[5], wyu[5];
@@ -250,9 +355,16 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             wyu[v] = sh.prim[(z + 1) & 1][wu][v][lane];
         }
         float hm[3][5], hp[3][5];
-        s3::hancock<LIM>(c, wD, wyd, wyu, wC, wN, hm, hp);
+        float xw[5] = {xD, 0.f, 0.f, xC, xN};
+        if constexpr (NFX > 0) {
+            xw[1] = sh.fx.xprim[(z + 1) & 1][wd][lane];
+            xw[2] = sh.fx.xprim[(z + 1) & 1][wu][lane];
+        }
+        float xo[6];
+        s3::hancock<LIM, NFX>(c, wD, wyd, wyu, wC, wN, hm, hp, xw, xo);
         // 3. x-faces of plane z+1: left face at this lane, right face from lane+1
         double dFxN[5];
+        double dxxN = 0.0;
         {
             float uL[5], Fl[5];
 #pragma unroll
@@ -264,15 +376,29 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             for (int v = 0; v < 5; ++v) {
                 dFxN[v] = (double)Fl[v] - (double)__shfl_down_sync(0xffffffffu, Fl[v], 1);
             }
+            if constexpr (NFX > 0) {
+                // this cell's minus value when the mass flows left, else the left cell's plus value
+                const float up_left = __shfl_up_sync(0xffffffffu, xo[3], 1);
+                const float fl = (Fl[0] < 0.f ? xo[0] : up_left) * Fl[0];
+                dxxN = (double)fl - (double)__shfl_down_sync(0xffffffffu, fl, 1);
+            }
         }
         // 4. z-face z+1/2
         float Gzhi[5];
         fast::riemann<3>(c.eos, RS, hzU, hm[2], 2, Gzhi);
+        float gzx_hi = 0.f;
+        if constexpr (NFX > 0) {
+            gzx_hi = (Gzhi[0] < 0.f ? xo[2] : xzU) * Gzhi[0];
+        }
         // 5. y-face states of plane z+1 for the neighbours
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
             sh.yface[(z + 1) & 1][w][0][v][lane] = hm[1][v];
             sh.yface[(z + 1) & 1][w][1][v][lane] = hp[1][v];
+        }
+        if constexpr (NFX > 0) {
+            sh.fx.xyface[(z + 1) & 1][w][0][lane] = xo[1];
+            sh.fx.xyface[(z + 1) & 1][w][1][lane] = xo[4];
         }
         // 6. y-face above this row, plane z
         const bool upd = z >= z0;
@@ -288,14 +414,19 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             for (int v = 0; v < 5; ++v) {
                 sh.gflux[z & 1][w][v][lane] = G[v];
             }
+            if constexpr (NFX > 0) {
+                // the upper row's bottom value when the mass flows down, else this row's top value
+                const float xu = G[0] < 0.f ? sh.fx.xyface[z & 1][wu][0][lane] : sh.fx.xyface[z & 1][w][1][lane];
+                sh.fx.xgflux[z & 1][w][lane] = xu * G[0];
+            }
         }
         __syncthreads();
         // 7. update of plane z
         if (upd && out_cell) {
-            double q[5], qn[5];
+            double q[5 + NFX], qn[5];
             const int64_t oo = ((int64_t)z * n1 + row) * pitch + col;
 #pragma unroll
-            for (int v = 0; v < 5; ++v) {
+            for (int v = 0; v < 5 + NFX; ++v) {
                 q[v] = __ldg(qin + oo + plane * v);
             }
 #pragma unroll
@@ -335,12 +466,24 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             for (int v = 0; v < 5; ++v) {
                 qout[oo + plane * v] = qn[v];
             }
+            double xnew = 0.0;
+            if constexpr (NFX > 0) {
+                const double gb = (double)sh.fx.xgflux[z & 1][wd][lane];
+                const double gt = (double)sh.fx.xgflux[z & 1][w][lane];
+                const double xn = fma(q[5], q[0], fma(cxyz[0], dxx, fma(cxyz[1], gb - gt, cxyz[2] * ((double)gzx_lo - (double)gzx_hi))));
+                xnew = xn / qn[0];
+                xnew = xnew < 0. ? 0. : (xnew > 1. ? 1. : xnew);
+                qout[oo + plane * 5] = xnew;
+            }
             // ghost images of border cells (boundary_distribute.hpp:42-76)
             const unsigned zm = (z < 2 * g.ng || z >= g.n[2] - 2 * g.ng)
                                     ? ghost_mask(z, g.n[2], g.ng, g.bc[4], g.bc[5])
                                     : 0u;
             if ((xym | zm) != 0u) {
                 store_images_3d(qout, plane, pitch, n0, n1, g.n[2], g.ng, col, row, z, xm, ym, zm, qn);
+                if constexpr (NFX > 0) {
+                    store_images_3d_scalar(qout + plane * 5, pitch, n0, n1, g.n[2], g.ng, col, row, z, xm, ym, zm, xnew);
+                }
             }
         }
         // slide the window
@@ -351,6 +494,13 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             hzU[v] = hp[2][v];
             dFx[v] = dFxN[v];
             Gzlo[v] = Gzhi[v];
+        }
+        if constexpr (NFX > 0) {
+            xC = xD;
+            xD = xN;
+            xzU = xo[5];
+            dxx = dxxN;
+            gzx_lo = gzx_hi;
         }
     }
 

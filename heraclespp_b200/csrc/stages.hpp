@@ -100,6 +100,8 @@ void step_strip2d_pair(const GridDev& g, const StateDev& in, const StateDev& out
 // 3-D column march (uniform Cartesian grids, uniform gravity); L <= 0 fits
 // the plane count per CTA to the resident CTAs.
 bool strip3d_eligible(const GridDev& g);
+// the column march with one passive scalar
+bool strip3d_fx_eligible(const GridDev& g);
 void step_strip3d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                   int slot, int out_buf, int L, cudaStream_t s);
 void step_strip2d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
