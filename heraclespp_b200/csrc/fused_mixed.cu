@@ -15,7 +15,7 @@ namespace hcl::fused {
 // 7 and 8 paired-column warp strips (fitted height, 32 rows); 9 fitted warp
 // strips in CTAs of 16 warps that march in step.  3-9 need a uniform
 // Cartesian grid, 7-8 an even ghost width.  With passive scalars: the tiles,
-// and for one scalar the 4-warp strips 3-6.
+// and for one scalar the 4-warp strips 3-6 (2-D) or the column march (3-D).
 // 3-D: 0 shared-memory tiles 8x8x4; 1 column march (uniform Cartesian grids).
 int mixed_shape_count(int ndim)
 {

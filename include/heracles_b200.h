@@ -278,8 +278,8 @@ int hcl_get_dt_log(hcl_handle* h, double* dts, int max_count, int* count);
  * resident warps, 7-8 paired-column warp strips (fitted, 32 rows; even ghost
  * width), 9 fitted warp strips in 16-warp CTAs that march in step.  3-D: 0
  * shared-memory tiles, 1 column march (uniform Cartesian grids).  With
- * passive scalars only the tiles qualify, and for one scalar in 2-D also
- * 3-6.  Returns the schedule in use through *used (may be NULL; -1 before
+ * passive scalars only the tiles qualify, and for one scalar also 3-6 in
+ * 2-D and 1 in 3-D.  Returns the schedule in use through *used (may be NULL; -1 before
  * the autotuner ran). */
 int hcl_set_schedule(hcl_handle* h, int schedule, int* used);
 
