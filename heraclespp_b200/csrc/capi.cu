@@ -2555,7 +2555,9 @@ std::mutex g_noalloc_mutex;
 double* g_noalloc_base[kNoAllocMaxDevices] = {};
 
 // Device address of this device's copy of the array, looked up on the first
-// call on each device (the caller has made that device current).
+// call on each device (the caller has made that device current) and kept for
+// the process: a cudaDeviceReset of that device after the first call leaves
+// the kept address stale, which the header states.
 int noalloc_scratch(int dev, double** out)
 {
     if (dev < 0 || dev >= kNoAllocMaxDevices) {

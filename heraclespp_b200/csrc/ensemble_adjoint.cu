@@ -9,6 +9,7 @@
 
 #include "adjoint_step.cuh"
 #include "ensemble.cuh"
+#include "per_device.hpp"
 #include "stages.hpp"
 
 namespace hcl::ensemble {
@@ -112,16 +113,19 @@ k_ens_reverse(const AdjProb* __restrict__ probs, const int* __restrict__ tile_pr
     }
 }
 
+// shared-memory opt-in and resident CTAs per SM, once per device
 template <class R>
 int blocks_per_sm()
 {
-    static int n = -1;
-    if (n < 0) {
+    static PerDevice cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return cache.get(dev, [] {
         cudaFuncSetAttribute(k_ens_reverse<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rev_smem<R>());
-        n = 0;
+        int n = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_ens_reverse<R>, kRevTile * kRevTile, rev_smem<R>());
-    }
-    return n;
+        return n;
+    });
 }
 
 template <class R>

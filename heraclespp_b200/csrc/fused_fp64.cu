@@ -7,6 +7,7 @@
 #include <cstdint>
 
 #include "fused_step.cuh"
+#include "per_device.hpp"
 #include "physics_exact.cuh"
 #include "stages.hpp"
 
@@ -54,15 +55,17 @@ size_t exact_smem_bytes(const GridDev& g)
     }
 }
 
+// the current device's per-block shared-memory opt-in limit
 int smem_optin()
 {
-    static int bytes = [] {
-        int dev = 0, v = 0;
-        cudaGetDevice(&dev);
+    static PerDevice cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return cache.get(dev, [dev] {
+        int v = 0;
         cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
         return v;
-    }();
-    return bytes;
+    });
 }
 
 void configure_exact()

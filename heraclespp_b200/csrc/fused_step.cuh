@@ -32,6 +32,7 @@
 #include <type_traits>
 
 #include "hcl_device.cuh"
+#include "per_device.hpp"
 #include "physics_exact.cuh"
 #include "physics_fast.cuh"
 #include "stages.hpp"
@@ -717,7 +718,7 @@ __device__ __forceinline__ void fused_step_body(const GridDev& g, const StateDev
         // (hydro_reconstruction.hpp:105-109), made conservative with the face
         // density before the predictor, advanced by the predictor's mass
         // fluxes (extrapolation_reconstruction.hpp:315-337) and turned back
-        // into fractions with the predicted face density (:459-469)
+        // into fractions with the predicted face density (:329-339)
         for (int f = 0; f < nfx; ++f) {
             const R* xs = sx + f * S::NP;
             R xf[2][ND];
@@ -1349,12 +1350,14 @@ struct FusedLauncher {
     static bool use_occ(int nfx)
     {
         if constexpr (kMinBlocks > 0) {
-            static const int per_sm = [] {
-                int dev = 0, v = 0;
-                cudaGetDevice(&dev);
+            static PerDevice cache;
+            int dev = 0;
+            cudaGetDevice(&dev);
+            const int per_sm = cache.get(dev, [dev] {
+                int v = 0;
                 cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
                 return v;
-            }();
+            });
             return (size_t)kMinBlocks * (smem(nfx) + 1024 + 256) <= (size_t)per_sm;
         }
         return false;

@@ -6,6 +6,7 @@
 
 #include "fused_strip2d.cuh"
 #include "fused_strip2d_pair.cuh"
+#include "per_device.hpp"
 #include "stages.hpp"
 
 namespace hcl::fused {
@@ -30,52 +31,47 @@ bool strip2d_pair_eligible(const GridDev& g)
 
 namespace {
 
-// Resident CTAs of one strip kernel on the whole device (queried once).
+// Resident CTAs of a strip kernel on the current device (`blocks` threads,
+// `smem` bytes of dynamic shared memory, opted in first when non-zero),
+// computed once per device.
+int resident_on_device(PerDevice& cache, const void* fn, int threads, int smem)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return cache.get(dev, [&] {
+        if (smem > 0) {
+            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        }
+        int per_sm = 0, nsm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, (size_t)smem);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        return per_sm > 0 && nsm > 0 ? per_sm * nsm : 148;
+    });
+}
+
 template <int LIM, int RS>
 int resident_blocks()
 {
-    static int cached = 0;
-    if (cached == 0) {
-        int per_sm = 0, nsm = 0, dev = 0;
-        cudaGetDevice(&dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip2d<LIM, RS>, 128, 0);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cached = per_sm > 0 && nsm > 0 ? per_sm * nsm : 148;
-    }
-    return cached;
+    static PerDevice cache;
+    return resident_on_device(cache, reinterpret_cast<const void*>(k_strip2d<LIM, RS>), 128, 0);
 }
 
 template <int LIM, int RS>
 int resident_blocks_fx()
 {
-    static int cached = 0;
-    if (cached == 0) {
-        int per_sm = 0, nsm = 0, dev = 0;
-        cudaGetDevice(&dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip2d<LIM, RS, 1>, 128, 0);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cached = per_sm > 0 && nsm > 0 ? per_sm * nsm : 148;
-    }
-    return cached;
+    static PerDevice cache;
+    return resident_on_device(cache, reinterpret_cast<const void*>(k_strip2d<LIM, RS, 1>), 128, 0);
 }
 
 constexpr int kSyncSmem = kStripSyncWarps * kStripRingDoubles * (int)sizeof(double);
 
-// Resident CTAs of the in-step strip kernel (one per SM), queried once.
+// Resident CTAs of the in-step strip kernel (one per SM).
 template <int LIM, int RS>
 int resident_blocks_sync()
 {
-    static int cached = 0;
-    if (cached == 0) {
-        int per_sm = 0, nsm = 0, dev = 0;
-        cudaGetDevice(&dev);
-        cudaFuncSetAttribute(k_strip2d_sync<LIM, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSyncSmem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip2d_sync<LIM, RS>, 32 * kStripSyncWarps,
-                                                      kSyncSmem);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cached = per_sm > 0 && nsm > 0 ? per_sm * nsm : 148;
-    }
-    return cached;
+    static PerDevice cache;
+    return resident_on_device(cache, reinterpret_cast<const void*>(k_strip2d_sync<LIM, RS>), 32 * kStripSyncWarps,
+                              kSyncSmem);
 }
 
 // sync: CTAs of 16 warps marching in step (k_strip2d_sync); otherwise CTAs
@@ -123,15 +119,8 @@ void launch_l(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl
 template <int LIM, int RS>
 int resident_blocks_pair()
 {
-    static int cached = 0;
-    if (cached == 0) {
-        int per_sm = 0, nsm = 0, dev = 0;
-        cudaGetDevice(&dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip2d_pair<LIM, RS>, 128, 0);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cached = per_sm > 0 && nsm > 0 ? per_sm * nsm : 148;
-    }
-    return cached;
+    static PerDevice cache;
+    return resident_on_device(cache, reinterpret_cast<const void*>(k_strip2d_pair<LIM, RS>), 128, 0);
 }
 
 template <int LIM, int RS>

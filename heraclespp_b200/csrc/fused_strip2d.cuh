@@ -112,7 +112,7 @@ __device__ __forceinline__ void cons_and_flux(const fast::Eos& e, const float w[
 // from its primitives xw = {row below, this row, row above}: limited slopes,
 // times the face density before the predictor, plus the predictor's
 // increment from the face states' mass fluxes, divided by the predicted face
-// density (extrapolation_reconstruction.hpp:315-337, :459-469).
+// density (extrapolation_reconstruction.hpp:315-337, :329-339).
 template <int LIM, int NFX = 0>
 __device__ __forceinline__ void strip_hancock(const StripCtx& c, const float wd[4], const float wc[4], const float wu[4],
                                               float hxL[4], float hxR[4], float hyB[4], float hyT[4],

@@ -6,6 +6,7 @@
 #include <algorithm>
 
 #include "fused_strip3d.cuh"
+#include "per_device.hpp"
 #include "stages.hpp"
 
 namespace hcl::fused {
@@ -29,15 +30,17 @@ void launch_lrf(const GridDev& g, const StateDev& in, const StateDev& out, StepC
                 int slot, int out_buf, int L, cudaStream_t s)
 {
     constexpr int kSmem = (int)sizeof(S3SharedT<NFX>);
-    static int resident = 0;
-    if (resident == 0) {
+    // shared-memory opt-in and resident CTAs, once per device
+    static PerDevice cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int resident = cache.get(dev, [&] {
         cudaFuncSetAttribute(k_strip3d<LIM, RS, NFX>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
-        int per_sm = 0, nsm = 0, dev = 0;
-        cudaGetDevice(&dev);
+        int per_sm = 0, nsm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_strip3d<LIM, RS, NFX>, kS3Threads, kSmem);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        resident = std::max(1, per_sm) * (nsm > 0 ? nsm : 148);
-    }
+        return std::max(1, per_sm) * (nsm > 0 ? nsm : 148);
+    });
     const int ncol = ((g.nx[0] + 27) / 28) * ((g.nx[1] + 11) / 12);
     if (L <= 0) {
         // plane count per CTA that minimises waves x (planes + 2 start-up planes)

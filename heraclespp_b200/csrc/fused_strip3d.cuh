@@ -84,7 +84,7 @@ __device__ __forceinline__ void cons_and_flux(const fast::Eos& e, const float w[
 // z) and xo[3..5] (plus faces) from its primitives xw = {centre, y-, y+, z-,
 // z+}: limited slopes, times the face density before the predictor, plus the
 // predictor's increment from the face states' mass fluxes, divided by the
-// predicted face density (extrapolation_reconstruction.hpp:315-337, :459-469).
+// predicted face density (extrapolation_reconstruction.hpp:315-337, :329-339).
 template <int LIM, int NFX = 0>
 __device__ __forceinline__ void hancock(const Ctx& c, const float wc[5], const float wyd[5], const float wyu[5],
                                         const float wzd[5], const float wzu[5], float hm[3][5], float hp[3][5],

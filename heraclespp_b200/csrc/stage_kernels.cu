@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(kThreads, kHeavyMinBlocks) k_hancock(GridDev g
     }
 }
 
-// extrapolation_reconstruction.hpp:459-469 "passive_scalar_extrapolation"
+// extrapolation_reconstruction.hpp:329-339 "passive_scalar_extrapolation"
 template <int ND>
 __global__ void k_passive_extrap(GridDev g, Box bx, const double* __restrict__ rho_rec, double* __restrict__ fx_rec)
 {

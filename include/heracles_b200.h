@@ -169,7 +169,11 @@ int hcl_hydro_reconstruction(hcl_handle* h, int ng_eff, double dt, const double*
  * ghosts (2-D, nfx = 0: N <= 349525; 3-D: N <= 174762); larger grids get
  * HCL_ERR_CONFIG.  The first call on a device looks the array up
  * (cudaGetSymbolAddress) and switches to the handle's device for it; make
- * that first call before any stream capture.  Nothing in the scratch needs to
+ * that first call before any stream capture.  The looked-up address is kept
+ * for the life of the process: after a cudaDeviceReset of that device (or an
+ * unload and reload of this library's module) it no longer names the array,
+ * so do not call this entry point on a device that was reset after its first
+ * call.  Nothing in the scratch needs to
  * start at zero (each call writes every entry it reads).  The array is shared
  * by all handles on a device: calls whose work overlaps in time on one device
  * (different streams, threads or handles) race on it; order them. */

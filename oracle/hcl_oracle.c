@@ -930,7 +930,7 @@ void or_hydro_reconstruction(const or_ctx* c, int ng_eff, double dt, const doubl
     }
 
     if (nfx > 0) {
-        /* "passive_scalar_extrapolation" :459-469 */
+        /* "passive_scalar_extrapolation" :329-339 */
 #pragma omp parallel for collapse(2) schedule(static)
         for (int k = b[2]; k < e[2]; ++k) {
             for (int j = b[1]; j < e[1]; ++j) {

@@ -85,16 +85,21 @@ def oracle_lib_path() -> Path:
     return HERE / "liboracle.so"
 
 
-def build_oracle(ref: bool | None = None) -> None:
-    """Builds liboracle.so, and oracle/_ref when the reference tree exists."""
+def build_oracle(ref: bool = True) -> None:
+    """Builds liboracle.so and, with ref, oracle/_ref (the recipe skips the
+    reference build when the reference sources are absent)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
-    if ref is None:
-        ref = Path(os.environ.get("HCL_REF_SRC", "/root/reference/src")).is_dir()
     if ref:
-        env = dict(os.environ)
-        if "HCL_REF_SRC" in env:
-            env["REF_SRC"] = env["HCL_REF_SRC"]
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True, env=env)
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+
+
+def reference_root() -> Path | None:
+    """The reference checkout the oracle recipe reads (HCL_REF_SRC or the
+    recipe's default), or None when it is absent."""
+    out = subprocess.run(["make", "-s", "-C", str(HERE), "print-ref-root"], check=True, capture_output=True,
+                         text=True).stdout.strip()
+    root = Path(out) if out else None
+    return root if root is not None and (root / "src").is_dir() else None
 
 
 _LIB = None

@@ -3,7 +3,6 @@
 Tests marked ``gpu`` need a CUDA device and the built product library; the
 rest run on CPU (oracle pins, host-side logic, C-ABI exports, gloo ranks).
 """
-import os
 import sys
 from pathlib import Path
 
@@ -32,11 +31,9 @@ def oracle_built():
 def ref_cell_available():
     p = ROOT / "oracle" / "_ref" / "libref_cell_2d.so"
     if not p.exists():
-        src = Path(os.environ.get("HCL_REF_SRC", "/root/reference/src"))
-        if src.is_dir():
-            from oracle import build_oracle
+        from oracle import build_oracle
 
-            build_oracle(ref=True)
+        build_oracle(ref=True)  # a no-op for the reference part when its sources are absent
     if not p.exists():
         pytest.skip("oracle/_ref not built (reference sources absent)")
     return True

@@ -1,7 +1,8 @@
 """Generates the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a container that has the reference tree (default /root/reference,
-override with HCL_REF_ROOT) after ``make -C oracle ref``:
+Run where the reference tree is present (the checkout the oracle recipe
+reads: HCL_REF_SRC=<checkout>/src or the recipe's default) after
+``make -C oracle ref``:
 
     python tests/golden/make_golden.py
 
@@ -14,7 +15,6 @@ Outputs (small, committed):
                           thermodynamics/perfect_gas.*) on seeded states.
 """
 import importlib.util
-import os
 import sys
 from pathlib import Path
 
@@ -22,8 +22,12 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF_ROOT = Path(os.environ.get("HCL_REF_ROOT", "/root/reference"))
 sys.path.insert(0, str(ROOT))
+from oracle import reference_root  # noqa: E402
+
+REF_ROOT = reference_root()
+if REF_ROOT is None:
+    raise SystemExit("reference checkout not found: set HCL_REF_SRC to its src/ directory")
 
 SOLVERS = ["HLL", "HLLC", "Low Mach"]
 LIMS = ["Constant", "VanLeer", "Minmod", "VanAlbada"]

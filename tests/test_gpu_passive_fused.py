@@ -1,7 +1,7 @@
 """Passive scalars in the fused tile kernels: hcl_run on handles with nfx > 0
 (and no pressure fix) steps with k_fused_step, which carries the scalars'
 face reconstruction, Hancock predictor (extrapolation_reconstruction.hpp:
-315-337, :459-469) and upwind Godunov update (godunov_scheme.hpp:118-123,
+315-337, :329-339) and upwind Godunov update (godunov_scheme.hpp:118-123,
 :262-301).  The FP64 kernel equals the oracle's main loop bit for bit; the
 FP32-mixed kernel stays within a small tolerance of it."""
 import numpy as np
