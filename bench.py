@@ -54,6 +54,8 @@ def parse():
                    help="skip the passive-scalar (stage-composed loop) measurement")
     p.add_argument("--no-rt3d", action="store_true", help="skip the 3-D Rayleigh-Taylor measurement")
     p.add_argument("--rt3d-steps", type=int, default=500, help="steps of the 3-D Rayleigh-Taylor measurement")
+    p.add_argument("--accuracy-steps", type=int, default=1000,
+                   help="KH steps over which the mixed step is compared with the FP64 step (the config's 1000)")
     return p.parse_args()
 
 
@@ -137,6 +139,47 @@ def time_fused(torch, d, steps, warmup):
     e1.synchronize()
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) * 1e-3, r
+
+
+def field_errors(mixed, ref, ng):
+    """Error of the FP32-mixed state against the FP64 one, per stored field,
+    over the interior cells: relative L1 (sum |a-b| / sum |b|), relative
+    L-infinity (max |a-b| / max |b|) and the largest per-cell relative error
+    of the positive fields (rho, E)."""
+    rho_a, m_a, E_a = mixed
+    rho_b, m_b, E_b = ref
+    nd = m_a.shape[0]
+    inner = tuple(slice(ng, -ng) if n > 1 else slice(None) for n in rho_a.shape)
+    pairs = [("rho", rho_a, rho_b)] + [(f"rhou_{k}", m_a[k], m_b[k]) for k in range(nd)] + [("E", E_a, E_b)]
+    out = {}
+    for name, a, b in pairs:
+        a = a[inner]
+        b = b[inner]
+        diff = np.abs(a - b)
+        e = {"rel_l1": float(np.sum(diff) / np.sum(np.abs(b))),
+             "rel_linf": float(np.max(diff) / np.max(np.abs(b)))}
+        if name in ("rho", "E"):
+            e["max_cell_rel"] = float(np.max(diff / np.abs(b)))
+        out[name] = e
+    return out
+
+
+def kh_accuracy(prim, steps):
+    """KH 2048^2 over `steps` steps: the FP32-mixed step with its own CFL dts,
+    then the FP64 step with the same dt sequence; errors per field."""
+    dm, _ = kh_domain("fp32_mixed")
+    dm.set_state_from_prim(*prim)
+    dm.run(cfl=0.4, nsteps=steps)
+    dts = dm.dt_log()[:steps]
+    mixed = dm.get_state()
+    dm.close()
+    d64, _ = kh_domain("fp64")
+    d64.set_state_from_prim(*prim)
+    d64.run(nsteps=steps, dts=dts)
+    ref = d64.get_state()
+    d64.close()
+    return {"steps_compared": int(len(dts)), "reference": "FP64 fused step (bit-equal to the oracle), same dts",
+            "fields": field_errors(mixed, ref, 2)}
 
 
 def read_traffic():
@@ -305,7 +348,7 @@ def rt3d_cost(torch, steps=500, nx=(256, 256, 512)):
     e1.synchronize()
     t_mixed = e0.elapsed_time(e1) * 1e-3
     dts = dm.dt_log()[:steps]
-    rho_m = dm.get_state()[0]
+    st_m = dm.get_state()
     dm.close()
     d64 = Domain(3, list(nx), precision="fp64", **kw)
     d64.set_state_from_prim(*prim)
@@ -318,18 +361,15 @@ def rt3d_cost(torch, steps=500, nx=(256, 256, 512)):
     e1.record(stream)
     e1.synchronize()
     t_64 = e0.elapsed_time(e1) * 1e-3
-    rho_64 = d64.get_state()[0]
+    st_64 = d64.get_state()
     d64.close()
-    ng = 2
-    a = rho_m[ng:-ng, ng:-ng, ng:-ng]
-    b = rho_64[ng:-ng, ng:-ng, ng:-ng]
     out["fp32_mixed"] = {"mcups": steps * cells / t_mixed * 1e-6, "ms_per_step": t_mixed / steps * 1e3,
                          "achieved_gbs": 80 * cells / (t_mixed / steps) * 1e-9}
     out["fp64"] = {"mcups": steps * cells / t_64 * 1e-6, "ms_per_step": t_64 / steps * 1e3,
                    "achieved_gbs": 80 * cells / (t_64 / steps) * 1e-9}
     out["speedup_mixed_vs_fp64"] = t_64 / t_mixed
-    out["rel_l1_rho_mixed_vs_fp64"] = float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
-    out["rel_linf_rho_mixed_vs_fp64"] = float(np.max(np.abs(a - b) / np.abs(b)))
+    out["accuracy"] = {"steps_compared": int(len(dts)), "reference": "FP64 fused step, same dts",
+                       "fields": field_errors(st_m, st_64, 2)}
     return out
 
 
@@ -497,23 +537,14 @@ def run_ours(args):
     with ClockSampler(int(os.environ.get("HCL_NVSMI_INDEX", dev_index))) as clk:
         el_mixed, r_mixed = time_fused(torch, d, args.steps, args.warmup)
     launches = hb.kernel_launch_count() - launches0 - args.warmup
-    dts = d.dt_log()
-    rho_mixed = d.get_state()[0]
 
-    # ---- FP64 fused step, same workload and the same dt sequence ----------
+    # ---- FP64 fused step, same workload ---------------------------------------
     d64, _ = kh_domain("fp64")
     d64.set_state_from_prim(*prim)
     el_64, _ = time_fused(torch, d64, args.steps, args.warmup)
-    # accuracy of mixed vs FP64 with identical dts over warmup+steps steps
-    d64.set_state_from_prim(*prim)
-    d64.run(nsteps=len(dts), dts=dts)
-    rho64 = d64.get_state()[0]
-    ng = 2
-    a = rho_mixed[0, ng:-ng, ng:-ng]
-    b = rho64[0, ng:-ng, ng:-ng]
-    l1 = float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
-    linf = float(np.max(np.abs(a - b) / np.abs(b)))
     d64.close()
+    # accuracy of mixed vs FP64 over the config's step count, every field
+    accuracy = kh_accuracy(prim, args.accuracy_steps)
 
     # ---- end to end through the C ABI with host buffers ----------------------
     pinned = [torch.empty(s, dtype=torch.float64).pin_memory() for s in (d.shape3, (2,) + d.shape3, d.shape3)]
@@ -535,15 +566,26 @@ def run_ours(args):
     e1.synchronize()
     el_e2e = e0.elapsed_time(e1) * 1e-3
     state_bytes = sum(int(np.prod(t_.shape)) * 8 for t_ in pinned)
+    # the same with the whole state copied in and out around every single step
+    n1 = max(1, min(args.steps, 10))
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(n1):
+        d.set_state(*[t_.numpy() for t_ in pinned])
+        d.run(cfl=0.4, nsteps=1)
+        d.get_state(out=tuple(t_.numpy() for t_ in pinned))
+    e1.record(stream)
+    e1.synchronize()
+    el_e2e1 = e0.elapsed_time(e1) * 1e-3
 
     # ---- cross-rank aggregation -------------------------------------------
-    el_max, el64_max, e2e_max = el_mixed, el_64, el_e2e
+    el_max, el64_max, e2e_max, e2e1_max = el_mixed, el_64, el_e2e, el_e2e1
     if world > 1:
         import torch.distributed as dist
 
-        t = torch.tensor([el_mixed, el_64, el_e2e], dtype=torch.float64, device="cuda")
+        t = torch.tensor([el_mixed, el_64, el_e2e, el_e2e1], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el_max, el64_max, e2e_max = (float(v) for v in t.tolist())
+        el_max, el64_max, e2e_max, e2e1_max = (float(v) for v in t.tolist())
 
     value = world * args.steps * CELLS / el_max * 1e-6
     value64 = world * args.steps * CELLS / el64_max * 1e-6
@@ -560,8 +602,7 @@ def run_ours(args):
                    "e2e_steps_per_call": chunk, "schedule": d.schedule()},
         "fp64": {"value": value64, "ms_per_step": el64_max / args.steps * 1e3, "unit": "Mcell-updates/s"},
         "speedup_mixed_vs_fp64": value / value64,
-        "accuracy": {"rel_l1_rho_mixed_vs_fp64": l1, "rel_linf_rho_mixed_vs_fp64": linf,
-                     "steps_compared": int(len(dts))},
+        "accuracy": accuracy,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic,
                      "peak_spec": HBM_SPEC_GBS, "frac_of_spec": achieved / HBM_SPEC_GBS,
@@ -570,6 +611,9 @@ def run_ours(args):
                      "bytes_per_cell": BYTES_PER_CELL, "cells_per_launch": CELLS},
         "e2e": {"value": e2e_val, "unit": "Mcell-updates/s", "h2d_bytes_per_step": state_bytes / chunk,
                 "d2h_bytes_per_step": state_bytes / chunk + 96},
+        "e2e_state_copied_every_step": {"value": world * n1 * CELLS / e2e1_max * 1e-6, "unit": "Mcell-updates/s",
+                                        "steps": n1, "h2d_bytes_per_step": state_bytes,
+                                        "d2h_bytes_per_step": state_bytes + 96},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }

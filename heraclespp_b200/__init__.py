@@ -366,7 +366,8 @@ class Ensemble:
         return int(s.value or 0)
 
     def run(self, nsteps, *, cfl=0.4, checkpoint_every=0, strip_rows=0, blocks_per_sm=0, use_graph=True,
-            adjoint_precision="fp64", check_status=True, warps_per_cta=0):
+            adjoint_precision="fp64", check_status=True, warps_per_cta=0, barrier_spin_limit=0,
+            barrier_extra_arrivals=0):
         from ._native import EnsembleParams, EnsembleResult
 
         p = EnsembleParams()
@@ -378,6 +379,8 @@ class Ensemble:
         p.use_graph = 1 if use_graph else 0
         p.adjoint_precision = _key(PRECISION, adjoint_precision, "precision")
         p.warps_per_cta = int(warps_per_cta)
+        p.barrier_spin_limit = int(barrier_spin_limit)
+        p.barrier_extra_arrivals = int(barrier_extra_arrivals)
         r = EnsembleResult()
         rc = lib().hcl_ensemble_run(self.e, C.byref(p), C.byref(r))
         if check_status:

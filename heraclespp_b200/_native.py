@@ -113,6 +113,8 @@ class EnsembleParams(C.Structure):
         ("use_graph", C.c_int),
         ("adjoint_precision", C.c_int),
         ("warps_per_cta", C.c_int),
+        ("barrier_spin_limit", C.c_longlong),
+        ("barrier_extra_arrivals", C.c_int),
     ]
 
 

@@ -1938,7 +1938,8 @@ struct hcl_ensemble {
     int lim = 0, rs = 0;
     int L = 0, bps = 0, nw = 4; // tuned schedule: strip rows, CTAs per SM, warps per CTA
     int64_t cells = 0;
-    std::map<std::tuple<int, int, int, int, int>, cudaGraphExec_t> graphs; // (nsteps, step0, L, bps, nw)
+    // (nsteps, step0, L, bps, nw, barrier spin limit, extra barrier arrivals)
+    std::map<std::tuple<int, int, int, int, int, long long, unsigned int>, cudaGraphExec_t> graphs;
     // batched reverse pass: problem tables, tile work list, dts of all problems
     hcl::ensemble::AdjProb* d_adjprobs = nullptr;
     hcl::ensemble::Prob* d_rec_probs = nullptr;
@@ -2010,7 +2011,7 @@ int ensemble_build_items(hcl_ensemble* e, int L)
 }
 
 int ensemble_launch(hcl_ensemble* e, const hcl::ensemble::Prob* probs, int nsteps, int step0, int L, int bps, int nw,
-                    int use_graph, double cfl, int* graphed)
+                    int use_graph, double cfl, int* graphed, long long spin_limit = 0, int extra_arrivals = 0)
 {
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->h[0]->cfg.device);
@@ -2023,6 +2024,8 @@ int ensemble_launch(hcl_ensemble* e, const hcl::ensemble::Prob* probs, int nstep
     ep.L = L;
     ep.nitems = e->nitems;
     ep.nprob = (int)e->h.size();
+    ep.spin_limit = spin_limit > 0 ? spin_limit : hcl::ensemble::kSpinLimit;
+    ep.extra_arrivals = (unsigned int)(extra_arrivals > 0 ? extra_arrivals : 0);
     auto issue = [&]() -> cudaError_t {
         cudaError_t err = cudaMemsetAsync(e->d_barrier, 0, sizeof(unsigned int), e->stream);
         if (err == cudaSuccess) {
@@ -2036,7 +2039,7 @@ int ensemble_launch(hcl_ensemble* e, const hcl::ensemble::Prob* probs, int nstep
     };
     *graphed = 0;
     if (use_graph && probs == e->d_probs) {
-        const auto key = std::make_tuple(nsteps, step0, L, bps, nw);
+        const auto key = std::make_tuple(nsteps, step0, L, bps, nw, ep.spin_limit, ep.extra_arrivals);
         auto it = e->graphs.find(key);
         if (it == e->graphs.end()) {
             cudaGraph_t graph;
@@ -2294,7 +2297,8 @@ int hcl_ensemble_run(hcl_ensemble* e, const hcl_ensemble_params* p, hcl_ensemble
             }
         }
         int graphed = 0;
-        if ((rc = ensemble_launch(e, e->d_probs, len, done, e->L, e->bps, e->nw, p->use_graph, p->cfl, &graphed))) {
+        if ((rc = ensemble_launch(e, e->d_probs, len, done, e->L, e->bps, e->nw, p->use_graph, p->cfl, &graphed,
+                                  p->barrier_spin_limit, p->barrier_extra_arrivals))) {
             return rc;
         }
         graphed_all &= graphed;
@@ -2461,6 +2465,7 @@ int hcl_ensemble_adjoint(hcl_ensemble* e, const double* const* lam_final, double
     ep.dts = e->d_adj_dts;
     ep.dts_stride = N;
     ep.seg_mode = 1;
+    ep.spin_limit = hcl::ensemble::kSpinLimit;
     HCL_CUDA(cudaMemsetAsync(e->d_status, 0, sizeof(int), s));
     // the segment loop (2 persistent launches per checkpoint segment) is
     // captured in a CUDA graph and replayed; it is rebuilt for every call

@@ -21,11 +21,12 @@
 
 namespace hcl::ensemble {
 
-constexpr long long kSpinLimit = 1ll << 26;
-
 // Returns the same answer to every thread of the CTA (thread 0 decides), so a
 // CTA leaves the step loop as a whole and no warp is left half-exited.
-__device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int target, int* status)
+// Thread 0 polls at most spin_limit times (each poll sleeps ~64 ns), then
+// records HCL_ERR_TIMEOUT; a CTA that sees any error recorded stops waiting.
+__device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int target, int* status,
+                                             long long spin_limit = kSpinLimit)
 {
     __shared__ int go_on;
     __syncthreads();
@@ -39,7 +40,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int t
                 ok = 0;
                 break;
             }
-            if (++spins > kSpinLimit) {
+            if (++spins > spin_limit) {
                 atomicExch(status, 6); // HCL_ERR_TIMEOUT
                 ok = 0;
                 break;
@@ -114,7 +115,7 @@ k_ensemble(const Prob* __restrict__ probs, const int* __restrict__ item_prob, Pa
                 atomicExch(status, 4);
             }
         }
-        if (!grid_barrier(barrier, (unsigned)((s + 1) * gridDim.x), status)) {
+        if (!grid_barrier(barrier, (unsigned)((s + 1) * gridDim.x) + ep.extra_arrivals, status, ep.spin_limit)) {
             return;
         }
     }

@@ -142,6 +142,10 @@ struct Prob {
     int64_t seg_stride; // segment mode: state s at q[0] + s * seg_stride
 };
 
+// polls of the ensemble's step barrier before it records HCL_ERR_TIMEOUT
+// (each poll sleeps ~64 ns: a few seconds in all)
+constexpr long long kSpinLimit = 1ll << 26;
+
 struct Params {
     double cfl;
     int nsteps;
@@ -153,6 +157,8 @@ struct Params {
     const double* dts; // [nprob][dts_stride], indexed by iteration
     int dts_stride;
     int seg_mode;      // 1: step s reads state s and writes state s+1 of each segment buffer
+    long long spin_limit;         // polls of the step barrier before HCL_ERR_TIMEOUT (> 0)
+    unsigned int extra_arrivals;  // arrivals the step barrier waits for beyond the CTAs (tests only)
 };
 
 // Reverse pass of a batch: one problem's segment states, adjoint buffers,

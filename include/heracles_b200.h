@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define HCL_ABI_VERSION 3
+#define HCL_ABI_VERSION 4
 
 /* ---- status codes ------------------------------------------------------ */
 enum hcl_status {
@@ -356,6 +356,11 @@ typedef struct hcl_ensemble_params {
     int use_graph;            /* 1: capture the persistent launch in a CUDA graph and replay it */
     int adjoint_precision;    /* HCL_FP64 or HCL_FP32_MIXED reverse sweep for hcl_ensemble_adjoint */
     int warps_per_cta;        /* 0: autotune; 4 or 16 warps per CTA of the persistent launch */
+    long long barrier_spin_limit; /* polls of the step barrier before it gives up with HCL_ERR_TIMEOUT
+                                   * (every CTA then returns); 0: 2^26 polls, a few seconds */
+    int barrier_extra_arrivals;   /* failure-path tests only: the step barrier waits for this many
+                                   * arrivals beyond the CTA count, which never come, so it runs out
+                                   * its limit; 0 in normal use */
 } hcl_ensemble_params;
 
 typedef struct hcl_ensemble_result {

@@ -38,7 +38,7 @@ def test_abi_version_and_errors_without_device():
     from heraclespp_b200._native import Config
 
     L = lib()
-    assert L.hcl_abi_version() == 3
+    assert L.hcl_abi_version() == 4
     cfg = Config()
     L.hcl_config_default(C.byref(cfg))
     # reference defaults (utils/param.cpp): gamma 5/3, VanLeer, HLL, Nghost 2

@@ -33,4 +33,11 @@ def test_bench_json_line():
     assert r["traffic"] is None or r["traffic"] > 0
     assert d["gpu_launches"] >= 5
     assert "sm_mhz" in d["clocks"] and "reasons" in d["clocks"]
-    assert d["accuracy"]["rel_l1_rho_mixed_vs_fp64"] < 1e-6
+    acc = d["accuracy"]
+    assert acc["steps_compared"] == 1000
+    assert set(acc["fields"]) == {"rho", "rhou_0", "rhou_1", "E"}
+    # the density bar (1e-6 relative L1) after the workload's 1000 steps
+    assert acc["fields"]["rho"]["rel_l1"] < 1e-6
+    for name, e in acc["fields"].items():
+        assert e["rel_l1"] >= 0 and e["rel_linf"] >= 0, name
+    assert d["e2e_state_copied_every_step"]["value"] > 0

@@ -216,11 +216,14 @@ def test_strip_passive_scalar_schedules():
     assert out[3][1].min() >= 0.0 and out[3][1].max() <= 1.0
 
 
-def test_column_march_passive_scalar():
-    """One passive scalar in the 3-D column march (schedule 1): within 1e-6
-    of the FP32-mixed tile kernel and within 1e-5 of the FP64 oracle
-    (relative L1, density and scalar), the scalar in [0, 1]."""
-    kw = dict(gamma=1.4, limiter="Minmod", riemann="HLL",
+@pytest.mark.parametrize("limiter,riemann", [("Minmod", "HLL"), ("VanLeer", "HLLC"), ("VanAlbada", "Low Mach"),
+                                             ("Constant", "HLLC")])
+def test_column_march_passive_scalar(limiter, riemann):
+    """One passive scalar in the 3-D column march (schedule 1), for several
+    limiter x Riemann solver instantiations of the kernel: within 1e-6 of
+    the FP32-mixed tile kernel and within 1e-5 of the FP64 oracle (relative
+    L1, density and scalar), the scalar in [0, 1]."""
+    kw = dict(gamma=1.4, limiter=limiter, riemann=riemann,
               bc=["Periodic", "Periodic", "NullGradient", "Reflexive", "Reflexive", "Reflexive"], g=(0.0, 0.0, -0.1))
     nx = [40, 30, 36]
     steps = 20
