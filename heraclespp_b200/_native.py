@@ -25,7 +25,7 @@ BCS = {"NullGradient": 0, "Periodic": 1, "Reflexive": 2}
 GEOMS = {"Cartesian": 0, "Spherical": 1}
 GRAVITY = {"Uniform": 0, "Point_mass": 1, "Internal_mass": 2}
 EOS = {"PerfectGas": 0, "RadGas": 1}
-PRECISION = {"fp64": 0, "fp32_mixed": 1}
+PRECISION = {"fp64": 0, "fp32_mixed": 1, "fp64_fast": 2}
 
 # Every entry point declared in include/heracles_b200.h.
 EXPORTS = [

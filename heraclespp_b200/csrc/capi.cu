@@ -396,7 +396,7 @@ int validate(const hcl_config* c)
         c->gravity != HCL_GRAVITY_INTERNAL_MASS) {
         return fail(HCL_ERR_CONFIG, "Unknown gravity id %d", c->gravity);
     }
-    if (c->precision != HCL_FP64 && c->precision != HCL_FP32_MIXED) {
+    if (c->precision != HCL_FP64 && c->precision != HCL_FP32_MIXED && c->precision != HCL_FP64_FAST) {
         return fail(HCL_ERR_CONFIG, "Unknown precision id %d", c->precision);
     }
     if (c->eos != HCL_EOS_PERFECT_GAS && c->eos != HCL_EOS_RAD_GAS) {
@@ -469,6 +469,8 @@ void launch_step(hcl_handle* h, const RunParamsDev& rp, int64_t counter, StepCtl
     }
     if (h->cfg.precision == HCL_FP64) {
         hcl::fused::step_exact(h->g, h->st[in_buf], h->st[out_buf], ctl, rp, slot, out_buf, s);
+    } else if (h->cfg.precision == HCL_FP64_FAST) {
+        hcl::fused::step_fast64(h->g, h->st[in_buf], h->st[out_buf], ctl, rp, slot, out_buf, s);
     } else {
         hcl::fused::step_mixed(h->g, h->st[in_buf], h->st[out_buf], ctl, rp, slot, out_buf, shape, s);
     }
@@ -706,6 +708,7 @@ int hcl_create(const hcl_config* cfg, hcl_handle** out)
     }
     HCL_CUDA(cudaSetDevice(cfg->device));
     hcl::fused::configure_exact();
+    hcl::fused::configure_fast64();
     hcl::fused::configure_mixed();
     hcl::adjoint::configure();
     HCL_CUDA(cudaGetLastError());
@@ -1543,6 +1546,9 @@ int hcl_run(hcl_handle* h, const hcl_run_params* p, hcl_run_result* r)
     if (ctl.err == HCL_ERR_NEGATIVE_DT) {
         return fail(HCL_ERR_NEGATIVE_DT, "Error: the time step is negative");
     }
+    if (ctl.err == HCL_ERR_TIMEOUT) {
+        return fail(HCL_ERR_TIMEOUT, "a bounded device-side wait for a staged state row gave up");
+    }
     return HCL_OK;
 }
 
@@ -1693,6 +1699,9 @@ int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p)
         g.riemann == HCL_RIEMANN_LOW_MACH || g.nfx > 0 || h->cfg.pressure_fix || g.eos != HCL_EOS_PERFECT_GAS) {
         return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian uniform grids, uniform gravity, HLL/HLLC, nfx = 0, "
                                     "no pressure fix, the perfect-gas EOS");
+    }
+    if (p->precision != HCL_FP64 && p->precision != HCL_FP32_MIXED) {
+        return fail(HCL_ERR_CONFIG, "the reverse sweep runs in HCL_FP64 or HCL_FP32_MIXED");
     }
     int rc;
     StepCtl ctl;
@@ -1874,6 +1883,9 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
             if (h->cfg.precision == HCL_FP64) {
                 hcl::fused::step_exact(g, state_at(h->adj_seg, base + j), state_at(h->adj_seg, base + j + 1),
                                        h->adj_ctl, rp, j % 6, 1, a);
+            } else if (h->cfg.precision == HCL_FP64_FAST) {
+                hcl::fused::step_fast64(g, state_at(h->adj_seg, base + j), state_at(h->adj_seg, base + j + 1),
+                                        h->adj_ctl, rp, j % 6, 1, a);
             } else {
                 hcl::fused::step_mixed(g, state_at(h->adj_seg, base + j), state_at(h->adj_seg, base + j + 1),
                                        h->adj_ctl, rp, j % 6, 1, h->mixed_shape < 0 ? 0 : h->mixed_shape, a);

@@ -13,13 +13,14 @@ namespace hcl::fused {
 // 0-2 shared-memory tiles 16x16, 32x8, 32x16; 3-5 warp strips of 32, 64,
 // 128 rows; 6 warp strips whose height fits one wave of resident warps;
 // 7 and 8 paired-column warp strips (fitted height, 32 rows); 9 fitted warp
-// strips in CTAs of 16 warps that march in step.  3-9 need a uniform
-// Cartesian grid, 7-8 an even ghost width.  With passive scalars: the tiles,
+// strips in CTAs of 16 warps that march in step, rows staged by TMA; 10 the
+// same with per-lane cp.async staging.  3-10 need a uniform Cartesian grid,
+// 7-9 an even ghost width.  With passive scalars: the tiles,
 // and for one scalar the 4-warp strips 3-6 (2-D) or the column march (3-D).
 // 3-D: 0 shared-memory tiles 8x8x4; 1 column march (uniform Cartesian grids).
 int mixed_shape_count(int ndim)
 {
-    return ndim == 2 ? 10 : (ndim == 3 ? 2 : 1);
+    return ndim == 2 ? 11 : (ndim == 3 ? 2 : 1);
 }
 
 size_t mixed_smem_bytes(const GridDev& g, int shape)
@@ -55,7 +56,10 @@ bool mixed_shape_valid(const GridDev& g, int shape)
     if (shape < 3) {
         return true;
     }
-    return (shape < 7 || shape == 9) ? strip2d_eligible(g) : strip2d_pair_eligible(g);
+    if (shape == 9) {
+        return strip2d_tma_eligible(g);
+    }
+    return (shape < 7 || shape == 10) ? strip2d_eligible(g) : strip2d_pair_eligible(g);
 }
 
 void configure_mixed()
@@ -75,13 +79,13 @@ void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepC
         FusedLauncher<1, false, 256, 1, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
         break;
     case 2:
-        if (shape == 9 && strip2d_eligible(g)) {
-            step_strip2d(g, in, out, ctl, rp, slot, out_buf, 0, true, s);
+        if ((shape == 9 && strip2d_tma_eligible(g)) || (shape == 10 && strip2d_eligible(g))) {
+            step_strip2d(g, in, out, ctl, rp, slot, out_buf, 0, true, shape == 9, s);
         } else if (shape >= 7 && shape < 9 && strip2d_pair_eligible(g)) {
             step_strip2d_pair(g, in, out, ctl, rp, slot, out_buf, shape == 7 ? 0 : 32, s);
         } else if (shape >= 3 && (strip2d_eligible(g) || (shape <= 6 && strip2d_fx_eligible(g)))) {
             step_strip2d(g, in, out, ctl, rp, slot, out_buf, shape == 3 ? 32 : (shape == 4 ? 64 : (shape == 5 ? 128 : 0)),
-                         false, s);
+                         false, false, s);
         } else if (shape == 1) {
             FusedLauncher<2, false, 32, 8, 1>::launch(g, in, out, ctl, rp, slot, out_buf, s);
         } else if (shape == 2) {

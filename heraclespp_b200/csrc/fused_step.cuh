@@ -518,7 +518,20 @@ __device__ __forceinline__ void fused_step_body(const GridDev& g, const StateDev
                 const R vc = sp[v * S::NP + lc];
                 const R vp = sp[v * S::NP + lc + lstride[idim]];
                 const R vm = sp[v * S::NP + lc - lstride[idim]];
-                if constexpr (EXACT) {
+                if constexpr (EXACT && EOSK == EOS_PERFECT_GAS_FAST) {
+                    // fast FP64 on a uniform grid: the limiter of the raw
+                    // differences, halved (positive homogeneity, as below)
+                    if (g.uniform_cart) {
+                        const double sh = 0.5 * exact::slope(g.limiter, vp - vc, vc - vm, EOSK);
+                        fp[0][idim][v] = vc - sh;
+                        fp[1][idim][v] = vc + sh;
+                    } else {
+                        const double slope =
+                            exact::slope(g.limiter, (vp - vc) / ((dl + dl_p) / 2), (vc - vm) / ((dl_m + dl) / 2), EOSK);
+                        fp[0][idim][v] = vc - ((dl / 2) * slope);
+                        fp[1][idim][v] = vc + ((dl / 2) * slope);
+                    }
+                } else if constexpr (EXACT) {
                     const double slope = exact::slope(g.limiter, (vp - vc) / ((dl + dl_p) / 2), (vc - vm) / ((dl_m + dl) / 2));
                     fp[0][idim][v] = vc - ((dl / 2) * slope);
                     fp[1][idim][v] = vc + ((dl / 2) * slope);
@@ -731,7 +744,8 @@ __device__ __forceinline__ void fused_step_body(const GridDev& g, const StateDev
                     const double dl = g.dx[idim][gcc[idim]];
                     const double dl_m = g.dx[idim][gcc[idim] - 1];
                     const double dl_p = g.dx[idim][gcc[idim] + 1];
-                    const double slope = exact::slope(g.limiter, (vp - vc) / ((dl + dl_p) / 2), (vc - vm) / ((dl_m + dl) / 2));
+                    const double slope = exact::slope(g.limiter, (vp - vc) / ((dl + dl_p) / 2), (vc - vm) / ((dl_m + dl) / 2),
+                                                      EOSK);
                     xf[0][idim] = vc - ((dl / 2) * slope);
                     xf[1][idim] = vc + ((dl / 2) * slope);
                 } else if (g.uniform_cart) {
@@ -1373,29 +1387,43 @@ struct FusedLauncher {
         const int bytes = std::max(optin - (int)fa.sharedSizeBytes, (int)smem());
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     }
-    static void launch(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
-                       int slot, int out_buf, cudaStream_t s)
+    // the kernel of one compile-time EOS kind (occupancy-bounded when it pays)
+    template <int EOSK>
+    static void launch_kind(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl,
+                            const RunParamsDev& rp, int slot, int out_buf, cudaStream_t s)
     {
         const size_t sm = smem(g.nfx);
         const int nt0 = (g.nx[0] + S::T0 - 1) / S::T0;
         const int nt1 = (g.nx[1] + S::T1 - 1) / S::T1;
         const int nt2 = (g.nx[2] + S::T2 - 1) / S::T2;
         const int blocks = nt0 * nt1 * nt2;
-        const bool occ = use_occ(g.nfx);
-        if (EXACT && g.eos == EOS_RAD_GAS) {
-            if (occ) {
-                k_fused_step_occ<ND, EXACT, TX, TY, TZ, EOS_RAD_GAS><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp,
-                                                                                            slot, out_buf);
-            } else {
-                k_fused_step<ND, EXACT, TX, TY, TZ, EOS_RAD_GAS><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot,
-                                                                                            out_buf);
-            }
-        } else if (occ) {
-            k_fused_step_occ<ND, EXACT, TX, TY, TZ><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot, out_buf);
+        if (use_occ(g.nfx)) {
+            k_fused_step_occ<ND, EXACT, TX, TY, TZ, EOSK><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot, out_buf);
         } else {
-            k_fused_step<ND, EXACT, TX, TY, TZ><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot, out_buf);
+            k_fused_step<ND, EXACT, TX, TY, TZ, EOSK><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot, out_buf);
         }
         ++g_launches;
+    }
+    static void launch(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                       int slot, int out_buf, cudaStream_t s)
+    {
+        if constexpr (EXACT) {
+            if (g.eos == EOS_RAD_GAS) {
+                launch_kind<EOS_RAD_GAS>(g, in, out, ctl, rp, slot, out_buf, s);
+                return;
+            }
+        }
+        launch_kind<EOS_PERFECT_GAS>(g, in, out, ctl, rp, slot, out_buf, s);
+    }
+    // fast FP64: the perfect gas in its fast forms (translation units built
+    // with FMA contraction)
+    static void configure_fast()
+    {
+        static_assert(EXACT, "fast FP64 runs the FP64 kernels");
+        set_max_dynamic(reinterpret_cast<const void*>(k_fused_step<ND, EXACT, TX, TY, TZ, EOS_PERFECT_GAS_FAST>));
+        if constexpr (kMinBlocks > 0) {
+            set_max_dynamic(reinterpret_cast<const void*>(k_fused_step_occ<ND, EXACT, TX, TY, TZ, EOS_PERFECT_GAS_FAST>));
+        }
     }
 };
 

@@ -29,6 +29,7 @@
 #include "hcl_device.cuh"
 #include "physics_fast.cuh"
 #include "stages.hpp"
+#include "tma_ring.cuh"
 
 namespace hcl::fused {
 
@@ -232,11 +233,20 @@ constexpr int kStripRingDoubles = 8 * 4 * 32;
 // strip_hancock, upwind fluxes from the Riemann mass fluxes
 // (godunov_scheme.hpp:262-301), the update in FP64 divided by the new density
 // and clamped to [0, 1], stored with the same ghost images.
-template <int LIM, int RS, int SYNC = 0, int XIMG = 1, int NFX = 0>
+// TMA: the ring rows are staged by the Tensor Memory Accelerator (tma_ring.cuh):
+// lane 0 issues one box per row through `tmap` (the input state), the lanes
+// wait on the slot's mbarrier (`bars`, 8 per warp; `phase` holds the parity
+// each slot waits for next, `timeout` is set when a bounded wait gave up).
+// Rows past r1 + 1 are not loaded.  Needs NFX == 0 and an even ghost width
+// (the box's first column c0 - 2 must start on a 16-byte boundary).
+template <int LIM, int RS, int SYNC = 0, int XIMG = 1, int NFX = 0, bool TMA = false>
 __device__ __forceinline__ void strip_work(const GridDev& g, const double* __restrict__ qin, double* __restrict__ qout,
                                            int64_t plane, int pitch, double dt, int sx, int sy, int L, double& inv_max,
-                                           int64_t& bad_cell, StripRingN<4 + NFX> ring)
+                                           int64_t& bad_cell, StripRingN<4 + NFX> ring,
+                                           const CUtensorMap* tmap = nullptr, uint64_t* bars = nullptr,
+                                           unsigned* phase = nullptr, bool* timeout = nullptr)
 {
+    static_assert(!TMA || NFX == 0, "the TMA ring carries the 4 hydro variables");
     const int lane = threadIdx.x & 31;
     const int n0 = g.n[0], n1 = g.n[1];
     const int c0 = g.ng + kStripLanesOut * sx;
@@ -291,6 +301,26 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             q[v] = ring[r & 7][v][lane];
         }
     };
+    // TMA staging: one box {32 columns, 1 row, 4 variables} per row, issued by
+    // lane 0 after the warp has finished reading the slot's previous row
+    unsigned ph = TMA ? *phase : 0u;
+    bool tmo = false;
+    auto tma_issue = [&](int r) {
+        __syncwarp();
+        if (lane == 0) {
+            uint64_t* bar = bars + (r & 7);
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(bar, kTmaRowBytes);
+            tma_load_3d(&ring[r & 7][0][0], tmap, bar, c0 - 2, min(max(r, 0), n1 - 1), 0);
+        }
+    };
+    auto tma_wait = [&](int r) {
+        const int sl = r & 7;
+        if (!mbar_wait_bounded(bars + sl, (ph >> sl) & 1u)) {
+            tmo = true;
+        }
+        ph ^= 1u << sl;
+    };
 
     // preamble: rows r0-2 .. r0+1 -> primitives; Hancock of rows r0-1 and r0
     float wB[4], wC[4], wD[4];
@@ -303,10 +333,19 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         double q[4 + NFX];
         float wA[4], hyB[4];
         float xA = 0.f, xB = 0.f;
-        for (int rr = r0 - 2; rr <= r0 + 3; ++rr) {
-            stage_row(rr);
+        if constexpr (TMA) {
+            for (int rr = r0 - 2; rr <= min(r0 + 3, r1 + 1); ++rr) {
+                tma_issue(rr);
+            }
+            for (int rr = r0 - 2; rr <= r0 + 1; ++rr) {
+                tma_wait(rr);
+            }
+        } else {
+            for (int rr = r0 - 2; rr <= r0 + 3; ++rr) {
+                stage_row(rr);
+            }
+            asm volatile("cp.async.wait_group 2;\n" ::: "memory"); // rows r0-2 .. r0+1 landed
         }
-        asm volatile("cp.async.wait_group 2;\n" ::: "memory"); // rows r0-2 .. r0+1 landed
         ring_row(r0 - 2, q);
         strip_prim(gm1, q, wA);
         if constexpr (NFX > 0) {
@@ -362,8 +401,15 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         double q[4 + NFX];
         float wN[4];
         float xN = 0.f;
-        stage_row(r + 4);
-        asm volatile("cp.async.wait_group 2;\n" ::: "memory"); // rows up to r+2 landed
+        if constexpr (TMA) {
+            if (r + 4 <= r1 + 1) {
+                tma_issue(r + 4);
+            }
+            tma_wait(r + 2); // rows up to r+2 landed
+        } else {
+            stage_row(r + 4);
+            asm volatile("cp.async.wait_group 2;\n" ::: "memory"); // rows up to r+2 landed
+        }
         ring_row(r, q);
         {
             double qn2[4 + NFX];
@@ -513,7 +559,15 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             }
         }
     }
-    asm volatile("cp.async.wait_all;\n" ::: "memory"); // the ring is reused by the next strip
+    if constexpr (TMA) {
+        // every issued row (up to r1 + 1) has been waited for
+        *phase = ph;
+        if (tmo) {
+            *timeout = true;
+        }
+    } else {
+        asm volatile("cp.async.wait_all;\n" ::: "memory"); // the ring is reused by the next strip
+    }
     const double inv_d = (double)inv_f;
     inv_max = inv_d > inv_max ? inv_d : (isnan(inv_d) ? inv_d : inv_max);
     (void)wB;
@@ -628,11 +682,20 @@ k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
 constexpr int kStripSyncRows = 64;
 constexpr int kStripSyncWarps = 16;
 
-template <int LIM, int RS>
+// Dynamic shared memory of k_strip2d_sync: 16 row rings; with TMA also one
+// mbarrier per ring slot and the slack to put the rings on a 1 KB boundary.
+constexpr int kStripSyncSmem = kStripSyncWarps * kStripRingDoubles * (int)sizeof(double);
+constexpr int kStripSyncSmemTma = kStripSyncSmem + kStripSyncWarps * 8 * (int)sizeof(uint64_t) + 1024;
+
+// TMA: the rows come in through the Tensor Memory Accelerator (`tmap` is a
+// 3-D tiled map of the input state: columns, rows, variables); otherwise
+// per-lane cp.async and `tmap` is unused.
+template <int LIM, int RS, bool TMA = false>
 __global__ void __launch_bounds__(32 * kStripSyncWarps, 1)
-k_strip2d_sync(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
+k_strip2d_sync(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L,
+               const __grid_constant__ CUtensorMap tmap)
 {
-    extern __shared__ __align__(16) double s_sync_rings[]; // [kStripSyncWarps][kStripRingDoubles]
+    extern __shared__ __align__(16) double s_sync_rings[]; // [kStripSyncWarps][kStripRingDoubles] (+ mbarriers)
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const Decision dec = decide(ctl, slot, rp);
@@ -647,14 +710,34 @@ k_strip2d_sync(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev 
     const int nitems = ncolw * nstrip;
     double inv_max = 0.0;
     int64_t bad_cell = -1;
-    const StripRing ring = reinterpret_cast<StripRing>(s_sync_rings + warp * kStripRingDoubles);
+    double* rings = s_sync_rings;
+    uint64_t* bars = nullptr;
+    unsigned phase = 0u;
+    bool timeout = false;
+    if constexpr (TMA) {
+        // rings on a 1 KB boundary, then 8 mbarriers per warp
+        const unsigned base = smem_u32(s_sync_rings);
+        rings = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(s_sync_rings) +
+                                          (((base + 1023u) & ~1023u) - base));
+        bars = reinterpret_cast<uint64_t*>(rings + kStripSyncWarps * kStripRingDoubles) + warp * 8;
+        if (lane == 0) {
+            for (int k = 0; k < 8; ++k) {
+                mbar_init(bars + k, 1u);
+            }
+            mbar_init_fence();
+            tma_prefetch_map(&tmap);
+        }
+        __syncwarp();
+    }
+    const StripRing ring = reinterpret_cast<StripRing>(rings + warp * kStripRingDoubles);
     // the CTA takes strips in groups of 16 (one per warp); every warp of the
     // CTA runs the same loop, so the barrier sequences match
     for (int base = blockIdx.x * kStripSyncWarps; base < nitems; base += gridDim.x * kStripSyncWarps) {
         const int w = base + warp;
         if (w < nitems) {
-            strip_work<LIM, RS, kStripSyncRows>(g, in.q, out.q, in.plane, in.pitch, dec.dt, w % ncolw, w / ncolw, L,
-                                                inv_max, bad_cell, ring);
+            strip_work<LIM, RS, kStripSyncRows, 1, 0, TMA>(g, in.q, out.q, in.plane, in.pitch, dec.dt, w % ncolw,
+                                                           w / ncolw, L, inv_max, bad_cell, ring, &tmap, bars, &phase,
+                                                           &timeout);
         } else {
             strip_idle<kStripSyncRows>(L);
         }
@@ -672,6 +755,12 @@ k_strip2d_sync(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev 
     if (bad_cell >= 0) {
         atomicMin(&ctl->bad_cell, (unsigned long long)bad_cell);
         ctl->err = 4;
+        ctl->errflag[(slot + 1) & 1] = 1;
+        ctl->final_buf = out_buf;
+    }
+    if (TMA && __any_sync(0xffffffffu, timeout) && lane == 0) {
+        // a staged row never arrived: stop the run with HCL_ERR_TIMEOUT
+        ctl->err = 6;
         ctl->errflag[(slot + 1) & 1] = 1;
         ctl->final_buf = out_buf;
     }

@@ -24,7 +24,10 @@ enum : int { RS_HLL = 0, RS_HLLC = 1, RS_SPLITTING = 2 };
 enum : int { BC_NULLGRADIENT = 0, BC_PERIODIC = 1, BC_REFLEXIVE = 2 };
 enum : int { GEOM_CARTESIAN = 0, GEOM_SPHERICAL = 1 };
 enum : int { GRAV_UNIFORM = 0, GRAV_POINT_MASS = 1, GRAV_INTERNAL_MASS = 2 };
-enum : int { EOS_PERFECT_GAS = 0, EOS_RAD_GAS = 1 };
+// EOS_PERFECT_GAS_FAST: the perfect gas in the fast-FP64 kernels (P = (gamma-1) e
+// without the temperature round trip, one reciprocal per state); a compile-time
+// kind of the fused kernels only, never a configured EOS.
+enum : int { EOS_PERFECT_GAS = 0, EOS_RAD_GAS = 1, EOS_PERFECT_GAS_FAST = 2 };
 
 // Everything a kernel needs to know about the grid and the physics plugins.
 // Passed by value (it lives in the kernel parameter space).

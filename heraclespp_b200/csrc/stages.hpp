@@ -81,6 +81,11 @@ void step_exact(const GridDev& g, const StateDev& in, const StateDev& out, StepC
                 int slot, int out_buf, cudaStream_t s);
 void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                 int slot, int out_buf, int shape, cudaStream_t s);
+// fast FP64 (HCL_FP64_FAST): the FP64 tile kernels with the fast perfect-gas
+// forms, built with FMA contraction
+void step_fast64(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
+                 int slot, int out_buf, cudaStream_t s);
+void configure_fast64();
 int mixed_shape_count(int ndim);
 bool mixed_shape_valid(const GridDev& g, int shape);
 // Dynamic shared memory of the fused tile kernels for g (g.nfx passive
@@ -104,8 +109,11 @@ bool strip3d_eligible(const GridDev& g);
 bool strip3d_fx_eligible(const GridDev& g);
 void step_strip3d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                   int slot, int out_buf, int L, cudaStream_t s);
+// sync: 16-warp CTAs marching in step; tma: their rows staged by the Tensor
+// Memory Accelerator where strip2d_tma_eligible (per-lane cp.async otherwise)
 void step_strip2d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
-                  int slot, int out_buf, int L, bool sync, cudaStream_t s);
+                  int slot, int out_buf, int L, bool sync, bool tma, cudaStream_t s);
+bool strip2d_tma_eligible(const GridDev& g);
 void configure_exact();
 void configure_mixed();
 int conservation_partials_doubles(int ndim);

@@ -1,0 +1,104 @@
+// tma_ring.cuh -- TMA row staging for the warp-strip kernels (sm_100a).
+//
+// A warp's row ring (8 slots of one x-row segment: 4 variables x 32 doubles,
+// 1 KB) is filled by the Tensor Memory Accelerator: one elected lane issues a
+// single 3-D cp.async.bulk.tensor per row (box {32 doubles, 1 row, 4
+// variables} of the FP64 state, whose planes are the tensor's third
+// dimension), and completion is tracked by one mbarrier per slot (expect-tx
+// of the box's bytes).  The lanes wait on the slot's mbarrier phase before
+// reading it.  The tensor map covers this GPU's own state buffer only and the
+// copies carry no cluster multicast.
+//
+// Every wait is bounded: after kTmaWaitPolls failed polls it gives up and
+// reports false, and the kernel records HCL_ERR_TIMEOUT instead of hanging.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace hcl::fused {
+
+// x-row segment of one ring slot: 32 lanes x 4 variables of FP64
+constexpr unsigned kTmaRowBytes = 4u * 32u * 8u;
+// polls of one mbarrier wait before it gives up (each try_wait also
+// suspends the thread for a hardware-defined time)
+constexpr int kTmaWaitPolls = 1 << 22;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// makes initialised mbarriers visible to the async (TMA) proxy
+__device__ __forceinline__ void mbar_init_fence()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+// orders this thread's earlier generic-proxy accesses of shared memory
+// before later async-proxy ones (a slot read by the lanes, then refilled)
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// One box of a 3-D tiled tensor map into shared memory; completes `bar`'s
+// transaction count.  x * 8 bytes must be a multiple of 16 (x even for FP64).
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+        "[%2];\n" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch_map(const CUtensorMap* map)
+{
+    asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n"
+        " .reg .pred p;\n"
+        " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+
+// Waits for the phase of `bar` with the given parity to complete; false when
+// kTmaWaitPolls polls were not enough.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity)
+{
+    if (mbar_try_wait(bar, parity)) {
+        return true;
+    }
+    for (int i = 1; i < kTmaWaitPolls; ++i) {
+        if (mbar_try_wait(bar, parity)) {
+            return true;
+        }
+    }
+    return false;
+}
+
+} // namespace hcl::fused

@@ -6,7 +6,7 @@
 // Options (the reference fixes these at CMake time, CMakeLists.txt:11-79):
 //   --ndim=1|2|3  --geometry=Cartesian|Spherical  --gravity=Uniform|Point_mass|Internal_mass
 //   --eos=PerfectGas|RadGas
-//   --setup=<name>  --precision=fp64|fp32_mixed  --device=N  --output=<file>
+//   --setup=<name>  --precision=fp64|fp32_mixed|fp64_fast  --device=N  --output=<file>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -56,7 +56,7 @@ int main(int argc, char** argv)
     opt.gravity = grav == "Point_mass"      ? HCL_GRAVITY_POINT_MASS
                   : grav == "Internal_mass" ? HCL_GRAVITY_INTERNAL_MASS
                                             : HCL_GRAVITY_UNIFORM;
-    opt.precision = prec == "fp32_mixed" ? HCL_FP32_MIXED : HCL_FP64;
+    opt.precision = prec == "fp32_mixed" ? HCL_FP32_MIXED : (prec == "fp64_fast" ? HCL_FP64_FAST : HCL_FP64);
     opt.eos = opt_value(argc, argv, "--eos", "PerfectGas") == "RadGas" ? HCL_EOS_RAD_GAS : HCL_EOS_PERFECT_GAS;
     opt.device = std::atoi(opt_value(argc, argv, "--device", "0").c_str());
     opt.setup = setup.c_str();

@@ -6,9 +6,11 @@ run the kernels on the benchmark's own grids and work distribution:
 
 * Kelvin-Helmholtz 2048^2 (periodic, van Leer, HLLC, CFL 0.4): the plain FP64
   fused step for 10 steps bit for bit against the oracle (every field, ghost
-  cells included, and the CFL dt sequence); the FP32-mixed step on schedule 9
+  cells included, and the CFL dt sequence); fast FP64 for 10 steps within
+  1e-12 relative L1 per field; the FP32-mixed step on schedule 9
   (one 16-warp CTA per SM, 2368 strips of 64 rows) for 20 steps with the
-  oracle's dts, relative L1 and L-infinity per field.
+  oracle's dts, relative L1 and L-infinity per field; its rows staged by TMA
+  (schedule 9) or by per-lane cp.async (schedule 10) give the same bits.
 * Rayleigh-Taylor 256x256x512 (reflecting z walls, g_z = -0.1, Minmod, HLL):
   the FP64 fused step (8x8x4 tiles) for 3 steps bit for bit, the FP32-mixed
   column march (440 CTAs x 256 planes) for 3 steps with the oracle's dts.
@@ -78,6 +80,21 @@ def test_kh2048_fp64_fused_bitwise(kh):
         assert np.array_equal(got[name], ref), name
 
 
+def test_kh2048_fast64_within_1e12(kh):
+    """Fast FP64 on the benchmark grid: 10 steps with the oracle's dts, every
+    field within 1e-12 relative L1 (ghost cells included)."""
+    from heraclespp_b200 import Domain
+
+    prim, (rho, rhou, E), _, dts = kh
+    d = Domain(2, KH_NX, precision="fp64_fast", **KH_KW)
+    d.set_state_from_prim(*prim)
+    d.run(nsteps=10, dts=dts[:10])
+    got = fields(*d.get_state())
+    d.close()
+    for name, ref in fields(rho, rhou, E).items():
+        assert rel_l1(got[name], ref) < 1e-12, name
+
+
 def test_kh2048_mixed_schedule9_every_field(kh):
     from heraclespp_b200 import Domain
 
@@ -96,6 +113,16 @@ def test_kh2048_mixed_schedule9_every_field(kh):
         l1 = rel_l1(got[name], ref[name])
         assert l1 < l1_bound[name], (name, l1)
         assert rel_linf(got[name], ref[name]) < 1e-3, name
+    # schedule 10 stages the same rows by per-lane cp.async instead of TMA:
+    # the same bits
+    d = Domain(2, KH_NX, precision="fp32_mixed", **KH_KW)
+    assert d.set_schedule(10) == 10
+    d.set_state_from_prim(*prim)
+    d.run(nsteps=20, dts=dts)
+    got10 = fields(*d.get_state())
+    d.close()
+    for name in ref:
+        assert np.array_equal(got10[name], got[name]), name
 
 
 @pytest.fixture(scope="module")

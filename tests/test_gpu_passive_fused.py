@@ -124,8 +124,9 @@ def test_fused_passive_scalars_mixed_close_to_fp64(ndim, nx, nfx, bc, extra, ste
         allowed = (0, 1) if (ndim == 3 and nfx == 1) else (0,)
     assert d.schedule() in allowed
     if ndim == 2:
-        with pytest.raises(hb.HclError):
-            d.set_schedule(9)
+        for sched in (9, 10):
+            with pytest.raises(hb.HclError):
+                d.set_schedule(sched)
     o.run(rho, rhou, E, fx, dts=d.dt_log(), max_iter=steps)
     fx_d = np.zeros_like(fx)
     r_d, m_d, E_d = d.get_state(fx=fx_d)

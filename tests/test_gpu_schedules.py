@@ -16,7 +16,7 @@ CASES_2D = {
 }
 
 
-@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9])
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
 @pytest.mark.parametrize("name", list(CASES_2D))
 def test_mixed_schedule_matches_oracle(name, schedule):
     o, d, (rho0, u0, P0) = make_pair(name, "fp32_mixed")
@@ -37,20 +37,22 @@ def test_mixed_schedule_matches_oracle(name, schedule):
 
 @pytest.mark.parametrize("name", list(CASES_2D))
 def test_in_step_strips_equal_independent_strips_bitwise(name):
-    """Schedule 9 (16-warp CTAs marching in step, idle warps keeping the
-    barrier sequence) runs the same per-cell arithmetic as schedule 6: equal
-    states and dt sequences bit for bit."""
+    """Schedules 9 and 10 (16-warp CTAs marching in step, idle warps keeping
+    the barrier sequence; rows staged by TMA in 9, by per-lane cp.async in 10)
+    run the same per-cell arithmetic as schedule 6: equal states and dt
+    sequences bit for bit."""
     out = []
-    for schedule in (6, 9):
+    for schedule in (6, 9, 10):
         _, d, (rho0, u0, P0) = make_pair(name, "fp32_mixed")
         assert d.set_schedule(schedule) == schedule
         d.set_state_from_prim(rho0, u0, P0)
         r = d.run(cfl=0.4, nsteps=25)
         out.append((r.t, d.get_state()))
-    (t6, s6), (t9, s9) = out
-    assert t6 == t9
-    for a, b in zip(s6, s9):
-        assert np.array_equal(a, b)
+    (t6, s6) = out[0]
+    for t, st in out[1:]:
+        assert t == t6
+        for a, b in zip(s6, st):
+            assert np.array_equal(a, b)
 
 
 def test_strip_with_gravity_and_reflexive_walls():
@@ -70,7 +72,7 @@ def test_strip_with_gravity_and_reflexive_walls():
     u0[1][s3] = np.broadcast_to(0.01 * np.cos(4 * np.pi * X) * np.exp(-((Y - 0.5) / 0.1) ** 2), rho0[s3].shape)
     rho, rhou, E, fx = o.init_from_prim(rho0, u0, P0)
     _, _, _, dts = o.run(rho, rhou, E, fx, cfl=0.4, max_iter=40, record_dts=True)
-    for schedule in (0, 4, 7, 9):
+    for schedule in (0, 4, 7, 9, 10):
         d = Domain(2, [40, 70], precision="fp32_mixed", **kw)
         d.set_schedule(schedule)
         d.set_state_from_prim(rho0, u0, P0)
