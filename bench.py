@@ -14,8 +14,9 @@ Metric: Mcell-updates/s = steps x interior cells / time (src/main.cpp:570-581).
 
 With --gpus N > 1 under torchrun each rank runs an independent replica of the
 single-domain step ("replicas only"); value is the sum over ranks, timing the
-max over ranks.  --impl reference times the CPU oracle (the reference's FP64
-algorithm restated in C, OpenMP on the host cores) on a bounded sample.
+max over ranks.  --impl reference times the reference's own FP64 array code
+(compiled from its sources against host Kokkos/MPI stand-ins, OpenMP on the
+host cores; the C oracle where that build is absent) on a bounded sample.
 """
 from __future__ import annotations
 
@@ -212,17 +213,31 @@ def measured_peaks():
 
 
 def cpu_baseline(budget_s, cells_full=CELLS):
-    """The CPU oracle (reference FP64 algorithm) on the full KH 2048^2 grid,
-    OpenMP over all host cores, for as many steps as fit in budget_s."""
+    """The reference's FP64 CPU path on the full KH 2048^2 grid, on all host
+    cores, for as many steps as fit in budget_s.  Kind "reference": the
+    reference's own array code (hydro/, mesh/, boundary*, analysis/ compiled
+    from its sources against the host Kokkos/MPI stand-ins, OpenMP loops;
+    oracle/_ref/libref_step_2d_cart.so) driven in the order of its time loop.
+    Kind "port" (when that library is absent): the oracle, the same algorithm
+    restated in C with OpenMP."""
     from heraclespp_b200 import setups
-    from oracle import Oracle
+    from oracle import Oracle, RefStep, ref_step_path
 
     ncores = os.cpu_count() or 1
-    Oracle.set_threads(ncores)
-    o = Oracle(2, [NX, NX], gamma=1.4, limiter="VanLeer", riemann="HLLC", bc=["Periodic"] * 4)
-    grid = setups.Grid.from_domain(o)
-    rho, u, P = setups.kelvin_helmholtz(grid)
-    rho, rhou, E, fx = o.init_from_prim(rho, u, P)
+    kw = dict(gamma=1.4, limiter="VanLeer", riemann="HLLC", bc=["Periodic"] * 4)
+    if ref_step_path(2).exists():
+        RefStep.set_threads(2, "Cartesian", ncores)
+        o = RefStep(2, [NX, NX], **kw)
+        kind, what = "reference", "the reference's own array code on the host Kokkos/MPI stand-ins"
+        threads = o.threads()
+    else:
+        Oracle.set_threads(ncores)
+        o = Oracle(2, [NX, NX], **kw)
+        kind, what = "port", "the FP64 oracle (C restatement)"
+        threads = Oracle.get_threads()
+    init = Oracle(2, [NX, NX], **kw)
+    grid = setups.Grid.from_domain(init)
+    rho, rhou, E, fx = init.init_from_prim(*setups.kelvin_helmholtz(grid))
     t0 = time.perf_counter()
     o.run(rho, rhou, E, fx, cfl=0.4, max_iter=1)
     one = time.perf_counter() - t0
@@ -230,9 +245,8 @@ def cpu_baseline(budget_s, cells_full=CELLS):
     t0 = time.perf_counter()
     o.run(rho, rhou, E, fx, cfl=0.4, max_iter=n)
     el = time.perf_counter() - t0
-    return {"value": n * cells_full / el * 1e-6, "unit": "Mcell-updates/s", "cores": Oracle.get_threads(),
-            "kind": "port",
-            "sample": f"{n} full steps of KH 2048^2 (FP64 oracle, {Oracle.get_threads()} OpenMP threads), {el:.1f} s"}
+    return {"value": n * cells_full / el * 1e-6, "unit": "Mcell-updates/s", "cores": threads, "kind": kind,
+            "sample": f"{n} full steps of KH 2048^2 with {what}, {threads} OpenMP threads, {el:.1f} s"}
 
 
 def adjoint_cost(torch, nsteps=400, n=512, k=32):

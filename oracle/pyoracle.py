@@ -487,3 +487,187 @@ class RefCell:
 
     def slope(self, limiter, diffR, diffL):
         return self.lib.ref_slope(_id(LIMITERS, limiter), float(diffR), float(diffL))
+
+
+# ---- the reference's own array code (oracle/_ref/libref_step_*.so) ----------------
+
+class _RsConfig(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int * 3),
+        ("ng", C.c_int),
+        ("nfx", C.c_int),
+        ("xmin", C.c_double * 3),
+        ("xmax", C.c_double * 3),
+        ("gamma", C.c_double),
+        ("mmw", C.c_double),
+        ("limiter", C.c_char_p),
+        ("riemann", C.c_char_p),
+        ("bc", C.c_char_p * 6),
+        ("bc_priority", C.c_char_p),
+        ("gravity", C.c_int),
+        ("g", C.c_double * 3),
+        ("central_mass", C.c_double),
+    ]
+
+
+def ref_step_path(ndim: int, geom: str = "Cartesian") -> Path:
+    tag = "sph" if geom == "Spherical" else "cart"
+    return HERE / "_ref" / f"libref_step_{int(ndim)}d_{tag}.so"
+
+
+_RS_LIBS: dict = {}
+
+
+def _rs_lib(ndim, geom):
+    key = (int(ndim), geom)
+    if key in _RS_LIBS:
+        return _RS_LIBS[key]
+    path = ref_step_path(ndim, geom)
+    if not path.exists():
+        raise FileNotFoundError(f"{path} not built (make -C oracle ref-step where the reference sources are)")
+    L = C.CDLL(str(path))
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    L.rs_create.argtypes = [C.POINTER(_RsConfig)]
+    L.rs_create.restype = vp
+    L.rs_destroy.argtypes = [vp]
+    L.rs_set_threads.argtypes = [i]
+    L.rs_get_threads.restype = i
+    L.rs_grid.argtypes = [vp, vp, vp, vp, vp]
+    L.rs_conv_prim_to_cons.argtypes = [vp, i, vp, vp, vp, vp, vp]
+    L.rs_conv_cons_to_prim.argtypes = [vp, i, vp, vp, vp, vp, vp]
+    L.rs_hydro_reconstruction.argtypes = [vp, i, d] + [vp] * 8
+    L.rs_godunov.argtypes = [vp, i, d] + [vp] * 12
+    L.rs_boundaries.argtypes = [vp, vp, vp, vp, vp]
+    L.rs_time_step.argtypes = [vp, i, vp, vp, vp]
+    L.rs_time_step.restype = d
+    L.rs_min_internal_energy.argtypes = [vp, vp, vp, vp]
+    L.rs_min_internal_energy.restype = d
+    L.rs_run.argtypes = [vp, vp, vp, vp, vp, d, d, i, vp, C.POINTER(i), vp]
+    L.rs_run.restype = i
+    _RS_LIBS[key] = L
+    return L
+
+
+class RefStep:
+    """The reference's own classes for one domain (MUSCLHancockHydroReconstruction,
+    the Godunov scheme of its factory, DistributedBoundaryCondition on one rank,
+    time_step, the conversions), run on the host through the Kokkos/MPI
+    stand-ins of oracle/ref_array.  Same keyword arguments and array shapes as
+    Oracle (uniform and point-mass gravity, perfect gas)."""
+
+    def __init__(self, ndim, nx, *, ng=2, nfx=0, geom="Cartesian", gamma=1.4, mmw=1.0, limiter="VanLeer",
+                 riemann="HLLC", bc=("Periodic",) * 6, gravity="Uniform", g=(0.0, 0.0, 0.0), central_mass=1.0,
+                 xmin=(0.0, 0.0, 0.0), xmax=(1.0, 1.0, 1.0), bc_priority=""):
+        if gravity not in ("Uniform", "Point_mass"):
+            raise ValueError("RefStep wraps the uniform and point-mass gravities")
+        self.lib = _rs_lib(ndim, geom)
+        cfg = _RsConfig()
+        nx3 = (list(nx) + [1, 1, 1])[:3]
+        for d in range(3):
+            cfg.nx[d] = int(nx3[d])
+            cfg.xmin[d] = float(xmin[d])
+            cfg.xmax[d] = float(xmax[d])
+            cfg.g[d] = float(g[d])
+        cfg.ng, cfg.nfx, cfg.gamma, cfg.mmw = int(ng), int(nfx), float(gamma), float(mmw)
+        self._keep = [s.encode() for s in [limiter, riemann, bc_priority] + (list(bc) + ["Periodic"] * 6)[:6]]
+        cfg.limiter, cfg.riemann, cfg.bc_priority = self._keep[0], self._keep[1], self._keep[2]
+        for f in range(6):
+            cfg.bc[f] = self._keep[3 + f]
+        cfg.gravity = 1 if gravity == "Point_mass" else 0
+        cfg.central_mass = float(central_mass)
+        self.h = self.lib.rs_create(C.byref(cfg))
+        if not self.h:
+            raise ValueError("the reference rejected this configuration (see stderr)")
+        self.ndim, self.nfx = int(ndim), int(nfx)
+        self.n = tuple(int(v) + (2 * ng if k < ndim else 0) for k, v in enumerate(nx3))
+        self.ncells = self.n[0] * self.n[1] * self.n[2]
+
+    def __del__(self):
+        try:
+            self.lib.rs_destroy(self.h)
+        except Exception:
+            pass
+
+    @property
+    def shape3(self):
+        return (self.n[2], self.n[1], self.n[0])
+
+    def zeros(self, ncomp=None):
+        return np.zeros(self.shape3) if ncomp is None else np.zeros((ncomp,) + self.shape3)
+
+    @staticmethod
+    def set_threads(ndim, geom, n):
+        _rs_lib(ndim, geom).rs_set_threads(int(n))
+
+    def threads(self):
+        return int(self.lib.rs_get_threads())
+
+    def grid(self):
+        dx = np.zeros(sum(self.n))
+        xc = np.zeros(sum(self.n))
+        ds = np.zeros((3,) + self.shape3)
+        dv = np.zeros(self.shape3)
+        self.lib.rs_grid(self.h, _p(dx), _p(xc), _p(ds), _p(dv))
+        out = {"ds": ds, "dv": dv}
+        off = 0
+        for d in range(3):
+            out[f"dx{d}"] = dx[off:off + self.n[d]]
+            out[f"x{d}c"] = xc[off:off + self.n[d]]
+            off += self.n[d]
+        return out
+
+    def conv_prim_to_cons(self, ng_eff, rho, u, P):
+        rhou, E = self.zeros(self.ndim), self.zeros()
+        self.lib.rs_conv_prim_to_cons(self.h, ng_eff, _p(rho), _p(u), _p(P), _p(rhou), _p(E))
+        return rhou, E
+
+    def conv_cons_to_prim(self, ng_eff, rho, rhou, E):
+        u, P = self.zeros(self.ndim), self.zeros()
+        self.lib.rs_conv_cons_to_prim(self.h, ng_eff, _p(rho), _p(rhou), _p(E), _p(u), _p(P))
+        return u, P
+
+    def hydro_reconstruction(self, ng_eff, dt, rho, u, P, fx=None):
+        nd, nfx = self.ndim, self.nfx
+        rho_rec = np.zeros((nd, 2) + self.shape3)
+        rhou_rec = np.zeros((nd, nd, 2) + self.shape3)
+        E_rec = np.zeros((nd, 2) + self.shape3)
+        fx_rec = np.zeros((max(nfx, 1), nd, 2) + self.shape3)
+        if fx is None:
+            fx = self.zeros(max(nfx, 1))
+        self.lib.rs_hydro_reconstruction(self.h, ng_eff, dt, _p(rho), _p(u), _p(P), _p(fx), _p(rho_rec), _p(rhou_rec),
+                                         _p(E_rec), _p(fx_rec))
+        return rho_rec, rhou_rec, E_rec, fx_rec
+
+    def godunov(self, ng_eff, dt, rho, rhou, E, rho_rec, rhou_rec, E_rec, fx=None, fx_rec=None):
+        nfx = max(self.nfx, 1)
+        if fx is None:
+            fx = self.zeros(nfx)
+        if fx_rec is None:
+            fx_rec = np.zeros((nfx, self.ndim, 2) + self.shape3)
+        rho_new, rhou_new, E_new, fx_new = self.zeros(), self.zeros(self.ndim), self.zeros(), self.zeros(nfx)
+        self.lib.rs_godunov(self.h, ng_eff, dt, _p(rho), _p(rhou), _p(E), _p(fx), _p(rho_rec), _p(rhou_rec),
+                            _p(E_rec), _p(fx_rec), _p(rho_new), _p(rhou_new), _p(E_new), _p(fx_new))
+        return rho_new, rhou_new, E_new, fx_new
+
+    def boundaries(self, rho, rhou, E, fx=None):
+        if fx is None:
+            fx = self.zeros(max(self.nfx, 1))
+        self.lib.rs_boundaries(self.h, _p(rho), _p(rhou), _p(E), _p(fx))
+
+    def time_step(self, ng_eff, rho, u, P):
+        return self.lib.rs_time_step(self.h, ng_eff, _p(rho), _p(u), _p(P))
+
+    def min_internal_energy(self, rho, rhou, E):
+        return self.lib.rs_min_internal_energy(self.h, _p(rho), _p(rhou), _p(E))
+
+    def run(self, rho, rhou, E, fx=None, *, cfl=0.4, t_end=1e30, max_iter=10000, record_dts=False):
+        """The reference's time loop (main.cpp:354-531 without outputs), in
+        place.  Returns (t, iter, status, dts)."""
+        if fx is None:
+            fx = self.zeros(max(self.nfx, 1))
+        t = C.c_double(0.0)
+        it = C.c_int(0)
+        rec = np.zeros(max_iter) if record_dts else None
+        st = self.lib.rs_run(self.h, _p(rho), _p(rhou), _p(E), _p(fx), float(cfl), float(t_end), int(max_iter),
+                             C.byref(t), C.byref(it), _p(rec))
+        return t.value, it.value, st, (rec[: it.value] if record_dts else None)
