@@ -289,6 +289,35 @@ class Domain:
         check(lib().hcl_adjoint_backward(self.h, _ptr(lam_final), _ptr(grad), 1 if device else 0))
         return grad
 
+    def get_prim(self, with_temperature=True, fx=None):
+        """(rho, u, P, T) over all cells (reference layout), as main() holds
+        them when it writes an output; fx (nfx, ...) is filled when given."""
+        rho = self.zeros()
+        u = self.zeros(self.ndim)
+        P = self.zeros()
+        T = self.zeros() if with_temperature else None
+        check(lib().hcl_get_prim(self.h, _ptr(rho), _ptr(u), _ptr(P), _ptr(T), _ptr(fx), 0))
+        return rho, u, P, T
+
+    def set_clock(self, t, iteration):
+        check(lib().hcl_set_clock(self.h, float(t), int(iteration)))
+
+    def write_output(self, directory, prefix, output_id, *, iter_output_id=-1, time_output_id=-1, iteration=0,
+                     t=0.0):
+        """One output with the reference's dataset set (hcl_write_output):
+        <directory>/<prefix>_<output_id:08d>.hclraw and <prefix>.xmf."""
+        check(lib().hcl_write_output(self.h, str(directory).encode(), str(prefix).encode(), int(output_id),
+                                     int(iter_output_id), int(time_output_id), int(iteration), float(t)))
+
+    def read_restart(self, path):
+        """Restart from an output file of the same grid (hcl_read_restart):
+        sets the state and the clock; returns the file's counters."""
+        out = [C.c_int(-1) for _ in range(4)]
+        t = C.c_double(0.0)
+        check(lib().hcl_read_restart(self.h, str(path).encode(), *[C.byref(o) for o in out], C.byref(t)))
+        return {"output_id": out[0].value, "iter_output_id": out[1].value, "time_output_id": out[2].value,
+                "iter": out[3].value, "current_time": t.value}
+
     def set_schedule(self, schedule):
         """Forces a schedule of the mixed kernel (-1: autotune); returns the one in use."""
         used = C.c_int()

@@ -38,7 +38,8 @@ EXPORTS = [
     "hcl_adjoint_forward", "hcl_adjoint_backward", "hcl_adjoint_dts", "hcl_set_schedule",
     "hcl_ensemble_create", "hcl_ensemble_destroy", "hcl_ensemble_handle", "hcl_ensemble_stream",
     "hcl_ensemble_run", "hcl_ensemble_adjoint", "hcl_pressure_fix", "hcl_internal_mass_gravity",
-    "hcl_set_stage_loop",
+    "hcl_set_stage_loop", "hcl_temperature", "hcl_get_prim", "hcl_set_clock", "hcl_get_config",
+    "hcl_write_output", "hcl_read_restart",
 ]
 
 
@@ -194,6 +195,13 @@ def lib():
     L.hcl_adjoint_dts.argtypes = [H, vp, i, C.POINTER(i)]
     L.hcl_set_schedule.argtypes = [H, i, C.POINTER(i)]
     L.hcl_set_stage_loop.argtypes = [H, i]
+    L.hcl_temperature.argtypes = [H, i, vp, vp, vp, vp]
+    L.hcl_get_prim.argtypes = [H, vp, vp, vp, vp, vp, i]
+    L.hcl_set_clock.argtypes = [H, d, i]
+    L.hcl_get_config.argtypes = [H, C.POINTER(Config)]
+    L.hcl_write_output.argtypes = [H, C.c_char_p, C.c_char_p, i, i, i, i, d]
+    L.hcl_read_restart.argtypes = [H, C.c_char_p, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i),
+                                   C.POINTER(d)]
     L.hcl_ensemble_create.argtypes = [C.POINTER(Config), i, C.POINTER(vp)]
     L.hcl_ensemble_destroy.argtypes = [vp]
     L.hcl_ensemble_handle.argtypes = [vp, i, C.POINTER(H)]

@@ -149,6 +149,8 @@ struct hcl_handle {
     // reference-layout state of the stage-composed loop (passive scalars or
     // pressure fix): one allocation, carved by stage_buffers()
     double* sl_mem = nullptr;
+    // output scratch of hcl_get_prim: rho, rhou, E, u, P, T in the reference layout
+    double* io_mem = nullptr;
     double *sl_rho = nullptr, *sl_rhou = nullptr, *sl_E = nullptr, *sl_fx = nullptr, *sl_u = nullptr, *sl_P = nullptr;
     double *sl_rho_rec = nullptr, *sl_rhou_rec = nullptr, *sl_E_rec = nullptr, *sl_fx_rec = nullptr;
     double *sl_rho_new = nullptr, *sl_rhou_new = nullptr, *sl_E_new = nullptr, *sl_fx_new = nullptr;
@@ -177,6 +179,7 @@ void free_handle(hcl_handle* h)
     for (auto& kv : h->graphs) {
         cudaGraphExecDestroy(kv.second);
     }
+    cudaFree(h->io_mem);
     for (int d = 0; d < 3; ++d) {
         cudaFree(h->dx_nodes[d]);
         cudaFree(h->ddx[d]);
@@ -795,6 +798,18 @@ int hcl_destroy(hcl_handle* h)
     return HCL_OK;
 }
 
+int hcl_get_config(const hcl_handle* h, hcl_config* out)
+{
+    if (!h || !out) {
+        return fail(HCL_ERR_ARGUMENT, "null handle or output");
+    }
+    *out = h->cfg;
+    for (int d = 0; d < 3; ++d) {
+        out->nodes[d] = nullptr;
+    }
+    return HCL_OK;
+}
+
 int hcl_get_extents(const hcl_handle* h, int n_wg[3], int64_t* ncells)
 {
     if (!h) {
@@ -909,6 +924,18 @@ int hcl_conv_cons_to_prim(hcl_handle* h, int ng_eff, const double* rho, const do
         return fail(HCL_ERR_ARGUMENT, "null array");
     }
     hcl::stage::conv_cons_to_prim(h->g, ng_eff, rho, rhou, E, u, P, pick(h, stream));
+    HCL_LAUNCH_CHECK();
+    return HCL_OK;
+}
+
+int hcl_temperature(hcl_handle* h, int ng_eff, const double* rho, const double* P, double* T, void* stream)
+{
+    HCL_CHECK_HANDLE(h);
+    HCL_CHECK_NGEFF(h, ng_eff);
+    if (!rho || !P || !T) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    hcl::stage::temperature(h->g, ng_eff, rho, P, T, pick(h, stream));
     HCL_LAUNCH_CHECK();
     return HCL_OK;
 }
@@ -1179,6 +1206,73 @@ int hcl_get_state(hcl_handle* h, double* rho, double* rhou, double* E, double* f
     HCL_CUDA(cudaGetLastError());
     HCL_CUDA(cudaStreamSynchronize(h->stream));
     return HCL_OK;
+}
+
+int hcl_get_prim(hcl_handle* h, double* rho, double* u, double* P, double* T, double* fx, int memory)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!rho || !u || !P) {
+        return fail(HCL_ERR_ARGUMENT, "null array");
+    }
+    if (!h->state_valid) {
+        return fail(HCL_ERR_CONFIG, "no state set");
+    }
+    const size_t N = (size_t)h->g.N, nd = (size_t)h->g.ndim;
+    int rc;
+    if (!h->io_mem && (rc = dalloc(&h->io_mem, N * (4 + 2 * nd)))) {
+        return rc;
+    }
+    double* d_rho = h->io_mem;
+    double* d_rhou = d_rho + N;
+    double* d_E = d_rhou + N * nd;
+    double* d_u = d_E + N;
+    double* d_P = d_u + N * nd;
+    double* d_T = d_P + N;
+    if ((rc = hcl_get_state(h, d_rho, d_rhou, d_E, nullptr, HCL_DEVICE))) {
+        return rc;
+    }
+    cudaStream_t s = h->stream;
+    // main.cpp:526 and :317-318: cons -> prim and the temperature over all ghosts
+    hcl::stage::conv_cons_to_prim(h->g, h->g.ng, d_rho, d_rhou, d_E, d_u, d_P, s);
+    hcl::stage::temperature(h->g, h->g.ng, d_rho, d_P, d_T, s);
+    HCL_LAUNCH_CHECK();
+    const cudaMemcpyKind kind = memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    HCL_CUDA(cudaMemcpyAsync(rho, d_rho, sizeof(double) * N, kind, s));
+    HCL_CUDA(cudaMemcpyAsync(u, d_u, sizeof(double) * N * nd, kind, s));
+    HCL_CUDA(cudaMemcpyAsync(P, d_P, sizeof(double) * N, kind, s));
+    if (T) {
+        HCL_CUDA(cudaMemcpyAsync(T, d_T, sizeof(double) * N, kind, s));
+    }
+    if (fx && h->g.nfx > 0) {
+        if (stage_mode(h)) {
+            HCL_CUDA(cudaMemcpyAsync(fx, h->sl_fx, sizeof(double) * N * h->g.nfx, kind, s));
+        } else {
+            hcl::fused::unpack_fx(h->g, h->st[h->cur], fx, kind, s);
+            HCL_CUDA(cudaGetLastError());
+        }
+    }
+    HCL_CUDA(cudaStreamSynchronize(s));
+    return HCL_OK;
+}
+
+int hcl_set_clock(hcl_handle* h, double t, int iter)
+{
+    HCL_CHECK_HANDLE(h);
+    if (!h->state_valid) {
+        return fail(HCL_ERR_CONFIG, "no state set");
+    }
+    if (iter < 0) {
+        return fail(HCL_ERR_ARGUMENT, "negative iteration count");
+    }
+    if (stage_mode(h)) {
+        h->sl_t = t;
+        h->sl_iter = iter;
+        h->sl_toid = h->sl_ioid = -1;
+        h->sl_status = 0;
+        h->sl_dts.clear();
+        return HCL_OK;
+    }
+    return restart_clock(h, t, iter);
 }
 
 int hcl_set_state_from_prim(hcl_handle* h, const double* rho, const double* u, const double* P, const double* fx)

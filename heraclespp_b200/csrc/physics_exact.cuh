@@ -111,6 +111,15 @@ __device__ __forceinline__ double temp_from_evol(const Eos& e, double rho, doubl
 {
     return evol * e.mmw * kMp * e.gamma_m1 / (rho * kKb);
 }
+// compute_temp_from_pres of the configured EOS (perfect_gas.hpp:64-68,
+// rad_gas.hpp:71-89)
+__device__ __forceinline__ double temperature(const Eos& e, double rho, double P)
+{
+    if (e.kind == EOS_RAD_GAS) {
+        return rad::temp_from_pres(e, rho, P);
+    }
+    return temp_from_pres(e, rho, P);
+}
 __device__ __forceinline__ double evol_from_pres(const Eos& e, double rho, double P)
 {
     if (e.kind == EOS_PERFECT_GAS_FAST) {

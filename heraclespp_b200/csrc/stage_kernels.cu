@@ -121,6 +121,20 @@ __global__ void k_cons_to_prim(GridDev g, Box bx, const double* __restrict__ rho
     }
 }
 
+// analysis/temperature.hpp:18-25 "fill_temperature_array"
+__global__ void k_temperature(GridDev g, Box bx, const double* __restrict__ rho, const double* __restrict__ P,
+                              double* __restrict__ T)
+{
+    const exact::Eos eos = exact::eos_of(g);
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < bx.count;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int i, j, k;
+        box_ijk(bx, idx, i, j, k);
+        const int64_t c = lidx(g, i, j, k);
+        T[c] = exact::temperature(eos, rho[c], P[c]);
+    }
+}
+
 // limited_linear_reconstruction.hpp:46-64 "face_reconstruction":
 // var_rec(c, s, idim) = rec[c + N*s + 2N*idim]
 template <int ND>
@@ -865,6 +879,13 @@ void conv_cons_to_prim(const GridDev& g, int ng_eff, const double* rho, const do
     dispatch_nd(g.ndim, [&](auto nd) {
         k_cons_to_prim<decltype(nd)::value><<<grid_for(bx.count), kThreads, 0, s>>>(g, bx, rho, rhou, E, u, P);
     });
+    ++g_launches;
+}
+
+void temperature(const GridDev& g, int ng_eff, const double* rho, const double* P, double* T, cudaStream_t s)
+{
+    const Box bx = make_box(g, ng_eff);
+    k_temperature<<<grid_for(bx.count), kThreads, 0, s>>>(g, bx, rho, P, T);
     ++g_launches;
 }
 

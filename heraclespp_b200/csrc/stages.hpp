@@ -21,6 +21,8 @@ void conv_prim_to_cons(const GridDev& g, int ng_eff, const double* rho, const do
                        double* rhou, double* E, cudaStream_t s);
 void conv_cons_to_prim(const GridDev& g, int ng_eff, const double* rho, const double* rhou, const double* E,
                        double* u, double* P, cudaStream_t s);
+// analysis/temperature.hpp:18-25 on the range with ng_eff ghost layers
+void temperature(const GridDev& g, int ng_eff, const double* rho, const double* P, double* T, cudaStream_t s);
 void face_reconstruction(const GridDev& g, int ng_eff, const double* var, double* var_rec, cudaStream_t s);
 void hydro_reconstruction(const GridDev& g, int ng_eff, double dt, const double* rho, const double* u,
                           const double* P, const double* fx, double* rho_rec, double* rhou_rec, double* E_rec,

@@ -7,6 +7,12 @@
 //   --ndim=1|2|3  --geometry=Cartesian|Spherical  --gravity=Uniform|Point_mass|Internal_mass
 //   --eos=PerfectGas|RadGas
 //   --setup=<name>  --precision=fp64|fp32_mixed|fp64_fast  --device=N  --output=<file>
+//   --output-dir=<dir> [--prefix=<name>]: outputs with the reference's dataset
+//     set at its cadence (main.cpp:312-346, :357-385, :533-561): one at the
+//     start when [Output] iter_frequency or time_frequency is set, then after
+//     every step that reaches an output iteration or time, at t_end and at
+//     max_iter (hcl_write_output: <dir>/<prefix>_<id>.hclraw and <prefix>.xmf).
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -52,6 +58,8 @@ int main(int argc, char** argv)
     const std::string prec = opt_value(argc, argv, "--precision", "fp64");
     const std::string setup = opt_value(argc, argv, "--setup", "shock_tube");
     const std::string output = opt_value(argc, argv, "--output", "");
+    const std::string outdir = opt_value(argc, argv, "--output-dir", "");
+    const std::string prefix = opt_value(argc, argv, "--prefix", "result");
     opt.geometry = geom == "Spherical" ? HCL_GEOM_SPHERICAL : HCL_GEOM_CARTESIAN;
     opt.gravity = grav == "Point_mass"      ? HCL_GRAVITY_POINT_MASS
                   : grav == "Internal_mass" ? HCL_GRAVITY_INTERNAL_MASS
@@ -77,7 +85,65 @@ int main(int argc, char** argv)
 
     const auto start = std::chrono::steady_clock::now();
     hcl_run_result res{};
-    rc = hcl_run(h, &run, &res);
+    if (outdir.empty()) {
+        rc = hcl_run(h, &run, &res);
+    } else {
+        // the time loop in chunks that end where main() writes an output
+        int output_id = -1, iter_output_id = -1, time_output_id = -1;
+        int iter = 0;
+        double t = 0.0;
+        const double t_end = run.t_end;
+        if (run.iter_frequency > 0 || run.time_frequency > 0) {
+            ++iter_output_id;
+            ++output_id;
+            if ((rc = hcl_write_output(h, outdir.c_str(), prefix.c_str(), output_id, iter_output_id, time_output_id,
+                                       iter, t))) {
+                return die("output", rc);
+            }
+        }
+        for (;;) {
+            hcl_run_params p = run;
+            p.iter_frequency = 0;
+            p.time_frequency = 0.0;
+            p.nsteps = 0;
+            int next_iter = -1;
+            double next_time = -1.0;
+            if (run.iter_frequency > 0) {
+                next_iter = (iter_output_id + 1) * run.iter_frequency;
+                p.nsteps = std::max(1, next_iter - iter);
+            }
+            if (run.time_frequency > 0) {
+                next_time = run.time_first_output + (time_output_id + 1) * run.time_frequency;
+                p.t_end = std::min(t_end, next_time);
+            }
+            rc = hcl_run(h, &p, &res);
+            if (rc) {
+                break;
+            }
+            iter = res.iter;
+            t = res.t;
+            bool out = false;
+            if (next_iter >= 0 && iter >= next_iter) {
+                ++iter_output_id;
+                out = true;
+            }
+            if (next_time >= 0 && t >= next_time) {
+                ++time_output_id;
+                out = true;
+            }
+            const bool done = t >= t_end || iter >= run.max_iter;
+            if (out || done) {
+                ++output_id;
+                if ((rc = hcl_write_output(h, outdir.c_str(), prefix.c_str(), output_id, iter_output_id,
+                                           time_output_id, iter, t))) {
+                    return die("output", rc);
+                }
+            }
+            if (done) {
+                break;
+            }
+        }
+    }
     const auto end = std::chrono::steady_clock::now();
     if (rc) {
         std::cerr << "Time = " << res.t << ", iteration = " << res.iter << ": " << hcl_last_error() << '\n';

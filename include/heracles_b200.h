@@ -126,6 +126,8 @@ int hcl_destroy(hcl_handle* h);
 const char* hcl_last_error(void);
 int hcl_abi_version(void);
 
+/* The configuration the handle was created with (node pointers not kept). */
+int hcl_get_config(const hcl_handle* h, hcl_config* out);
 /* Extents with ghosts (Nx_local_wg, grid.cpp:119) and cell count. */
 int hcl_get_extents(const hcl_handle* h, int n_wg[3], int64_t* ncells);
 /* Interior extents (Nx_glob_ng; 1 on inactive dims) and ghost width. */
@@ -147,6 +149,9 @@ int hcl_conv_prim_to_cons(hcl_handle* h, int ng_eff, const double* rho, const do
 /* conv_cons_to_prim (hydro/array_conversion.hpp:106-172) */
 int hcl_conv_cons_to_prim(hcl_handle* h, int ng_eff, const double* rho, const double* rhou, const double* E,
                           double* u, double* P, void* stream);
+/* temperature (analysis/temperature.hpp:18-25): T = compute_temp_from_pres(rho,
+ * P) of the configured EOS over the range with ng_eff ghost layers. */
+int hcl_temperature(hcl_handle* h, int ng_eff, const double* rho, const double* P, double* T, void* stream);
 /* IFaceReconstruction::execute (hydro/face_reconstruction.hpp:40-43,
  * limited_linear_reconstruction.hpp:46-64): var -> var_rec(.., 2, ndim) */
 int hcl_face_reconstruction(hcl_handle* h, int ng_eff, const double* var, double* var_rec, void* stream);
@@ -233,6 +238,15 @@ int hcl_get_state(hcl_handle* h, double* rho, double* rhou, double* E, double* f
  * full extent; ghost entries are ignored. */
 int hcl_set_state_from_prim(hcl_handle* h, const double* rho, const double* u, const double* P,
                             const double* fx);
+
+/* The primitive arrays main() holds when it writes an output (main.cpp:526 and
+ * :317-318): rho, u (ndim components), P and, when T is not NULL, the
+ * temperature, over all cells including ghosts (reference layout), plus the
+ * passive scalars when fx is not NULL.  Host or device destination. */
+int hcl_get_prim(hcl_handle* h, double* rho, double* u, double* P, double* T, double* fx, int memory);
+/* Sets the time and the iteration count of the loop without touching the state
+ * (a restart from an output: main.cpp:234-248 reads iter and current_time). */
+int hcl_set_clock(hcl_handle* h, double t, int iter);
 
 /* Parameters of the time loop (utils/param.cpp:40-50, main.cpp:354-385). */
 typedef struct hcl_run_params {
@@ -389,6 +403,31 @@ int hcl_ensemble_run(hcl_ensemble* e, const hcl_ensemble_params* p, hcl_ensemble
  * buffer layout as hcl_adjoint_backward).  The problems' sweeps run
  * concurrently on their own streams. */
 int hcl_ensemble_adjoint(hcl_ensemble* e, const double* const* lam_final, double* const* grads, int memory);
+
+/* ---- outputs and restarts (host only) --------------------------------------- */
+/* The reference writes one HDF5 file per output through PDI
+ * (io/io.cpp:185-318 write_pdi, dataset set io/config.yaml.cpp:7-265) and
+ * restarts from one (read_pdi, io/io.hpp:40-53).  No HDF5 library is used
+ * here: the same datasets -- output_id, iter_output_id, time_output_id, iter,
+ * current_time, gamma, x0..x2 (nodes with ghosts), x0_ng..x2_ng (interior
+ * nodes), rho, ux0..ux{ndim-1}, P, E, T, fx0..fx{nfx-1} (interior cells,
+ * C order [nx2][nx1][nx0]) -- go into one raw file "<prefix>_<output_id,
+ * 8 digits>.hclraw": the magic "HCLRAW01", the byte length of a text index,
+ * the index (one line per dataset: name, type f64|i32, byte offset, extents),
+ * then little-endian data at 64-byte aligned offsets.  An XDMF file
+ * "<prefix>.xmf" lists every output written so far as a time series whose
+ * attributes point into the raw files (Format="Binary", Seek = offset), like
+ * the reference's XmlWriter (io/io.hpp:56-81) does into its HDF5 files. */
+int hcl_write_output(hcl_handle* h, const char* directory, const char* prefix, int output_id, int iter_output_id,
+                     int time_output_id, int iter, double t);
+/* Restart (main.cpp:225-246): reads rho, u, P, fx and the clock from an output
+ * file into a handle of the same grid (the file's nodes must equal the
+ * handle's, else HCL_ERR_CONFIG), sets the state from the primitives
+ * (conv_prim_to_cons + boundaries, as hcl_set_state_from_prim) and the clock
+ * (hcl_set_clock); returns the output counters through the pointers (each may
+ * be NULL). */
+int hcl_read_restart(hcl_handle* h, const char* path, int* output_id, int* iter_output_id, int* time_output_id,
+                     int* iter, double* t);
 
 /* ---- .ini front end (host only) ------------------------------------------ */
 /* Compile-time choices of the reference (CMake Heraclespp_NDIM, _GEOM,

@@ -125,3 +125,38 @@ def test_driver_runs_passive_scalars_and_pressure_fix(tmp_path):
     # cells have internal energy below 4x their kinetic energy)
     o.run(r2, m2, e2, fx2, cfl=0.4, t_end=0.2, max_iter=100000, time_frequency=0.1)
     assert not np.array_equal(e2, e)
+
+
+def test_driver_writes_outputs_at_the_reference_cadence(tmp_path):
+    """--output-dir: an output at the start, at t = 0.1 (time_frequency) and at
+    t_end, with the reference's dataset set; the last one holds the oracle's
+    final state (same dt clamps to the output times), and restarting from the
+    middle one with the library reaches the same final state."""
+    from heraclespp_b200 import Domain
+    from heraclespp_b200.output import read_output
+
+    ini = tmp_path / "shock_tube.ini"
+    ini.write_text(SOD_INI)
+    res = subprocess.run([str(DRIVER), str(ini), "--setup=shock_tube", f"--output-dir={tmp_path}",
+                          "--prefix=shock_tube"], capture_output=True, text=True, timeout=120)
+    assert res.returncode == 0, res.stderr
+    outs = [read_output(tmp_path / f"shock_tube_{k:08d}.hclraw") for k in range(3)]
+    assert not (tmp_path / "shock_tube_00000003.hclraw").exists()
+    assert [o["current_time"] for o in outs] == [0.0, 0.1, 0.2]
+    assert [o["time_output_id"] for o in outs] == [-1, 0, 1]
+    assert [o["output_id"] for o in outs] == [0, 1, 2]
+    t_o, it_o, rho_o, rhou_o, E_o = sod_oracle()
+    assert outs[2]["iter"] == it_o
+    assert np.array_equal(outs[2]["rho"][0, 0], rho_o[0, 0, 2:-2])
+    assert np.array_equal(outs[2]["E"][0, 0], E_o[0, 0, 2:-2])
+    assert "shock_tube_00000002.hclraw" in (tmp_path / "shock_tube.xmf").read_text()
+    # restart from t = 0.1 and run to t_end
+    d = Domain(1, [1024], gamma=1.4, limiter="Minmod", riemann="HLLC", bc=["NullGradient"] * 2)
+    meta = d.read_restart(tmp_path / "shock_tube_00000001.hclraw")
+    assert meta["current_time"] == 0.1 and meta["iter"] == outs[1]["iter"]
+    r = d.run(cfl=0.4, t_end=0.2, max_iter=100000)
+    assert r.t == 0.2
+    rho_r = d.get_state()[0]
+    # the restart goes through the primitives (main.cpp:225-246): close, not bitwise
+    assert float(np.abs(rho_r[0, 0, 2:-2] - rho_o[0, 0, 2:-2]).max()) < 1e-12
+    d.close()
