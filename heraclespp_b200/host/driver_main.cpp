@@ -122,16 +122,20 @@ int main(int argc, char** argv)
             }
             iter = res.iter;
             t = res.t;
+            // the chunk ended on its own t_end (the dt of its last step was
+            // clamped to it, main.cpp:366-378) or on max_iter
+            const bool at_max = iter >= run.max_iter;
+            const bool at_t = res.finished && !at_max;
             bool out = false;
             if (next_iter >= 0 && iter >= next_iter) {
                 ++iter_output_id;
                 out = true;
             }
-            if (next_time >= 0 && t >= next_time) {
+            if (next_time >= 0 && at_t && p.t_end == next_time) {
                 ++time_output_id;
                 out = true;
             }
-            const bool done = t >= t_end || iter >= run.max_iter;
+            const bool done = at_max || (at_t && p.t_end == t_end);
             if (out || done) {
                 ++output_id;
                 if ((rc = hcl_write_output(h, outdir.c_str(), prefix.c_str(), output_id, iter_output_id,
