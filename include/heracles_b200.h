@@ -296,7 +296,9 @@ int hcl_get_dt_log(hcl_handle* h, double* dts, int max_count, int* count);
  * shared-memory tiles (16x16, 32x8, 32x16); on uniform Cartesian grids 3-5
  * warp strips of 32/64/128 rows, 6 warp strips fitted to one wave of
  * resident warps, 7-8 paired-column warp strips (fitted, 32 rows; even ghost
- * width), 9 fitted warp strips in 16-warp CTAs that march in step.  3-D: 0
+ * width), 9 fitted warp strips in 16-warp CTAs that march in step with their
+ * rows staged by the Tensor Memory Accelerator (even ghost width), 10 the same
+ * with per-lane cp.async staging.  3-D: 0
  * shared-memory tiles, 1 column march (uniform Cartesian grids).  With
  * passive scalars only the tiles qualify, and for one scalar also 3-6 in
  * 2-D and 1 in 3-D.  Returns the schedule in use through *used (may be NULL; -1 before
