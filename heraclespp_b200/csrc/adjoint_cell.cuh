@@ -184,7 +184,7 @@ HCL_HD R limiter(int lim, R dR, R dL, R* gR, R* gL)
 
 // ---- Riemann solvers (hydro/riemann_solver.hpp) on conservative states -------
 // Forward flux and reverse: given Fb, accumulate ULb, URb.  Solver 0 = HLL,
-// 1 = HLLC.
+// 1 = HLLC, 2 = the low-Mach splitting solver (riemann_solver.hpp:143-181).
 template <int ND, class R>
 HCL_HD void riemann(const Eos<R>& e, int solver, const R* UL, const R* UR, int l, R* F)
 {
@@ -195,6 +195,21 @@ HCL_HD void riemann(const Eos<R>& e, int solver, const R* UL, const R* UR, int l
     const R aL = std::sqrt(e.gamma * PL / UL[0]);
     const R aR = std::sqrt(e.gamma * PR / UR[0]);
     const R uL = WL[1 + l], uR = WR[1 + l];
+    if (solver == 2) {
+        const R a = R(1.1) * (UL[0] * aL > UR[0] * aR ? UL[0] * aL : UR[0] * aR);
+        const R ustar = R(0.5) * (uL + uR) - (PR - PL) / (R(2) * a);
+        const R amin = aL < aR ? aL : aR;
+        const R Ma = std::fabs(ustar) / amin;
+        const R theta = Ma < R(1) ? Ma : R(1);
+        const R Pstar = R(0.5) * (PL + PR) - R(0.5) * theta * a * (uR - uL);
+        const R* U = ustar > R(0) ? UL : UR;
+        for (int v = 0; v < ND + 2; ++v) {
+            F[v] = ustar * U[v];
+        }
+        F[1 + l] += Pstar;
+        F[1 + ND] += Pstar * ustar;
+        return;
+    }
     const R wsL = (uL - aL) < (uR - aR) ? (uL - aL) : (uR - aR);
     const R wsR = (uL + aL) > (uR + aR) ? (uL + aL) : (uR + aR);
     R FL[ND + 2], FR[ND + 2];
@@ -250,6 +265,78 @@ HCL_HD void riemann_rev(const Eos<R>& e, int solver, const R* UL, const R* UR, i
     const R aL = std::sqrt(cL2);
     const R aR = std::sqrt(cR2);
     const R uL = WL[1 + l], uR = WR[1 + l];
+    if (solver == 2) {
+        // forward values along the branches the forward evaluation took
+        const bool selLa = UL[0] * aL > UR[0] * aR;
+        const R a = R(1.1) * (selLa ? UL[0] * aL : UR[0] * aR);
+        const R ustar = R(0.5) * (uL + uR) - (PR - PL) / (R(2) * a);
+        const bool selLm = aL < aR;
+        const R amin = selLm ? aL : aR;
+        const R Ma = std::fabs(ustar) / amin;
+        const bool sub = Ma < R(1);
+        const R theta = sub ? Ma : R(1);
+        const R Pstar = R(0.5) * (PL + PR) - R(0.5) * theta * a * (uR - uL);
+        const bool left = ustar > R(0);
+        const R* U = left ? UL : UR;
+        R* Ub = left ? ULb : URb;
+        // F_v = ustar U_v (+ Pstar on the normal momentum, + Pstar ustar on E)
+        R ustarb = Fb[1 + ND] * Pstar;
+        const R Pstarb = Fb[1 + l] + Fb[1 + ND] * ustar;
+        for (int v = 0; v < NV; ++v) {
+            ustarb += Fb[v] * U[v];
+            Ub[v] += Fb[v] * ustar;
+        }
+        // Pstar = (PL + PR)/2 - theta a (uR - uL)/2
+        R WLb[NV], WRb[NV];
+        for (int v = 0; v < NV; ++v) {
+            WLb[v] = WRb[v] = R(0);
+        }
+        WLb[1 + ND] += R(0.5) * Pstarb;
+        WRb[1 + ND] += R(0.5) * Pstarb;
+        const R thetab = -R(0.5) * Pstarb * a * (uR - uL);
+        R ab = -R(0.5) * Pstarb * theta * (uR - uL);
+        WRb[1 + l] -= R(0.5) * Pstarb * theta * a;
+        WLb[1 + l] += R(0.5) * Pstarb * theta * a;
+        // theta = min(1, Ma); Ma = |ustar| / min(aL, aR)
+        R aLb = 0, aRb = 0;
+        if (sub) {
+            const R sgn = ustar > R(0) ? R(1) : (ustar < R(0) ? R(-1) : R(0));
+            ustarb += thetab * sgn / amin;
+            const R aminb = -thetab * Ma / amin;
+            if (selLm) {
+                aLb += aminb;
+            } else {
+                aRb += aminb;
+            }
+        }
+        // ustar = (uL + uR)/2 - (PR - PL)/(2a)
+        WLb[1 + l] += R(0.5) * ustarb;
+        WRb[1 + l] += R(0.5) * ustarb;
+        WRb[1 + ND] -= ustarb / (R(2) * a);
+        WLb[1 + ND] += ustarb / (R(2) * a);
+        ab += ustarb * (PR - PL) / (R(2) * a * a);
+        // a = 1.1 max(rhoL aL, rhoR aR)
+        if (selLa) {
+            WLb[0] += R(1.1) * ab * aL;
+            aLb += R(1.1) * ab * UL[0];
+        } else {
+            WRb[0] += R(1.1) * ab * aR;
+            aRb += R(1.1) * ab * UR[0];
+        }
+        if (aL > R(0)) {
+            const R c2b = aLb * R(0.5) / aL;
+            WLb[1 + ND] += c2b * e.gamma / UL[0];
+            ULb[0] -= c2b * cL2 / UL[0];
+        }
+        if (aR > R(0)) {
+            const R c2b = aRb * R(0.5) / aR;
+            WRb[1 + ND] += c2b * e.gamma / UR[0];
+            URb[0] -= c2b * cR2 / UR[0];
+        }
+        prim_from_cons_rev<ND>(e, UL, WLb, ULb);
+        prim_from_cons_rev<ND>(e, UR, WRb, URb);
+        return;
+    }
     const bool selL_min = (uL - aL) < (uR - aR);
     const bool selL_max = (uL + aL) > (uR + aR);
     const R wsL = selL_min ? (uL - aL) : (uR - aR);

@@ -1,6 +1,7 @@
 // adjoint_step.cuh -- discrete adjoint of one fused MUSCL-Hancock step.
 //
-// Forward step (Cartesian, uniform spacing, uniform gravity):
+// Forward step (Cartesian, uniform spacing; uniform gravity, or the point-mass
+// field g(i) along x0, which does not depend on the state):
 //   U'_c = U_c + sum_d c_d (F_{c-1/2,d} - F_{c+1/2,d}) + dt g-terms(U_c),
 //   F_{f,d} = Riemann(H_{L,d}, H_{R,d}),  H = Hancock face states built from the
 //   limited slopes of the primitive stencil of each cell, and ghosts of U' are
@@ -166,6 +167,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
         int x[3], own;
         decode_h(h, x, own);
         const int lc = lcell(x);
+        const int gi = gorg[0] + x[0]; // x0 index of the cell (gravity table)
         R fp[2][ND][NV];
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
@@ -219,7 +221,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 }
 #pragma unroll
                 for (int e = 0; e < ND; ++e) {
-                    const R gg = (R)(dth * g.g[e]);
+                    const R gg = (R)(dth * gravity_at(g, gi, e));
                     hs[1 + e] += gg * fc[s][d][0];
                     hs[1 + ND] += gg * fc[s][d][1 + e];
                 }
@@ -273,7 +275,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 UR[v] = base[v * S::Asize(d) + aRd];
                 ULb[v] = URb[v] = R(0);
             }
-            adj::riemann_rev<ND>(eos, g.riemann == 0 ? 0 : 1, UL, UR, d, Fb, ULb, URb);
+            adj::riemann_rev<ND>(eos, g.riemann, UL, UR, d, Fb, ULb, URb);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 bb[(NV + v) * S::Asize(d) + aLd] = ULb[v];
@@ -288,6 +290,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
         int x[3], own;
         decode_h(h, x, own);
         const int lc = lcell(x);
+        const int gi = gorg[0] + x[0]; // x0 index of the cell (gravity table)
         // gather this cell's face-state adjoints
         R Hb[2][ND][NV];
         bool any = false;
@@ -351,7 +354,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 }
 #pragma unroll
                 for (int e = 0; e < ND; ++e) {
-                    const R gg = (R)(dth * g.g[e]);
+                    const R gg = (R)(dth * gravity_at(g, gi, e));
                     cb[0] += gg * Hb[s][ip][1 + e];
                     cb[1 + e] += gg * Hb[s][ip][1 + ND];
                 }
@@ -444,8 +447,9 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
 #pragma unroll
             for (int e = 0; e < ND; ++e) {
                 // U'_m_e += dt g_e rho ; U'_E += dt g_e m_e   (godunov_scheme.hpp:258-260)
-                outv[0] += dt * g.g[e] * sl[(1 + e) * S::NP + p];
-                outv[1 + e] += dt * g.g[e] * sl[(1 + ND) * S::NP + p];
+                const double ge = gravity_at(g, ri, e);
+                outv[0] += dt * ge * sl[(1 + e) * S::NP + p];
+                outv[1 + e] += dt * ge * sl[(1 + ND) * S::NP + p];
             }
         }
         const int64_t oo = sidx(lam_in, g.n[1], ri, rj, rk);

@@ -1789,10 +1789,10 @@ int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p)
         return fail(HCL_ERR_CONFIG, "no state set");
     }
     const GridDev& g = h->g;
-    if (g.geom != HCL_GEOM_CARTESIAN || !g.uniform_cart || g.gravity != HCL_GRAVITY_UNIFORM ||
-        g.riemann == HCL_RIEMANN_LOW_MACH || g.nfx > 0 || h->cfg.pressure_fix || g.eos != HCL_EOS_PERFECT_GAS) {
-        return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian uniform grids, uniform gravity, HLL/HLLC, nfx = 0, "
-                                    "no pressure fix, the perfect-gas EOS");
+    if (g.geom != HCL_GEOM_CARTESIAN || !g.uniform_cart || g.gravity == HCL_GRAVITY_INTERNAL_MASS || g.nfx > 0 ||
+        h->cfg.pressure_fix || g.eos != HCL_EOS_PERFECT_GAS) {
+        return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian uniform grids, uniform or point-mass gravity, "
+                                    "every Riemann solver, nfx = 0, no pressure fix, the perfect-gas EOS");
     }
     if (p->precision != HCL_FP64 && p->precision != HCL_FP32_MIXED) {
         return fail(HCL_ERR_CONFIG, "the reverse sweep runs in HCL_FP64 or HCL_FP32_MIXED");

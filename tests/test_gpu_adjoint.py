@@ -159,7 +159,7 @@ def test_autograd_wrapper_gives_the_adjoint():
 
 
 @pytest.mark.parametrize("lim,solver,n", [("VanLeer", "HLLC", 20), ("Minmod", "HLL", 20), ("VanAlbada", "HLLC", 20),
-                                          ("VanLeer", "HLLC", 32)])
+                                          ("VanLeer", "HLLC", 32), ("VanLeer", "Low Mach", 20)])
 def test_adjoint_kernel_matches_loop_reference(tmp_path, lim, solver, n):
     """The tiled adjoint kernel (two 16-wide tiles per axis: the second ragged
     at n = 20, full at n = 32 where the last tile owns the domain's last face)
@@ -170,7 +170,7 @@ def test_adjoint_kernel_matches_loop_reference(tmp_path, lim, solver, n):
 
     lib = build_cell_lib(tmp_path / "libadjcheck.so")
     ids = {"VanLeer": 1, "Minmod": 2, "VanAlbada": 3}
-    ref = Ref(lib, lim=ids[lim], solver=0 if solver == "HLL" else 1)
+    ref = Ref(lib, lim=ids[lim], solver={"HLL": 0, "HLLC": 1, "Low Mach": 2}[solver])
     nsteps, dt = 5, 0.004
     U0 = smooth_state(n, seed=3)
     states = [U0]
@@ -194,3 +194,46 @@ def test_adjoint_kernel_matches_loop_reference(tmp_path, lim, solver, n):
     print(f"{lim}/{solver}: max |gpu - ref| {err.max():.3e} of {np.abs(lam_c).max():.3e}")
     # tiles and ghost folds cell by cell
     assert err.max() <= 1e-11 * np.abs(lam_c).max(), np.argwhere(err > 1e-11 * np.abs(lam_c).max())[:20]
+
+
+@pytest.mark.parametrize("riemann,gravity", [("Low Mach", "Uniform"), ("HLLC", "Point_mass")])
+def test_adjoint_other_physics_matches_finite_differences(riemann, gravity):
+    """The low-Mach splitting solver (riemann_solver.hpp:143-181) and the
+    point-mass gravity field g(i) along x0 (gravity.cpp:29-55, state
+    independent) in the reverse sweep: central differences of
+    J = 0.5 ||rho^N - target||^2 on a smooth 2-D state, 12 steps."""
+    n, nsteps = 40, 12
+    kw = dict(gamma=1.4, limiter="VanLeer", riemann=riemann, bc=["NullGradient", "Reflexive", "Periodic", "Periodic"],
+              gravity=gravity, central_mass=0.2 / 6.6743015e-11 if gravity == "Point_mass" else 1.0, g=(0.0, 0.0, 0.0),
+              xmin=(1.0, 0.0, 0.0), xmax=(2.0, 1.0, 1.0))
+    o = Oracle(2, [n, n], **{k: v for k, v in kw.items()})
+    grid = setups.Grid.from_domain(o)
+    rho, u, P = grid.alloc()
+    s3, (X, Y, Z), _ = grid.interior()
+    shape = rho[s3].shape
+    rho[s3] = np.broadcast_to(1 + 0.2 * np.sin(2 * np.pi * Y + 0.3) * np.cos(np.pi * X), shape)
+    P[s3] = np.broadcast_to(1 + 0.1 * np.cos(2 * np.pi * (X + Y)), shape)
+    u[0][s3] = np.broadcast_to(0.05 * np.sin(2 * np.pi * Y + 0.1) * (X - 1) * (2 - X), shape)
+    u[1][s3] = np.broadcast_to(0.05 * np.cos(np.pi * X + 0.5), shape)
+    prim = smooth_background(grid, (rho, u, P), amp=0.01)
+    r0, m0, E0, _ = o.init_from_prim(*prim)
+    U0 = np.concatenate([r0[None], m0, E0[None]])
+    d = Domain(2, [n, n], precision="fp64", **kw)
+    d.set_state(r0, m0, E0)
+    rr = d.run(cfl=0.4, nsteps=nsteps)
+    assert rr.iter == nsteps
+    dts = d.dt_log()[:nsteps]
+    rng = np.random.default_rng(5)
+    target = d.get_state()[0] * (1 + 0.01 * rng.uniform(-1, 1, r0.shape))
+    g = adjoint_grad(d, U0, dts, target, "fp64", 4)
+    ng = 2
+    errs = []
+    for _ in range(8):
+        v = np.zeros_like(U0)
+        v[:, :, ng:-ng, ng:-ng] = rng.uniform(-1, 1, (4, 1, n, n)) * np.abs(U0[:, :, ng:-ng, ng:-ng])
+        fd = fd_directional(d, o, U0, v, 3e-9, dts, target)
+        ad = float(np.sum(g * v))
+        errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
+    errs = np.array(errs)
+    print(f"{riemann}/{gravity}: FD rel err median {np.median(errs):.2e} max {errs.max():.2e}")
+    assert np.median(errs) < 1e-5, errs
