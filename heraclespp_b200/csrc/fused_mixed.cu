@@ -11,11 +11,12 @@ namespace hcl::fused {
 
 // Schedules selectable at run time for 2-D (the autotuner picks one):
 // 0-2 shared-memory tiles 16x16, 32x8, 32x16; 3-5 warp strips of 32, 64,
-// 128 rows; 6 warp strips whose height fits one wave of resident warps;
-// 7 and 8 paired-column warp strips (fitted height, 32 rows); 9 fitted warp
-// strips in CTAs of 16 warps that march in step, rows staged by TMA; 10 the
-// same with per-lane cp.async staging.  3-10 need a uniform Cartesian grid,
-// 7-9 an even ghost width.  With passive scalars: the tiles,
+// 128 rows; 6 warp strips whose height fits one wave of resident warps; 9
+// fitted warp strips in CTAs of 16 warps that march in step, rows staged by
+// TMA; 10 the same with per-lane cp.async staging.  3-10 need a uniform
+// Cartesian grid, 9 an even ghost width.  7 and 8 are unused (they were
+// paired-column strips, slower than 6 and 9, and were removed).
+// With passive scalars: the tiles,
 // and for one scalar the 4-warp strips 3-6 (2-D) or the column march (3-D).
 // 3-D: 0 shared-memory tiles 8x8x4; 1 column march (uniform Cartesian grids).
 int mixed_shape_count(int ndim)
@@ -59,7 +60,7 @@ bool mixed_shape_valid(const GridDev& g, int shape)
     if (shape == 9) {
         return strip2d_tma_eligible(g);
     }
-    return (shape < 7 || shape == 10) ? strip2d_eligible(g) : strip2d_pair_eligible(g);
+    return (shape < 7 || shape == 10) && strip2d_eligible(g);
 }
 
 void configure_mixed()
@@ -81,8 +82,6 @@ void step_mixed(const GridDev& g, const StateDev& in, const StateDev& out, StepC
     case 2:
         if ((shape == 9 && strip2d_tma_eligible(g)) || (shape == 10 && strip2d_eligible(g))) {
             step_strip2d(g, in, out, ctl, rp, slot, out_buf, 0, true, shape == 9, s);
-        } else if (shape >= 7 && shape < 9 && strip2d_pair_eligible(g)) {
-            step_strip2d_pair(g, in, out, ctl, rp, slot, out_buf, shape == 7 ? 0 : 32, s);
         } else if (shape >= 3 && (strip2d_eligible(g) || (shape <= 6 && strip2d_fx_eligible(g)))) {
             step_strip2d(g, in, out, ctl, rp, slot, out_buf, shape == 3 ? 32 : (shape == 4 ? 64 : (shape == 5 ? 128 : 0)),
                          false, false, s);

@@ -8,7 +8,6 @@
 #include <cstring>
 
 #include "fused_strip2d.cuh"
-#include "fused_strip2d_pair.cuh"
 #include "per_device.hpp"
 #include "stages.hpp"
 
@@ -48,13 +47,6 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 bool strip2d_tma_eligible(const GridDev& g)
 {
     return strip2d_eligible(g) && g.ng % 2 == 0 && tensor_map_encoder() != nullptr;
-}
-
-// The paired schedule loads and stores column pairs as 16-byte vectors: the
-// first column of a pair is even, which needs an even ghost width.
-bool strip2d_pair_eligible(const GridDev& g)
-{
-    return strip2d_eligible(g) && g.ng % 2 == 0;
 }
 
 namespace {
@@ -101,8 +93,9 @@ int resident_blocks_sync()
 }
 
 // 3-D tiled map of a 2-D FP64 state (columns, rows, the 4 hydro planes) with
-// the strip ring's box {32 columns, 1 row, 4 variables}; columns past n0 read
-// as zeros (they feed only lanes that write nothing).
+// the strip ring's box {32 columns, 2 rows, 4 variables}; columns past n0 and
+// rows past n1 read as zeros (they feed only lanes and rows that write
+// nothing).
 bool encode_strip_map(const GridDev& g, const StateDev& st, CUtensorMap* map)
 {
     const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
@@ -111,7 +104,7 @@ bool encode_strip_map(const GridDev& g, const StateDev& st, CUtensorMap* map)
     }
     const cuuint64_t dims[3] = {(cuuint64_t)g.n[0], (cuuint64_t)g.n[1], 4};
     const cuuint64_t strides[2] = {(cuuint64_t)st.pitch * sizeof(double), (cuuint64_t)st.plane * sizeof(double)};
-    const cuuint32_t box[3] = {32, 1, 4};
+    const cuuint32_t box[3] = {32, kTmaBoxRows, 4};
     const cuuint32_t estr[3] = {1, 1, 1};
     return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, st.q, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -167,63 +160,7 @@ void launch_l(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl
     }
 }
 
-template <int LIM, int RS>
-int resident_blocks_pair()
-{
-    static PerDevice cache;
-    return resident_on_device(cache, reinterpret_cast<const void*>(k_strip2d_pair<LIM, RS>), 128, 0);
-}
-
-template <int LIM, int RS>
-void launch_pair_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
-                    int slot, int out_buf, int L, cudaStream_t s)
-{
-    const int ncolw = (g.nx[0] + kPairLanesOut - 1) / kPairLanesOut;
-    const int resident = resident_blocks_pair<LIM, RS>();
-    if (L <= 0) {
-        const int per_col = std::max(1, resident * 4 / ncolw);
-        L = std::max(8, (g.nx[1] + per_col - 1) / per_col);
-    }
-    const int nstrip = (g.nx[1] + L - 1) / L;
-    const int warps = ncolw * nstrip;
-    const int blocks = std::min((warps + 3) / 4, resident);
-    k_strip2d_pair<LIM, RS><<<blocks, 128, 0, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
-}
-
-template <int LIM>
-void launch_pair_l(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
-                   int slot, int out_buf, int L, cudaStream_t s)
-{
-    if (g.riemann == RS_HLL) {
-        launch_pair_lr<LIM, RS_HLL>(g, in, out, ctl, rp, slot, out_buf, L, s);
-    } else if (g.riemann == RS_HLLC) {
-        launch_pair_lr<LIM, RS_HLLC>(g, in, out, ctl, rp, slot, out_buf, L, s);
-    } else {
-        launch_pair_lr<LIM, RS_SPLITTING>(g, in, out, ctl, rp, slot, out_buf, L, s);
-    }
-}
-
 } // namespace
-
-void step_strip2d_pair(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
-                       int slot, int out_buf, int L, cudaStream_t s)
-{
-    switch (g.limiter) {
-    case LIM_CONSTANT:
-        launch_pair_l<LIM_CONSTANT>(g, in, out, ctl, rp, slot, out_buf, L, s);
-        break;
-    case LIM_VANLEER:
-        launch_pair_l<LIM_VANLEER>(g, in, out, ctl, rp, slot, out_buf, L, s);
-        break;
-    case LIM_MINMOD:
-        launch_pair_l<LIM_MINMOD>(g, in, out, ctl, rp, slot, out_buf, L, s);
-        break;
-    default:
-        launch_pair_l<LIM_VANALBADA>(g, in, out, ctl, rp, slot, out_buf, L, s);
-        break;
-    }
-    ++g_launches;
-}
 
 void step_strip2d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                   int slot, int out_buf, int L, bool sync, bool tma, cudaStream_t s)

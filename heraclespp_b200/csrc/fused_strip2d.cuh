@@ -234,10 +234,11 @@ constexpr int kStripRingDoubles = 8 * 4 * 32;
 // (godunov_scheme.hpp:262-301), the update in FP64 divided by the new density
 // and clamped to [0, 1], stored with the same ghost images.
 // TMA: the ring rows are staged by the Tensor Memory Accelerator (tma_ring.cuh):
-// lane 0 issues one box per row through `tmap` (the input state), the lanes
-// wait on the slot's mbarrier (`bars`, 8 per warp; `phase` holds the parity
-// each slot waits for next, `timeout` is set when a bounded wait gave up).
-// Rows past r1 + 1 are not loaded.  Needs NFX == 0 and an even ghost width
+// lane 0 issues one box of two rows through `tmap` (the input state) into one
+// of the warp's 4 ring slots, the lanes wait on the slot's mbarrier (`bars`,
+// 4 per warp; `phase` counts the boxes the warp has waited for, which fixes
+// each slot's next parity; `timeout` is set when a bounded wait gave up).
+// Rows past r1 + 2 are not loaded.  Needs NFX == 0 and an even ghost width
 // (the box's first column c0 - 2 must start on a 16-byte boundary).
 template <int LIM, int RS, int SYNC = 0, int XIMG = 1, int NFX = 0, bool TMA = false>
 __device__ __forceinline__ void strip_work(const GridDev& g, const double* __restrict__ qin, double* __restrict__ qout,
@@ -295,31 +296,46 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
-    auto ring_row = [&](int r, double* q) {
-#pragma unroll
-        for (int v = 0; v < 4 + NFX; ++v) {
-            q[v] = ring[r & 7][v][lane];
-        }
-    };
-    // TMA staging: one box {32 columns, 1 row, 4 variables} per row, issued by
-    // lane 0 after the warp has finished reading the slot's previous row
-    unsigned ph = TMA ? *phase : 0u;
+    // TMA staging: box b of this strip holds rows r0-2+2b and r0-1+2b as
+    // [var][row][lane] in slot (nb0 + b) & 3; the k-th box a warp waits for
+    // completes its slot's phase with parity (k >> 2) & 1.  Boxes 0..nbox-1
+    // cover rows r0-2 .. r1+1 (the last may reach r1+2).
+    const unsigned nb0 = TMA ? *phase : 0u;
+    const int nbox = TMA ? ((r1 - r0 + 3) >> 1) + 1 : 0;
     bool tmo = false;
-    auto tma_issue = [&](int r) {
-        __syncwarp();
+    const unsigned ring_s = TMA ? smem_u32(&ring[0][0][0]) : 0u;
+    const unsigned bar_s = TMA ? smem_u32(bars) : 0u;
+    const double* ring_d = &ring[0][0][0];
+    auto tma_issue = [&](int b) {
+        __syncwarp(); // the warp is done with the slot's previous box
         if (lane == 0) {
-            uint64_t* bar = bars + (r & 7);
+            const unsigned sl = (nb0 + (unsigned)b) & 3u;
             fence_proxy_async_smem();
-            mbar_arrive_expect_tx(bar, kTmaRowBytes);
-            tma_load_3d(&ring[r & 7][0][0], tmap, bar, c0 - 2, min(max(r, 0), n1 - 1), 0);
+            mbar_arrive_expect_tx_s(bar_s + 8u * sl, kTmaBoxBytes);
+            tma_load_3d_s(ring_s + sl * kTmaBoxBytes, tmap, bar_s + 8u * sl, c0 - 2, r0 - 2 + 2 * b, 0);
         }
     };
-    auto tma_wait = [&](int r) {
-        const int sl = r & 7;
-        if (!mbar_wait_bounded(bars + sl, (ph >> sl) & 1u)) {
+    auto tma_wait = [&](int b) {
+        const unsigned k = nb0 + (unsigned)b;
+        if (!mbar_wait_bounded_s(bar_s + 8u * (k & 3u), (k >> 2) & 1u)) {
             tmo = true;
         }
-        ph ^= 1u << sl;
+    };
+    auto ring_row = [&](int r, double* q) {
+        if constexpr (TMA) {
+            const int rel = r - (r0 - 2);
+            const unsigned sl = (nb0 + (unsigned)(rel >> 1)) & 3u;
+            const double* base = ring_d + sl * (kTmaBoxBytes / 8u) + (rel & 1) * 32 + lane;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                q[v] = base[v * 64];
+            }
+        } else {
+#pragma unroll
+            for (int v = 0; v < 4 + NFX; ++v) {
+                q[v] = ring[r & 7][v][lane];
+            }
+        }
     };
 
     // preamble: rows r0-2 .. r0+1 -> primitives; Hancock of rows r0-1 and r0
@@ -334,12 +350,11 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         float wA[4], hyB[4];
         float xA = 0.f, xB = 0.f;
         if constexpr (TMA) {
-            for (int rr = r0 - 2; rr <= min(r0 + 3, r1 + 1); ++rr) {
-                tma_issue(rr);
+            for (int b = 0; b < min(4, nbox); ++b) {
+                tma_issue(b);
             }
-            for (int rr = r0 - 2; rr <= r0 + 1; ++rr) {
-                tma_wait(rr);
-            }
+            tma_wait(0); // rows r0-2, r0-1
+            tma_wait(1); // rows r0, r0+1
         } else {
             for (int rr = r0 - 2; rr <= r0 + 3; ++rr) {
                 stage_row(rr);
@@ -402,10 +417,12 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         float wN[4];
         float xN = 0.f;
         if constexpr (TMA) {
-            if (r + 4 <= r1 + 1) {
-                tma_issue(r + 4);
+            if ((i & 1) == 0) {
+                tma_wait((i >> 1) + 2); // rows r+2, r+3 landed
+                if ((i >> 1) + 4 < nbox) {
+                    tma_issue((i >> 1) + 4);
+                }
             }
-            tma_wait(r + 2); // rows up to r+2 landed
         } else {
             stage_row(r + 4);
             asm volatile("cp.async.wait_group 2;\n" ::: "memory"); // rows up to r+2 landed
@@ -560,8 +577,8 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         }
     }
     if constexpr (TMA) {
-        // every issued row (up to r1 + 1) has been waited for
-        *phase = ph;
+        // every issued box has been waited for
+        *phase = nb0 + (unsigned)nbox;
         if (tmo) {
             *timeout = true;
         }

@@ -61,10 +61,6 @@ namespace fused {
 // Output columns of one warp strip of the 2-D mixed kernel (32 lanes less a
 // 2-cell halo on each side).
 constexpr int kStripLanesOut = 28;
-// Output columns of one warp of the paired schedule (two columns per lane,
-// lanes 0 and 31 are the halo).
-constexpr int kPairLanesOut = 60;
-
 // State buffers of the fused path: nvar planes, each n2*n1*pitch doubles with
 // the x0 row padded to `pitch` (a multiple of 16 doubles).
 struct StateDev {
@@ -100,10 +96,6 @@ constexpr size_t kFusedStaticSmemMargin = 1024;
 bool strip2d_eligible(const GridDev& g);
 // 4-warp strips (schedules 3-6) with one passive scalar.
 bool strip2d_fx_eligible(const GridDev& g);
-// Paired schedule: two columns per lane in packed FP32 pairs (ng even).
-bool strip2d_pair_eligible(const GridDev& g);
-void step_strip2d_pair(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
-                       int slot, int out_buf, int L, cudaStream_t s);
 // 3-D column march (uniform Cartesian grids, uniform gravity); L <= 0 fits
 // the plane count per CTA to the resident CTAs.
 bool strip3d_eligible(const GridDev& g);

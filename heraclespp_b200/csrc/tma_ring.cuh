@@ -1,9 +1,9 @@
 // tma_ring.cuh -- TMA row staging for the warp-strip kernels (sm_100a).
 //
-// A warp's row ring (8 slots of one x-row segment: 4 variables x 32 doubles,
-// 1 KB) is filled by the Tensor Memory Accelerator: one elected lane issues a
-// single 3-D cp.async.bulk.tensor per row (box {32 doubles, 1 row, 4
-// variables} of the FP64 state, whose planes are the tensor's third
+// A warp's row ring (4 slots of two x-row segments: 4 variables x 2 rows x 32
+// doubles, 2 KB) is filled by the Tensor Memory Accelerator: one lane issues a
+// single 3-D cp.async.bulk.tensor per pair of rows (box {32 doubles, 2 rows,
+// 4 variables} of the FP64 state, whose planes are the tensor's third
 // dimension), and completion is tracked by one mbarrier per slot (expect-tx
 // of the box's bytes).  The lanes wait on the slot's mbarrier phase before
 // reading it.  The tensor map covers this GPU's own state buffer only and the
@@ -20,8 +20,9 @@
 
 namespace hcl::fused {
 
-// x-row segment of one ring slot: 32 lanes x 4 variables of FP64
-constexpr unsigned kTmaRowBytes = 4u * 32u * 8u;
+// one ring slot: 32 lanes x 2 rows x 4 variables of FP64
+constexpr unsigned kTmaBoxRows = 2u;
+constexpr unsigned kTmaBoxBytes = 4u * kTmaBoxRows * 32u * 8u;
 // polls of one mbarrier wait before it gives up (each try_wait also
 // suspends the thread for a hardware-defined time)
 constexpr int kTmaWaitPolls = 1 << 22;
@@ -69,6 +70,43 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
 __device__ __forceinline__ void tma_prefetch_map(const CUtensorMap* map)
 {
     asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+// the same operations on shared-memory addresses computed once
+__device__ __forceinline__ void mbar_arrive_expect_tx_s(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_load_3d_s(unsigned dst, const CUtensorMap* map, unsigned bar, int x, int y, int z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+        "[%2];\n" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait_s(unsigned bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n"
+        " .reg .pred p;\n"
+        " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+__device__ __forceinline__ bool mbar_wait_bounded_s(unsigned bar, unsigned parity)
+{
+    for (int i = 0; i < kTmaWaitPolls; ++i) {
+        if (mbar_try_wait_s(bar, parity)) {
+            return true;
+        }
+    }
+    return false;
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)

@@ -295,8 +295,7 @@ int hcl_get_dt_log(hcl_handle* h, double* dts, int max_count, int* count);
  * first run; -2: leaves the schedule unchanged (query).  2-D: 0-2
  * shared-memory tiles (16x16, 32x8, 32x16); on uniform Cartesian grids 3-5
  * warp strips of 32/64/128 rows, 6 warp strips fitted to one wave of
- * resident warps, 7-8 paired-column warp strips (fitted, 32 rows; even ghost
- * width), 9 fitted warp strips in 16-warp CTAs that march in step with their
+ * resident warps (7-8 unused), 9 fitted warp strips in 16-warp CTAs that march in step with their
  * rows staged by the Tensor Memory Accelerator (even ghost width), 10 the same
  * with per-lane cp.async staging.  3-D: 0
  * shared-memory tiles, 1 column march (uniform Cartesian grids).  With

@@ -16,7 +16,7 @@ CASES_2D = {
 }
 
 
-@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 4, 5, 6, 9, 10])
 @pytest.mark.parametrize("name", list(CASES_2D))
 def test_mixed_schedule_matches_oracle(name, schedule):
     o, d, (rho0, u0, P0) = make_pair(name, "fp32_mixed")
@@ -72,7 +72,7 @@ def test_strip_with_gravity_and_reflexive_walls():
     u0[1][s3] = np.broadcast_to(0.01 * np.cos(4 * np.pi * X) * np.exp(-((Y - 0.5) / 0.1) ** 2), rho0[s3].shape)
     rho, rhou, E, fx = o.init_from_prim(rho0, u0, P0)
     _, _, _, dts = o.run(rho, rhou, E, fx, cfl=0.4, max_iter=40, record_dts=True)
-    for schedule in (0, 4, 7, 9, 10):
+    for schedule in (0, 4, 9, 10):
         d = Domain(2, [40, 70], precision="fp32_mixed", **kw)
         d.set_schedule(schedule)
         d.set_state_from_prim(rho0, u0, P0)
