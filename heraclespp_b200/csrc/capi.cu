@@ -568,12 +568,12 @@ int get_graph(hcl_handle* h, const RunParamsDev& rp, int k, cudaGraphExec_t* out
     return HCL_OK;
 }
 
-// Handles whose time loop is composed of the FP64 stage entry points: the
-// FP32-mixed kernels carry no pressure fix, and passive scalars too many for
-// the fused tile's shared memory are not carried at all.
+// Handles whose time loop is composed of the FP64 stage entry points: those
+// that ask for it, and passive scalars too many for the fused tile's shared
+// memory (the tiles carry the pressure fix in every precision).
 bool stage_mode(const hcl_handle* h)
 {
-    if (h->force_stage || (h->cfg.pressure_fix != 0 && h->cfg.precision == HCL_FP32_MIXED)) {
+    if (h->force_stage) {
         return true;
     }
     if (h->cfg.nfx == 0) {

@@ -40,6 +40,11 @@ size_t mixed_smem_bytes(const GridDev& g, int shape)
 
 bool mixed_shape_valid(const GridDev& g, int shape)
 {
+    if (g.pressure_fix) {
+        // the pressure fix rides in the shared-memory tiles only
+        return (g.ndim == 2 ? shape < 3 : shape == 0) &&
+               mixed_smem_bytes(g, shape) + kFusedStaticSmemMargin <= (size_t)smem_optin();
+    }
     if (g.nfx > 0) {
         // passive scalars ride in the shared-memory tiles and, one of them,
         // in the 4-warp strips

@@ -855,7 +855,8 @@ __device__ __forceinline__ void fused_step_body(const GridDev& g, const StateDev
     __syncthreads();
 
     // ---- phase 4: Godunov update, ghost images, health, CFL -----------------
-    // pressure_fix.hpp:19-172 on one interior cell (FP64): q the old state,
+    // pressure_fix.hpp:19-172 on one interior cell (FP64; in the FP32-mixed
+    // tiles from the FP32 predicted face states): q the old state,
     // qn the Godunov update, whose energy it may replace.  The face states are
     // the predicted ones in shared memory, the neighbours' old states come
     // from global memory; expression order as in the reference (the energy is
@@ -1127,10 +1128,9 @@ __device__ __forceinline__ void fused_step_body(const GridDev& g, const StateDev
             }
         }
 
-        if constexpr (EXACT) {
-            if (g.pressure_fix) {
-                pressure_fix_cell(x0, x1, x2, gi, gj, gk, cgl, q, qn);
-            }
+        // FP32-mixed tiles: the same FP64 arithmetic on their FP32 face states
+        if (g.pressure_fix) {
+            pressure_fix_cell(x0, x1, x2, gi, gj, gk, cgl, q, qn);
         }
 
         // health check (main.cpp:397-425) and CFL of the new state (time_step.hpp:55-77)

@@ -275,12 +275,14 @@ typedef struct hcl_run_result {
  * everything on the device: CFL dt reduced inside the step kernel, dt clamps,
  * health check and ghost filling in place; steps are replayed from CUDA graphs.
  * Synchronises at the end (and between graph chunks when nsteps <= 0).
- * Passive scalars (nfx > 0) ride in the fused shared-memory tile kernels
- * (FP64 or FP32-mixed); the state then includes fx.  Handles with
- * pressure_fix, or with more passive scalars than the tile's shared memory
- * holds, run the same loop composed of the FP64 stage entry points
- * (reconstruction, Godunov, pressure fix, boundaries, cons->prim) in the
- * reference's order, with dt and the health check read back each step. */
+ * Passive scalars (nfx > 0) and the pressure fix ride in the fused
+ * shared-memory tile kernels (FP64, fast FP64 and FP32-mixed, which applies
+ * the fix in FP64 to its FP32 face states); the state then includes fx.
+ * Handles with more passive scalars than the tile's shared memory holds, and
+ * handles set to it by hcl_set_stage_loop, run the same loop composed of the
+ * FP64 stage entry points (reconstruction, Godunov, pressure fix, boundaries,
+ * cons->prim) in the reference's order, with dt and the health check read
+ * back each step. */
 int hcl_run(hcl_handle* h, const hcl_run_params* p, hcl_run_result* r);
 /* One step of the fused kernel with the given dt (no CFL clamp logic, no
  * synchronisation): the building block the adapters use. */
