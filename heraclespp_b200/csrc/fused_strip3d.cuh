@@ -12,8 +12,7 @@
 //    x-faces of plane z+1, the z-face z+1/2 and the y-faces of plane z, and
 //    updates plane z in FP64 with the ghost images, the health check and the
 //    CFL contribution.  One CTA barrier per plane orders the shared planes.
-// Lanes 2..29 and warps 2..13 write; the others are the stencil halo, and
-// the halo warps do only the part of a step their neighbours read.
+// Lanes 2..29 and warps 2..13 write; the others are the stencil halo.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -296,13 +295,6 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
         }
     };
     const int wd = max(w - 1, 0), wu = min(w + 1, kS3Warps - 1);
-    // Roles of the rows along y (warp-uniform): the outermost halo rows (0 and
-    // 15) only supply primitives for their neighbours' y-slopes; rows 1 and 14
-    // also build Hancock states for their y-face states, and row 1 solves the
-    // y-face above it; rows 2..13 (the written rows) do everything.
-    const bool hancock_row = w >= 1 && w < kS3Warps - 1;
-    const bool xz_row = w >= 2 && w < kS3Warps - 2;
-    const bool yabove_row = w >= 1 && w < kS3Warps - 2;
 
     // window: wC = P[z], wD = P[z+1]; qN = U[z+2] in flight
     float wC[5], wD[5];
@@ -356,41 +348,24 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
         }
         load(z + 3, qN);
         // 2. Hancock of plane z+1 (y-neighbours' primitives of plane z+1 were shared last step)
-        float hm[3][5], hp[3][5];
-        float xo[6];
-        if (hancock_row) {
-            float wyd[5], wyu[5];
+        float wyd[5], wyu[5];
 #pragma unroll
-            for (int v = 0; v < 5; ++v) {
-                wyd[v] = sh.prim[(z + 1) & 1][wd][v][lane];
-                wyu[v] = sh.prim[(z + 1) & 1][wu][v][lane];
-            }
-            float xw[5] = {xD, 0.f, 0.f, xC, xN};
-            if constexpr (NFX > 0) {
-                xw[1] = sh.fx.xprim[(z + 1) & 1][wd][lane];
-                xw[2] = sh.fx.xprim[(z + 1) & 1][wu][lane];
-            }
-            s3::hancock<LIM, NFX>(c, wD, wyd, wyu, wC, wN, hm, hp, xw, xo);
-        } else {
-#pragma unroll
-            for (int v = 0; v < 5; ++v) {
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    hm[d][v] = hp[d][v] = 0.f;
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                xo[k] = 0.f;
-            }
+        for (int v = 0; v < 5; ++v) {
+            wyd[v] = sh.prim[(z + 1) & 1][wd][v][lane];
+            wyu[v] = sh.prim[(z + 1) & 1][wu][v][lane];
         }
+        float hm[3][5], hp[3][5];
+        float xw[5] = {xD, 0.f, 0.f, xC, xN};
+        if constexpr (NFX > 0) {
+            xw[1] = sh.fx.xprim[(z + 1) & 1][wd][lane];
+            xw[2] = sh.fx.xprim[(z + 1) & 1][wu][lane];
+        }
+        float xo[6];
+        s3::hancock<LIM, NFX>(c, wD, wyd, wyu, wC, wN, hm, hp, xw, xo);
         // 3. x-faces of plane z+1: left face at this lane, right face from lane+1
         double dFxN[5];
         double dxxN = 0.0;
-        // 4. z-face z+1/2
-        float Gzhi[5];
-        float gzx_hi = 0.f;
-        if (xz_row) {
+        {
             float uL[5], Fl[5];
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
@@ -407,32 +382,27 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
                 const float fl = (Fl[0] < 0.f ? xo[0] : up_left) * Fl[0];
                 dxxN = (double)fl - (double)__shfl_down_sync(0xffffffffu, fl, 1);
             }
-            fast::riemann<3>(c.eos, RS, hzU, hm[2], 2, Gzhi);
-            if constexpr (NFX > 0) {
-                gzx_hi = (Gzhi[0] < 0.f ? xo[2] : xzU) * Gzhi[0];
-            }
-        } else {
-#pragma unroll
-            for (int v = 0; v < 5; ++v) {
-                dFxN[v] = 0.0;
-                Gzhi[v] = 0.f;
-            }
+        }
+        // 4. z-face z+1/2
+        float Gzhi[5];
+        fast::riemann<3>(c.eos, RS, hzU, hm[2], 2, Gzhi);
+        float gzx_hi = 0.f;
+        if constexpr (NFX > 0) {
+            gzx_hi = (Gzhi[0] < 0.f ? xo[2] : xzU) * Gzhi[0];
         }
         // 5. y-face states of plane z+1 for the neighbours
-        if (hancock_row) {
 #pragma unroll
-            for (int v = 0; v < 5; ++v) {
-                sh.yface[(z + 1) & 1][w][0][v][lane] = hm[1][v];
-                sh.yface[(z + 1) & 1][w][1][v][lane] = hp[1][v];
-            }
-            if constexpr (NFX > 0) {
-                sh.fx.xyface[(z + 1) & 1][w][0][lane] = xo[1];
-                sh.fx.xyface[(z + 1) & 1][w][1][lane] = xo[4];
-            }
+        for (int v = 0; v < 5; ++v) {
+            sh.yface[(z + 1) & 1][w][0][v][lane] = hm[1][v];
+            sh.yface[(z + 1) & 1][w][1][v][lane] = hp[1][v];
+        }
+        if constexpr (NFX > 0) {
+            sh.fx.xyface[(z + 1) & 1][w][0][lane] = xo[1];
+            sh.fx.xyface[(z + 1) & 1][w][1][lane] = xo[4];
         }
         // 6. y-face above this row, plane z
         const bool upd = z >= z0;
-        if (upd && yabove_row) {
+        if (upd) {
             float yL[5], yR[5], G[5];
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
