@@ -308,12 +308,8 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     const double* ring_d = &ring[0][0][0];
     auto tma_issue = [&](int b) {
         __syncwarp(); // the warp is done with the slot's previous box
-        if (lane == 0) {
-            const unsigned sl = (nb0 + (unsigned)b) & 3u;
-            fence_proxy_async_smem();
-            mbar_arrive_expect_tx_s(bar_s + 8u * sl, kTmaBoxBytes);
-            tma_load_3d_s(ring_s + sl * kTmaBoxBytes, tmap, bar_s + 8u * sl, c0 - 2, r0 - 2 + 2 * b, 0);
-        }
+        const unsigned sl = (nb0 + (unsigned)b) & 3u;
+        tma_box_elected(ring_s + sl * kTmaBoxBytes, tmap, bar_s + 8u * sl, kTmaBoxBytes, c0 - 2, r0 - 2 + 2 * b, 0);
     };
     auto tma_wait = [&](int b) {
         const unsigned k = nb0 + (unsigned)b;

@@ -85,6 +85,27 @@ __device__ __forceinline__ void tma_load_3d_s(unsigned dst, const CUtensorMap* m
         "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z)
         : "memory");
 }
+// One box into shared memory by one elected lane of the (converged) warp:
+// expect-tx on the slot's mbarrier and the copy, both predicated on the
+// election, so the warp takes no divergent branch.  The proxy fence orders
+// the warp's earlier generic reads of the slot before the async write.
+__device__ __forceinline__ void tma_box_elected(unsigned dst, const CUtensorMap* map, unsigned bar, unsigned bytes,
+                                                int x, int y, int z)
+{
+    asm volatile(
+        "{\n"
+        " .reg .pred P;\n"
+        " .reg .b32 L;\n"
+        " elect.sync L|P, 0xffffffff;\n"
+        " @P fence.proxy.async.shared::cta;\n"
+        " @P mbarrier.arrive.expect_tx.shared::cta.b64 _, [%2], %3;\n"
+        " @P cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%4, %5, "
+        "%6}], [%2];\n"
+        "}\n" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(bytes), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait_s(unsigned bar, unsigned parity)
 {
     unsigned ok;
