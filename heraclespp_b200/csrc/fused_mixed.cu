@@ -17,7 +17,8 @@ namespace hcl::fused {
 // Cartesian grid, 9 an even ghost width.  7 and 8 are unused (they were
 // paired-column strips, slower than 6 and 9, and were removed).
 // With passive scalars: the tiles,
-// and for one scalar the 4-warp strips 3-6 (2-D) or the column march (3-D).
+// and for one or two scalars the 4-warp strips 3-6 (2-D), for one the column
+// march (3-D).
 // 3-D: 0 shared-memory tiles 8x8x4; 1 column march (uniform Cartesian grids).
 int mixed_shape_count(int ndim)
 {

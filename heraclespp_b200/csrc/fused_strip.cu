@@ -18,10 +18,11 @@ bool strip2d_eligible(const GridDev& g)
     return g.ndim == 2 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM && g.nfx == 0;
 }
 
-// Strips with one passive scalar (schedules 3-6 only).
+// Strips with one or two passive scalars (schedules 3-6 only).
 bool strip2d_fx_eligible(const GridDev& g)
 {
-    return g.ndim == 2 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM && g.nfx == 1;
+    return g.ndim == 2 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM &&
+           (g.nfx == 1 || g.nfx == 2);
 }
 
 // cuTensorMapEncodeTiled from the driver (no link against libcuda), looked
@@ -51,6 +52,13 @@ bool strip2d_tma_eligible(const GridDev& g)
 
 namespace {
 
+// dynamic shared memory of the 4-warp strip kernel with nfx passive scalars
+// (the rings of one scalar are static)
+constexpr int fx_ring_smem(int nfx)
+{
+    return nfx > 1 ? 4 * 8 * (4 + nfx) * 32 * (int)sizeof(double) : 0;
+}
+
 // Resident CTAs of a strip kernel on the current device (`blocks` threads,
 // `smem` bytes of dynamic shared memory, opted in first when non-zero),
 // computed once per device.
@@ -76,11 +84,11 @@ int resident_blocks()
     return resident_on_device(cache, reinterpret_cast<const void*>(k_strip2d<LIM, RS>), 128, 0);
 }
 
-template <int LIM, int RS>
+template <int LIM, int RS, int NFX>
 int resident_blocks_fx()
 {
     static PerDevice cache;
-    return resident_on_device(cache, reinterpret_cast<const void*>(k_strip2d<LIM, RS, 1>), 128, 0);
+    return resident_on_device(cache, reinterpret_cast<const void*>(k_strip2d<LIM, RS, NFX>), 128, fx_ring_smem(NFX));
 }
 
 // Resident CTAs of the in-step strip kernel (one per SM).
@@ -119,14 +127,15 @@ void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCt
                int out_buf, int L, bool sync, bool tma, cudaStream_t s)
 {
     const int ncolw = (g.nx[0] + kStripLanesOut - 1) / kStripLanesOut;
-    const bool fx = g.nfx == 1;
+    const bool fx = g.nfx > 0;
     sync = sync && !fx;
     CUtensorMap map;
     std::memset(&map, 0, sizeof(map));
     tma = tma && sync && strip2d_tma_eligible(g) && encode_strip_map(g, in, &map);
     const int wpb = sync ? kStripSyncWarps : 4;
     const int resident = sync ? (tma ? resident_blocks_sync<LIM, RS, true>() : resident_blocks_sync<LIM, RS, false>())
-                              : (fx ? resident_blocks_fx<LIM, RS>() : resident_blocks<LIM, RS>());
+                              : (fx ? (g.nfx == 2 ? resident_blocks_fx<LIM, RS, 2>() : resident_blocks_fx<LIM, RS, 1>())
+                                    : resident_blocks<LIM, RS>());
     if (L <= 0) {
         const int per_col = std::max(1, resident * wpb / ncolw);
         L = std::max(8, (g.nx[1] + per_col - 1) / per_col);
@@ -140,6 +149,8 @@ void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCt
     } else if (sync) {
         k_strip2d_sync<LIM, RS, false>
             <<<blocks, 32 * kStripSyncWarps, kStripSyncSmem, s>>>(g, in, out, ctl, rp, slot, out_buf, L, map);
+    } else if (fx && g.nfx == 2) {
+        k_strip2d<LIM, RS, 2><<<blocks, 128, fx_ring_smem(2), s>>>(g, in, out, ctl, rp, slot, out_buf, L);
     } else if (fx) {
         k_strip2d<LIM, RS, 1><<<blocks, 128, 0, s>>>(g, in, out, ctl, rp, slot, out_buf, L);
     } else {

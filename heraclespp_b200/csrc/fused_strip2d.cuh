@@ -109,11 +109,11 @@ __device__ __forceinline__ void cons_and_flux(const fast::Eos& e, const float w[
 }
 
 // Hancock face states of one cell: x-left, x-right, y-bottom, y-top (conservative).
-// NFX = 1: also the passive scalar's face values xo[4] (same order, fractions)
-// from its primitives xw = {row below, this row, row above}: limited slopes,
-// times the face density before the predictor, plus the predictor's
-// increment from the face states' mass fluxes, divided by the predicted face
-// density (extrapolation_reconstruction.hpp:315-337, :329-339).
+// NFX > 0: also each passive scalar k's face values xo[4k..4k+3] (same order,
+// fractions) from its primitives xw[3k..3k+2] = {row below, this row, row
+// above}: limited slopes, times the face density before the predictor, plus
+// the predictor's increment from the face states' mass fluxes, divided by the
+// predicted face density (extrapolation_reconstruction.hpp:315-337, :329-339).
 template <int LIM, int NFX = 0>
 __device__ __forceinline__ void strip_hancock(const StripCtx& c, const float wd[4], const float wc[4], const float wu[4],
                                               float hxL[4], float hxR[4], float hyB[4], float hyT[4],
@@ -159,16 +159,21 @@ __device__ __forceinline__ void strip_hancock(const StripCtx& c, const float wd[
         }
     }
     if constexpr (NFX > 0) {
-        const float xl = __shfl_up_sync(0xffffffffu, xw[1], 1);
-        const float xr = __shfl_down_sync(0xffffffffu, xw[1], 1);
-        const float sx = half_lim_fast<LIM>(xr - xw[1], xw[1] - xl);
-        const float sy = half_lim_fast<LIM>(xw[2] - xw[1], xw[1] - xw[0]);
-        const float pf[4] = {xw[1] - sx, xw[1] + sx, xw[1] - sy, xw[1] + sy};
-        const float xinc = fmaf(c.cthx, pf[0] * FxL[0] - pf[1] * FxR[0], c.cthy * (pf[2] * FyB[0] - pf[3] * FyT[0]));
         const float rho_pre[4] = {fxL[0], fxR[0], fyB[0], fyT[0]};
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            xo[f] = __fdividef(fmaf(pf[f], rho_pre[f], xinc), outs[f][0]);
+        for (int k = 0; k < NFX; ++k) {
+            const float* xk = xw + 3 * k;
+            const float xl = __shfl_up_sync(0xffffffffu, xk[1], 1);
+            const float xr = __shfl_down_sync(0xffffffffu, xk[1], 1);
+            const float sx = half_lim_fast<LIM>(xr - xk[1], xk[1] - xl);
+            const float sy = half_lim_fast<LIM>(xk[2] - xk[1], xk[1] - xk[0]);
+            const float pf[4] = {xk[1] - sx, xk[1] + sx, xk[1] - sy, xk[1] + sy};
+            const float xinc =
+                fmaf(c.cthx, pf[0] * FxL[0] - pf[1] * FxR[0], c.cthy * (pf[2] * FyB[0] - pf[3] * FyT[0]));
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                xo[4 * k + f] = __fdividef(fmaf(pf[f], rho_pre[f], xinc), outs[f][0]);
+            }
         }
     }
 }
@@ -229,8 +234,8 @@ constexpr int kStripRingDoubles = 8 * 4 * 32;
 // XIMG: border columns with up to XIMG x images (1: Periodic, Reflexive; 2:
 // also NullGradient with two ghost layers) store them without a divergent
 // branch.
-// NFX = 1: one passive scalar (state plane 4) rides along: face values from
-// strip_hancock, upwind fluxes from the Riemann mass fluxes
+// NFX > 0: the passive scalars (state planes 4..3+NFX) ride along: face
+// values from strip_hancock, upwind fluxes from the Riemann mass fluxes
 // (godunov_scheme.hpp:262-301), the update in FP64 divided by the new density
 // and clamped to [0, 1], stored with the same ghost images.
 // TMA: the ring rows are staged by the Tensor Memory Accelerator (tma_ring.cuh):
@@ -338,13 +343,18 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
     float wB[4], wC[4], wD[4];
     float hxL[4], hxR[4], hyT[4];
     double Glo[4];
-    // passive scalar: primitives of rows r, r+1; face values of row r (x-left,
-    // x-right, y-top); upwind flux of the y-face r-1/2
-    float xC = 0.f, xD = 0.f, xoL = 0.f, xoR = 0.f, xoT = 0.f, gx_lo = 0.f;
+    // passive scalars (index k): primitives of rows r, r+1; face values of
+    // row r (x-left, x-right, y-top); upwind flux of the y-face r-1/2
+    constexpr int NX = NFX > 0 ? NFX : 1;
+    float xC[NX], xD[NX], xoL[NX], xoR[NX], xoT[NX], gx_lo[NX];
+#pragma unroll
+    for (int k = 0; k < NX; ++k) {
+        xC[k] = xD[k] = xoL[k] = xoR[k] = xoT[k] = gx_lo[k] = 0.f;
+    }
     {
         double q[4 + NFX];
         float wA[4], hyB[4];
-        float xA = 0.f, xB = 0.f;
+        float xA[NX], xB[NX];
         if constexpr (TMA) {
             for (int b = 0; b < min(4, nbox); ++b) {
                 tma_issue(b);
@@ -359,27 +369,40 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         }
         ring_row(r0 - 2, q);
         strip_prim(gm1, q, wA);
-        if constexpr (NFX > 0) {
-            xA = (float)q[4];
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            xA[k] = (float)q[4 + k];
         }
         ring_row(r0 - 1, q);
         strip_prim(gm1, q, wB);
-        if constexpr (NFX > 0) {
-            xB = (float)q[4];
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            xB[k] = (float)q[4 + k];
         }
         ring_row(r0, q);
         strip_prim(gm1, q, wC);
-        if constexpr (NFX > 0) {
-            xC = (float)q[4];
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            xC[k] = (float)q[4 + k];
         }
         ring_row(r0 + 1, q);
         strip_prim(gm1, q, wD);
-        if constexpr (NFX > 0) {
-            xD = (float)q[4];
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            xD[k] = (float)q[4 + k];
         }
         float t0[4], t1[4], t2[4], tT[4];
-        const float xw0[3] = {xA, xB, xC}, xw1[3] = {xB, xC, xD};
-        float xo0[4], xo1[4];
+        float xw0[3 * NX], xw1[3 * NX];
+#pragma unroll
+        for (int k = 0; k < NX; ++k) {
+            xw0[3 * k] = xA[k];
+            xw0[3 * k + 1] = xB[k];
+            xw0[3 * k + 2] = xC[k];
+            xw1[3 * k] = xB[k];
+            xw1[3 * k + 1] = xC[k];
+            xw1[3 * k + 2] = xD[k];
+        }
+        float xo0[4 * NX], xo1[4 * NX];
         strip_hancock<LIM, NFX>(c, wA, wB, wC, t0, t1, t2, tT, xw0, xo0); // row r0-1: keep its top face
         strip_hancock<LIM, NFX>(c, wB, wC, wD, hxL, hxR, hyB, hyT, xw1, xo1); // row r0
         float G[4];
@@ -388,11 +411,12 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         for (int v = 0; v < 4; ++v) {
             Glo[v] = (double)G[v];
         }
-        if constexpr (NFX > 0) {
-            gx_lo = (G[0] < 0.f ? xo1[2] : xo0[3]) * G[0];
-            xoL = xo1[0];
-            xoR = xo1[1];
-            xoT = xo1[3];
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            gx_lo[k] = (G[0] < 0.f ? xo1[4 * k + 2] : xo0[4 * k + 3]) * G[0];
+            xoL[k] = xo1[4 * k];
+            xoR[k] = xo1[4 * k + 1];
+            xoT[k] = xo1[4 * k + 3];
         }
     }
     // window: wC = P[r], wD = P[r+1]; ring rows r+3, r+4 in flight.  Two rows
@@ -411,7 +435,7 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         }
         double q[4 + NFX];
         float wN[4];
-        float xN = 0.f;
+        float xN[NX];
         if constexpr (TMA) {
             if ((i & 1) == 0) {
                 tma_wait((i >> 1) + 2); // rows r+2, r+3 landed
@@ -428,14 +452,21 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             double qn2[4 + NFX];
             ring_row(r + 2, qn2);
             strip_prim(gm1, qn2, wN);
-            if constexpr (NFX > 0) {
-                xN = (float)qn2[4];
+#pragma unroll
+            for (int k = 0; k < NFX; ++k) {
+                xN[k] = (float)qn2[4 + k];
             }
         }
         // Hancock of row r+1
         float nxL[4], nxR[4], nyB[4], nyT[4];
-        const float xw[3] = {xC, xD, xN};
-        float nxo[4];
+        float xw[3 * NX];
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            xw[3 * k] = xC[k];
+            xw[3 * k + 1] = xD[k];
+            xw[3 * k + 2] = xN[k];
+        }
+        float nxo[4 * NX];
         strip_hancock<LIM, NFX>(c, wC, wD, wN, nxL, nxR, nyB, nyT, xw, nxo);
         // y-face r+1/2
         float G[4];
@@ -445,10 +476,11 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
         for (int v = 0; v < 4; ++v) {
             Ghi[v] = (double)G[v];
         }
-        float gx_hi = 0.f;
-        if constexpr (NFX > 0) {
+        float gx_hi[NX];
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
             // the upper cell's bottom face when the mass flows down, else the lower cell's top face
-            gx_hi = (G[0] < 0.f ? nxo[2] : xoT) * G[0];
+            gx_hi[k] = (G[0] < 0.f ? nxo[4 * k + 2] : xoT[k]) * G[0];
         }
         // x-faces of row r: left face at this lane, right face from lane+1
         float uL[4], Fl[4];
@@ -463,12 +495,13 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             Fld[v] = (double)Fl[v];
             Frd[v] = __shfl_down_sync(0xffffffffu, Fld[v], 1);
         }
-        float fx_l = 0.f, fx_r = 0.f;
-        if constexpr (NFX > 0) {
+        float fx_l[NX], fx_r[NX];
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
             // left face: this cell's left value when the mass flows left, else the left cell's right value
-            const float up_left = __shfl_up_sync(0xffffffffu, xoR, 1);
-            fx_l = (Fl[0] < 0.f ? xoL : up_left) * Fl[0];
-            fx_r = __shfl_down_sync(0xffffffffu, fx_l, 1);
+            const float up_left = __shfl_up_sync(0xffffffffu, xoR[k], 1);
+            fx_l[k] = (Fl[0] < 0.f ? xoL[k] : up_left) * Fl[0];
+            fx_r[k] = __shfl_down_sync(0xffffffffu, fx_l[k], 1);
         }
         if (out_lane) {
             // Godunov update of row r in FP64 (godunov_scheme.hpp:159-163, 258-260)
@@ -508,19 +541,23 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             for (int v = 0; v < 4; ++v) {
                 qout[oo + plane * v] = qn[v];
             }
-            double xnew = 0.0;
-            if constexpr (NFX > 0) {
-                const double xn = fma(q[4], q[0], fma(cx, (double)fx_l - (double)fx_r, cy * ((double)gx_lo - (double)gx_hi)));
-                xnew = xn / qn[0];
-                xnew = xnew < 0. ? 0. : (xnew > 1. ? 1. : xnew);
-                qout[oo + plane * 4] = xnew;
+            double xnew[NX];
+#pragma unroll
+            for (int k = 0; k < NFX; ++k) {
+                const double xn = fma(q[4 + k], q[0], fma(cx, (double)fx_l[k] - (double)fx_r[k],
+                                                          cy * ((double)gx_lo[k] - (double)gx_hi[k])));
+                double xv = xn / qn[0];
+                xv = xv < 0. ? 0. : (xv > 1. ? 1. : xv);
+                xnew[k] = xv;
+                qout[oo + plane * (4 + k)] = xv;
             }
             const unsigned ym = (r < 2 * g.ng || r >= n1 - 2 * g.ng) ? ghost_mask(r, n1, g.ng, g.bc[2], g.bc[3]) : 0u;
             if (ym != 0u || !x_fast) {
                 if ((xm | ym) != 0u) {
                     store_images_2d(qout, plane, pitch, n0, n1, g.ng, col, r, xm, ym, qn);
-                    if constexpr (NFX > 0) {
-                        store_images_2d_scalar(qout + plane * 4, pitch, n0, n1, g.ng, col, r, xm, ym, xnew);
+#pragma unroll
+                    for (int k = 0; k < NFX; ++k) {
+                        store_images_2d_scalar(qout + plane * (4 + k), pitch, n0, n1, g.ng, col, r, xm, ym, xnew[k]);
                     }
                 }
             } else if (x_any) {
@@ -529,8 +566,9 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
                 qout[og + plane] = x_flip ? -qn[1] : qn[1];
                 qout[og + 2 * plane] = qn[2];
                 qout[og + 3 * plane] = qn[3];
-                if constexpr (NFX > 0) {
-                    qout[og + 4 * plane] = xnew;
+#pragma unroll
+                for (int k = 0; k < NFX; ++k) {
+                    qout[og + (4 + k) * plane] = xnew[k];
                 }
                 if (XIMG > 1 && x_two) {
                     // the second image, or the first again
@@ -542,8 +580,9 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
                     qout[og2 + plane] = fl ? -qn[1] : qn[1];
                     qout[og2 + 2 * plane] = qn[2];
                     qout[og2 + 3 * plane] = qn[3];
-                    if constexpr (NFX > 0) {
-                        qout[og2 + 4 * plane] = xnew;
+#pragma unroll
+                    for (int k = 0; k < NFX; ++k) {
+                        qout[og2 + (4 + k) * plane] = xnew[k];
                     }
                 }
             }
@@ -558,13 +597,14 @@ __device__ __forceinline__ void strip_work(const GridDev& g, const double* __res
             hyT[v] = nyT[v];
             Glo[v] = Ghi[v];
         }
-        if constexpr (NFX > 0) {
-            xC = xD;
-            xD = xN;
-            xoL = nxo[0];
-            xoR = nxo[1];
-            xoT = nxo[3];
-            gx_lo = gx_hi;
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            xC[k] = xD[k];
+            xD[k] = xN[k];
+            xoL[k] = nxo[4 * k];
+            xoR[k] = nxo[4 * k + 1];
+            xoT[k] = nxo[4 * k + 3];
+            gx_lo[k] = gx_hi[k];
         }
         if constexpr (SYNC > 0) {
             if (i % SYNC == SYNC - 1 || i == L - 1) {
@@ -633,10 +673,11 @@ __device__ __forceinline__ void publish_decision(StepCtl* ctl, const Decision& d
     ctl->inv_dt_bits[(slot + 2) % 3] = 0ull;
 }
 
-// NFX = 1: one passive scalar (5-variable rings; three CTAs of 4 warps per SM
-// leave 170 registers for its window).
+// NFX = 1 or 2 passive scalars: (4+NFX)-variable rings; three CTAs of 4 warps
+// per SM leave 170 registers for one scalar's window, two CTAs 255 for two.
+// The rings of NFX = 2 (48 KB) are dynamic shared memory.
 template <int LIM, int RS, int NFX = 0>
-__global__ void __launch_bounds__(128, NFX > 0 ? 3 : 4)
+__global__ void __launch_bounds__(128, NFX > 1 ? 2 : (NFX > 0 ? 3 : 4))
 k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
 {
     const int lane = threadIdx.x & 31;
@@ -659,8 +700,16 @@ k_strip2d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     // grid-stride over the strips (the launcher sizes the grid to the
     // resident warps, so a warp usually takes one or two strips)
     const int wstride = gridDim.x * (blockDim.x >> 5);
-    __shared__ __align__(16) double s_ring[4][8 * (4 + NFX) * 32];
-    const StripRingN<4 + NFX> ring = reinterpret_cast<StripRingN<4 + NFX>>(s_ring[(threadIdx.x >> 5) & 3]);
+    double* ring_mem;
+    if constexpr (NFX > 1) {
+        extern __shared__ __align__(16) double s_ring_dyn[];
+        ring_mem = s_ring_dyn;
+    } else {
+        __shared__ __align__(16) double s_ring[4 * 8 * (4 + NFX) * 32];
+        ring_mem = s_ring;
+    }
+    const StripRingN<4 + NFX> ring =
+        reinterpret_cast<StripRingN<4 + NFX>>(ring_mem + ((threadIdx.x >> 5) & 3) * 8 * (4 + NFX) * 32);
     for (int w = wg; w < nitems; w += wstride) {
         strip_work<LIM, RS, 0, 1, NFX>(g, in.q, out.q, in.plane, in.pitch, dec.dt, w % ncolw, w / ncolw, L, inv_max,
                                        bad_cell, ring);

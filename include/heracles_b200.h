@@ -301,8 +301,8 @@ int hcl_get_dt_log(hcl_handle* h, double* dts, int max_count, int* count);
  * rows staged by the Tensor Memory Accelerator (even ghost width), 10 the same
  * with per-lane cp.async staging.  3-D: 0
  * shared-memory tiles, 1 column march (uniform Cartesian grids).  With
- * passive scalars only the tiles qualify, and for one scalar also 3-6 in
- * 2-D and 1 in 3-D.  Returns the schedule in use through *used (may be NULL; -1 before
+ * passive scalars only the tiles qualify, and for one or two scalars also
+ * 3-6 in 2-D, for one scalar 1 in 3-D.  Returns the schedule in use through *used (may be NULL; -1 before
  * the autotuner ran). */
 int hcl_set_schedule(hcl_handle* h, int schedule, int* used);
 
