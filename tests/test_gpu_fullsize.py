@@ -158,6 +158,26 @@ def test_rt3d_fp64_fused_bitwise(rt):
         assert np.array_equal(got[name], ref), name
 
 
+def test_rt3d_fast64_within_1e12(rt):
+    """Fast FP64 on the 3-D benchmark grid: 3 steps with the oracle's dts,
+    every field within 1e-12 relative L1 (the transverse momenta on the scale
+    of the vertical one)."""
+    from heraclespp_b200 import Domain
+
+    prim, (rho, rhou, E), dts = rt
+    d = Domain(3, RT_NX, precision="fp64_fast", **RT_KW)
+    d.set_state_from_prim(*prim)
+    d.run(nsteps=3, dts=dts)
+    got = fields(*d.get_state())
+    d.close()
+    ref = fields(rho, rhou, E)
+    for name in ("rho", "E", "rhou_2"):
+        assert rel_l1(got[name], ref[name]) < 1e-12, name
+    scale = float(np.sum(np.abs(ref["rhou_2"])))
+    for name in ("rhou_0", "rhou_1"):
+        assert float(np.sum(np.abs(got[name] - ref[name]))) / scale < 1e-12, name
+
+
 def test_rt3d_mixed_column_march_every_field(rt):
     from heraclespp_b200 import Domain
 
