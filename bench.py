@@ -4,9 +4,10 @@
 Workload: 2-D Cartesian KH on [0,1]^2, 2048x2048 cells, periodic, gamma=1.4,
 van Leer slopes, HLLC, CFL 0.4 (synthetic seeded initial state).  A "step" is
 one time step of the whole grid.  The headline arm is the FP32-mixed fused
-step; the plain FP64 fused step is measured in the same run, and the relative
-L1 density error of the mixed result against the FP64 result after the timed
-steps (same dt sequence) is reported.
+step; the plain FP64 and the fast FP64 fused steps are measured in the same
+run, and the relative L1 and L-infinity errors of every stored field of the
+mixed (and fast FP64) result against the FP64 result after the config's 1000
+steps (same dt sequence) are reported.
 
 Metric: Mcell-updates/s = steps x interior cells / time (src/main.cpp:570-581).
 
@@ -80,65 +81,142 @@ def kh_domain(precision):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock, power and clock-event (throttle) reasons of this GPU, sampled
+    from a thread through NVML every millisecond or so (read-only queries),
+    with nvidia-smi every 200 ms where NVML is not importable.  `window(t0, t1)`
+    marks the timed region on the host clock; the summary keeps the samples
+    inside it (the nearest one on each side when the region is shorter than
+    the sampling period)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, pci_bus_id=None):
         self.gpu = gpu_index
-        self.samples = []
+        self.pci = pci_bus_id
+        self.samples = []  # (host time, sm MHz, max sm MHz, power W, set of reasons)
+        self.source = None
+        self._win = None
         self._stop = threading.Event()
         self._t = None
 
-    def _run(self):
+    def _nvml(self):
+        import pynvml as nv
+
+        nv.nvmlInit()
+        h = nv.nvmlDeviceGetHandleByPciBusId(self.pci.encode()) if self.pci else nv.nvmlDeviceGetHandleByIndex(self.gpu)
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        self.source = "nvml"
+        try:
+            while not self._stop.is_set():
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                pw = nv.nvmlDeviceGetPowerUsage(h) * 1e-3
+                self.samples.append((time.perf_counter(), float(sm), float(smax), pw,
+                                     {k for k, b in bits.items() if r & b}))
+                self._stop.wait(0.001)
+        finally:
+            nv.nvmlShutdown()
+
+    def _smi(self):
+        self.source = "nvidia-smi"
+        gid = self.pci if self.pci else str(self.gpu)
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                out = subprocess.run(["nvidia-smi", f"--id={gid}", f"--query-gpu={self.FIELDS}",
                                       "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
                 if out.returncode == 0 and out.stdout.strip():
-                    self.samples.append([s.strip() for s in out.stdout.strip().split(",")])
+                    f = [x.strip() for x in out.stdout.strip().split(",")]
+                    num = lambda x: float(x) if x.replace(".", "").isdigit() else None  # noqa: E731
+                    rs = {nm for k, nm in enumerate(self.REASONS) if len(f) > 5 + k and f[5 + k].lower().startswith("active")}
+                    self.samples.append((time.perf_counter(), num(f[1]), num(f[2]), num(f[3]), rs))
             except Exception:
                 pass
             self._stop.wait(0.2)
 
+    def _run(self):
+        try:
+            import pynvml  # noqa: F401
+        except ImportError:
+            self._smi()
+            return
+        try:
+            self._nvml()
+        except Exception:
+            self._smi()
+
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
+        # let the first samples arrive before the caller's timed region
+        t_end = time.perf_counter() + 0.5
+        while not self.samples and time.perf_counter() < t_end:
+            time.sleep(0.005)
         return self
 
     def __exit__(self, *a):
+        # a few samples after the region, then stop
+        time.sleep(0.01)
         self._stop.set()
         self._t.join(timeout=10)
 
+    def window(self, t0, t1):
+        self._win = (t0, t1)
+
     def summary(self):
-        if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        smax = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for s in self.samples:
-            for k, nm in enumerate(names):
-                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
-                    reasons.add(nm)
+        samples = list(self.samples)
+        if self._win is not None and samples:
+            t0, t1 = self._win
+            inside = [s for s in samples if t0 <= s[0] <= t1]
+            if not inside:
+                before = [s for s in samples if s[0] < t0][-1:]
+                after = [s for s in samples if s[0] > t1][:1]
+                inside = before + after
+            samples = inside
+        if not samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0,
+                    "source": self.source}
+        sm = [s[1] for s in samples if s[1] is not None]
+        smax = [s[2] for s in samples if s[2] is not None]
+        pw = [s[3] for s in samples if s[3] is not None]
+        reasons = set().union(*[s[4] for s in samples])
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+                "power_w_median": round(float(np.median(pw)), 1) if pw else None,
+                "reasons": sorted(reasons), "samples": len(samples), "source": self.source}
 
 
-def time_fused(torch, d, steps, warmup):
+def pci_bus_id(torch, dev):
+    """NVML's PCI bus id string of a CUDA device (the same GPU whatever
+    CUDA_VISIBLE_DEVICES renumbers)."""
+    try:
+        p = torch.cuda.get_device_properties(dev)
+        return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+    except Exception:
+        return None
+
+
+def time_fused(torch, d, steps, warmup, clk=None):
     """Device time of `steps` fused steps (CUDA events on the library's stream)."""
     stream = torch.cuda.ExternalStream(d.stream_handle())
     d.run(cfl=0.4, nsteps=warmup)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
     e0.record(stream)
     r = d.run(cfl=0.4, nsteps=steps)
     e1.record(stream)
     e1.synchronize()
+    t1 = time.perf_counter()
     torch.cuda.synchronize()
+    if clk is not None:
+        clk.window(t0, t1)
     return e0.elapsed_time(e1) * 1e-3, r
 
 
@@ -569,8 +647,8 @@ def run_ours(args):
         import torch.distributed as dist
 
         dist.barrier()
-    with ClockSampler(int(os.environ.get("HCL_NVSMI_INDEX", dev_index))) as clk:
-        el_mixed, r_mixed = time_fused(torch, d, args.steps, args.warmup)
+    with ClockSampler(int(os.environ.get("HCL_NVSMI_INDEX", dev_index)), pci_bus_id(torch, dev_index)) as clk:
+        el_mixed, r_mixed = time_fused(torch, d, args.steps, args.warmup, clk)
     launches = hb.kernel_launch_count() - launches0 - args.warmup
 
     # ---- FP64 fused step, same workload ---------------------------------------

@@ -24,3 +24,24 @@ def test_reference_arm_json_line():
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_clock_summary_keeps_the_timed_window():
+    """The clock record keeps the samples taken inside the timed region, or
+    the nearest one on each side of a region shorter than the sampling
+    period, and unions the throttle reasons seen there."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    c = bench.ClockSampler(0)
+    c.source = "test"
+    c.samples = [(0.0, 1000.0, 1965.0, 300.0, set()), (1.0, 1965.0, 1965.0, 900.0, {"sw_power_cap"}),
+                 (1.5, 1950.0, 1965.0, 950.0, set()), (3.0, 800.0, 1965.0, 200.0, {"hw_slowdown"})]
+    c.window(0.9, 1.6)
+    s = c.summary()
+    assert s["samples"] == 2 and s["sm_mhz"] == 1957.5 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"]
+    c.window(1.6, 1.7)  # no sample inside: the neighbours on both sides
+    s = c.summary()
+    assert s["samples"] == 2 and s["reasons"] == ["hw_slowdown"] and s["sm_mhz"] == 1375.0
+    assert bench.ClockSampler(0).summary()["reasons"] == ["unsampled"]
