@@ -159,10 +159,15 @@ HCL_HD R limiter(int lim, R dR, R dL, R* gR, R* gL)
         return R(0);
     }
     if (lim == 1) { // van Leer: 2RL/(R+L)
+        // partials 2 (L/(R+L))^2 and 2 (R/(R+L))^2, formed from the ratios
+        // (each in (0, 1) when RL > 0) so that tiny differences neither
+        // overflow 1/(R+L)^2 nor underflow L^2 into 0 * inf
         const R s = dR + dL;
         const R is = R(1) / s;
-        *gR = R(2) * dL * dL * is * is;
-        *gL = R(2) * dR * dR * is * is;
+        const R a = dL * is;
+        const R b = dR * is;
+        *gR = R(2) * a * a;
+        *gL = R(2) * b * b;
         return R(2) * prod * is;
     }
     if (lim == 2) { // minmod
@@ -173,12 +178,20 @@ HCL_HD R limiter(int lim, R dR, R dL, R* gR, R* gL)
         *gL = R(1);
         return dL;
     }
-    // van Albada: RL(R+L)/(R^2+L^2)
+    // van Albada: RL(R+L)/(R^2+L^2).  Its partials
+    // L^2 (L^2 + 2RL - R^2) / (R^2+L^2)^2 and R^2 (R^2 + 2RL - L^2) / (R^2+L^2)^2
+    // are homogeneous of degree 0: formed from R and L scaled by
+    // 1/max(|R|, |L|), so that tiny differences do not overflow them
     const R N = prod * (dR + dL);
     const R D = dR * dR + dL * dL;
     const R iD = R(1) / D;
-    *gR = ((R(2) * dR * dL + dL * dL) * D - N * R(2) * dR) * iD * iD;
-    *gL = ((R(2) * dR * dL + dR * dR) * D - N * R(2) * dL) * iD * iD;
+    const R im = R(1) / std::fmax(std::fabs(dR), std::fabs(dL));
+    const R r = dR * im;
+    const R l = dL * im;
+    const R d = r * r + l * l;
+    const R id2 = R(1) / (d * d);
+    *gR = l * l * (l * l + R(2) * r * l - r * r) * id2;
+    *gL = r * r * (r * r + R(2) * r * l - l * l) * id2;
     return N * iD;
 }
 

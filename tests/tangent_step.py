@@ -70,6 +70,49 @@ class _Sqrt(torch.autograd.Function):
         return t / (2 * s)
 
 
+class _Limited(torch.autograd.Function):
+    """The reference's limited slope phi(R, L) (slope_limiters.hpp:38-66,
+    value bit for bit) with the tangent of the branch it took, from the
+    closed-form partials: van Leer 2RL/(R+L) has 2 (L/(R+L))^2 and
+    2 (R/(R+L))^2, minmod takes R where R/L < 1 and L otherwise, and the
+    slope is 0 (tangent 0) unless R*L > 0.  Differentiating the reference's
+    ratio form instead overflows for tiny L ((R/L + 1)^2 = inf), which gives
+    NaN tangents in nearly flat regions."""
+
+    @staticmethod
+    def forward(R, L, kind):
+        cond = L * R > 0
+        Ls = torch.where(cond, L, torch.ones_like(L))
+        ratio = R / Ls
+        if kind == 0:
+            val = (1.0 / 2) * (R + L) * (4 * ratio) / ((ratio + 1) * (ratio + 1))
+        else:
+            # fmin(1, ratio) with ratio == 1 on the constant branch (slope L)
+            val = 2 * torch.where(ratio < 1, ratio, torch.ones_like(ratio)) / (1 + ratio) * (L + R) / 2
+        return torch.where(cond, val, torch.zeros_like(val))
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        R, L, kind = inputs
+        ctx.kind = kind
+        ctx.save_for_forward(R, L)
+
+    @staticmethod
+    def jvp(ctx, Rt, Lt, _kind_t):
+        R, L = ctx.saved_tensors
+        cond = L * R > 0
+        one = torch.ones_like(R)
+        if ctx.kind == 0:
+            s = torch.where(cond, R + L, one)
+            a = L / s
+            b = R / s
+            t = 2 * a * a * Rt + 2 * b * b * Lt
+        else:
+            ratio = R / torch.where(cond, L, one)
+            t = torch.where(ratio < 1, Rt, Lt)
+        return torch.where(cond, t, torch.zeros_like(t))
+
+
 def _min(a, b):
     return torch.where(a < b, a, b)
 
@@ -137,16 +180,7 @@ class TangentStep:
 
     # ---- slopes (slope_limiters.hpp:38-66) ----------------------------------
     def slope(self, R, L):
-        cond = L * R > 0
-        Ls = torch.where(cond, L, torch.ones_like(L))
-        ratio = R / Ls
-        if self.limiter == "VanLeer":
-            val = (1.0 / 2) * (R + L) * (4 * ratio) / ((ratio + 1) * (ratio + 1))
-        else:
-            # fmin(1, ratio): at ratio == 1 the adjoint differentiates the
-            # slope as L, which is the constant branch
-            val = 2 * torch.where(ratio < 1, ratio, torch.ones_like(ratio)) / (1 + ratio) * (L + R) / 2
-        return torch.where(cond, val, torch.zeros_like(val))
+        return _Limited.apply(R, L, 0 if self.limiter == "VanLeer" else 1)
 
     def faces(self, q, d):
         """(minus face, plus face) of q along d (limited_linear_reconstruction.hpp:46-64)."""

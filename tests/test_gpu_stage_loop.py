@@ -112,6 +112,23 @@ def test_stage_loop_matches_oracle_bitwise(ndim, nx, nfx, pf, eps, steps, fails,
     assert d.conservation_sums()[0] == pytest.approx(o.integrate(rho), rel=1e-14)
 
 
+def sheared_layers(o, lo, uy=0.1, seed=5):
+    """2-D flow that varies along x only, with a transverse velocity u_y(x)
+    and pressure 10^U(lo, -1) per column.  The 2-D pressure fix (with the
+    reference's cross terms) acts on it without driving an internal energy
+    negative, which it does on the fully 2-D low-energy flow."""
+    rng = np.random.default_rng(seed)
+    grid = setups.Grid.from_domain(o)
+    rho, u, P = grid.alloc()
+    s3, (X, Y, Z), _ = grid.interior()
+    shape = rho[s3].shape
+    rho[s3] = np.broadcast_to(1.0 + 0.2 * np.sin(2 * np.pi * X), shape)
+    u[0][s3] = np.broadcast_to(1.0 + 0.5 * np.sin(4 * np.pi * X), shape)
+    u[1][s3] = np.broadcast_to(uy * np.cos(2 * np.pi * X), shape)
+    P[s3] = np.broadcast_to(10.0 ** rng.uniform(lo, -1, (1, 1, shape[-1])), shape)
+    return rho, u, P
+
+
 @pytest.mark.parametrize("ndim,nx,nfx,eps", [(1, [200], 0, 3e-3), (1, [200], 1, 3e-3), (2, [36, 28], 1, 3e-3)])
 def test_mixed_pressure_fix_in_fused_tiles(ndim, nx, nfx, eps):
     """FP32-mixed handles with the pressure fix run the fused tile kernel
@@ -122,7 +139,8 @@ def test_mixed_pressure_fix_in_fused_tiles(ndim, nx, nfx, eps):
     kw = dict(gamma=1.4, limiter="Minmod", riemann="HLLC", bc=bc)
     o = Oracle(ndim, nx, nfx=nfx, **kw)
     d = Domain(ndim, nx, nfx=nfx, pressure_fix=True, eps_pf=eps, precision="fp32_mixed", **kw)
-    rho, rhou, E, fx = o.init_from_prim(*smooth_low_energy(o, -2.5))
+    prim = smooth_low_energy(o, -3) if ndim == 1 else sheared_layers(o, -3)
+    rho, rhou, E, fx = o.init_from_prim(*prim)
     if nfx:
         grid = setups.Grid.from_domain(o)
         s3, (X, Y, Z), _ = grid.interior()
@@ -131,14 +149,18 @@ def test_mixed_pressure_fix_in_fused_tiles(ndim, nx, nfx, eps):
     d.set_state(rho, rhou, E, fx=fx if nfx else None)
     steps = 30
     r = d.run(cfl=0.4, max_iter=steps)
-    assert r.iter == steps
+    assert r.iter == steps and r.status == 0
     if ndim == 2:
         assert d.schedule() in (0, 1, 2)
     dts = d.dt_log()[:steps]
     ref = [a.copy() for a in (rho, rhou, E, fx)]
-    o.run(rho, rhou, E, fx, dts=dts, max_iter=steps, pressure_fix=True, eps_pf=eps)
+    t_o, it_o, st_o, _ = o.run(rho, rhou, E, fx, dts=dts, max_iter=steps, pressure_fix=True, eps_pf=eps)
+    assert st_o == 0 and it_o == steps
     o.run(*ref, dts=dts, max_iter=steps)
     r_d, m_d, E_d = d.get_state()
     rel = lambda a, b: float(np.abs(a - b).sum() / np.abs(b).sum())  # noqa: E731
+    print(f"mixed vs oracle with the fix: rho {rel(r_d, rho):.2e} E {rel(E_d, E):.2e}; "
+          f"oracle without the fix: E {rel(ref[2], E):.2e}")
+    assert rel(ref[2], E) > 1e-4  # the fix acts
     assert rel(r_d, rho) < 1e-5 and rel(E_d, E) < 1e-5
     assert rel(E_d, E) < 0.1 * rel(ref[2], E)
