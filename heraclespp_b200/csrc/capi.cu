@@ -1576,6 +1576,25 @@ int hcl_run(hcl_handle* h, const hcl_run_params* p, hcl_run_result* r)
     }
     const int K = p->graph_chunk > 0 ? (p->graph_chunk + 5) / 6 * 6 : 60;
     const int shape = h->mixed_shape < 0 ? 0 : h->mixed_shape;
+    // A run of a fixed step count replays the largest of these graphs that
+    // fits, again and again, then launches the last < 6 steps singly.  All of
+    // them are built (captured once per run parameters) on the first such
+    // call, so that later calls of any step count replay graphs only.
+    int sizes[4] = {K, 24, 12, 6};
+    int nsizes = 1;
+    for (int i = 1; i < 4; ++i) {
+        if (sizes[i] < K) {
+            sizes[nsizes++] = sizes[i];
+        }
+    }
+    if (nsteps > 0) {
+        for (int i = 0; i < nsizes; ++i) {
+            cudaGraphExec_t exec;
+            if ((rc = get_graph(h, rp, sizes[i], &exec))) {
+                return rc;
+            }
+        }
+    }
 
     auto single = [&]() {
         launch_step(h, rp, h->counter, h->ctl, (int)(h->counter & 1), shape, h->stream);
@@ -1590,15 +1609,21 @@ int hcl_run(hcl_handle* h, const hcl_run_params* p, hcl_run_result* r)
             ++done;
         }
         const int remaining = nsteps > 0 ? nsteps - done : K;
-        if (remaining >= K) {
+        int chunk = 0;
+        for (int i = 0; i < nsizes && chunk == 0; ++i) {
+            if (remaining >= sizes[i]) {
+                chunk = sizes[i];
+            }
+        }
+        if (chunk > 0) {
             cudaGraphExec_t exec;
-            if ((rc = get_graph(h, rp, K, &exec))) {
+            if ((rc = get_graph(h, rp, chunk, &exec))) {
                 return rc;
             }
             HCL_CUDA(cudaGraphLaunch(exec, h->stream));
-            hcl::g_launches += K;
-            h->counter += K;
-            done += K;
+            hcl::g_launches += chunk;
+            h->counter += chunk;
+            done += chunk;
         } else {
             while (done < nsteps) {
                 single();

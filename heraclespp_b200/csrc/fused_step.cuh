@@ -29,6 +29,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <type_traits>
 
 #include "hcl_device.cuh"
@@ -36,6 +37,7 @@
 #include "physics_exact.cuh"
 #include "physics_fast.cuh"
 #include "stages.hpp"
+#include "tma_ring.cuh"
 
 namespace hcl::fused {
 
@@ -331,9 +333,14 @@ constexpr int fused_min_blocks()
     return (EXACT && ND == 2) ? 3 : 0;
 }
 
+// tma (2-D and 3-D): the FP64 tile plus its halo arrives as one tensor box
+// ({L0, L1, L2, NV} of `tmap`, the input state's hydro planes) issued by one
+// thread into the face buffer, which phase 2 overwrites only after phase 1
+// has read it; otherwise every thread loads its cells directly.
 template <int ND, bool EXACT, int TX, int TY, int TZ, int EOSK>
 __device__ __forceinline__ void fused_step_body(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl,
-                                                const RunParamsDev& rp, int slot, int out_buf)
+                                                const RunParamsDev& rp, int slot, int out_buf,
+                                                const CUtensorMap* tmap = nullptr, int tma = 0)
 {
     using S = Shape<ND, TX, TY, TZ>;
     using R = std::conditional_t<EXACT, double, float>;
@@ -413,6 +420,43 @@ __device__ __forceinline__ void fused_step_body(const GridDev& g, const StateDev
     const fast::Eos feos{(float)g.gamma, (float)g.gamma_m1, (float)(1.0 / g.gamma_m1)};
 
     // ---- phase 1: state tile + halo -> primitives --------------------------
+    // The box lands at the first 128-byte boundary of the face buffer (the
+    // alignment a tensor copy's shared-memory destination needs; the dynamic
+    // shared memory itself starts after the kernel's static shared memory).
+    static_assert(NV * S::NP * sizeof(double) + 128 <= (S::A_TOTAL + S::F_TOTAL) * sizeof(R),
+                  "the staged box fits the face and flux buffers");
+    const unsigned sa_s = smem_u32(sa);
+    double* stage = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(sa) + ((128u - (sa_s & 127u)) & 127u));
+    bool staged = false;
+    if constexpr (ND >= 2) {
+        // uniform over the CTA: the destination and the box's x origin are
+        // aligned as a tensor copy needs them, else the direct loads run
+        const bool aligned = (smem_u32(stage) & 127u) == 0u && ((gorg[0] - 2) & 1) == 0;
+        if (tma && aligned) {
+            __shared__ uint64_t tile_bar;
+            if (tid == 0) {
+                mbar_init(&tile_bar, 1);
+                mbar_init_fence();
+            }
+            __syncthreads();
+            if (tid == 0) {
+                mbar_arrive_expect_tx(&tile_bar, (unsigned)(NV * S::NP * sizeof(double)));
+                if constexpr (ND == 2) {
+                    tma_load_3d(stage, tmap, &tile_bar, gorg[0] - 2, gorg[1] - 2, 0);
+                } else {
+                    tma_load_4d(stage, tmap, &tile_bar, gorg[0] - 2, gorg[1] - 2, gorg[2] - 2, 0);
+                }
+            }
+            staged = true;
+            const bool arrived = mbar_wait_bounded(&tile_bar, 0);
+            if (__syncthreads_or(!arrived) && tid == 0) {
+                // the box never arrived: stop the run with HCL_ERR_TIMEOUT
+                ctl->err = 6;
+                ctl->errflag[(slot + 1) & 1] = 1;
+                ctl->final_buf = out_buf;
+            }
+        }
+    }
     for (int p = tid; p < S::NP; p += NT) {
         const int lx = p % S::L0;
         const int ly = (p / S::L0) % S::L1;
@@ -422,9 +466,21 @@ __device__ __forceinline__ void fused_step_body(const GridDev& g, const StateDev
         const int gk = ND >= 3 ? min(max(gorg[2] - 2 + lz, 0), g.n[2] - 1) : 0;
         const int64_t o = sidx(in, g.n[1], gi, gj, gk);
         double q[NV];
+        if (staged) {
+            // the box slot of the same (clamped) cell: cells past the array's
+            // end repeat its last cell, as the direct loads do (the box's
+            // origin is never below 0)
+            const int bp = (gi - (gorg[0] - 2)) +
+                           S::L0 * ((ND >= 2 ? gj - (gorg[1] - 2) : 0) + S::L1 * (ND >= 3 ? gk - (gorg[2] - 2) : 0));
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            q[v] = __ldg(in.q + o + in.plane * v);
+            for (int v = 0; v < NV; ++v) {
+                q[v] = stage[v * S::NP + bp];
+            }
+        } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                q[v] = __ldg(in.q + o + in.plane * v);
+            }
         }
         if constexpr (EXACT) {
             double pr[NV];
@@ -1316,18 +1372,20 @@ __device__ __forceinline__ void fused_step_body(const GridDev& g, const StateDev
 
 template <int ND, bool EXACT, int TX, int TY, int TZ, int EOSK = EOS_PERFECT_GAS>
 __global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1))
-k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf)
+k_fused_step(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf,
+             const __grid_constant__ CUtensorMap tmap, int tma)
 {
-    fused_step_body<ND, EXACT, TX, TY, TZ, EOSK>(g, in, out, ctl, rp, slot, out_buf);
+    fused_step_body<ND, EXACT, TX, TY, TZ, EOSK>(g, in, out, ctl, rp, slot, out_buf, &tmap, tma);
 }
 
 // the same step with the occupancy bound above (instantiated where it is > 0)
 template <int ND, bool EXACT, int TX, int TY, int TZ, int EOSK = EOS_PERFECT_GAS>
 __global__ void __launch_bounds__(TX*(ND >= 2 ? TY : 1)*(ND >= 3 ? TZ : 1),
                                   fused_min_blocks<ND, EXACT, TX, TY, TZ>() > 0 ? fused_min_blocks<ND, EXACT, TX, TY, TZ>() : 1)
-k_fused_step_occ(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf)
+k_fused_step_occ(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf,
+                 const __grid_constant__ CUtensorMap tmap, int tma)
 {
-    fused_step_body<ND, EXACT, TX, TY, TZ, EOSK>(g, in, out, ctl, rp, slot, out_buf);
+    fused_step_body<ND, EXACT, TX, TY, TZ, EOSK>(g, in, out, ctl, rp, slot, out_buf, &tmap, tma);
 }
 
 template <int ND, bool EXACT, int TX, int TY, int TZ>
@@ -1360,7 +1418,7 @@ struct FusedLauncher {
         }
     }
     // the occupancy-bounded kernel pays off when that many CTAs fit the SM's
-    // shared memory (1 KB reserved per CTA, 256 B static)
+    // shared memory (1 KB reserved per CTA, up to 512 B static)
     static bool use_occ(int nfx)
     {
         if constexpr (kMinBlocks > 0) {
@@ -1372,7 +1430,7 @@ struct FusedLauncher {
                 cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
                 return v;
             });
-            return (size_t)kMinBlocks * (smem(nfx) + 1024 + 256) <= (size_t)per_sm;
+            return (size_t)kMinBlocks * (smem(nfx) + 1024 + 512) <= (size_t)per_sm;
         }
         return false;
     }
@@ -1397,10 +1455,18 @@ struct FusedLauncher {
         const int nt1 = (g.nx[1] + S::T1 - 1) / S::T1;
         const int nt2 = (g.nx[2] + S::T2 - 1) / S::T2;
         const int blocks = nt0 * nt1 * nt2;
+        // the tile + halo box of the input state for TMA staging (2-D and 3-D;
+        // its x origin gorg[0] - 2 = ng - 2 + T0 k is 16-byte aligned for an
+        // even ghost width)
+        CUtensorMap map;
+        std::memset(&map, 0, sizeof(map));
+        const int box[3] = {S::L0, S::L1, S::L2};
+        const int tma = (ND >= 2 && g.ng % 2 == 0 && encode_tile_map(g, in, S::NV, box, &map)) ? 1 : 0;
         if (use_occ(g.nfx)) {
-            k_fused_step_occ<ND, EXACT, TX, TY, TZ, EOSK><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot, out_buf);
+            k_fused_step_occ<ND, EXACT, TX, TY, TZ, EOSK>
+                <<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot, out_buf, map, tma);
         } else {
-            k_fused_step<ND, EXACT, TX, TY, TZ, EOSK><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot, out_buf);
+            k_fused_step<ND, EXACT, TX, TY, TZ, EOSK><<<blocks, S::TVOL, sm, s>>>(g, in, out, ctl, rp, slot, out_buf, map, tma);
         }
         ++g_launches;
     }

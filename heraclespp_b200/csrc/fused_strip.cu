@@ -50,6 +50,34 @@ bool strip2d_tma_eligible(const GridDev& g)
     return strip2d_eligible(g) && g.ng % 2 == 0 && tensor_map_encoder() != nullptr;
 }
 
+bool encode_tile_map(const GridDev& g, const StateDev& st, int nv, const int box[3], CUtensorMap* map)
+{
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || g.ndim < 2 || (reinterpret_cast<uintptr_t>(st.q) & 15u) != 0 || (st.pitch * sizeof(double)) % 16 != 0 ||
+        (st.plane * sizeof(double)) % 16 != 0) {
+        return false;
+    }
+    const int rank = g.ndim + 1;
+    cuuint64_t dims[4], strides[3];
+    cuuint32_t bx[4], estr[4] = {1, 1, 1, 1};
+    dims[0] = (cuuint64_t)g.n[0];
+    dims[1] = (cuuint64_t)g.n[1];
+    bx[0] = (cuuint32_t)box[0];
+    bx[1] = (cuuint32_t)box[1];
+    strides[0] = (cuuint64_t)st.pitch * sizeof(double);
+    if (g.ndim == 3) {
+        dims[2] = (cuuint64_t)g.n[2];
+        bx[2] = (cuuint32_t)box[2];
+        strides[1] = (cuuint64_t)st.pitch * g.n[1] * sizeof(double);
+    }
+    dims[rank - 1] = (cuuint64_t)nv;
+    bx[rank - 1] = (cuuint32_t)nv;
+    strides[rank - 2] = (cuuint64_t)st.plane * sizeof(double);
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank, st.q, dims, strides, bx, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 namespace {
 
 // dynamic shared memory of the 4-warp strip kernel with nfx passive scalars

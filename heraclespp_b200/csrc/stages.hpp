@@ -2,6 +2,7 @@
 // step, shared between the translation units of the library.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -108,6 +109,11 @@ void step_strip3d(const GridDev& g, const StateDev& in, const StateDev& out, Ste
 void step_strip2d(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp,
                   int slot, int out_buf, int L, bool sync, bool tma, cudaStream_t s);
 bool strip2d_tma_eligible(const GridDev& g);
+// Tiled tensor map of a state's first nv planes for the fused tile kernels'
+// TMA staging: dims n0 x n1 (x n2) x nv, box {box[0], box[1], (box[2]), nv}
+// (2-D and 3-D).  False where the driver offers no encoder, or the base or a
+// stride is not a multiple of 16 bytes.
+bool encode_tile_map(const GridDev& g, const StateDev& st, int nv, const int box[3], CUtensorMap* map);
 void configure_exact();
 void configure_mixed();
 int conservation_partials_doubles(int ndim);

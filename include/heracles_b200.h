@@ -257,7 +257,11 @@ typedef struct hcl_run_params {
     double time_frequency;    /* [Output] time_frequency (0 = off): dt is clamped to output times */
     double time_first_output; /* [Output] time_first_output */
     int nsteps;               /* steps to take in this call (<= 0: until t_end / max_iter) */
-    int graph_chunk;          /* steps per CUDA-graph replay (0 = default) */
+    int graph_chunk;          /* steps per CUDA-graph replay (0 = 60; rounded up to a multiple
+                                 of 6).  A run of a fixed step count replays that graph and,
+                                 for its remainder, graphs of 24, 12 and 6 steps (all captured
+                                 on the handle's first fixed-count run), then launches the last
+                                 < 6 steps singly */
     int fixed_dt;             /* 1: use dts[] (host, one per step) instead of the CFL dt */
     const double* dts;
 } hcl_run_params;

@@ -85,4 +85,9 @@ double t_limiter(int lim, double R, double L, double* gR, double* gL)
     return limiter<double>(lim, R, L, gR, gL);
 }
 
+double t_limiter_on(int lim, int active, double R, double L, double* gR, double* gL)
+{
+    return limiter_on<double>(lim, active != 0, R, L, gR, gL);
+}
+
 } // extern "C"

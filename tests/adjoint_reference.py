@@ -14,6 +14,8 @@ from pathlib import Path
 import numpy as np
 
 NG = 2
+KB = 1.380649e-23  # units.hpp: Boltzmann constant
+MP = 1.672649e-27  # units.hpp: proton mass
 ROOT = Path(__file__).resolve().parents[1]
 
 
@@ -34,6 +36,8 @@ def build_cell_lib(out):
     L.t_c2p_rev.argtypes = [d, vp, vp, vp]
     L.t_limiter.argtypes = [i, d, d, C.POINTER(d), C.POINTER(d)]
     L.t_limiter.restype = d
+    L.t_limiter_on.argtypes = [i, i, d, d, C.POINTER(d), C.POINTER(d)]
+    L.t_limiter_on.restype = d
     return L
 
 
@@ -67,12 +71,17 @@ class Ref:
         self.g = gamma
         self.lim = lim
         self.solver = solver
+        self.dx = (1.0, 1.0)  # cell spacing of the step being evaluated
 
     # ---- per-cell wrappers -----------------------------------------------
     def c2p(self, U):
-        W = np.zeros(4)
-        self.L.t_c2p_fwd(self.g, p(U), W.ctypes.data_as(C.c_void_p))
-        return W
+        """Primitives rounded as the forward FP64 step rounds them (the
+        perfect gas's temperature round trip, mmw = 1), which is where the
+        FP64 sweep takes its branch decisions from."""
+        rho, m0, m1, E = (float(x) for x in U)
+        ek = (m0 * m0 + m1 * m1) / rho / 2
+        T = (E - ek) * MP * (self.g - 1.0) / (rho * KB)
+        return np.array([rho, m0 / rho, m1 / rho, rho * KB * T / MP])
 
     def c2p_rev(self, U, Wb):
         Ub = np.zeros(4)
@@ -110,9 +119,17 @@ class Ref:
                              b.ctypes.data_as(C.c_void_p))
         return a, b
 
-    def limiter(self, R, L):
+    def limiter(self, R, L, dx=None):
+        """phi(R, L) of raw differences and its partials.  With the cell
+        spacing dx the branch is the forward step's: the sign of
+        (R/dx)*(L/dx), as it forms the limiter's arguments (the raw product
+        can underflow to 0 where that one does not)."""
         gR, gL = C.c_double(), C.c_double()
-        phi = self.L.t_limiter(self.lim, float(R), float(L), C.byref(gR), C.byref(gL))
+        if dx is None:
+            phi = self.L.t_limiter(self.lim, float(R), float(L), C.byref(gR), C.byref(gL))
+        else:
+            active = 1 if (float(L) / dx) * (float(R) / dx) > 0 else 0
+            phi = self.L.t_limiter_on(self.lim, active, float(R), float(L), C.byref(gR), C.byref(gL))
         return phi, gR.value, gL.value
 
     # ---- grid helpers ------------------------------------------------------
@@ -146,7 +163,7 @@ class Ref:
             fl = np.zeros(4)
             fr = np.zeros(4)
             for v in range(4):
-                phi, _, _ = self.limiter(W[v, j + dj, i + di] - wc[v], wc[v] - W[v, j - dj, i - di])
+                phi, _, _ = self.limiter(W[v, j + dj, i + di] - wc[v], wc[v] - W[v, j - dj, i - di], self.dx[d])
                 fl[v] = wc[v] - 0.5 * phi
                 fr[v] = wc[v] + 0.5 * phi
             fp[(0, d)] = fl
@@ -160,6 +177,7 @@ class Ref:
         return H, fp
 
     def step(self, U, dt, dx):
+        self.dx = dx
         n1, n0 = U.shape[1] - 2 * NG, U.shape[2] - 2 * NG
         cth = [0.5 * dt / dx[0], 0.5 * dt / dx[1]]
         W = np.zeros_like(U)
@@ -185,6 +203,7 @@ class Ref:
     def step_adjoint(self, U, lam_out, dt, dx):
         """lam_out: adjoint of the interior outputs (ghost entries ignored).
         Returns the adjoint of the full input U (ghost entries folded)."""
+        self.dx = dx
         n1, n0 = U.shape[1] - 2 * NG, U.shape[2] - 2 * NG
         cth = [0.5 * dt / dx[0], 0.5 * dt / dx[1]]
         c = [dt / dx[0], dt / dx[1]]
@@ -226,7 +245,7 @@ class Ref:
             for d, (dj, di) in enumerate(((0, 1), (1, 0))):
                 for v in range(4):
                     wc = W[v, j, i]
-                    _, gR, gL = self.limiter(W[v, j + dj, i + di] - wc, wc - W[v, j - dj, i - di])
+                    _, gR, gL = self.limiter(W[v, j + dj, i + di] - wc, wc - W[v, j - dj, i - di], self.dx[d])
                     phib = 0.5 * (fpb[(1, d)][v] - fpb[(0, d)][v])
                     Wb[v, j, i] += fpb[(0, d)][v] + fpb[(1, d)][v] - phib * gR + phib * gL
                     Wb[v, j + dj, i + di] += phib * gR

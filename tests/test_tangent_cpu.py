@@ -112,3 +112,36 @@ def test_dot_product_against_loop_adjoint(cell_lib, lim, solver, rs):
         tl = float(np.sum(lam[:, NG:NG + n, NG:NG + n] * JV.numpy()))
         ad = float(np.sum(g[:, NG:NG + n, NG:NG + n] * v))
         assert ad == pytest.approx(tl, rel=1e-11, abs=1e-13)
+
+
+@pytest.mark.parametrize("steps", [15, 23, 30])
+def test_dot_product_on_plain_gresho(cell_lib, steps):
+    """One step from the plain Gresho vortex (64^2) after some oracle steps,
+    where flat and solid-body regions leave slope differences at rounding
+    level: the loop reference adjoint takes its primitives with the forward's
+    rounding and each limiter's branch from the forward's test on the
+    differences divided by the spacing (after 15 and 23 steps a raw product
+    underflows to 0 where that one is a positive subnormal), as the FP64
+    sweep does, so <J v, lambda> = <v, J^T lambda> to rounding."""
+    from heraclespp_b200 import setups
+
+    n, g = 64, 5.0 / 3.0
+    o = Oracle(2, [n, n], gamma=g, limiter="VanLeer", riemann="HLLC", bc=["Periodic"] * 4)
+    rho, rhou, E, _ = o.init_from_prim(*setups.gresho_vortex(setups.Grid.from_domain(o)))
+    o.run(rho, rhou, E, max_iter=steps)
+    *_, dts = o.run(*[a.copy() for a in (rho, rhou, E)], max_iter=1, record_dts=True)
+    dt = float(dts[0])
+    U = np.concatenate([rho[None], rhou, E[None]])[:, 0]
+    ref = Ref(cell_lib, gamma=g, lim=1, solver=1)
+    rng = np.random.default_rng(steps)
+    lam = np.zeros_like(U)
+    lam[:, NG:-NG, NG:-NG] = rng.normal(size=(4, n, n))
+    grad = ref.step_adjoint(U, lam, dt, (1.0 / n, 1.0 / n))
+    ts = TangentStep.from_grid(o.grid(), g, "VanLeer", "HLLC")
+    Ui = torch.from_numpy(np.ascontiguousarray(U[:, NG:-NG, NG:-NG]))
+    for _ in range(3):
+        v = rng.uniform(-1, 1, (4, n, n))
+        _, JV = ts.jvp(Ui, torch.from_numpy(v), [dt])
+        tl = float(np.sum(lam[:, NG:-NG, NG:-NG] * JV.numpy()))
+        ad = float(np.sum(grad[:, NG:-NG, NG:-NG] * v))
+        assert ad == pytest.approx(tl, rel=1e-12)
