@@ -306,19 +306,8 @@ HCL_HD void riemann(const Eos<R>& e, int solver, const R* UL, const R* UR, int l
     F[1 + ND] = Fk[1 + ND] + S * (Es - U[1 + ND]);
 }
 
-// The selections a Riemann evaluation took; riemann_rev differentiates along
-// them when given, and otherwise takes them from its own evaluation.
-struct RiemannBranch {
-    bool valid;
-    bool min_left, max_left; // HLL/HLLC: wsL from the left state, wsR from the left state
-    bool neg_l, pos_r;       // HLL: wsL < 0, wsR > 0
-    bool left, sup;          // HLLC and low Mach: u* > 0; HLLC: wsL wsR > 0
-    bool a_left, amin_left, sub; // low Mach: rho a from the left, min(aL, aR) = aL, Ma < 1
-};
-
 template <int ND, class R>
-HCL_HD void riemann_rev(const Eos<R>& e, int solver, const R* UL, const R* UR, int l, const R* Fb, R* ULb, R* URb,
-                        const RiemannBranch* br = nullptr)
+HCL_HD void riemann_rev(const Eos<R>& e, int solver, const R* UL, const R* UR, int l, const R* Fb, R* ULb, R* URb)
 {
     constexpr int NV = ND + 2;
     R WL[NV], WR[NV];
@@ -332,16 +321,16 @@ HCL_HD void riemann_rev(const Eos<R>& e, int solver, const R* UL, const R* UR, i
     const R uL = WL[1 + l], uR = WR[1 + l];
     if (solver == 2) {
         // forward values along the branches the forward evaluation took
-        const bool selLa = br ? br->a_left : UL[0] * aL > UR[0] * aR;
+        const bool selLa = UL[0] * aL > UR[0] * aR;
         const R a = R(1.1) * (selLa ? UL[0] * aL : UR[0] * aR);
         const R ustar = R(0.5) * (uL + uR) - (PR - PL) / (R(2) * a);
-        const bool selLm = br ? br->amin_left : aL < aR;
+        const bool selLm = aL < aR;
         const R amin = selLm ? aL : aR;
         const R Ma = std::fabs(ustar) / amin;
-        const bool sub = br ? br->sub : Ma < R(1);
+        const bool sub = Ma < R(1);
         const R theta = sub ? Ma : R(1);
         const R Pstar = R(0.5) * (PL + PR) - R(0.5) * theta * a * (uR - uL);
-        const bool left = br ? br->left : ustar > R(0);
+        const bool left = ustar > R(0);
         const R* U = left ? UL : UR;
         R* Ub = left ? ULb : URb;
         // F_v = ustar U_v (+ Pstar on the normal momentum, + Pstar ustar on E)
@@ -402,8 +391,8 @@ HCL_HD void riemann_rev(const Eos<R>& e, int solver, const R* UL, const R* UR, i
         prim_from_cons_rev<ND>(e, UR, WRb, URb);
         return;
     }
-    const bool selL_min = br ? br->min_left : (uL - aL) < (uR - aR);
-    const bool selL_max = br ? br->max_left : (uL + aL) > (uR + aR);
+    const bool selL_min = (uL - aL) < (uR - aR);
+    const bool selL_max = (uL + aL) > (uR + aR);
     const R wsL = selL_min ? (uL - aL) : (uR - aR);
     const R wsR = selL_max ? (uL + aL) : (uR + aR);
     R FL[NV], FR[NV];
@@ -416,8 +405,8 @@ HCL_HD void riemann_rev(const Eos<R>& e, int solver, const R* UL, const R* UR, i
     }
     R wsLb = 0, wsRb = 0;
     if (solver == 0) {
-        const bool cl = br ? br->neg_l : wsL < R(0);
-        const bool cr = br ? br->pos_r : wsR > R(0);
+        const bool cl = wsL < R(0);
+        const bool cr = wsR > R(0);
         const R sl = cl ? wsL : R(0);
         const R sr = cr ? wsR : R(0);
         const R inv = R(1) / (sr - sl);
@@ -450,7 +439,7 @@ HCL_HD void riemann_rev(const Eos<R>& e, int solver, const R* UL, const R* UR, i
         const R num = PR - PL + rcL * uL - rcR * uR;
         const R den = rcL - rcR;
         const R ustar = num / den;
-        const bool left = br ? br->left : ustar > R(0);
+        const bool left = ustar > R(0);
         const R S = left ? wsL : wsR;
         const R* U = left ? UL : UR;
         const R* W = left ? WL : WR;
@@ -459,7 +448,7 @@ HCL_HD void riemann_rev(const Eos<R>& e, int solver, const R* UL, const R* UR, i
         R* Fkb = left ? FLb : FRb;
         const R un = W[1 + l];
         R ustarb = 0, pstarb = 0, Sb = 0;
-        if (br ? br->sup : wsL * wsR > R(0)) {
+        if (wsL * wsR > R(0)) {
             for (int v = 0; v < NV; ++v) {
                 Fkb[v] += Fb[v];
             }

@@ -61,7 +61,8 @@ __device__ __forceinline__ void prim_forward_rounding(const GridDev& g, const do
     for (int d = 1; d < ND; ++d) {
         norm = __dadd_rn(norm, __dmul_rn(q[1 + d], q[1 + d]));
     }
-    const double ek = __ddiv_rn(__ddiv_rn(norm, q[0]), 2.0);
+    // halving is exact: x * 0.5 rounds as x / 2 does
+    const double ek = __dmul_rn(__ddiv_rn(norm, q[0]), 0.5);
     const double evol = __dsub_rn(q[1 + ND], ek);
     w[0] = q[0];
 #pragma unroll
@@ -72,13 +73,8 @@ __device__ __forceinline__ void prim_forward_rounding(const GridDev& g, const do
     w[1 + ND] = __ddiv_rn(__dmul_rn(__dmul_rn(q[0], kKb), T), __dmul_rn(g.mmw, kMp));
 }
 
-// The forward FP64 step's face states and Riemann branches, rounded as the
-// forward rounds them (fused_step.cuh phase 2 and physics_exact.cuh on a
-// Cartesian grid: division-form limiters of slope_limiters.hpp:18-87, the
-// temperature round trip of perfect_gas.hpp:46-78, the Hancock increments of
-// extrapolation_reconstruction.hpp:222-312 added direction by direction),
-// written with round-to-nearest intrinsics so that no contraction changes
-// them.  The FP64 sweep linearises at these states and takes these branches.
+// Round-to-nearest FP64 operations that no contraction changes, for the
+// values the FP64 sweep must round exactly as the forward step does.
 namespace fwd {
 __device__ __forceinline__ double mul(double a, double b)
 {
@@ -95,98 +91,6 @@ __device__ __forceinline__ double sub(double a, double b)
 __device__ __forceinline__ double div(double a, double b)
 {
     return __ddiv_rn(a, b);
-}
-// perfect_gas.hpp:46-56: e from P through the temperature
-__device__ __forceinline__ double evol_from_pres(const GridDev& g, double rho, double P)
-{
-    const double T = div(mul(mul(P, g.mmw), kMp), mul(rho, kKb));
-    return div(mul(mul(rho, kKb), T), mul(mul(g.mmw, kMp), g.gamma_m1));
-}
-template <int ND>
-__device__ __forceinline__ double ek_prim(const double* p)
-{
-    double norm = mul(p[1], p[1]);
-#pragma unroll
-    for (int d = 1; d < ND; ++d) {
-        norm = add(norm, mul(p[1 + d], p[1 + d]));
-    }
-    return div(mul(p[0], norm), 2.0);
-}
-template <int ND>
-__device__ __forceinline__ void to_cons(const GridDev& g, const double* p, double* c)
-{
-    c[0] = p[0];
-#pragma unroll
-    for (int d = 0; d < ND; ++d) {
-        c[1 + d] = mul(p[0], p[1 + d]);
-    }
-    c[1 + ND] = add(evol_from_pres(g, p[0], p[1 + ND]), ek_prim<ND>(p));
-}
-template <int ND>
-__device__ __forceinline__ void flux_prim(const GridDev& g, const double* p, int l, double* f)
-{
-    const double P = p[1 + ND];
-    const double E = add(ek_prim<ND>(p), evol_from_pres(g, p[0], P));
-    f[0] = mul(p[0], p[1 + l]);
-#pragma unroll
-    for (int d = 0; d < ND; ++d) {
-        f[1 + d] = mul(mul(p[0], p[1 + l]), p[1 + d]);
-    }
-    f[1 + l] = add(f[1 + l], P);
-    f[1 + ND] = mul(p[1 + l], add(E, P));
-}
-// slope_limiters.hpp:18-87 in their division forms
-__device__ __forceinline__ double slope(int lim, double dR, double dL)
-{
-    if (lim == LIM_CONSTANT || !(mul(dL, dR) > 0)) {
-        return 0;
-    }
-    const double ratio = div(dR, dL);
-    const double r1 = add(ratio, 1.0);
-    if (lim == LIM_VANLEER) {
-        return div(mul(mul(0.5, add(dR, dL)), mul(4.0, ratio)), mul(r1, r1));
-    }
-    if (lim == LIM_MINMOD) {
-        return div(mul(div(mul(2.0, fmin(1., ratio)), add(1.0, ratio)), add(dL, dR)), 2.0);
-    }
-    return div(mul(mul(0.5, add(dR, dL)), mul(2.0, ratio)), add(mul(ratio, ratio), 1.0));
-}
-// Branches of the forward Riemann solve of one face (riemann_solver.hpp:22-181;
-// selections at ties as adj::riemann_rev takes them)
-template <int ND>
-__device__ __forceinline__ adj::RiemannBranch riemann_branch(const GridDev& g, int solver, const double* UL,
-                                                             const double* UR, int l)
-{
-    double pL[ND + 2], pR[ND + 2];
-    prim_forward_rounding<ND>(g, UL, pL);
-    prim_forward_rounding<ND>(g, UR, pR);
-    const double PL = pL[1 + ND], PR = pR[1 + ND];
-    const double aL = __dsqrt_rn(div(mul(g.gamma, PL), pL[0]));
-    const double aR = __dsqrt_rn(div(mul(g.gamma, PR), pR[0]));
-    const double uL = pL[1 + l], uR = pR[1 + l];
-    adj::RiemannBranch b{};
-    b.valid = true;
-    if (solver == RS_SPLITTING) {
-        b.a_left = mul(pL[0], aL) > mul(pR[0], aR);
-        const double a = mul(1.1, b.a_left ? mul(pL[0], aL) : mul(pR[0], aR));
-        const double ustar = sub(div(add(uL, uR), 2.0), mul(div(1.0, mul(2.0, a)), sub(PR, PL)));
-        b.amin_left = aL < aR;
-        b.sub = div(fabs(ustar), fmin(aL, aR)) < 1.0;
-        b.left = ustar > 0;
-        return b;
-    }
-    b.min_left = sub(uL, aL) < sub(uR, aR);
-    b.max_left = add(uL, aL) > add(uR, aR);
-    const double wsL = b.min_left ? sub(uL, aL) : sub(uR, aR);
-    const double wsR = b.max_left ? add(uL, aL) : add(uR, aR);
-    b.neg_l = wsL < 0;
-    b.pos_r = wsR > 0;
-    const double rcL = mul(pL[0], sub(wsL, uL));
-    const double rcR = mul(pR[0], sub(wsR, uR));
-    const double ustar = div(sub(add(sub(PR, PL), mul(rcL, uL)), mul(rcR, uR)), sub(rcL, rcR));
-    b.left = ustar > 0;
-    b.sup = mul(wsL, wsR) > 0;
-    return b;
 }
 } // namespace fwd
 
@@ -314,72 +218,48 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
         return (x[0] + 2) + S::L0 * ((ND >= 2 ? x[1] + 2 : 0) + S::L1 * (ND >= 3 ? x[2] + 2 : 0));
     };
 
-    // FP64 sweep: the face states of one cell as the forward step rounds them
-    // (fwd::), stored like phase 2's
-    auto hancock_forward_rounding = [&](const int x[3], int own, int lc, int gi) {
-        (void)gi;
-        const int gc[3] = {gorg[0] + x[0], ND >= 2 ? gorg[1] + x[1] : 0, ND >= 3 ? gorg[2] + x[2] : 0};
-        int gcc[3];
+    // ---- phase 2: forward Hancock face states (recomputed) -----------------
+    for (int h = tid; h < S::HCOUNT; h += NT) {
+        int x[3], own;
+        decode_h(h, x, own);
+        const int lc = lcell(x);
+        const int gi = gorg[0] + x[0]; // x0 index of the cell (gravity table)
+        R fp[2][ND][NV];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            gcc[d] = d < ND ? min(max(gc[d], 1), g.n[d] - 2) : 0;
-        }
-        double fp[2][ND][NV];
-#pragma unroll
-        for (int idim = 0; idim < ND; ++idim) {
-            const double dl = g.dx[idim][gcc[idim]];
-            const double dl_m = g.dx[idim][gcc[idim] - 1];
-            const double dl_p = g.dx[idim][gcc[idim] + 1];
+        for (int d = 0; d < ND; ++d) {
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-                const double vc = sw[v * S::NP + lc];
-                const double vp = sw[v * S::NP + lc + lstride[idim]];
-                const double vm = sw[v * S::NP + lc - lstride[idim]];
-                const double sl = fwd::slope(g.limiter, fwd::div(fwd::sub(vp, vc), fwd::div(fwd::add(dl, dl_p), 2.0)),
-                                             fwd::div(fwd::sub(vc, vm), fwd::div(fwd::add(dl_m, dl), 2.0)));
-                const double hs = fwd::mul(fwd::div(dl, 2.0), sl);
-                fp[0][idim][v] = fwd::sub(vc, hs);
-                fp[1][idim][v] = fwd::add(vc, hs);
+                const R wc = sw[v * S::NP + lc];
+                R gR, gL;
+                // the value only: a branch taken differently at a raw product
+                // that underflows changes it by less than 1e-270
+                const R phi = adj::limiter(g.limiter, sw[v * S::NP + lc + lstride[d]] - wc,
+                                           wc - sw[v * S::NP + lc - lstride[d]], &gR, &gL);
+                fp[0][d][v] = wc - R(0.5) * phi;
+                fp[1][d][v] = wc + R(0.5) * phi;
             }
         }
-        double fc[2][ND][NV];
+        R fc[2][ND][NV];
 #pragma unroll
-        for (int idim = 0; idim < ND; ++idim) {
+        for (int d = 0; d < ND; ++d) {
 #pragma unroll
-            for (int sd = 0; sd < 2; ++sd) {
-                fwd::to_cons<ND>(g, fp[sd][idim], fc[sd][idim]);
+            for (int s = 0; s < 2; ++s) {
+                adj::cons_from_prim<ND>(eos, fp[s][d], fc[s][d]);
             }
         }
-        const double dxs[3] = {g.dx[0][gcc[0]], g.dx[1][gcc[1]], g.dx[2][gcc[2]]};
-        const double dv_c = fwd::mul(fwd::mul(dxs[0], dxs[1]), dxs[2]);
+        R inc[NV];
 #pragma unroll
-        for (int idim = 0; idim < ND; ++idim) {
-            double a3[3] = {dxs[0], dxs[1], dxs[2]};
-            a3[idim] = 1;
-            const double ds = fwd::mul(fwd::mul(a3[0], a3[1]), a3[2]);
-            double fL[NV], fR[NV];
-            fwd::flux_prim<ND>(g, fp[0][idim], idim, fL);
-            fwd::flux_prim<ND>(g, fp[1][idim], idim, fR);
-            const double dtodv = fwd::div(dth, dv_c);
+        for (int v = 0; v < NV; ++v) {
+            inc[v] = R(0);
+        }
 #pragma unroll
-            for (int ipos = 0; ipos < ND; ++ipos) {
+        for (int d = 0; d < ND; ++d) {
+            R fL[NV], fR[NV];
+            adj::flux_prim<ND>(eos, fp[0][d], d, fL);
+            adj::flux_prim<ND>(eos, fp[1][d], d, fR);
 #pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    const double inc = fwd::mul(dtodv, fwd::sub(fwd::mul(fL[v], ds), fwd::mul(fR[v], ds)));
-                    fc[0][ipos][v] = fwd::add(fc[0][ipos][v], inc);
-                    fc[1][ipos][v] = fwd::add(fc[1][ipos][v], inc);
-                }
-            }
-            const double gd = gravity_at(g, gcc[0], idim);
-#pragma unroll
-            for (int ipos = 0; ipos < ND; ++ipos) {
-#pragma unroll
-                for (int sd = 0; sd < 2; ++sd) {
-                    const double rho_old = fp[sd][ipos][0];
-                    const double rhou_old = fwd::mul(fp[sd][ipos][0], fp[sd][ipos][1 + idim]);
-                    fc[sd][ipos][1 + idim] = fwd::add(fc[sd][ipos][1 + idim], fwd::mul(fwd::mul(dth, gd), rho_old));
-                    fc[sd][ipos][1 + ND] = fwd::add(fc[sd][ipos][1 + ND], fwd::mul(fwd::mul(dth, gd), rhou_old));
-                }
+            for (int v = 0; v < NV; ++v) {
+                inc[v] += cth[d] * (fL[v] - fR[v]);
             }
         }
 #pragma unroll
@@ -391,85 +271,21 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
             const int a = ax + S::Adim(d, 0) * (ay + S::Adim(d, 1) * az);
             R* base = sa + S::Aoff(d);
 #pragma unroll
-            for (int sd = 0; sd < 2; ++sd) {
+            for (int s = 0; s < 2; ++s) {
+                R hs[NV];
 #pragma unroll
                 for (int v = 0; v < NV; ++v) {
-                    base[(sd * NV + v) * S::Asize(d) + a] = (R)fc[sd][d][v];
+                    hs[v] = fc[s][d][v] + inc[v];
                 }
-            }
-        }
-    };
-
-    // ---- phase 2: forward Hancock face states (recomputed) -----------------
-    for (int h = tid; h < S::HCOUNT; h += NT) {
-        int x[3], own;
-        decode_h(h, x, own);
-        const int lc = lcell(x);
-        const int gi = gorg[0] + x[0]; // x0 index of the cell (gravity table)
-        if constexpr (std::is_same<R, double>::value) {
-            hancock_forward_rounding(x, own, lc, gi);
-        } else {
-            R fp[2][ND][NV];
 #pragma unroll
-            for (int d = 0; d < ND; ++d) {
+                for (int e = 0; e < ND; ++e) {
+                    const R gg = (R)(dth * gravity_at(g, gi, e));
+                    hs[1 + e] += gg * fc[s][d][0];
+                    hs[1 + ND] += gg * fc[s][d][1 + e];
+                }
 #pragma unroll
                 for (int v = 0; v < NV; ++v) {
-                    const R wc = sw[v * S::NP + lc];
-                    R gR, gL;
-                    const R phi = adj::limiter(g.limiter, sw[v * S::NP + lc + lstride[d]] - wc,
-                                               wc - sw[v * S::NP + lc - lstride[d]], &gR, &gL);
-                    fp[0][d][v] = wc - R(0.5) * phi;
-                    fp[1][d][v] = wc + R(0.5) * phi;
-                }
-            }
-            R fc[2][ND][NV];
-#pragma unroll
-            for (int d = 0; d < ND; ++d) {
-#pragma unroll
-                for (int s = 0; s < 2; ++s) {
-                    adj::cons_from_prim<ND>(eos, fp[s][d], fc[s][d]);
-                }
-            }
-            R inc[NV];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                inc[v] = R(0);
-            }
-#pragma unroll
-            for (int d = 0; d < ND; ++d) {
-                R fL[NV], fR[NV];
-                adj::flux_prim<ND>(eos, fp[0][d], d, fL);
-                adj::flux_prim<ND>(eos, fp[1][d], d, fR);
-#pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    inc[v] += cth[d] * (fL[v] - fR[v]);
-                }
-            }
-#pragma unroll
-            for (int d = 0; d < ND; ++d) {
-                if (own >= 0 && own != d) {
-                    continue;
-                }
-                const int ax = x[0] + (d == 0), ay = x[1] + (d == 1), az = x[2] + (d == 2);
-                const int a = ax + S::Adim(d, 0) * (ay + S::Adim(d, 1) * az);
-                R* base = sa + S::Aoff(d);
-#pragma unroll
-                for (int s = 0; s < 2; ++s) {
-                    R hs[NV];
-#pragma unroll
-                    for (int v = 0; v < NV; ++v) {
-                        hs[v] = fc[s][d][v] + inc[v];
-                    }
-#pragma unroll
-                    for (int e = 0; e < ND; ++e) {
-                        const R gg = (R)(dth * gravity_at(g, gi, e));
-                        hs[1 + e] += gg * fc[s][d][0];
-                        hs[1 + ND] += gg * fc[s][d][1 + e];
-                    }
-#pragma unroll
-                    for (int v = 0; v < NV; ++v) {
-                        base[(s * NV + v) * S::Asize(d) + a] = hs[v];
-                    }
+                    base[(s * NV + v) * S::Asize(d) + a] = hs[v];
                 }
             }
         }
@@ -517,11 +333,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 UR[v] = base[v * S::Asize(d) + aRd];
                 ULb[v] = URb[v] = R(0);
             }
-            adj::RiemannBranch br{};
-            if constexpr (std::is_same<R, double>::value) {
-                br = fwd::riemann_branch<ND>(g, g.riemann, UL, UR, d);
-            }
-            adj::riemann_rev<ND>(eos, g.riemann, UL, UR, d, Fb, ULb, URb, br.valid ? &br : nullptr);
+            adj::riemann_rev<ND>(eos, g.riemann, UL, UR, d, Fb, ULb, URb);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 bb[(NV + v) * S::Asize(d) + aLd] = ULb[v];
@@ -558,31 +370,37 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
         if (!any) {
             continue;
         }
-        // recompute slopes and face primitives; the FP64 sweep takes each
-        // limiter's branch from the forward's R*L > 0, formed from the
-        // differences divided by the cell spacing as the forward forms them
+        // recompute slopes and face primitives.  The FP64 sweep takes each
+        // limiter's branch from the forward's R*L > 0, which the forward forms
+        // from the differences divided by the half-spacings (dl + dl_p)/2 and
+        // (dl_m + dl)/2.  Where the raw product is too small for those
+        // quotients' product to stay above the subnormal range (1.0e-33 x
+        // 3.1e-292 underflows to 0, (64 x 1.0e-33) x (64 x 3.1e-292) does
+        // not), the test is evaluated as the forward rounds it; elsewhere both
+        // products have the same sign.  The FP32 sweep decides on its own
+        // differences.
         R fp[2][ND][NV], gRs[ND][NV], gLs[ND][NV];
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
-            double dl = 0, dl_m = 0, dl_p = 0;
-            if constexpr (std::is_same<R, double>::value) {
-                const int gd = min(max((d == 0 ? gorg[0] : (d == 1 ? gorg[1] : gorg[2])) + x[d], 1), g.n[d] - 2);
-                dl = g.dx[d][gd];
-                dl_m = g.dx[d][gd - 1];
-                dl_p = g.dx[d][gd + 1];
-            }
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 const R wc = sw[v * S::NP + lc];
-                const R wp = sw[v * S::NP + lc + lstride[d]];
-                const R wm = sw[v * S::NP + lc - lstride[d]];
+                const R dR = sw[v * S::NP + lc + lstride[d]] - wc;
+                const R dL = wc - sw[v * S::NP + lc - lstride[d]];
                 R phi;
                 if constexpr (std::is_same<R, double>::value) {
-                    const double Rs = fwd::div(fwd::sub(wp, wc), fwd::div(fwd::add(dl, dl_p), 2.0));
-                    const double Ls = fwd::div(fwd::sub(wc, wm), fwd::div(fwd::add(dl_m, dl), 2.0));
-                    phi = adj::limiter_on(g.limiter, fwd::mul(Ls, Rs) > 0, wp - wc, wc - wm, &gRs[d][v], &gLs[d][v]);
+                    const double prod = dR * dL;
+                    bool active = prod > 0;
+                    if (fabs(prod) * (g.inv_dx[d] * g.inv_dx[d]) <= 1e-270) {
+                        const int gd = min(max(gorg[d] + x[d], 1), g.n[d] - 2);
+                        const double dl = g.dx[d][gd];
+                        const double hR = fwd::div(fwd::add(dl, g.dx[d][gd + 1]), 2.0);
+                        const double hL = fwd::div(fwd::add(g.dx[d][gd - 1], dl), 2.0);
+                        active = fwd::mul(fwd::div(dL, hL), fwd::div(dR, hR)) > 0;
+                    }
+                    phi = adj::limiter_on(g.limiter, active, dR, dL, &gRs[d][v], &gLs[d][v]);
                 } else {
-                    phi = adj::limiter(g.limiter, wp - wc, wc - wm, &gRs[d][v], &gLs[d][v]);
+                    phi = adj::limiter(g.limiter, dR, dL, &gRs[d][v], &gLs[d][v]);
                 }
                 fp[0][d][v] = wc - R(0.5) * phi;
                 fp[1][d][v] = wc + R(0.5) * phi;

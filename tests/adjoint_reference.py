@@ -128,8 +128,9 @@ class Ref:
         if dx is None:
             phi = self.L.t_limiter(self.lim, float(R), float(L), C.byref(gR), C.byref(gL))
         else:
-            active = 1 if (float(L) / dx) * (float(R) / dx) > 0 else 0
-            phi = self.L.t_limiter_on(self.lim, active, float(R), float(L), C.byref(gR), C.byref(gL))
+            prod = float(R) * float(L)
+            active = prod > 0 if abs(prod) > 1e-270 * (dx * dx) else (float(L) / dx) * (float(R) / dx) > 0
+            phi = self.L.t_limiter_on(self.lim, 1 if active else 0, float(R), float(L), C.byref(gR), C.byref(gL))
         return phi, gR.value, gL.value
 
     # ---- grid helpers ------------------------------------------------------

@@ -5,9 +5,10 @@ FP64 restatement of the step (tests/tangent_step.py) on the same device:
 <g, v> = <lambda, J v> must hold to rounding for every direction v.
 
 Unlike central differences, the two sides differentiate the same branches
-(limiter zero when R*L <= 0, wave-speed and star-side selections), so the test
-holds on the plain Gresho vortex too, whose flat and solid-body regions sit on
-the limiter's kink, and at the full 512^2 x 400-step size of the adjoint
+(limiter zero unless R*L > 0 as the forward forms it, wave-speed and
+star-side selections), so the test holds on the plain Gresho vortex too, whose
+flat and solid-body regions sit on the limiter's kink with slope differences
+at rounding level, and at the full 512^2 x 400-step size of the adjoint
 workload with checkpoints every 32 steps."""
 import numpy as np
 import pytest
@@ -63,4 +64,4 @@ def test_adjoint_dot_product(n, nsteps, k, smooth, ndir):
         errs.append(abs(ad - tl) / abs(tl))
     errs = np.array(errs)
     print(f"  <g, v> vs <lambda, J v>: rel err median {np.median(errs):.2e} max {errs.max():.2e}")
-    assert np.max(errs) < 1e-9, errs
+    assert np.median(errs) < 1e-12 and np.max(errs) < 1e-10, errs
