@@ -47,12 +47,12 @@ struct AdjShape {
 // FP64 step rounds them (physics_exact.cuh to_prim for the perfect gas:
 // hydro/euler_equations.hpp:41-65, :111-122 with the temperature round trip of
 // thermodynamics/perfect_gas.hpp:58-78), written with round-to-nearest
-// intrinsics so that no contraction changes them.  The FP64 sweep takes its
-// branch decisions (the limiter's R*L > 0, the Riemann solver's wave-speed
-// and star-side selections) from these values: at rounding-level ties, which
-// flat and solid-body regions produce, they are then the branches the forward
-// step took.  The derivatives are those of P = (gamma - 1) e, which equal the
-// round trip's.
+// intrinsics so that no contraction changes them.  The FP64 sweep takes the
+// limiters' branches from the differences of these values (phase 4), so that
+// at rounding-level ties, which flat and solid-body regions produce, they are
+// the branches the forward step took; the Riemann selections it takes on the
+// face states it builds from them.  The derivatives are those of
+// P = (gamma - 1) e, which equal the round trip's.
 template <int ND>
 __device__ __forceinline__ void prim_forward_rounding(const GridDev& g, const double* q, double* w)
 {

@@ -1,4 +1,5 @@
-// tma_ring.cuh -- TMA row staging for the warp-strip kernels (sm_100a).
+// tma_ring.cuh -- TMA staging helpers (sm_100a): the row rings of the
+// warp-strip kernels and the tile + halo box of the fused tile kernels.
 //
 // A warp's row ring (4 slots of two x-row segments: 4 variables x 2 rows x 32
 // doubles, 2 KB) is filled by the Tensor Memory Accelerator: one lane issues a
@@ -43,13 +44,6 @@ __device__ __forceinline__ void mbar_init_fence()
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
 
-// orders this thread's earlier generic-proxy accesses of shared memory
-// before later async-proxy ones (a slot read by the lanes, then refilled)
-__device__ __forceinline__ void fence_proxy_async_smem()
-{
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-}
-
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
@@ -83,20 +77,8 @@ __device__ __forceinline__ void tma_prefetch_map(const CUtensorMap* map)
     asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
-// the same operations on shared-memory addresses computed once
-__device__ __forceinline__ void mbar_arrive_expect_tx_s(unsigned bar, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void tma_load_3d_s(unsigned dst, const CUtensorMap* map, unsigned bar, int x, int y, int z)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
-        "[%2];\n" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z)
-        : "memory");
-}
-// One box into shared memory by one elected lane of the (converged) warp:
+// On shared-memory addresses computed once: one box into shared memory by
+// one elected lane of the (converged) warp:
 // expect-tx on the slot's mbarrier and the copy, both predicated on the
 // election, so the warp takes no divergent branch.  The proxy fence orders
 // the warp's earlier generic reads of the slot before the async write.
