@@ -376,7 +376,8 @@ def adjoint_cost(torch, nsteps=400, n=512, k=32):
         cells = n * n
         algo = cells * (nsteps * ADJ_BYTES_PER_CELL_STEP + (nsteps // k) * 64)
         out[prec] = {"forward_ms": fwd, "gradient_ms": adj, "adj_over_fwd": adj / fwd,
-                     "gradient_algorithmic_gb": algo * 1e-9, "gradient_achieved_gbs": algo / (adj * 1e-3) * 1e-9}
+                     "gradient_algorithmic_gb": algo * 1e-9, "gradient_achieved_gbs": algo / (adj * 1e-3) * 1e-9,
+                     "schedule": d.schedule()}
         d.close()
     return out
 
