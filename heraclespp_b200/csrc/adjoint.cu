@@ -21,12 +21,12 @@ struct Launcher {
                              (int)smem());
     }
     static void launch(const GridDev& g, const StateDev& U, const StateDev& lo, const StateDev& li, double dt,
-                       cudaStream_t s)
+                       const StateDev& lz, cudaStream_t s)
     {
         const int nt0 = (g.nx[0] + S::T0 - 1) / S::T0;
         const int nt1 = (g.nx[1] + S::T1 - 1) / S::T1;
         const int nt2 = (g.nx[2] + S::T2 - 1) / S::T2;
-        k_adjoint_step<ND, R, TX, TY, TZ, NT><<<nt0 * nt1 * nt2, NT, smem(), s>>>(g, U, lo, li, dt);
+        k_adjoint_step<ND, R, TX, TY, TZ, NT><<<nt0 * nt1 * nt2, NT, smem(), s>>>(g, U, lo, li, dt, lz);
         ++g_launches;
     }
 };
@@ -55,23 +55,23 @@ void configure()
 }
 
 void step(const GridDev& g, const StateDev& U, const StateDev& lam_out, const StateDev& lam_in, double dt, bool fp64,
-          cudaStream_t s)
+          const StateDev& lam_zero, cudaStream_t s)
 {
     if (fp64) {
         if (g.ndim == 1) {
-            L1d::launch(g, U, lam_out, lam_in, dt, s);
+            L1d::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
         } else if (g.ndim == 2) {
-            L2d::launch(g, U, lam_out, lam_in, dt, s);
+            L2d::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
         } else {
-            L3d::launch(g, U, lam_out, lam_in, dt, s);
+            L3d::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
         }
     } else {
         if (g.ndim == 1) {
-            L1f::launch(g, U, lam_out, lam_in, dt, s);
+            L1f::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
         } else if (g.ndim == 2) {
-            L2f::launch(g, U, lam_out, lam_in, dt, s);
+            L2f::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
         } else {
-            L3f::launch(g, U, lam_out, lam_in, dt, s);
+            L3f::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
         }
     }
 }
@@ -114,28 +114,6 @@ void zero_ghosts(const GridDev& g, const StateDev& lam, cudaStream_t s)
         k_zero_ghosts<2><<<blocks, 256, 0, s>>>(g, lam);
     } else {
         k_zero_ghosts<3><<<blocks, 256, 0, s>>>(g, lam);
-    }
-    ++g_launches;
-}
-
-void fold_zero(const GridDev& g, const StateDev& lam, double* zero, int64_t zero_count, cudaStream_t s)
-{
-    const int64_t count = (int64_t)g.nx[0] * g.nx[1] * g.nx[2];
-    if (count > (int64_t)0xffffffffll) { // beyond the kernel's 32-bit cell index
-        cudaMemsetAsync(zero, 0, sizeof(double) * (size_t)zero_count, s);
-        fold(g, lam, s);
-        return;
-    }
-    int blocks = (int)((std::max(count, zero_count / 2) + 255) / 256);
-    if (blocks > 148 * 8) {
-        blocks = 148 * 8;
-    }
-    if (g.ndim == 1) {
-        k_fold_ghosts_zero<1><<<blocks, 256, 0, s>>>(g, lam, zero, zero_count);
-    } else if (g.ndim == 2) {
-        k_fold_ghosts_zero<2><<<blocks, 256, 0, s>>>(g, lam, zero, zero_count);
-    } else {
-        k_fold_ghosts_zero<3><<<blocks, 256, 0, s>>>(g, lam, zero, zero_count);
     }
     ++g_launches;
 }

@@ -97,9 +97,15 @@ __device__ __forceinline__ double div(double a, double b)
 // The reverse sweep of one tile (index `tile` in x-fastest tile order) by the
 // whole CTA; smem_raw holds AdjShape::smem() bytes.  It starts with a CTA
 // barrier, so a CTA may run several tiles back to back.
+// redirect: a contribution to a ghost cell goes straight to the interior cell
+// the ghost is filled from (bc_source in each dimension, the normal momentum
+// negated for a Reflexive face), so that lam_in needs no fold afterwards.
+// lam_zero (optional): a third adjoint buffer, which the CTA clears on its own
+// interior tile for the next step to add into.
 template <int ND, class R, int TX, int TY, int TZ, int NT>
 __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U, const StateDev& lam_out,
-                                             const StateDev& lam_in, double dt, int tile, unsigned char* smem_raw)
+                                             const StateDev& lam_in, double dt, int tile, unsigned char* smem_raw,
+                                             const StateDev* lam_zero = nullptr, bool redirect = false)
 {
     using S = Shape<ND, TX, TY, TZ>;
     constexpr int NV = S::NV;
@@ -135,6 +141,20 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
     const int gorg[3] = {g.ng + t0[0], ND >= 2 ? g.ng + t0[1] : 0, ND >= 3 ? g.ng + t0[2] : 0};
     const int lstride[3] = {1, S::L0, S::L0 * S::L1};
     auto ntile_d = [&](int d) { return (g.nx[d] + S::T(d) - 1) / S::T(d); };
+
+    if (lam_zero) {
+        // this tile's interior cells of the buffer the next step adds into
+        for (int c = tid; c < S::TVOL; c += NT) {
+            const int x0 = c % S::T0, x1 = (c / S::T0) % S::T1, x2 = c / (S::T0 * S::T1);
+            if (t0[0] + x0 < g.nx[0] && (ND < 2 || t0[1] + x1 < g.nx[1]) && (ND < 3 || t0[2] + x2 < g.nx[2])) {
+                const int64_t o = sidx(*lam_zero, g.n[1], gorg[0] + x0, gorg[1] + x1, gorg[2] + x2);
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    lam_zero->q[o + lam_zero->plane * v] = 0.0;
+                }
+            }
+        }
+    }
 
     // ---- phase 1: primitives, lambda', zero adjoint buffers --------------
     for (int p = tid; p < S::NP; p += NT) {
@@ -533,7 +553,24 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 outv[1 + e] += dt * ge * sl[(1 + ND) * S::NP + p];
             }
         }
-        const int64_t oo = sidx(lam_in, g.n[1], ri, rj, rk);
+        int si = ri, sj = rj, sk = rk;
+        int fl[3] = {0, 0, 0};
+        if (redirect) {
+            si = bc_source(ri, g.n[0], g.ng, g.bc[0], g.bc[1], &fl[0]);
+            if (ND >= 2) {
+                sj = bc_source(rj, g.n[1], g.ng, g.bc[2], g.bc[3], &fl[1]);
+            }
+            if (ND >= 3) {
+                sk = bc_source(rk, g.n[2], g.ng, g.bc[4], g.bc[5], &fl[2]);
+            }
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+                if (fl[d]) {
+                    outv[1 + d] = -outv[1 + d];
+                }
+            }
+        }
+        const int64_t oo = sidx(lam_in, g.n[1], si, sj, sk);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             if (outv[v] != 0.0) {
@@ -555,10 +592,10 @@ constexpr int adj_min_blocks()
 
 template <int ND, class R, int TX, int TY, int TZ, int NT>
 __global__ void __launch_bounds__(NT, adj_min_blocks<R, NT>())
-k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt)
+k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt, StateDev lam_zero)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    adjoint_tile<ND, R, TX, TY, TZ, NT>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw);
+    adjoint_tile<ND, R, TX, TY, TZ, NT>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw, &lam_zero, true);
 }
 
 // Transpose of the boundary fill: every interior cell gathers the adjoints of
@@ -621,120 +658,6 @@ template <int ND>
 __global__ void k_fold_ghosts(GridDev g, StateDev lam)
 {
     fold_cells<ND>(g, lam, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
-}
-
-// Adds the adjoints of cell (gi, gj, gk)'s ghost images into the cell, in the
-// order of fold_cells (z images outer, then y, then x; slots in order, the
-// normal-momentum entry negated for a flipped dimension).  xm, ym, zm:
-// fused::ghost_mask of the cell's indices (0 for an inactive dimension).
-template <int ND>
-__device__ __forceinline__ void fold_cell_masks(const GridDev& g, const StateDev& lam, int gi, int gj, int gk,
-                                                unsigned xm, unsigned ym, unsigned zm)
-{
-    const int64_t oc = sidx(lam, g.n[1], gi, gj, gk);
-    double acc[ND + 2];
-#pragma unroll
-    for (int v = 0; v < ND + 2; ++v) {
-        acc[v] = lam.q[oc + lam.plane * v];
-    }
-    unsigned zb = zm & 0xffffu;
-    int pz = gk, fz = 0;
-    bool self_z = true;
-    for (;;) {
-        unsigned yb = ym & 0xffffu;
-        int py = gj, fy = 0;
-        bool self_y = true;
-        for (;;) {
-            unsigned xb = xm & 0xffffu;
-            int px = gi, fx = 0;
-            bool self_x = true;
-            for (;;) {
-                if (!(self_x && self_y && self_z)) {
-                    const int64_t og = sidx(lam, g.n[1], px, py, pz);
-                    const int fl[3] = {fx, fy, fz};
-                    acc[0] += lam.q[og];
-#pragma unroll
-                    for (int d = 0; d < ND; ++d) {
-                        const double v = lam.q[og + lam.plane * (1 + d)];
-                        acc[1 + d] += fl[d] ? -v : v;
-                    }
-                    acc[1 + ND] += lam.q[og + lam.plane * (1 + ND)];
-                }
-                if (xb == 0u) {
-                    break;
-                }
-                const int k = __ffs(xb) - 1;
-                xb &= xb - 1u;
-                px = fused::ghost_slot(k, g.n[0], g.ng);
-                fx = (xm >> (16 + k)) & 1u;
-                self_x = false;
-            }
-            if (yb == 0u) {
-                break;
-            }
-            const int k = __ffs(yb) - 1;
-            yb &= yb - 1u;
-            py = fused::ghost_slot(k, g.n[1], g.ng);
-            fy = (ym >> (16 + k)) & 1u;
-            self_y = false;
-        }
-        if (zb == 0u) {
-            break;
-        }
-        const int k = __ffs(zb) - 1;
-        zb &= zb - 1u;
-        pz = fused::ghost_slot(k, g.n[2], g.ng);
-        fz = (zm >> (16 + k)) & 1u;
-        self_z = false;
-    }
-#pragma unroll
-    for (int v = 0; v < ND + 2; ++v) {
-        lam.q[oc + lam.plane * v] = acc[v];
-    }
-}
-
-// The fold of one step's input adjoint (the transpose of the ghost fill, as
-// fold_cells), one thread per interior cell with 32-bit index arithmetic
-// (interior cell count < 2^32; the launcher checks), the image gather only
-// for the cells that have images (within ng of a face).  Then the zeroing of
-// the buffer the next step adds into (the step's own output adjoint, read by
-// nobody after it), in 16-byte stores.
-template <int ND>
-__global__ void k_fold_ghosts_zero(GridDev g, StateDev lam, double* __restrict__ zero, int64_t zero_count)
-{
-    const unsigned nx0 = (unsigned)g.nx[0], nx1 = (unsigned)g.nx[1];
-    const unsigned count = nx0 * nx1 * (unsigned)g.nx[2];
-    for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
-        const unsigned ii = idx % nx0;
-        const unsigned row = idx / nx0;
-        const int gi = g.ng + (int)ii;
-        const int gj = ND >= 2 ? g.ng + (int)(row % nx1) : 0;
-        const int gk = ND >= 3 ? g.ng + (int)(row / nx1) : 0;
-        const unsigned xm = fused::ghost_mask(gi, g.n[0], g.ng, g.bc[0], g.bc[1]);
-        const unsigned ym = ND >= 2 ? fused::ghost_mask(gj, g.n[1], g.ng, g.bc[2], g.bc[3]) : 0u;
-        const unsigned zm = ND >= 3 ? fused::ghost_mask(gk, g.n[2], g.ng, g.bc[4], g.bc[5]) : 0u;
-        if ((xm | ym | zm) != 0u) {
-            fold_cell_masks<ND>(g, lam, gi, gj, gk, xm, ym, zm);
-        }
-    }
-    const int64_t first = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    // a leading double when the buffer starts off a 16-byte boundary, then
-    // pairs, then a trailing double when one is left
-    const int64_t head = (reinterpret_cast<uintptr_t>(zero) & 15u) ? 1 : 0;
-    const int64_t pairs = (zero_count - head) / 2;
-    double2* z2 = reinterpret_cast<double2*>(zero + head);
-    for (int64_t i = first; i < pairs; i += stride) {
-        z2[i] = make_double2(0.0, 0.0);
-    }
-    if (first == 0) {
-        if (head) {
-            zero[0] = 0.0;
-        }
-        if (head + 2 * pairs < zero_count) {
-            zero[zero_count - 1] = 0.0;
-        }
-    }
 }
 
 } // namespace hcl::adjoint

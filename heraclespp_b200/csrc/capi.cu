@@ -1950,7 +1950,7 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
             HCL_CUDA(cudaEventCreateWithFlags(&h->adj_ev_rev[b], cudaEventDisableTiming));
         }
     }
-    if (!h->adj_lam && (rc = dalloc(&h->adj_lam, sz * 2))) {
+    if (!h->adj_lam && (rc = dalloc(&h->adj_lam, sz * 3))) {
         return rc;
     }
     if (!h->adj_ctl && (rc = dalloc(&h->adj_ctl, 1))) {
@@ -1972,8 +1972,10 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
         st.q = base + sz * idx;
         return st;
     };
-    StateDev lam[2] = {state_at(h->adj_lam, 0), state_at(h->adj_lam, 1)};
-    HCL_CUDA(cudaMemsetAsync(h->adj_lam, 0, sizeof(double) * sz * 2, s));
+    // three adjoint buffers in rotation: a step reads one, adds into the
+    // second (zero) and clears the third for the step after it
+    StateDev lam[3] = {state_at(h->adj_lam, 0), state_at(h->adj_lam, 1), state_at(h->adj_lam, 2)};
+    HCL_CUDA(cudaMemsetAsync(h->adj_lam, 0, sizeof(double) * sz * 3, s));
     hcl::fused::pack_state(g, lam[0], lam_final, lam_final + g.N, lam_final + g.N * (nd + 1),
                            memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
     // the reference layout packs rho, rhou (nd planes), E contiguously: rhou at +N, E at +N*(nd+1)
@@ -2023,7 +2025,7 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
     if ((rc = recompute(h->adj_nck - 1))) {
         return rc;
     }
-    int cur = 0;
+    int ra = 0, rb = 1, rc3 = 2; // read, add into, clear
     for (int sg = h->adj_nck - 1; sg >= 0; --sg) {
         if (sg > 0 && (rc = recompute(sg - 1))) {
             return rc;
@@ -2036,19 +2038,22 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
         // backward through the segment
         for (int j = len - 1; j >= 0; --j) {
             const int n = first + j;
-            // lam[cur ^ 1] holds zeros here: from the initial clear, then from the
-            // previous step's fold_zero, which cleared the adjoint it had just read
-            hcl::adjoint::step(g, state_at(h->adj_seg, base + j), lam[cur], lam[cur ^ 1], h->adj_dts[n], fp64_sweep,
+            // lam[rb] holds zeros here: from the initial clear, then from the
+            // step before the previous one, which cleared it after the step
+            // before that had read it
+            hcl::adjoint::step(g, state_at(h->adj_seg, base + j), lam[ra], lam[rb], h->adj_dts[n], fp64_sweep, lam[rc3],
                                s);
-            hcl::adjoint::fold_zero(g, lam[cur ^ 1], lam[cur].q, (int64_t)sz, s);
-            cur ^= 1;
+            const int t = ra;
+            ra = rb;
+            rb = rc3;
+            rc3 = t;
         }
         HCL_CUDA(cudaEventRecord(h->adj_ev_rev[b], s));
     }
     HCL_LAUNCH_CHECK();
     // the gradient lives on the interior cells; ghost entries are zero
-    hcl::adjoint::zero_ghosts(g, lam[cur], s);
-    hcl::fused::unpack_state(g, lam[cur], grad, grad + g.N, grad + g.N * (nd + 1),
+    hcl::adjoint::zero_ghosts(g, lam[ra], s);
+    hcl::fused::unpack_state(g, lam[ra], grad, grad + g.N, grad + g.N * (nd + 1),
                              memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
     HCL_LAUNCH_CHECK();
     return HCL_OK;

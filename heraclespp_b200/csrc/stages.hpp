@@ -206,14 +206,15 @@ cudaError_t launch(int lim, int rs, int nw, int grid, const Prob* probs, const i
 namespace adjoint {
 
 void configure();
-// One adjoint step: lam_in (zeroed by the caller) += (dU^{n+1}/dU^n)^T lam_out,
-// with U = U^n and lam_out already folded onto interior cells.
+// One adjoint step: lam_in (zero on entry) += (dU^{n+1}/dU^n)^T lam_out, with
+// U = U^n and lam_out on interior cells (ghost entries zero); the
+// contributions to ghost cells land on the interior cells they are filled
+// from, so lam_in comes out folded.  The interior of lam_zero is cleared for
+// the next step (a buffer neither read nor written by this one).
 void step(const GridDev& g, const fused::StateDev& U, const fused::StateDev& lam_out, const fused::StateDev& lam_in,
-          double dt, bool fp64, cudaStream_t s);
+          double dt, bool fp64, const fused::StateDev& lam_zero, cudaStream_t s);
 // Transpose of the boundary fill, in place on interior cells.
 void fold(const GridDev& g, const fused::StateDev& lam, cudaStream_t s);
-// fold of lam, and zero_count doubles of `zero` set to 0 in the same launch
-void fold_zero(const GridDev& g, const fused::StateDev& lam, double* zero, int64_t zero_count, cudaStream_t s);
 void zero_ghosts(const GridDev& g, const fused::StateDev& lam, cudaStream_t s);
 
 } // namespace adjoint
