@@ -43,12 +43,20 @@ void launch_lrf(const GridDev& g, const StateDev& in, const StateDev& out, StepC
     });
     const int ncol = ((g.nx[0] + 27) / 28) * ((g.nx[1] + 11) / 12);
     if (L <= 0) {
-        // plane count per CTA that minimises waves x (planes + 2 start-up planes)
-        long best = -1;
+        // plane count per CTA that minimises (waves + 1/2) x (planes + 3): the
+        // start-up planes of each CTA, and half a CTA of imbalance in the last
+        // wave.  Chunks of at least 80 planes (RT 256^2 x 512: 2, 4, 6 and 8
+        // chunks of the z column took 1.992, 1.963, 1.961 and 1.972 ms per
+        // step; waves x (planes + 2) had picked 2)
+        double best = -1;
+        const int Lmin = std::min(80, g.nx[2]);
         for (int nzc = 1; nzc <= std::max(1, g.nx[2] / 4); ++nzc) {
             const int Lc = (g.nx[2] + nzc - 1) / nzc;
+            if (Lc < Lmin) {
+                break;
+            }
             const long waves = ((long)ncol * nzc + resident - 1) / resident;
-            const long cost = waves * (Lc + 2);
+            const double cost = (waves + 0.5) * (Lc + 3);
             if (best < 0 || cost < best) {
                 best = cost;
                 L = Lc;
