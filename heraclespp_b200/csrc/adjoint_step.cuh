@@ -13,8 +13,10 @@
 // the limited slopes of every cell it touched, and of the primitive recovery,
 // and adds the result for every cell of its halo-extended tile into lam_in
 // with atomics (neighbouring tiles overlap by the stencil width).  The
-// transpose of the boundary fill (ghost adjoints folded onto their interior
-// sources) is a separate gather kernel.
+// transpose of the boundary fill is applied as the contributions are made: a
+// contribution to a ghost cell goes to the interior cell the ghost is filled
+// from.  The gather kernel k_fold_ghosts folds the ghosts of the final
+// adjoint the caller supplies.
 #pragma once
 
 #include <cuda_runtime.h>

@@ -135,7 +135,7 @@ struct hcl_handle {
     // discrete adjoint: checkpoints, segment states, adjoint state, dts
     double* adj_ckpt = nullptr;   // nck states
     double* adj_seg = nullptr;    // k+1 states
-    double* adj_lam = nullptr;    // 2 states
+    double* adj_lam = nullptr;    // 3 states
     double* adj_ddts = nullptr;   // device copy of the dts
     StepCtl* adj_ctl = nullptr;
     std::vector<double> adj_dts;
@@ -2522,7 +2522,7 @@ int hcl_ensemble_adjoint(hcl_ensemble* e, const double* const* lam_final, double
             }
             h->adj_cap_seg = 2 * (k + 1);
         }
-        if (!h->adj_lam && (rc = dalloc(&h->adj_lam, sz * 2))) {
+        if (!h->adj_lam && (rc = dalloc(&h->adj_lam, sz * 3))) {
             return rc;
         }
         if (!h->adj_ctl && (rc = dalloc(&h->adj_ctl, 1))) {
@@ -2538,6 +2538,8 @@ int hcl_ensemble_adjoint(hcl_ensemble* e, const double* const* lam_final, double
         A.lam[0].q = h->adj_lam;
         A.lam[1] = h->st[0];
         A.lam[1].q = h->adj_lam + sz;
+        A.lam[2] = h->st[0];
+        A.lam[2].q = h->adj_lam + 2 * sz;
         A.ckpt = h->adj_ckpt;
         A.ctl = h->adj_ctl;
         A.tile0 = (int)tiles.size();
@@ -2576,7 +2578,7 @@ int hcl_ensemble_adjoint(hcl_ensemble* e, const double* const* lam_final, double
     for (size_t q = 0; q < np; ++q) {
         const GridDev& g = e->h[q]->g;
         const int nd = g.ndim;
-        HCL_CUDA(cudaMemsetAsync(ap[q].lam[0].q, 0, sizeof(double) * ap[q].sz * 2, s));
+        HCL_CUDA(cudaMemsetAsync(ap[q].lam[0].q, 0, sizeof(double) * ap[q].sz * 3, s));
         hcl::fused::pack_state(g, ap[q].lam[0], lam_final[q], lam_final[q] + g.N, lam_final[q] + g.N * (nd + 1), kin,
                                s);
         hcl::adjoint::fold(g, ap[q].lam[0], s);
@@ -2634,7 +2636,7 @@ int hcl_ensemble_adjoint(hcl_ensemble* e, const double* const* lam_final, double
                 err = hcl::ensemble::reverse(fp64, rev_bps * nsm, e->d_adjprobs, e->d_tiles, prm, e->d_barrier,
                                              e->d_status, s);
             }
-            cur ^= len & 1;
+            cur = (cur + len) % 3;
         }
         return err;
     };

@@ -2,8 +2,10 @@
 // launches: per checkpoint segment one launch of the ensemble's own forward
 // kernel recomputes every problem's segment states (segment mode, recorded
 // dts), then one cooperative launch sweeps every problem's segment back, step
-// by step, with two grid barriers per step (adjoint tiles of all problems;
-// transpose of the ghost fill together with zeroing the next step's buffer).
+// by step, with one grid barrier per step.  Three adjoint buffers rotate: step
+// j reads lam[a] (the adjoint of its output), adds into lam[b] (its input),
+// with each ghost's contribution sent to the interior cell the ghost is
+// filled from, and clears the interior of lam[c], which step j-1 adds into.
 // Same per-tile code and flags as the single-problem adjoint (adjoint.cu).
 #include <cuda_runtime.h>
 
@@ -59,22 +61,16 @@ k_ens_reverse(const AdjProb* __restrict__ probs, const int* __restrict__ tile_pr
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ GridDev sg; // the tile's grid, read from shared memory by the tile code
-    const int64_t gtid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t gsize = (int64_t)gridDim.x * blockDim.x;
+    // lam[cur] holds the adjoint of the segment's last output state and the
+    // interior of lam[cur + 1] is zero: the host clears all three buffers
+    // before the first segment, and the last step of a segment clears the
+    // buffer the next segment's first step adds into
     int cur = ap.cur;
     unsigned int phase = 0;
-    // the adjoint of the first step's input starts at zero
-    for (int p = 0; p < ap.nprob; ++p) {
-        double* q = probs[p].lam[cur ^ 1].q;
-        for (int64_t i = gtid; i < probs[p].sz; i += gsize) {
-            q[i] = 0.0;
-        }
-    }
-    if (!grid_barrier(barrier, (++phase) * gridDim.x, status)) {
-        return;
-    }
     for (int j = ap.len - 1; j >= 0; --j) {
         const int n = ap.first + j;
+        const int nxt = cur == 2 ? 0 : cur + 1;
+        const int clr = nxt == 2 ? 0 : nxt + 1;
         int loaded = -1;
         for (int item = blockIdx.x; item < ap.ntiles; item += gridDim.x) {
             const int p = tile_prob[item];
@@ -90,26 +86,12 @@ k_ens_reverse(const AdjProb* __restrict__ probs, const int* __restrict__ tile_pr
             fused::StateDev U = P.seg0;
             U.q += P.sz * j;
             adjoint::adjoint_tile<2, R, kRevTile, kRevTile, 1, kRevTile * kRevTile>(
-                sg, U, P.lam[cur], P.lam[cur ^ 1], P.dts[n], item - P.tile0, smem_raw);
+                sg, U, P.lam[cur], P.lam[nxt], P.dts[n], item - P.tile0, smem_raw, &P.lam[clr], true);
         }
         if (!grid_barrier(barrier, (++phase) * gridDim.x, status)) {
             return;
         }
-        // fold this step's input adjoint; zero the buffer the next step adds into
-        // (this step's output adjoint, read only by the tiles above)
-        for (int p = 0; p < ap.nprob; ++p) {
-            adjoint::fold_cells<2>(probs[p].g, probs[p].lam[cur ^ 1], gtid, gsize);
-            if (j > 0) {
-                double* q = probs[p].lam[cur].q;
-                for (int64_t i = gtid; i < probs[p].sz; i += gsize) {
-                    q[i] = 0.0;
-                }
-            }
-        }
-        if (!grid_barrier(barrier, (++phase) * gridDim.x, status)) {
-            return;
-        }
-        cur ^= 1;
+        cur = nxt;
     }
 }
 

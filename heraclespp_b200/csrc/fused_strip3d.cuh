@@ -12,7 +12,12 @@
 //    x-faces of plane z+1, the z-face z+1/2 and the y-faces of plane z, and
 //    updates plane z in FP64 with the ghost images, the health check and the
 //    CFL contribution.  One CTA barrier per plane orders the shared planes.
-// Lanes 2..29 and warps 2..13 write; the others are the stencil halo.
+// Lanes 2..29 and warps 2..13 write; the others are the stencil halo.  The
+// halo warps solve no x- or z-face and update nothing; warp 1 solves the
+// y-face above it, which row 2 reads.  (Skipping the Hancock states of warps
+// 0 and 15 as well, whose neighbours read only their primitives, measured
+// 2.25 against 1.93 ms per step on RT 256^2 x 512: the branch around the
+// predictor cost more than the work it saved.)
 #pragma once
 
 #include <cuda_runtime.h>
@@ -295,6 +300,9 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
         }
     };
     const int wd = max(w - 1, 0), wu = min(w + 1, kS3Warps - 1);
+    // warp-uniform roles of the halo warps (see the file comment)
+    const bool w_update = w >= 2 && w < kS3Warps - 2;
+    const bool w_yface = w >= 1 && w < kS3Warps - 2;
 
     // window: wC = P[z], wD = P[z+1]; qN = U[z+2] in flight
     float wC[5], wD[5];
@@ -363,9 +371,11 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
         float xo[6];
         s3::hancock<LIM, NFX>(c, wD, wyd, wyu, wC, wN, hm, hp, xw, xo);
         // 3. x-faces of plane z+1: left face at this lane, right face from lane+1
-        double dFxN[5];
+        double dFxN[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
         double dxxN = 0.0;
-        {
+        float Gzhi[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+        float gzx_hi = 0.f;
+        if (w_update) {
             float uL[5], Fl[5];
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
@@ -382,13 +392,11 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
                 const float fl = (Fl[0] < 0.f ? xo[0] : up_left) * Fl[0];
                 dxxN = (double)fl - (double)__shfl_down_sync(0xffffffffu, fl, 1);
             }
-        }
-        // 4. z-face z+1/2
-        float Gzhi[5];
-        fast::riemann<3>(c.eos, RS, hzU, hm[2], 2, Gzhi);
-        float gzx_hi = 0.f;
-        if constexpr (NFX > 0) {
-            gzx_hi = (Gzhi[0] < 0.f ? xo[2] : xzU) * Gzhi[0];
+            // 4. z-face z+1/2
+            fast::riemann<3>(c.eos, RS, hzU, hm[2], 2, Gzhi);
+            if constexpr (NFX > 0) {
+                gzx_hi = (Gzhi[0] < 0.f ? xo[2] : xzU) * Gzhi[0];
+            }
         }
         // 5. y-face states of plane z+1 for the neighbours
 #pragma unroll
@@ -402,7 +410,7 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
         }
         // 6. y-face above this row, plane z
         const bool upd = z >= z0;
-        if (upd) {
+        if (upd && w_yface) {
             float yL[5], yR[5], G[5];
 #pragma unroll
             for (int v = 0; v < 5; ++v) {

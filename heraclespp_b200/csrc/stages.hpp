@@ -175,7 +175,7 @@ struct AdjProb {
     GridDev g;
     fused::StateDev seg0;  // segment state 0; state j at seg0.q + j * sz
     int64_t sz;            // doubles per state buffer
-    fused::StateDev lam[2];
+    fused::StateDev lam[3];  // rotating adjoint buffers (see reverse())
     const double* ckpt;    // checkpoints, sz apart
     StepCtl* ctl;          // control block of the recomputation
     const double* dts;     // dts of the forward run
@@ -187,7 +187,8 @@ struct AdjParams {
     int ntiles;  // work items (16x16 tiles) over all problems
     int first;   // step index of the segment's first state
     int len;     // steps in the segment
-    int cur;     // lam[cur] holds the adjoint of the segment's last output state
+    int cur;     // lam[cur] holds the adjoint of the segment's last output state;
+                 // lam[(cur + 1) % 3] is zero on the interior
 };
 
 int reverse_blocks_per_sm(bool fp64);
