@@ -11,13 +11,13 @@ namespace hcl::adjoint {
 
 namespace {
 
-template <int ND, class R, int TX, int TY, int TZ, int NT>
+template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH = false>
 struct Launcher {
     using S = Shape<ND, TX, TY, TZ>;
     static size_t smem() { return AdjShape<ND, R, TX, TY, TZ>::smem(); }
     static void configure()
     {
-        cudaFuncSetAttribute(k_adjoint_step<ND, R, TX, TY, TZ, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem());
     }
     static void launch(const GridDev& g, const StateDev& U, const StateDev& lo, const StateDev& li, double dt,
@@ -26,7 +26,7 @@ struct Launcher {
         const int nt0 = (g.nx[0] + S::T0 - 1) / S::T0;
         const int nt1 = (g.nx[1] + S::T1 - 1) / S::T1;
         const int nt2 = (g.nx[2] + S::T2 - 1) / S::T2;
-        k_adjoint_step<ND, R, TX, TY, TZ, NT><<<nt0 * nt1 * nt2, NT, smem(), s>>>(g, U, lo, li, dt, lz);
+        k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH><<<nt0 * nt1 * nt2, NT, smem(), s>>>(g, U, lo, li, dt, lz);
         ++g_launches;
     }
 };
@@ -35,44 +35,63 @@ struct Launcher {
 // so the 320 Hancock cells and the 400 stencil cells of a tile take about one
 // round each (measured 8 % faster than 256 threads); the FP64 sweep keeps 256
 // threads and two CTAs per SM.
-using L1d = Launcher<1, double, 128, 1, 1, 128>;
-using L2d = Launcher<2, double, 16, 16, 1, 256>;
-using L3d = Launcher<3, double, 8, 4, 4, 128>;
-using L1f = Launcher<1, float, 128, 1, 1, 128>;
-using L2f = Launcher<2, float, 16, 16, 1, 384>;
-using L3f = Launcher<3, float, 8, 4, 4, 128>;
+template <bool SPH>
+struct Launchers {
+    using L1d = Launcher<1, double, 128, 1, 1, 128, SPH>;
+    using L2d = Launcher<2, double, 16, 16, 1, 256, SPH>;
+    using L3d = Launcher<3, double, 8, 4, 4, 128, SPH>;
+    using L1f = Launcher<1, float, 128, 1, 1, 128, SPH>;
+    using L2f = Launcher<2, float, 16, 16, 1, 384, SPH>;
+    using L3f = Launcher<3, float, 8, 4, 4, 128, SPH>;
+
+    static void configure()
+    {
+        L1d::configure();
+        L2d::configure();
+        L3d::configure();
+        L1f::configure();
+        L2f::configure();
+        L3f::configure();
+    }
+
+    static void step(const GridDev& g, const StateDev& U, const StateDev& lam_out, const StateDev& lam_in, double dt,
+                     bool fp64, const StateDev& lam_zero, cudaStream_t s)
+    {
+        if (fp64) {
+            if (g.ndim == 1) {
+                L1d::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
+            } else if (g.ndim == 2) {
+                L2d::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
+            } else {
+                L3d::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
+            }
+        } else {
+            if (g.ndim == 1) {
+                L1f::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
+            } else if (g.ndim == 2) {
+                L2f::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
+            } else {
+                L3f::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
+            }
+        }
+    }
+};
 
 } // namespace
 
 void configure()
 {
-    L1d::configure();
-    L2d::configure();
-    L3d::configure();
-    L1f::configure();
-    L2f::configure();
-    L3f::configure();
+    Launchers<false>::configure();
+    Launchers<true>::configure();
 }
 
 void step(const GridDev& g, const StateDev& U, const StateDev& lam_out, const StateDev& lam_in, double dt, bool fp64,
           const StateDev& lam_zero, cudaStream_t s)
 {
-    if (fp64) {
-        if (g.ndim == 1) {
-            L1d::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
-        } else if (g.ndim == 2) {
-            L2d::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
-        } else {
-            L3d::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
-        }
+    if (g.geom == GEOM_SPHERICAL) {
+        Launchers<true>::step(g, U, lam_out, lam_in, dt, fp64, lam_zero, s);
     } else {
-        if (g.ndim == 1) {
-            L1f::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
-        } else if (g.ndim == 2) {
-            L2f::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
-        } else {
-            L3f::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
-        }
+        Launchers<false>::step(g, U, lam_out, lam_in, dt, fp64, lam_zero, s);
     }
 }
 

@@ -147,6 +147,92 @@ HCL_HD void flux_prim_rev(const Eos<R>& e, const R* W, int l, const R* Fb, R* Wb
     Wb[1 + ND] += Pb;
 }
 
+// ---- spherical geometric source terms (hydro/source_terms.hpp:16-77) -----------
+// The momentum sources of one direction d of a cell from its two face states
+// W_L, W_R along d in primitive form, as the predictor
+// (extrapolation_reconstruction.hpp:145-303, k = dt/2 / dv) and the update
+// (godunov_scheme.hpp:165-256, k = dt / dv on the predicted states) add them:
+//  d = 0: m_r  += k (P_L + P_R)/2 (dS_p - dS)
+//         m_r  += k (rho_L u_o,L^2 + rho_R u_o,R^2)/2 (dS_p - dS)/2     (o = theta, phi)
+//         m_o  -= k rf (rho_R u_o,R u_r,R dS_p + rho_L u_o,L u_r,L dS)
+//  d = 1: m_th += k (P_L + P_R)/2 (dS_p - dS)
+//         m_th += k (rho_L u_ph,L^2 + rho_R u_ph,R^2)/2 cot (dS_p - dS)/2  (3-D)
+//         m_ph -= k sf (rho_R u_ph,R u_th,R dS_p + rho_L u_ph,L u_th,L dS)  (3-D)
+// with dS, dS_p the areas of the cell's minus and plus faces along d,
+// rf = (r_+ - r_-)/(r_+ + r_-) of the cell's radial faces, cot the cotangent
+// of its mid polar angle and sf = (sin th_+ - sin th_-)/(sin th_+ + sin th_-).
+template <class R>
+struct SphGeo {
+    R k;
+    R dS, dSp;
+    R rf, cot, sf;
+};
+
+template <int ND, class R>
+HCL_HD void sph_source(const SphGeo<R>& s, int d, const R* WL, const R* WR, R* S)
+{
+    const R dd = s.dSp - s.dS;
+    if (d == 0) {
+        S[1] += s.k * (WL[1 + ND] + WR[1 + ND]) / R(2) * dd;
+        for (int o = 1; o < ND; ++o) {
+            S[1] += s.k * ((WL[0] * WL[1 + o] * WL[1 + o]) + (WR[0] * WR[1 + o] * WR[1 + o])) / R(2) * dd / R(2);
+            S[1 + o] -= s.k * s.rf * ((WR[0] * WR[1 + o] * WR[1] * s.dSp) + (WL[0] * WL[1 + o] * WL[1] * s.dS));
+        }
+    } else if (d == 1 && ND >= 2) {
+        S[2] += s.k * (WL[1 + ND] + WR[1 + ND]) / R(2) * dd;
+        if (ND == 3) {
+            S[2] += s.k * ((WL[0] * WL[3] * WL[3]) + (WR[0] * WR[3] * WR[3])) / R(2) * s.cot * dd / R(2);
+            S[3] -= s.k * s.sf * ((WR[0] * WR[3] * WR[2] * s.dSp) + (WL[0] * WL[3] * WL[2] * s.dS));
+        }
+    }
+}
+
+// Accumulates into WLb, WRb the transpose of sph_source's Jacobian applied to Sb.
+template <int ND, class R>
+HCL_HD void sph_source_rev(const SphGeo<R>& s, int d, const R* WL, const R* WR, const R* Sb, R* WLb, R* WRb)
+{
+    const R dd = s.dSp - s.dS;
+    if (d == 0) {
+        const R a = s.k * dd / R(2) * Sb[1];
+        WLb[1 + ND] += a;
+        WRb[1 + ND] += a;
+        const R b = s.k * dd / R(4) * Sb[1];
+        for (int o = 1; o < ND; ++o) {
+            WLb[0] += b * WL[1 + o] * WL[1 + o];
+            WLb[1 + o] += b * R(2) * WL[0] * WL[1 + o];
+            WRb[0] += b * WR[1 + o] * WR[1 + o];
+            WRb[1 + o] += b * R(2) * WR[0] * WR[1 + o];
+            const R c = -s.k * s.rf * Sb[1 + o];
+            const R cR = c * s.dSp, cL = c * s.dS;
+            WRb[0] += cR * WR[1 + o] * WR[1];
+            WRb[1 + o] += cR * WR[0] * WR[1];
+            WRb[1] += cR * WR[0] * WR[1 + o];
+            WLb[0] += cL * WL[1 + o] * WL[1];
+            WLb[1 + o] += cL * WL[0] * WL[1];
+            WLb[1] += cL * WL[0] * WL[1 + o];
+        }
+    } else if (d == 1 && ND >= 2) {
+        const R a = s.k * dd / R(2) * Sb[2];
+        WLb[1 + ND] += a;
+        WRb[1 + ND] += a;
+        if (ND == 3) {
+            const R b = s.k * s.cot * dd / R(4) * Sb[2];
+            WLb[0] += b * WL[3] * WL[3];
+            WLb[3] += b * R(2) * WL[0] * WL[3];
+            WRb[0] += b * WR[3] * WR[3];
+            WRb[3] += b * R(2) * WR[0] * WR[3];
+            const R c = -s.k * s.sf * Sb[3];
+            const R cR = c * s.dSp, cL = c * s.dS;
+            WRb[0] += cR * WR[3] * WR[2];
+            WRb[3] += cR * WR[0] * WR[2];
+            WRb[2] += cR * WR[0] * WR[3];
+            WLb[0] += cL * WL[3] * WL[2];
+            WLb[3] += cL * WL[0] * WL[2];
+            WLb[2] += cL * WL[0] * WL[3];
+        }
+    }
+}
+
 // ---- limiters on raw differences (hydro/slope_limiters.hpp) --------------------
 // phi(R, L) and its partials; zero when R*L <= 0.
 template <class R>

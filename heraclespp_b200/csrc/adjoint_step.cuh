@@ -104,7 +104,12 @@ __device__ __forceinline__ double div(double a, double b)
 // negated for a Reflexive face), so that lam_in needs no fold afterwards.
 // lam_zero (optional): a third adjoint buffer, which the CTA clears on its own
 // interior tile for the next step to add into.
-template <int ND, class R, int TX, int TY, int TZ, int NT>
+// SPH: spherical geometry (uniform spacing per coordinate): the flux
+// differences carry each face's area over the cell's volume
+// (extrapolation_reconstruction.hpp:130-142, godunov_scheme.hpp:157-163) and
+// the geometric source terms enter the predictor and the update
+// (adj::sph_source).
+template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH = false>
 __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U, const StateDev& lam_out,
                                              const StateDev& lam_in, double dt, int tile, unsigned char* smem_raw,
                                              const StateDev* lam_zero = nullptr, bool redirect = false)
@@ -143,6 +148,33 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
     const int gorg[3] = {g.ng + t0[0], ND >= 2 ? g.ng + t0[1] : 0, ND >= 3 ? g.ng + t0[2] : 0};
     const int lstride[3] = {1, S::L0, S::L0 * S::L1};
     auto ntile_d = [&](int d) { return (g.nx[d] + S::T(d) - 1) / S::T(d); };
+    // spherical geometry of the cell at global index (i, j, k), clamped into
+    // the arrays (cells beyond them carry no adjoint)
+    auto geo_cell = [&](int i, int j, int k) {
+        return lidx(g, min(max(i, 0), g.n[0] - 1), min(max(j, 0), g.n[1] - 1), min(max(k, 0), g.n[2] - 1));
+    };
+    // source-term factors along d of that cell; kfac is dt (update) or dt/2
+    // (predictor) and is divided by the cell's volume
+    auto sph_geo = [&](int i, int j, int k, int d, double kfac) {
+        adj::SphGeo<R> sg;
+        const int64_t c = geo_cell(i, j, k);
+        const int64_t cp = geo_cell(i + (d == 0), j + (d == 1), k + (d == 2));
+        sg.k = (R)(kfac / g.dv[c]);
+        sg.dS = (R)g.ds[c + g.N * d];
+        sg.dSp = (R)g.ds[cp + g.N * d];
+        const int ic = min(max(i, 0), g.n[0] - 1);
+        const double x0 = g.x[0][ic], x0p = g.x[0][ic + 1];
+        sg.rf = (R)((x0p - x0) / (x0p + x0));
+        sg.cot = R(0);
+        sg.sf = R(0);
+        if (ND == 3) { // the polar-angle factors enter the 3-D terms only
+            const int jc = min(max(j, 0), g.n[1] - 1);
+            const double sm = g.sin1[jc], sp = g.sin1[jc + 1];
+            sg.cot = (R)g.cot_mid1[jc];
+            sg.sf = (R)((sp - sm) / (sp + sm));
+        }
+        return sg;
+    };
 
     if (lam_zero) {
         // this tile's interior cells of the buffer the next step adds into
@@ -246,6 +278,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
         decode_h(h, x, own);
         const int lc = lcell(x);
         const int gi = gorg[0] + x[0]; // x0 index of the cell (gravity table)
+        const int gj = gorg[1] + x[1], gk = gorg[2] + x[2];
         R fp[2][ND][NV];
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
@@ -279,9 +312,19 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
             R fL[NV], fR[NV];
             adj::flux_prim<ND>(eos, fp[0][d], d, fL);
             adj::flux_prim<ND>(eos, fp[1][d], d, fR);
+            if constexpr (SPH) {
+                const adj::SphGeo<R> sg = sph_geo(gi, gj, gk, d, dth);
+                const R cl = sg.k * sg.dS, cr = sg.k * sg.dSp;
 #pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                inc[v] += cth[d] * (fL[v] - fR[v]);
+                for (int v = 0; v < NV; ++v) {
+                    inc[v] += cl * fL[v] - cr * fR[v];
+                }
+                adj::sph_source<ND>(sg, d, fp[0][d], fp[1][d], inc);
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    inc[v] += cth[d] * (fL[v] - fR[v]);
+                }
             }
         }
 #pragma unroll
@@ -336,10 +379,24 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
             const int lcL = lcR - lstride[d];
             R Fb[NV];
             bool nz = false;
+            if constexpr (SPH) {
+                // the face enters U'_R with +dt dS / dv_R and U'_L with -dt dS / dv_L
+                const int i1 = gorg[0] + x[0], j1 = gorg[1] + x[1], k1 = gorg[2] + x[2];
+                const int64_t cR = geo_cell(i1, j1, k1);
+                const int64_t cL = geo_cell(i1 - (d == 0), j1 - (d == 1), k1 - (d == 2));
+                const double area = g.ds[cR + g.N * d];
+                const double kR = dt / g.dv[cR] * area, kL = dt / g.dv[cL] * area;
 #pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                Fb[v] = (R)(cfull[d] * (sl[v * S::NP + lcR] - sl[v * S::NP + lcL]));
-                nz |= Fb[v] != R(0);
+                for (int v = 0; v < NV; ++v) {
+                    Fb[v] = (R)(kR * sl[v * S::NP + lcR] - kL * sl[v * S::NP + lcL]);
+                    nz |= Fb[v] != R(0);
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    Fb[v] = (R)(cfull[d] * (sl[v * S::NP + lcR] - sl[v * S::NP + lcL]));
+                    nz |= Fb[v] != R(0);
+                }
             }
             if (!nz) {
                 continue;
@@ -371,6 +428,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
         decode_h(h, x, own);
         const int lc = lcell(x);
         const int gi = gorg[0] + x[0]; // x0 index of the cell (gravity table)
+        const int gj = gorg[1] + x[1], gk = gorg[2] + x[2];
         // gather this cell's face-state adjoints
         R Hb[2][ND][NV];
         bool any = false;
@@ -386,6 +444,43 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 for (int v = 0; v < NV; ++v) {
                     Hb[s][d][v] = has ? bb[(s * NV + v) * S::Asize(d) + a] : R(0);
                     any |= Hb[s][d][v] != R(0);
+                }
+            }
+        }
+        if constexpr (SPH) {
+            // the update's source terms on this cell's predicted states
+            // (godunov_scheme.hpp:165-256), for the tile's own cells
+            if (own < 0) {
+                R lamc[NV];
+                bool lz = false;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    lamc[v] = (R)sl[v * S::NP + lc];
+                    lz |= lamc[v] != R(0);
+                }
+                if (lz) {
+                    any = true;
+#pragma unroll
+                    for (int d = 0; d < (ND < 2 ? ND : 2); ++d) {
+                        const int ax = x[0] + (d == 0), ay = x[1] + (d == 1), az = x[2] + (d == 2);
+                        const int a = ax + S::Adim(d, 0) * (ay + S::Adim(d, 1) * az);
+                        const R* base = sa + S::Aoff(d);
+                        R H[2][NV], pH[2][NV], pHb[2][NV];
+#pragma unroll
+                        for (int s = 0; s < 2; ++s) {
+#pragma unroll
+                            for (int v = 0; v < NV; ++v) {
+                                H[s][v] = base[(s * NV + v) * S::Asize(d) + a];
+                                pHb[s][v] = R(0);
+                            }
+                            adj::prim_from_cons<ND>(eos, H[s], pH[s]);
+                        }
+                        adj::sph_source_rev<ND>(sph_geo(gi, gj, gk, d, dt), d, pH[0], pH[1], lamc, pHb[0], pHb[1]);
+#pragma unroll
+                        for (int s = 0; s < 2; ++s) {
+                            adj::prim_from_cons_rev<ND>(eos, H[s], pHb[s], Hb[s][d]);
+                        }
+                    }
                 }
             }
         }
@@ -467,10 +562,21 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
             R Fb0[NV], Fb1[NV];
+            if constexpr (SPH) {
+                const adj::SphGeo<R> sg = sph_geo(gi, gj, gk, d, dth);
+                const R cl = sg.k * sg.dS, cr = sg.k * sg.dSp;
 #pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                Fb0[v] = cth[d] * Sb[v];
-                Fb1[v] = -cth[d] * Sb[v];
+                for (int v = 0; v < NV; ++v) {
+                    Fb0[v] = cl * Sb[v];
+                    Fb1[v] = -cr * Sb[v];
+                }
+                adj::sph_source_rev<ND>(sg, d, fp[0][d], fp[1][d], Sb, fpb[0][d], fpb[1][d]);
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    Fb0[v] = cth[d] * Sb[v];
+                    Fb1[v] = -cth[d] * Sb[v];
+                }
             }
             adj::flux_prim_rev<ND>(eos, fp[0][d], d, Fb0, fpb[0][d]);
             adj::flux_prim_rev<ND>(eos, fp[1][d], d, Fb1, fpb[1][d]);
@@ -592,12 +698,12 @@ constexpr int adj_min_blocks()
     return sizeof(R) == 8 ? (NT <= 256 ? 2 : 1) : (NT <= 256 ? 3 : (NT <= 384 ? 3 : 1));
 }
 
-template <int ND, class R, int TX, int TY, int TZ, int NT>
+template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH>
 __global__ void __launch_bounds__(NT, adj_min_blocks<R, NT>())
 k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt, StateDev lam_zero)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    adjoint_tile<ND, R, TX, TY, TZ, NT>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw, &lam_zero, true);
+    adjoint_tile<ND, R, TX, TY, TZ, NT, SPH>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw, &lam_zero, true);
 }
 
 // Transpose of the boundary fill: every interior cell gathers the adjoints of

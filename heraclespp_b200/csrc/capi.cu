@@ -334,15 +334,14 @@ void build_grid_host(hcl_handle* h)
     g.eos = c.eos;
     g.pressure_fix = c.pressure_fix;
     g.eps_pf = c.eps_pf;
-    // uniform Cartesian spacing (to 1e-12 relative) enables the fast forms of
-    // the mixed kernel
-    int uniform = c.geometry == HCL_GEOM_CARTESIAN;
-    for (int d = 0; d < nd && uniform; ++d) {
+    // uniform spacing (to 1e-12 relative): with Cartesian geometry it enables
+    // the fast forms of the mixed kernel; the adjoint needs it in any geometry
+    int uniform = 1;
+    for (int d = 0; d < nd; ++d) {
         const double ref = h->hdx[d][c.nghost];
-        for (int i = 0; i < n[d]; ++i) {
+        for (int i = 0; i < n[d] && uniform; ++i) {
             if (std::fabs(h->hdx[d][i] - ref) > 1e-12 * std::fabs(ref)) {
                 uniform = 0;
-                break;
             }
         }
         g.inv_dx[d] = 1.0 / ref;
@@ -351,7 +350,8 @@ void build_grid_host(hcl_handle* h)
         g.inv_dx_f[d] = (float)g.inv_dx[d];
     }
     g.cfl_kc2 = (float)(0.5 * g.gamma * g.gamma_m1);
-    g.uniform_cart = uniform;
+    g.uniform_dx = uniform;
+    g.uniform_cart = uniform && c.geometry == HCL_GEOM_CARTESIAN;
 }
 
 int validate(const hcl_config* c)
@@ -1814,10 +1814,11 @@ int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p)
         return fail(HCL_ERR_CONFIG, "no state set");
     }
     const GridDev& g = h->g;
-    if (g.geom != HCL_GEOM_CARTESIAN || !g.uniform_cart || g.gravity == HCL_GRAVITY_INTERNAL_MASS || g.nfx > 0 ||
-        h->cfg.pressure_fix || g.eos != HCL_EOS_PERFECT_GAS) {
-        return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian uniform grids, uniform or point-mass gravity, "
-                                    "every Riemann solver, nfx = 0, no pressure fix, the perfect-gas EOS");
+    if (!g.uniform_dx || g.gravity == HCL_GRAVITY_INTERNAL_MASS || g.nfx > 0 || h->cfg.pressure_fix ||
+        g.eos != HCL_EOS_PERFECT_GAS) {
+        return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian and spherical grids of uniform spacing, uniform "
+                                    "or point-mass gravity, every Riemann solver, nfx = 0, no pressure fix, the "
+                                    "perfect-gas EOS");
     }
     if (p->precision != HCL_FP64 && p->precision != HCL_FP32_MIXED) {
         return fail(HCL_ERR_CONFIG, "the reverse sweep runs in HCL_FP64 or HCL_FP32_MIXED");

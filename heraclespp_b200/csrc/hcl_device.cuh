@@ -60,7 +60,8 @@ struct GridDev {
     const double* sin1;       // sin(x1_j) per node j, source_terms.hpp:58-59
     const double* sin_xc1;    // sin(x1c_j) per j, time_step.hpp:67
     int uniform_cart;         // 1 when Cartesian with uniform dx per dim (to 1e-12)
-    double inv_dx[3];         // 1/dx per dim when uniform_cart
+    int uniform_dx;           // 1 when dx is uniform per dim (to 1e-12), any geometry
+    double inv_dx[3];         // 1/dx per dim when uniform_dx
     float inv_dx_f[3];        // the same rounded to FP32 (CFL of the mixed march kernels)
     float cfl_kc2;            // gamma (gamma - 1) / 2 in FP32 (same use)
 };

@@ -23,9 +23,37 @@ void riemann_rev_nd(int solver, double gamma, const double* UL, const double* UR
 {
     riemann_rev<ND>(eos_of(gamma), solver, UL, UR, l, Fb, ULb, URb);
 }
+SphGeo<double> geo_of(const double* g)
+{
+    return SphGeo<double>{g[0], g[1], g[2], g[3], g[4], g[5]};
+}
 } // namespace
 
 extern "C" {
+
+// geo = {k, dS, dS_p, rf, cot, sf}
+void t_sph_src(int nd, int d, const double* geo, const double* WL, const double* WR, double* S)
+{
+    if (nd == 1) {
+        sph_source<1>(geo_of(geo), d, WL, WR, S);
+    } else if (nd == 2) {
+        sph_source<2>(geo_of(geo), d, WL, WR, S);
+    } else {
+        sph_source<3>(geo_of(geo), d, WL, WR, S);
+    }
+}
+
+void t_sph_src_rev(int nd, int d, const double* geo, const double* WL, const double* WR, const double* Sb, double* WLb,
+                   double* WRb)
+{
+    if (nd == 1) {
+        sph_source_rev<1>(geo_of(geo), d, WL, WR, Sb, WLb, WRb);
+    } else if (nd == 2) {
+        sph_source_rev<2>(geo_of(geo), d, WL, WR, Sb, WLb, WRb);
+    } else {
+        sph_source_rev<3>(geo_of(geo), d, WL, WR, Sb, WLb, WRb);
+    }
+}
 
 void t_riemann_fwd(int nd, int solver, double gamma, const double* UL, const double* UR, int l, double* F)
 {

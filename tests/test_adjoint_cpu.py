@@ -29,6 +29,8 @@ def lib(tmp_path_factory):
     L.t_c2p_rev.argtypes = [d, vp, vp, vp]
     L.t_limiter.argtypes = [i, d, d, C.POINTER(d), C.POINTER(d)]
     L.t_limiter.restype = d
+    L.t_sph_src.argtypes = [i, i, vp, vp, vp, vp]
+    L.t_sph_src_rev.argtypes = [i, i, vp, vp, vp, vp, vp, vp]
     return L
 
 
@@ -172,3 +174,59 @@ def test_riemann_forward_forms_equal_the_oracle(lib, nd):
             lib.t_riemann_fwd(nd, solver, gamma, p(UL), p(UR), l, p(out))
             ref = o.riemann(name, UL, UR, l)
             np.testing.assert_allclose(out, ref, rtol=1e-12, atol=1e-12 * (1 + np.max(np.abs(ref))))
+
+
+def sph_sources_ref(nd, d, geo, WL, WR):
+    """The momentum sources of direction d as the step adds them, written from
+    the source terms of hydro/source_terms.hpp:16-77 and their call sites in
+    extrapolation_reconstruction.hpp:145-303 / godunov_scheme.hpp:165-256."""
+    k, dS, dSp, rf, cot, sf = geo
+    S = np.zeros(nd + 2)
+
+    def grad_pres(PL, PR):
+        return k * (PL + PR) / 2 * (dSp - dS)
+
+    def grad_u_r(rL, rR, uL, uR):
+        return k * ((rL * uL * uL) + (rR * uR * uR)) / 2 * (dSp - dS) / 2
+
+    def grad_u_idir_r(rL, rR, uLr, uRr, uLo, uRo):
+        return k * rf * ((rR * uRo * uRr * dSp) + (rL * uLo * uLr * dS))
+
+    if d == 0:
+        S[1] += grad_pres(WL[-1], WR[-1])
+        for o in range(1, nd):
+            S[1] += grad_u_r(WL[0], WR[0], WL[1 + o], WR[1 + o])
+            S[1 + o] -= grad_u_idir_r(WL[0], WR[0], WL[1], WR[1], WL[1 + o], WR[1 + o])
+    elif d == 1:
+        S[2] += grad_pres(WL[-1], WR[-1])
+        if nd == 3:
+            S[2] += k * ((WL[0] * WL[3] * WL[3]) + (WR[0] * WR[3] * WR[3])) / 2 * cot * (dSp - dS) / 2
+            S[3] -= k * sf * ((WR[0] * WR[3] * WR[2] * dSp) + (WL[0] * WL[3] * WL[2] * dS))
+    return S
+
+
+@pytest.mark.parametrize("nd", [1, 2, 3])
+def test_spherical_sources_and_reverse(lib, nd):
+    """Spherical source terms: the forward against the reference's formulas,
+    the reverse against central differences of the forward."""
+    rng = np.random.default_rng(40 + nd)
+    nv = nd + 2
+    for _ in range(40):
+        geo = np.array([rng.uniform(0.01, 0.2), rng.uniform(0.5, 2), rng.uniform(0.5, 2), rng.uniform(0.01, 0.3),
+                        rng.uniform(-2, 2), rng.uniform(-0.5, 0.5)])
+        WL = np.concatenate([[rng.uniform(0.3, 2)], rng.uniform(-1, 1, nd), [rng.uniform(0.3, 3)]])
+        WR = np.concatenate([[rng.uniform(0.3, 2)], rng.uniform(-1, 1, nd), [rng.uniform(0.3, 3)]])
+        for d in range(nd):
+            def f(x):
+                out = np.zeros(nv)
+                lib.t_sph_src(nd, d, p(geo), p(np.ascontiguousarray(x[:nv])), p(np.ascontiguousarray(x[nv:])),
+                              p(out))
+                return out
+
+            x = np.concatenate([WL, WR])
+            np.testing.assert_allclose(f(x), sph_sources_ref(nd, d, geo, WL, WR), rtol=1e-14, atol=1e-15)
+            J = jac_fd(f, x, nv)
+            b = rng.normal(size=nv)
+            gL, gR = np.zeros(nv), np.zeros(nv)
+            lib.t_sph_src_rev(nd, d, p(geo), p(WL), p(WR), p(b), p(gL), p(gR))
+            np.testing.assert_allclose(np.concatenate([gL, gR]), J.T @ b, rtol=1e-6, atol=1e-8)
