@@ -333,11 +333,14 @@ int hcl_get_stream(const hcl_handle* h, void** stream);
 
 /* ---- discrete adjoint of the fused step ------------------------------------ */
 /* Reverse-mode derivative of nsteps fused steps with dt held fixed per step
- * (recorded by the forward pass or given).  Supported: Cartesian uniform
- * grids, uniform gravity, HLL/HLLC, every limiter.  Branches (limiter sign
- * tests, wave-speed min/max, HLLC switches) are differentiated along the
- * branch the forward evaluation took.  No reference counterpart: the
- * reference has no adjoint. */
+ * (recorded by the forward pass or given).  Supported: Cartesian and
+ * spherical grids of uniform spacing per coordinate (the spherical face areas,
+ * volumes and geometric source terms included), uniform and point-mass
+ * gravity, HLL/HLLC/Low Mach, every limiter, ndim 1-3, nfx = 0, no pressure
+ * fix, the perfect-gas EOS; anything else returns HCL_ERR_CONFIG.  Branches
+ * (limiter sign tests, wave-speed min/max, HLLC switches) are differentiated
+ * along the branch the forward evaluation took.  No reference counterpart:
+ * the reference has no adjoint. */
 typedef struct hcl_adjoint_params {
     int nsteps;
     const double* dts;        /* host, nsteps values; NULL: CFL dt of this forward run (recorded) */
