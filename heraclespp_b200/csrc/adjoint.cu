@@ -21,12 +21,12 @@ struct Launcher {
                              (int)smem());
     }
     static void launch(const GridDev& g, const StateDev& U, const StateDev& lo, const StateDev& li, double dt,
-                       const StateDev& lz, cudaStream_t s)
+                       const StateDev& lz, double* gbar, cudaStream_t s)
     {
         const int nt0 = (g.nx[0] + S::T0 - 1) / S::T0;
         const int nt1 = (g.nx[1] + S::T1 - 1) / S::T1;
         const int nt2 = (g.nx[2] + S::T2 - 1) / S::T2;
-        k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH><<<nt0 * nt1 * nt2, NT, smem(), s>>>(g, U, lo, li, dt, lz);
+        k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH><<<nt0 * nt1 * nt2, NT, smem(), s>>>(g, U, lo, li, dt, lz, gbar);
         ++g_launches;
     }
 };
@@ -55,23 +55,23 @@ struct Launchers {
     }
 
     static void step(const GridDev& g, const StateDev& U, const StateDev& lam_out, const StateDev& lam_in, double dt,
-                     bool fp64, const StateDev& lam_zero, cudaStream_t s)
+                     bool fp64, const StateDev& lam_zero, double* gbar, cudaStream_t s)
     {
         if (fp64) {
             if (g.ndim == 1) {
-                L1d::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
+                L1d::launch(g, U, lam_out, lam_in, dt, lam_zero, gbar, s);
             } else if (g.ndim == 2) {
-                L2d::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
+                L2d::launch(g, U, lam_out, lam_in, dt, lam_zero, gbar, s);
             } else {
-                L3d::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
+                L3d::launch(g, U, lam_out, lam_in, dt, lam_zero, gbar, s);
             }
         } else {
             if (g.ndim == 1) {
-                L1f::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
+                L1f::launch(g, U, lam_out, lam_in, dt, lam_zero, gbar, s);
             } else if (g.ndim == 2) {
-                L2f::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
+                L2f::launch(g, U, lam_out, lam_in, dt, lam_zero, gbar, s);
             } else {
-                L3f::launch(g, U, lam_out, lam_in, dt, lam_zero, s);
+                L3f::launch(g, U, lam_out, lam_in, dt, lam_zero, gbar, s);
             }
         }
     }
@@ -86,13 +86,78 @@ void configure()
 }
 
 void step(const GridDev& g, const StateDev& U, const StateDev& lam_out, const StateDev& lam_in, double dt, bool fp64,
-          const StateDev& lam_zero, cudaStream_t s)
+          const StateDev& lam_zero, double* gbar, cudaStream_t s)
 {
     if (g.geom == GEOM_SPHERICAL) {
-        Launchers<true>::step(g, U, lam_out, lam_in, dt, fp64, lam_zero, s);
+        Launchers<true>::step(g, U, lam_out, lam_in, dt, fp64, lam_zero, gbar, s);
     } else {
-        Launchers<false>::step(g, U, lam_out, lam_in, dt, fp64, lam_zero, s);
+        Launchers<false>::step(g, U, lam_out, lam_in, dt, fp64, lam_zero, gbar, s);
     }
+}
+
+namespace {
+// Reverse of InternalMassGravity (gravity.cpp:59-128, the forward in
+// stage_kernels.cu k_internal_mass_gravity): g_r[i] = -G M_i / xc_i^2 for
+// i >= ng, M_i = M_c + sum over shells s of a(i, s) shell[s], with a(i, s) =
+// V(xc_{s+ng}^3 - x0_{s+ng}^3) for s + ng <= i plus V(x0_{s+ng+1}^3 -
+// xc_{s+ng}^3) for s + ng < i (V = 4 pi / 3), and shell[s] the dv-weighted
+// mean density of radial index s + ng over the interior (j, k).  With
+// c_i = gbar_i (-G / xc_i^2) and the suffix sums C_i = sum_{i' >= i} c_i':
+// shell_bar[s] = C_{s+ng} V(xc^3 - x0^3)_{s+ng} + C_{s+ng+1} V(x0_{s+ng+1}^3 - xc_{s+ng}^3),
+// and every cell of the shell gets shell_bar[s] dv / sum dv on its density
+// adjoint (on the interior cell a ghost is filled from).  One CTA.
+__global__ void k_internal_mass_reverse(GridDev g, const double* __restrict__ gbar, double* __restrict__ shell_bar,
+                                        StateDev lam)
+{
+    const int ng = g.ng;
+    const int n0 = g.n[0];
+    const int nsh = g.nx[0] + ng;
+    const double* x0 = g.x[0];
+    const double* xc = g.xc[0];
+    if (threadIdx.x == 0) {
+        const double vol_s3 = 4 * kPi / 3;
+        double C = 0.0;          // C_{i+1}
+        for (int i = n0 - 1; i >= ng; --i) {
+            const double Cn = C; // C_{i+1}
+            C += gbar[i] * (-kG / (xc[i] * xc[i]));
+            const int sidx_ = i - ng;
+            const double xc3 = xc[i] * xc[i] * xc[i];
+            const double x3 = x0[i] * x0[i] * x0[i];
+            const double x3p = x0[i + 1] * x0[i + 1] * x0[i + 1];
+            shell_bar[sidx_] = C * (vol_s3 * (xc3 - x3)) + Cn * (vol_s3 * (x3p - xc3));
+        }
+    }
+    __syncthreads();
+    const int g1 = g.ndim >= 2 ? ng : 0;
+    const int g2 = g.ndim >= 3 ? ng : 0;
+    for (int si = threadIdx.x; si < nsh; si += blockDim.x) {
+        const int i = si + ng;
+        double sd = 0;
+        for (int j = 0; j < g.nx[1]; ++j) {
+            for (int k = 0; k < g.nx[2]; ++k) {
+                sd += g.dv[lidx(g, i, j + g1, k + g2)];
+            }
+        }
+        const double f = shell_bar[si] / sd;
+        if (f == 0.0) {
+            continue;
+        }
+        int flip = 0;
+        const int src = bc_source(i, n0, ng, g.bc[0], g.bc[1], &flip); // a density: no sign change
+        for (int j = 0; j < g.nx[1]; ++j) {
+            for (int k = 0; k < g.nx[2]; ++k) {
+                const double w = f * g.dv[lidx(g, i, j + g1, k + g2)];
+                atomicAdd(&lam.q[sidx(lam, g.n[1], src, j + g1, k + g2)], w);
+            }
+        }
+    }
+}
+} // namespace
+
+void internal_mass_reverse(const GridDev& g, const double* gbar, double* shell_bar, const StateDev& lam, cudaStream_t s)
+{
+    k_internal_mass_reverse<<<1, 256, 0, s>>>(g, gbar, shell_bar, lam);
+    ++g_launches;
 }
 
 namespace {

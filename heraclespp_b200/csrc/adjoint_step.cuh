@@ -109,10 +109,14 @@ __device__ __forceinline__ double div(double a, double b)
 // (extrapolation_reconstruction.hpp:130-142, godunov_scheme.hpp:157-163) and
 // the geometric source terms enter the predictor and the update
 // (adj::sph_source).
+// gbar (optional, internal-mass gravity): gbar[i] += dJ/dg_r[i], the
+// derivative with respect to the radial gravity table the step read, over
+// the cells the tile's face states and output cells touch.
 template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH = false>
 __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U, const StateDev& lam_out,
                                              const StateDev& lam_in, double dt, int tile, unsigned char* smem_raw,
-                                             const StateDev* lam_zero = nullptr, bool redirect = false)
+                                             const StateDev* lam_zero = nullptr, bool redirect = false,
+                                             double* gbar = nullptr)
 {
     using S = Shape<ND, TX, TY, TZ>;
     constexpr int NV = S::NV;
@@ -540,6 +544,23 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
         for (int v = 0; v < NV; ++v) {
             Sb[v] = R(0);
         }
+        if (gbar) {
+            // H[s][ip]: m_0 += (dt/2) g_r rho_f, E += (dt/2) g_r m_0,f of the
+            // face state's conserved form (extrapolation_reconstruction.hpp:306-312)
+            double gs = 0.0;
+#pragma unroll
+            for (int ip = 0; ip < ND; ++ip) {
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    R fc[NV];
+                    adj::cons_from_prim<ND>(eos, fp[s][ip], fc);
+                    gs += (double)Hb[s][ip][1] * (double)fc[0] + (double)Hb[s][ip][1 + ND] * (double)fc[1];
+                }
+            }
+            if (gs != 0.0 && gi >= 0 && gi < g.n[0]) {
+                atomicAdd(&gbar[gi], dth * gs);
+            }
+        }
 #pragma unroll
         for (int ip = 0; ip < ND; ++ip) {
 #pragma unroll
@@ -660,6 +681,12 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 outv[0] += dt * ge * sl[(1 + e) * S::NP + p];
                 outv[1 + e] += dt * ge * sl[(1 + ND) * S::NP + p];
             }
+            if (gbar) {
+                const double gs = sl[1 * S::NP + p] * U.q[o] + sl[(1 + ND) * S::NP + p] * U.q[o + U.plane];
+                if (gs != 0.0) {
+                    atomicAdd(&gbar[ri], dt * gs);
+                }
+            }
         }
         int si = ri, sj = rj, sk = rk;
         int fl[3] = {0, 0, 0};
@@ -700,10 +727,10 @@ constexpr int adj_min_blocks()
 
 template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH>
 __global__ void __launch_bounds__(NT, adj_min_blocks<R, NT>())
-k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt, StateDev lam_zero)
+k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt, StateDev lam_zero, double* gbar)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    adjoint_tile<ND, R, TX, TY, TZ, NT, SPH>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw, &lam_zero, true);
+    adjoint_tile<ND, R, TX, TY, TZ, NT, SPH>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw, &lam_zero, true, gbar);
 }
 
 // Transpose of the boundary fill: every interior cell gathers the adjoints of

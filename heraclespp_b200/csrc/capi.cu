@@ -136,6 +136,8 @@ struct hcl_handle {
     double* adj_ckpt = nullptr;   // nck states
     double* adj_seg = nullptr;    // k+1 states
     double* adj_lam = nullptr;    // 3 states
+    double* adj_gmem = nullptr;   // internal-mass gravity: 2 (k+1) radial tables, dJ/dg_r, 2 shell scratches
+    int adj_cap_gmem = 0;         // doubles
     double* adj_ddts = nullptr;   // device copy of the dts
     StepCtl* adj_ctl = nullptr;
     std::vector<double> adj_dts;
@@ -208,6 +210,7 @@ void free_handle(hcl_handle* h)
     cudaFree(h->adj_ckpt);
     cudaFree(h->adj_seg);
     cudaFree(h->adj_lam);
+    cudaFree(h->adj_gmem);
     cudaFree(h->adj_ddts);
     cudaFree(h->adj_ctl);
     cudaFree(h->sl_mem);
@@ -1814,11 +1817,10 @@ int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p)
         return fail(HCL_ERR_CONFIG, "no state set");
     }
     const GridDev& g = h->g;
-    if (!g.uniform_dx || g.gravity == HCL_GRAVITY_INTERNAL_MASS || g.nfx > 0 || h->cfg.pressure_fix ||
-        g.eos != HCL_EOS_PERFECT_GAS) {
-        return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian and spherical grids of uniform spacing, uniform "
-                                    "or point-mass gravity, every Riemann solver, nfx = 0, no pressure fix, the "
-                                    "perfect-gas EOS");
+    if (!g.uniform_dx || g.nfx > 0 || h->cfg.pressure_fix || g.eos != HCL_EOS_PERFECT_GAS) {
+        return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian and spherical grids of uniform spacing, uniform, "
+                                    "point-mass or internal-mass gravity, every Riemann solver, nfx = 0, no pressure "
+                                    "fix, the perfect-gas EOS");
     }
     if (p->precision != HCL_FP64 && p->precision != HCL_FP32_MIXED) {
         return fail(HCL_ERR_CONFIG, "the reverse sweep runs in HCL_FP64 or HCL_FP32_MIXED");
@@ -1957,6 +1959,33 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
     if (!h->adj_ctl && (rc = dalloc(&h->adj_ctl, 1))) {
         return rc;
     }
+    // internal-mass gravity: the radial table of every segment state (the
+    // forward rebuilds it from each step's input density), dJ/dg_r of one
+    // reverse step, and shell scratch for the recompute and the reverse
+    const bool imass = g.gravity == HCL_GRAVITY_INTERNAL_MASS;
+    const int n0 = g.n[0];
+    const int nsh = g.nx[0] + g.ng;
+    const int gneed = imass ? 2 * (k + 1) * n0 + n0 + 2 * nsh : 0;
+    if (h->adj_cap_gmem < gneed) {
+        cudaFree(h->adj_gmem);
+        h->adj_gmem = nullptr;
+        h->adj_cap_gmem = 0;
+        if ((rc = dalloc(&h->adj_gmem, (size_t)gneed))) {
+            return rc;
+        }
+        h->adj_cap_gmem = gneed;
+    }
+    double* gtab = h->adj_gmem;
+    double* gbar = imass ? gtab + 2 * (k + 1) * n0 : nullptr;
+    double* shell_rev = imass ? gbar + n0 : nullptr;
+    double* shell_rec = imass ? shell_rev + nsh : nullptr;
+    auto grid_at = [&](int b, int j) {
+        GridDev gj = g;
+        if (imass) {
+            gj.g_r = gtab + ((size_t)b * (k + 1) + j) * n0;
+        }
+        return gj;
+    };
     if (h->adj_ddts_cap < N + 8) {
         cudaFree(h->adj_ddts);
         h->adj_ddts = nullptr;
@@ -2001,15 +2030,25 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
         HCL_CUDA(cudaMemcpyAsync(h->adj_seg + sz * base, h->adj_ckpt + sz * sg, sizeof(double) * sz,
                                  cudaMemcpyDeviceToDevice, a));
         hcl::fused::prologue(g, state_at(h->adj_seg, base), h->adj_ctl, 0.0, first, a);
-        for (int j = 0; j + 1 < len; ++j) {
+        for (int j = 0; j < len; ++j) {
+            const GridDev gj = grid_at(b, j);
+            if (imass) {
+                // the radial gravity of state j, which step j reads (main.cpp:309, :528)
+                const StateDev sj = state_at(h->adj_seg, base + j);
+                hcl::stage::internal_mass_gravity(g, sj.q, sj.pitch, h->cfg.central_mass, shell_rec,
+                                                  const_cast<double*>(gj.g_r), a);
+            }
+            if (j + 1 == len) {
+                break;
+            }
             if (h->cfg.precision == HCL_FP64) {
-                hcl::fused::step_exact(g, state_at(h->adj_seg, base + j), state_at(h->adj_seg, base + j + 1),
+                hcl::fused::step_exact(gj, state_at(h->adj_seg, base + j), state_at(h->adj_seg, base + j + 1),
                                        h->adj_ctl, rp, j % 6, 1, a);
             } else if (h->cfg.precision == HCL_FP64_FAST) {
-                hcl::fused::step_fast64(g, state_at(h->adj_seg, base + j), state_at(h->adj_seg, base + j + 1),
+                hcl::fused::step_fast64(gj, state_at(h->adj_seg, base + j), state_at(h->adj_seg, base + j + 1),
                                         h->adj_ctl, rp, j % 6, 1, a);
             } else {
-                hcl::fused::step_mixed(g, state_at(h->adj_seg, base + j), state_at(h->adj_seg, base + j + 1),
+                hcl::fused::step_mixed(gj, state_at(h->adj_seg, base + j), state_at(h->adj_seg, base + j + 1),
                                        h->adj_ctl, rp, j % 6, 1, h->mixed_shape < 0 ? 0 : h->mixed_shape, a);
             }
         }
@@ -2042,8 +2081,16 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
             // lam[rb] holds zeros here: from the initial clear, then from the
             // step before the previous one, which cleared it after the step
             // before that had read it
-            hcl::adjoint::step(g, state_at(h->adj_seg, base + j), lam[ra], lam[rb], h->adj_dts[n], fp64_sweep, lam[rc3],
-                               s);
+            if (imass) {
+                HCL_CUDA(cudaMemsetAsync(gbar, 0, sizeof(double) * n0, s));
+            }
+            const GridDev gj = grid_at(b, j);
+            hcl::adjoint::step(gj, state_at(h->adj_seg, base + j), lam[ra], lam[rb], h->adj_dts[n], fp64_sweep,
+                               lam[rc3], gbar, s);
+            if (imass) {
+                // the density of state j also enters through the gravity table step j read
+                hcl::adjoint::internal_mass_reverse(gj, gbar, shell_rev, lam[rb], s);
+            }
             const int t = ra;
             ra = rb;
             rb = rc3;

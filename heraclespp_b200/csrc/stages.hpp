@@ -212,8 +212,15 @@ void configure();
 // contributions to ghost cells land on the interior cells they are filled
 // from, so lam_in comes out folded.  The interior of lam_zero is cleared for
 // the next step (a buffer neither read nor written by this one).
+// gbar (internal-mass gravity, else nullptr): n0 doubles, zero on entry;
+// receives dJ/dg_r of the radial table g.g_r the step read.
 void step(const GridDev& g, const fused::StateDev& U, const fused::StateDev& lam_out, const fused::StateDev& lam_in,
-          double dt, bool fp64, const fused::StateDev& lam_zero, cudaStream_t s);
+          double dt, bool fp64, const fused::StateDev& lam_zero, double* gbar, cudaStream_t s);
+// Internal-mass gravity: adds to the density adjoint of lam the part that
+// flows through the step's gravity table (gbar from step()); shell_bar:
+// nx0 + ng doubles of scratch.
+void internal_mass_reverse(const GridDev& g, const double* gbar, double* shell_bar, const fused::StateDev& lam,
+                           cudaStream_t s);
 // Transpose of the boundary fill, in place on interior cells.
 void fold(const GridDev& g, const fused::StateDev& lam, cudaStream_t s);
 void zero_ghosts(const GridDev& g, const fused::StateDev& lam, cudaStream_t s);

@@ -335,8 +335,8 @@ int hcl_get_stream(const hcl_handle* h, void** stream);
 /* Reverse-mode derivative of nsteps fused steps with dt held fixed per step
  * (recorded by the forward pass or given).  Supported: Cartesian and
  * spherical grids of uniform spacing per coordinate (the spherical face areas,
- * volumes and geometric source terms included), uniform and point-mass
- * gravity, HLL/HLLC/Low Mach, every limiter, ndim 1-3, nfx = 0, no pressure
+ * volumes and geometric source terms included), uniform, point-mass and
+ * internal-mass gravity, HLL/HLLC/Low Mach, every limiter, ndim 1-3, nfx = 0, no pressure
  * fix, the perfect-gas EOS; anything else returns HCL_ERR_CONFIG.  Branches
  * (limiter sign tests, wave-speed min/max, HLLC switches) are differentiated
  * along the branch the forward evaluation took.  No reference counterpart:

@@ -28,6 +28,18 @@ CASES = {
     "sph_1d_pointmass": (1, [64], dict(gamma=1.4, limiter="VanAlbada", riemann="HLL", geometry="Spherical",
                                        bc=["Reflexive", "NullGradient"], gravity="Point_mass", central_mass=1e8,
                                        xmin=(0.2, 0.0, 0.0), xmax=(1.2, 1.0, 1.0)), 16),
+    # internal-mass gravity (gravity.cpp:59-128): g_r = -G M(r) / r^2 rebuilt
+    # from every step's input density, so the density also enters through the
+    # enclosed mass of every shell outside it; rho and P carry RHO_SCALE so
+    # that the gas's own mass (G M_gas ~ 0.05) is comparable to the central
+    # mass's pull
+    "sph_1d_internalmass": (1, [64], dict(gamma=1.4, limiter="VanLeer", riemann="HLLC", geometry="Spherical",
+                                          bc=["Reflexive", "NullGradient"], gravity="Internal_mass",
+                                          central_mass=2e7, xmin=(0.2, 0.0, 0.0), xmax=(1.2, 1.0, 1.0)), 16),
+    "sph_2d_internalmass": (2, [40, 24], dict(gamma=1.4, limiter="VanLeer", riemann="HLL", geometry="Spherical",
+                                              bc=["Reflexive", "NullGradient", "Reflexive", "Reflexive"],
+                                              gravity="Internal_mass", central_mass=2e7,
+                                              xmin=(0.2, 0.5, 0.0), xmax=(1.0, 2.6, 1.0)), 12),
     "sph_2d": (2, [40, 24], dict(gamma=1.4, limiter="VanLeer", riemann="HLLC", geometry="Spherical",
                                  bc=["Reflexive", "NullGradient", "Reflexive", "Reflexive"],
                                  xmin=(0.2, 0.5, 0.0), xmax=(1.0, 2.6, 1.0)), 12),
@@ -40,6 +52,9 @@ CASES = {
                                      bc=["Reflexive", "NullGradient", "Reflexive", "Reflexive", "Periodic", "Periodic"],
                                      xmin=(0.3, 0.6, 0.0), xmax=(1.0, 2.5, 1.5)), 10),
 }
+
+
+RHO_SCALE = {"sph_1d_internalmass": 1e8, "sph_2d_internalmass": 1e8}
 
 
 def interior(ndim):
@@ -80,8 +95,9 @@ def smooth_state(o, ndim, kw):
 def problem(name):
     ndim, nx, kw, nsteps = CASES[name]
     o = Oracle(ndim, nx, **oracle_kwargs(kw))
-    prim = smooth_state(o, ndim, kw)
-    rho, rhou, E, _ = o.init_from_prim(*prim)
+    rho0, u0, P0 = smooth_state(o, ndim, kw)
+    scale = RHO_SCALE.get(name, 1.0)
+    rho, rhou, E, _ = o.init_from_prim(rho0 * scale, u0, P0 * scale)
     U0 = np.concatenate([rho[None], rhou, E[None]])
     d = Domain(ndim, nx, precision="fp64", **kw)
     d.set_state(rho, rhou, E)
@@ -141,7 +157,7 @@ def test_spherical_adjoint_matches_finite_differences(name):
     d.close()
 
 
-@pytest.mark.parametrize("name", ["sph_1d", "sph_2d", "sph_3d"])
+@pytest.mark.parametrize("name", ["sph_1d", "sph_2d", "sph_3d", "sph_1d_internalmass"])
 def test_spherical_mixed_sweep_close_to_fp64(name):
     """The FP32 sweep decides the limiter and wave-speed branches on its own
     face states: where FP32 rounding moves an argument across a switch the two
