@@ -11,13 +11,13 @@ namespace hcl::adjoint {
 
 namespace {
 
-template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH = false>
+template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH = false, bool EXACTB = true>
 struct Launcher {
     using S = Shape<ND, TX, TY, TZ>;
     static size_t smem() { return AdjShape<ND, R, TX, TY, TZ>::smem(); }
     static void configure()
     {
-        cudaFuncSetAttribute(k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem());
     }
     static void launch(const GridDev& g, const StateDev& U, const StateDev& lo, const StateDev& li, double dt,
@@ -26,7 +26,7 @@ struct Launcher {
         const int nt0 = (g.nx[0] + S::T0 - 1) / S::T0;
         const int nt1 = (g.nx[1] + S::T1 - 1) / S::T1;
         const int nt2 = (g.nx[2] + S::T2 - 1) / S::T2;
-        k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH><<<nt0 * nt1 * nt2, NT, smem(), s>>>(g, U, lo, li, dt, lz, gbar);
+        k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB><<<nt0 * nt1 * nt2, NT, smem(), s>>>(g, U, lo, li, dt, lz, gbar);
         ++g_launches;
     }
 };
@@ -35,14 +35,14 @@ struct Launcher {
 // so the 320 Hancock cells and the 400 stencil cells of a tile take about one
 // round each (measured 8 % faster than 256 threads); the FP64 sweep keeps 256
 // threads and two CTAs per SM.
-template <bool SPH>
+template <bool SPH, bool EXACTB>
 struct Launchers {
-    using L1d = Launcher<1, double, 128, 1, 1, 128, SPH>;
-    using L2d = Launcher<2, double, 16, 16, 1, 256, SPH>;
-    using L3d = Launcher<3, double, 8, 4, 4, 128, SPH>;
-    using L1f = Launcher<1, float, 128, 1, 1, 128, SPH>;
-    using L2f = Launcher<2, float, 16, 16, 1, 384, SPH>;
-    using L3f = Launcher<3, float, 8, 4, 4, 128, SPH>;
+    using L1d = Launcher<1, double, 128, 1, 1, 128, SPH, EXACTB>;
+    using L2d = Launcher<2, double, 16, 16, 1, 256, SPH, EXACTB>;
+    using L3d = Launcher<3, double, 8, 4, 4, 128, SPH, EXACTB>;
+    using L1f = Launcher<1, float, 128, 1, 1, 128, SPH, true>;
+    using L2f = Launcher<2, float, 16, 16, 1, 384, SPH, true>;
+    using L3f = Launcher<3, float, 8, 4, 4, 128, SPH, true>;
 
     static void configure()
     {
@@ -81,17 +81,29 @@ struct Launchers {
 
 void configure()
 {
-    Launchers<false>::configure();
-    Launchers<true>::configure();
+    Launchers<false, true>::configure();
+    Launchers<true, true>::configure();
+    Launchers<false, false>::configure();
+    Launchers<true, false>::configure();
 }
 
 void step(const GridDev& g, const StateDev& U, const StateDev& lam_out, const StateDev& lam_in, double dt, bool fp64,
-          const StateDev& lam_zero, double* gbar, cudaStream_t s)
+          bool exact_branches, const StateDev& lam_zero, double* gbar, cudaStream_t s)
 {
+    // the FP32 sweep has one form: its instantiation does not depend on EXACTB
+    const bool eb = exact_branches || !fp64;
     if (g.geom == GEOM_SPHERICAL) {
-        Launchers<true>::step(g, U, lam_out, lam_in, dt, fp64, lam_zero, gbar, s);
+        if (eb) {
+            Launchers<true, true>::step(g, U, lam_out, lam_in, dt, fp64, lam_zero, gbar, s);
+        } else {
+            Launchers<true, false>::step(g, U, lam_out, lam_in, dt, fp64, lam_zero, gbar, s);
+        }
     } else {
-        Launchers<false>::step(g, U, lam_out, lam_in, dt, fp64, lam_zero, gbar, s);
+        if (eb) {
+            Launchers<false, true>::step(g, U, lam_out, lam_in, dt, fp64, lam_zero, gbar, s);
+        } else {
+            Launchers<false, false>::step(g, U, lam_out, lam_in, dt, fp64, lam_zero, gbar, s);
+        }
     }
 }
 

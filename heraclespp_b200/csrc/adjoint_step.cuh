@@ -112,7 +112,10 @@ __device__ __forceinline__ double div(double a, double b)
 // gbar (optional, internal-mass gravity): gbar[i] += dJ/dg_r[i], the
 // derivative with respect to the radial gravity table the step read, over
 // the cells the tile's face states and output cells touch.
-template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH = false>
+// EXACTB (FP64 sweep): take the primitives as the bit-exact FP64 forward
+// step rounds them and its limiter branch test (phases 1 and 4); for a
+// forward in other arithmetic (FP32-mixed, fast FP64) the plain forms.
+template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH = false, bool EXACTB = true>
 __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U, const StateDev& lam_out,
                                              const StateDev& lam_in, double dt, int tile, unsigned char* smem_raw,
                                              const StateDev* lam_zero = nullptr, bool redirect = false,
@@ -211,7 +214,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
         for (int v = 0; v < NV; ++v) {
             q[v] = (R)U.q[o + U.plane * v];
         }
-        if constexpr (std::is_same<R, double>::value) {
+        if constexpr (std::is_same<R, double>::value && EXACTB) {
             prim_forward_rounding<ND>(g, q, w);
         } else {
             adj::prim_from_cons<ND>(eos, q, w);
@@ -509,7 +512,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 const R dR = sw[v * S::NP + lc + lstride[d]] - wc;
                 const R dL = wc - sw[v * S::NP + lc - lstride[d]];
                 R phi;
-                if constexpr (std::is_same<R, double>::value) {
+                if constexpr (std::is_same<R, double>::value && EXACTB) {
                     const double prod = dR * dL;
                     bool active = prod > 0;
                     if (fabs(prod) * (g.inv_dx[d] * g.inv_dx[d]) <= 1e-270) {
@@ -725,12 +728,13 @@ constexpr int adj_min_blocks()
     return sizeof(R) == 8 ? (NT <= 256 ? 2 : 1) : (NT <= 256 ? 3 : (NT <= 384 ? 3 : 1));
 }
 
-template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH>
+template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH, bool EXACTB>
 __global__ void __launch_bounds__(NT, adj_min_blocks<R, NT>())
 k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt, StateDev lam_zero, double* gbar)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    adjoint_tile<ND, R, TX, TY, TZ, NT, SPH>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw, &lam_zero, true, gbar);
+    adjoint_tile<ND, R, TX, TY, TZ, NT, SPH, EXACTB>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw, &lam_zero, true,
+                                                     gbar);
 }
 
 // Transpose of the boundary fill: every interior cell gathers the adjoints of

@@ -2086,7 +2086,7 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
             }
             const GridDev gj = grid_at(b, j);
             hcl::adjoint::step(gj, state_at(h->adj_seg, base + j), lam[ra], lam[rb], h->adj_dts[n], fp64_sweep,
-                               lam[rc3], gbar, s);
+                               h->cfg.precision == HCL_FP64, lam[rc3], gbar, s);
             if (imass) {
                 // the density of state j also enters through the gravity table step j read
                 hcl::adjoint::internal_mass_reverse(gj, gbar, shell_rev, lam[rb], s);

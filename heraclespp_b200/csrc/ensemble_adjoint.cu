@@ -85,7 +85,8 @@ k_ens_reverse(const AdjProb* __restrict__ probs, const int* __restrict__ tile_pr
             }
             fused::StateDev U = P.seg0;
             U.q += P.sz * j;
-            adjoint::adjoint_tile<2, R, kRevTile, kRevTile, 1, kRevTile * kRevTile>(
+            // the forward is the ensemble's FP32-mixed kernel: no FP64 forward rounding to reproduce
+            adjoint::adjoint_tile<2, R, kRevTile, kRevTile, 1, kRevTile * kRevTile, false, false>(
                 sg, U, P.lam[cur], P.lam[nxt], P.dts[n], item - P.tile0, smem_raw, &P.lam[clr], true);
         }
         if (!grid_barrier(barrier, (++phase) * gridDim.x, status)) {

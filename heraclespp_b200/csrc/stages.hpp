@@ -214,8 +214,10 @@ void configure();
 // the next step (a buffer neither read nor written by this one).
 // gbar (internal-mass gravity, else nullptr): n0 doubles, zero on entry;
 // receives dJ/dg_r of the radial table g.g_r the step read.
+// exact_branches (FP64 sweep): the forward was the bit-exact FP64 step, whose
+// rounding of the primitives the sweep reproduces to take its branches.
 void step(const GridDev& g, const fused::StateDev& U, const fused::StateDev& lam_out, const fused::StateDev& lam_in,
-          double dt, bool fp64, const fused::StateDev& lam_zero, double* gbar, cudaStream_t s);
+          double dt, bool fp64, bool exact_branches, const fused::StateDev& lam_zero, double* gbar, cudaStream_t s);
 // Internal-mass gravity: adds to the density adjoint of lam the part that
 // flows through the step's gravity table (gbar from step()); shell_bar:
 // nx0 + ng doubles of scratch.
