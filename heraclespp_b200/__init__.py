@@ -281,9 +281,10 @@ class Domain:
         return out[: cnt.value]
 
     def adjoint_backward(self, lam_final, grad=None, device=False):
-        """lam_final, grad: one contiguous buffer of (ndim+2)*N doubles (rho, rhou, E)."""
+        """lam_final, grad: one contiguous buffer of (ndim+2+nfx)*N doubles
+        (rho, rhou, E, then the passive scalars' fractions)."""
         if grad is None:
-            grad = np.zeros(((self.ndim + 2),) + self.shape3)
+            grad = np.zeros(((self.ndim + 2 + self.nfx),) + self.shape3)
         if not device:
             lam_final = np.ascontiguousarray(lam_final, dtype=np.float64)
         check(lib().hcl_adjoint_backward(self.h, _ptr(lam_final), _ptr(grad), 1 if device else 0))

@@ -11,14 +11,26 @@ namespace hcl::adjoint {
 
 namespace {
 
+// the device's largest dynamic shared-memory opt-in per block
+int smem_optin()
+{
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return v;
+}
+
 template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH = false, bool EXACTB = true>
 struct Launcher {
     using S = Shape<ND, TX, TY, TZ>;
-    static size_t smem() { return AdjShape<ND, R, TX, TY, TZ>::smem(); }
+    static size_t smem(int nfx = 0) { return AdjShape<ND, R, TX, TY, TZ>::smem(nfx); }
     static void configure()
     {
         cudaFuncSetAttribute(k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem());
+        // with passive scalars the size depends on their count: allow the opt-in
+        cudaFuncSetAttribute(k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());
     }
     static void launch(const GridDev& g, const StateDev& U, const StateDev& lo, const StateDev& li, double dt,
                        const StateDev& lz, double* gbar, cudaStream_t s)
@@ -26,7 +38,13 @@ struct Launcher {
         const int nt0 = (g.nx[0] + S::T0 - 1) / S::T0;
         const int nt1 = (g.nx[1] + S::T1 - 1) / S::T1;
         const int nt2 = (g.nx[2] + S::T2 - 1) / S::T2;
-        k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB><<<nt0 * nt1 * nt2, NT, smem(), s>>>(g, U, lo, li, dt, lz, gbar);
+        if (g.nfx > 0) {
+            k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB, true>
+                <<<nt0 * nt1 * nt2, NT, smem(g.nfx), s>>>(g, U, lo, li, dt, lz, gbar);
+        } else {
+            k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB>
+                <<<nt0 * nt1 * nt2, NT, smem(), s>>>(g, U, lo, li, dt, lz, gbar);
+        }
         ++g_launches;
     }
 };
@@ -43,6 +61,14 @@ struct Launchers {
     using L1f = Launcher<1, float, 128, 1, 1, 128, SPH, true>;
     using L2f = Launcher<2, float, 16, 16, 1, 384, SPH, true>;
     using L3f = Launcher<3, float, 8, 4, 4, 128, SPH, true>;
+
+    static size_t smem(int ndim, bool fp64, int nfx)
+    {
+        if (fp64) {
+            return ndim == 1 ? L1d::smem(nfx) : (ndim == 2 ? L2d::smem(nfx) : L3d::smem(nfx));
+        }
+        return ndim == 1 ? L1f::smem(nfx) : (ndim == 2 ? L2f::smem(nfx) : L3f::smem(nfx));
+    }
 
     static void configure()
     {
@@ -85,6 +111,14 @@ void configure()
     Launchers<true, true>::configure();
     Launchers<false, false>::configure();
     Launchers<true, false>::configure();
+}
+
+int scalar_sweep_fits(int ndim, bool fp64, int nfx, size_t* need, size_t* avail)
+{
+    // the tile shapes do not depend on the geometry
+    *need = Launchers<false, true>::smem(ndim, fp64, nfx);
+    *avail = (size_t)smem_optin();
+    return *need <= *avail;
 }
 
 void step(const GridDev& g, const StateDev& U, const StateDev& lam_out, const StateDev& lam_in, double dt, bool fp64,
@@ -189,8 +223,7 @@ __global__ void k_zero_ghosts(GridDev g, StateDev lam)
         }
         if (ghost) {
             const int64_t o = sidx(lam, g.n[1], i, j, k);
-#pragma unroll
-            for (int v = 0; v < ND + 2; ++v) {
+            for (int v = 0; v < ND + 2 + g.nfx; ++v) {
                 lam.q[o + lam.plane * v] = 0.0;
             }
         }

@@ -38,10 +38,26 @@ using fused::StateDev;
 template <int ND, class R, int TX, int TY, int TZ>
 struct AdjShape {
     using S = Shape<ND, TX, TY, TZ>;
+    // per passive scalar: its face values on the A arrays ([2][A_d] per d)
+    static constexpr int XA = S::A_TOTAL / S::NV;
+    __host__ __device__ static constexpr int XAoff(int d) { return S::Aoff(d) / S::NV; }
+    // one value per face of the tile (the F_d arrays)
+    static constexpr int FS = S::F_TOTAL / S::NV;
+    __host__ __device__ static constexpr int FSoff(int d) { return S::Foff(d) / S::NV; }
     static constexpr size_t smem()
     {
         // W, Wb, lam: [NV][NP]; A, Ab: A_TOTAL each
         return sizeof(R) * (2 * (size_t)S::NV * S::NP + 2 * (size_t)S::A_TOTAL) + sizeof(double) * (size_t)S::NV * S::NP;
+    }
+    // with nfx passive scalars: the density and scalar adjoints of the new
+    // state's division ([1 + nfx][TVOL], FP64), the scalar primitives and
+    // their adjoints ([nfx][NP] each), the predicted face values and their
+    // adjoints ([nfx][XA] each) and the Riemann mass flux of every face [FS]
+    static constexpr size_t smem(int nfx)
+    {
+        return smem() + (nfx > 0 ? sizeof(double) * (size_t)(1 + nfx) * S::TVOL +
+                                       sizeof(R) * ((size_t)nfx * (2 * S::NP + 2 * XA) + FS)
+                                 : 0);
     }
 };
 
@@ -115,20 +131,46 @@ __device__ __forceinline__ double div(double a, double b)
 // EXACTB (FP64 sweep): take the primitives as the bit-exact FP64 forward
 // step rounds them and its limiter branch test (phases 1 and 4); for a
 // forward in other arithmetic (FP32-mixed, fast FP64) the plain forms.
-template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH = false, bool EXACTB = true>
+// FX: the g.nfx passive scalars (state planes NV .. NV + nfx - 1, mass
+// fractions) ride along; smem_raw then holds AdjShape::smem(g.nfx) bytes.
+// Their forward (extrapolation_reconstruction.hpp:87-88, :315-339,
+// godunov_scheme.hpp:262-301): face values x_f = x -/+ phi/2 from the limited
+// slopes, times the face density, plus the predictor's increment
+// sum_d c_d (x_{L,d} m_{L,d} - x_{R,d} m_{R,d}) (m: the mass fluxes of the
+// reconstructed face states), over the predicted face density; the update
+// rho'x' = rho x + sum_d c_d (x_up m - x_up m) with the upwind face value of
+// each face's Riemann mass flux m, and x' = clamp(rho'x' / rho', 0, 1).  Phases
+// 2b and 2c recompute the mass fluxes and each output cell's division; the
+// reverse of the division adds -lam_v v / rho' to the new density's adjoint
+// and the upwind fluxes add x_up lam to the mass flux, both on the faces of
+// the tile's own cells (phase 3, which also runs the Riemann reverse for the
+// scalar part of a face the next tile owns); phase 4 takes the predicted face
+// values back to the face densities, the mass fluxes of the reconstructed
+// states and the scalars' slopes.  Branches (limiters, the upwind choice, the
+// clamp) are those of the sweep's own recomputation.
+template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH = false, bool EXACTB = true, bool FX = false>
 __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U, const StateDev& lam_out,
                                              const StateDev& lam_in, double dt, int tile, unsigned char* smem_raw,
                                              const StateDev* lam_zero = nullptr, bool redirect = false,
                                              double* gbar = nullptr)
 {
     using S = Shape<ND, TX, TY, TZ>;
+    using AS = AdjShape<ND, R, TX, TY, TZ>;
     constexpr int NV = S::NV;
+    const int nfx = FX ? g.nfx : 0;
     __syncthreads(); // the previous tile of this CTA is done with the shared arrays
     double* sl = reinterpret_cast<double*>(smem_raw);       // lambda' [NV][NP] (FP64)
-    R* sw = reinterpret_cast<R*>(sl + NV * S::NP);          // primitives [NV][NP]
+    double* sgr = sl + NV * S::NP;                          // FX: new-density adjoint of the division [TVOL]
+    double* sgx = sgr + (FX ? S::TVOL : 0);                 // FX: adjoint of rho'x' [nfx][TVOL]
+    R* sw = reinterpret_cast<R*>(sgx + nfx * S::TVOL);      // primitives [NV][NP]
     R* swb = sw + NV * S::NP;                               // primitive adjoints [NV][NP]
     R* sa = swb + NV * S::NP;                               // face states per d [2][NV][A_d]
     R* sab = sa + S::A_TOTAL;                               // face-state adjoints
+    R* swx = sab + S::A_TOTAL;                              // FX: scalar primitives [nfx][NP]
+    R* swxb = swx + nfx * S::NP;                            // FX: their adjoints
+    R* sxa = swxb + nfx * S::NP;                            // FX: predicted face values [nfx][XA]
+    R* sxab = sxa + nfx * AS::XA;                           // FX: their adjoints
+    R* sfm = sxab + nfx * AS::XA;                           // FX: Riemann mass flux per face [FS]
 
     const int tid = threadIdx.x;
     const adj::Eos<R> eos{(R)g.gamma, (R)g.gamma_m1, (R)(1.0 / g.gamma_m1)};
@@ -193,6 +235,9 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 for (int v = 0; v < NV; ++v) {
                     lam_zero->q[o + lam_zero->plane * v] = 0.0;
                 }
+                for (int k = 0; k < nfx; ++k) {
+                    lam_zero->q[o + lam_zero->plane * (NV + k)] = 0.0;
+                }
             }
         }
     }
@@ -234,9 +279,16 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
             swb[v * S::NP + p] = R(0);
             sl[v * S::NP + p] = out_cell ? lam_out.q[ol + lam_out.plane * v] : 0.0;
         }
+        for (int k = 0; k < nfx; ++k) {
+            swx[k * S::NP + p] = (R)U.q[o + U.plane * (NV + k)];
+            swxb[k * S::NP + p] = R(0);
+        }
     }
     for (int a = tid; a < S::A_TOTAL; a += NT) {
         sab[a] = R(0);
+    }
+    for (int a = tid; a < nfx * AS::XA; a += NT) {
+        sxab[a] = R(0);
     }
     __syncthreads();
 
@@ -314,23 +366,71 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
         for (int v = 0; v < NV; ++v) {
             inc[v] = R(0);
         }
+        // FX: mass fluxes of the reconstructed face states and the predictor's
+        // coefficients of the left and right face along d
+        R mfl[ND], mfr[ND], ccl[ND], ccr[ND];
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
             R fL[NV], fR[NV];
             adj::flux_prim<ND>(eos, fp[0][d], d, fL);
             adj::flux_prim<ND>(eos, fp[1][d], d, fR);
+            mfl[d] = fL[0];
+            mfr[d] = fR[0];
             if constexpr (SPH) {
                 const adj::SphGeo<R> sg = sph_geo(gi, gj, gk, d, dth);
                 const R cl = sg.k * sg.dS, cr = sg.k * sg.dSp;
+                ccl[d] = cl;
+                ccr[d] = cr;
 #pragma unroll
                 for (int v = 0; v < NV; ++v) {
                     inc[v] += cl * fL[v] - cr * fR[v];
                 }
                 adj::sph_source<ND>(sg, d, fp[0][d], fp[1][d], inc);
             } else {
+                ccl[d] = ccr[d] = cth[d];
 #pragma unroll
                 for (int v = 0; v < NV; ++v) {
                     inc[v] += cth[d] * (fL[v] - fR[v]);
+                }
+            }
+        }
+        if constexpr (FX) {
+            // predicted face values of each scalar (written in the forms of the
+            // density's predictor, so that a scalar equal to 1 over the stencil
+            // gives face values of exactly 1, as in the forward step)
+            for (int k = 0; k < nfx; ++k) {
+                const R* xk = swx + k * S::NP;
+                R xf[2][ND];
+                R xinc = R(0);
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    const R xc = xk[lc];
+                    R gR, gL;
+                    const R phi = adj::limiter(g.limiter, xk[lc + lstride[d]] - xc, xc - xk[lc - lstride[d]], &gR, &gL);
+                    xf[0][d] = xc - R(0.5) * phi;
+                    xf[1][d] = xc + R(0.5) * phi;
+                }
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    if constexpr (SPH) {
+                        xinc += ccl[d] * (xf[0][d] * mfl[d]) - ccr[d] * (xf[1][d] * mfr[d]);
+                    } else {
+                        xinc += cth[d] * (xf[0][d] * mfl[d] - xf[1][d] * mfr[d]);
+                    }
+                }
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    if (own >= 0 && own != d) {
+                        continue;
+                    }
+                    const int ax = x[0] + (d == 0), ay = x[1] + (d == 1), az = x[2] + (d == 2);
+                    const int a = ax + S::Adim(d, 0) * (ay + S::Adim(d, 1) * az);
+                    R* xb = sxa + k * AS::XA + AS::XAoff(d);
+#pragma unroll
+                    for (int s2 = 0; s2 < 2; ++s2) {
+                        const R rho_pred = fc[s2][d][0] + inc[0];
+                        xb[s2 * S::Asize(d) + a] = (xf[s2][d] * fc[s2][d][0] + xinc) / rho_pred;
+                    }
                 }
             }
         }
@@ -364,6 +464,118 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
     }
     __syncthreads();
 
+    // tile-interior index of an own output cell, -1 for a cell outside the
+    // tile or beyond the domain
+    auto own_index = [&](const int x[3]) {
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            if (x[d] < 0 || x[d] >= S::T(d) || t0[d] + x[d] >= g.nx[d]) {
+                return -1;
+            }
+        }
+        return x[0] + S::T0 * (x[1] + S::T1 * x[2]);
+    };
+    // update coefficient of the left (side 0) or right (side 1) face along d
+    // of tile cell x: dt dS / dV of that cell (dt/dx on Cartesian grids)
+    auto upd_coef = [&](const int x[3], int d, int side) -> double {
+        if constexpr (SPH) {
+            const int i1 = gorg[0] + x[0], j1 = gorg[1] + x[1], k1 = gorg[2] + x[2];
+            const int64_t c = geo_cell(i1, j1, k1);
+            const int64_t cf = side ? geo_cell(i1 + (d == 0), j1 + (d == 1), k1 + (d == 2)) : c;
+            return dt / g.dv[c] * g.ds[cf + g.N * d];
+        } else {
+            return dt * g.inv_dx[d];
+        }
+    };
+    // A index along d of tile cell x (the H cells -1 .. T_d along d)
+    auto a_index = [&](const int x[3], int d) {
+        return (x[0] + (d == 0)) + S::Adim(d, 0) * ((x[1] + (d == 1)) + S::Adim(d, 1) * (x[2] + (d == 2)));
+    };
+    auto a_step = [&](int d) { return d == 0 ? 1 : (d == 1 ? S::Adim(d, 0) : S::Adim(d, 0) * S::Adim(d, 1)); };
+    if constexpr (FX) {
+        // ---- phase 2b: Riemann mass flux of every face of the tile -------------
+        if (nfx > 0) {
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+                const R* base = sa + S::Aoff(d);
+                for (int f = tid; f < S::Fsize(d); f += NT) {
+                    int x[3];
+                    x[0] = f % S::Fdim(d, 0);
+                    x[1] = (f / S::Fdim(d, 0)) % S::Fdim(d, 1);
+                    x[2] = f / (S::Fdim(d, 0) * S::Fdim(d, 1));
+                    const int aRd = a_index(x, d);
+                    const int aLd = aRd - a_step(d);
+                    R UL[NV], UR[NV], F[NV];
+#pragma unroll
+                    for (int v = 0; v < NV; ++v) {
+                        UL[v] = base[(NV + v) * S::Asize(d) + aLd];
+                        UR[v] = base[v * S::Asize(d) + aRd];
+                    }
+                    adj::riemann<ND>(eos, g.riemann, UL, UR, d, F);
+                    sfm[AS::FSoff(d) + f] = F[0];
+                }
+            }
+            __syncthreads();
+            // ---- phase 2c: each own output cell's division rho'x' / rho' ---------
+            // (godunov_scheme.hpp:294-301): the clamp's branch, the adjoint of
+            // rho'x' and the division's part of the new density's adjoint
+            for (int c = tid; c < S::TVOL; c += NT) {
+                int x[3] = {c % S::T0, (c / S::T0) % S::T1, c / (S::T0 * S::T1)};
+                if (own_index(x) < 0) {
+                    sgr[c] = 0.0;
+                    for (int k = 0; k < nfx; ++k) {
+                        sgx[k * S::TVOL + c] = 0.0;
+                    }
+                    continue;
+                }
+                const int lc = lcell(x);
+                double cl[ND], cr[ND];
+                R ml[ND], mr[ND];
+                int fl_[ND], fr_[ND];
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    cl[d] = upd_coef(x, d, 0);
+                    cr[d] = upd_coef(x, d, 1);
+                    fl_[d] = x[0] + S::Fdim(d, 0) * (x[1] + S::Fdim(d, 1) * x[2]);
+                    const int st = d == 0 ? 1 : (d == 1 ? S::Fdim(d, 0) : S::Fdim(d, 0) * S::Fdim(d, 1));
+                    fr_[d] = fl_[d] + st;
+                    ml[d] = sfm[AS::FSoff(d) + fl_[d]];
+                    mr[d] = sfm[AS::FSoff(d) + fr_[d]];
+                }
+                const R rc = sw[lc];
+                R rn = rc;
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    rn += (R)cl[d] * ml[d] - (R)cr[d] * mr[d];
+                }
+                const int64_t ol = sidx(lam_out, g.n[1], gorg[0] + x[0], gorg[1] + x[1], gorg[2] + x[2]);
+                double extra = 0.0;
+                for (int k = 0; k < nfx; ++k) {
+                    const R* xa = sxa + k * AS::XA;
+                    R rx = swx[k * S::NP + lc] * rc;
+#pragma unroll
+                    for (int d = 0; d < ND; ++d) {
+                        const R* xd = xa + AS::XAoff(d);
+                        const int a = a_index(x, d);
+                        // left face: this cell's left value when the mass flows
+                        // left, else the left cell's right value; right face alike
+                        const R xl = ml[d] < R(0) ? xd[a] : xd[S::Asize(d) + a - a_step(d)];
+                        const R xr = mr[d] < R(0) ? xd[a + a_step(d)] : xd[S::Asize(d) + a];
+                        rx += (R)cl[d] * (xl * ml[d]) - (R)cr[d] * (xr * mr[d]);
+                    }
+                    const R v = rx / rn;
+                    const bool free_ = !(v < R(0)) && !(v > R(1));
+                    const double lv = free_ ? lam_out.q[ol + lam_out.plane * (NV + k)] : 0.0;
+                    const double lrx = lv / (double)rn;
+                    sgx[k * S::TVOL + c] = lrx;
+                    extra -= lrx * (double)v;
+                }
+                sgr[c] = extra;
+            }
+            __syncthreads();
+        }
+    }
+
     // ---- phase 3: adjoint of each owned face through the Riemann solver ---------
     // A tile owns the left face of each of its interior cells; the last tile
     // along d also owns the domain's last face (the right face of the last
@@ -378,15 +590,24 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
             x[0] = f % S::Fdim(d, 0);
             x[1] = (f / S::Fdim(d, 0)) % S::Fdim(d, 1);
             x[2] = f / (S::Fdim(d, 0) * S::Fdim(d, 1));
-            if (x[d] == S::T(d) && !last_d) {
-                continue; // owned by the next tile along d
+            // the next tile along d owns the face x_d = T_d; with passive
+            // scalars this tile still runs the Riemann reverse for the part of
+            // that face's mass-flux adjoint its own cell contributes
+            const bool owned = !(x[d] == S::T(d) && !last_d);
+            if (!owned && (!FX || nfx == 0)) {
+                continue;
             }
             // cells R = x and L = x - e_d (R may be the slab cell x_d = T_d)
             const int lcR = lcell(x);
             const int lcL = lcR - lstride[d];
             R Fb[NV];
             bool nz = false;
-            if constexpr (SPH) {
+            if (!owned) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    Fb[v] = R(0);
+                }
+            } else if constexpr (SPH) {
                 // the face enters U'_R with +dt dS / dv_R and U'_L with -dt dS / dv_L
                 const int i1 = gorg[0] + x[0], j1 = gorg[1] + x[1], k1 = gorg[2] + x[2];
                 const int64_t cR = geo_cell(i1, j1, k1);
@@ -403,6 +624,35 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 for (int v = 0; v < NV; ++v) {
                     Fb[v] = (R)(cfull[d] * (sl[v * S::NP + lcR] - sl[v * S::NP + lcL]));
                     nz |= Fb[v] != R(0);
+                }
+            }
+            if constexpr (FX) {
+                // scalar part from the tile's own cells on either side: the
+                // division's density adjoint and the upwind fluxes x_up m
+                int xl[3] = {x[0], x[1], x[2]};
+                xl[d] -= 1;
+                const int tR = own_index(x), tL = own_index(xl);
+                if (nfx > 0 && (tR >= 0 || tL >= 0)) {
+                    const R m = sfm[AS::FSoff(d) + f];
+                    const int aR = a_index(x, d), aL = aR - a_step(d);
+                    const double cR = tR >= 0 ? upd_coef(x, d, 0) : 0.0;  // R's left face
+                    const double cL = tL >= 0 ? upd_coef(xl, d, 1) : 0.0; // L's right face
+                    double gm = (tR >= 0 ? cR * sgr[tR] : 0.0) - (tL >= 0 ? cL * sgr[tL] : 0.0);
+                    // upwind value: the right cell's left value when the mass flows left
+                    const int slot = m < R(0) ? aR : S::Asize(d) + aL;
+                    for (int k = 0; k < nfx; ++k) {
+                        const double lf = (tR >= 0 ? cR * sgx[k * S::TVOL + tR] : 0.0) -
+                                          (tL >= 0 ? cL * sgx[k * S::TVOL + tL] : 0.0);
+                        if (lf != 0.0) {
+                            const int xo = k * AS::XA + AS::XAoff(d) + slot;
+                            gm += lf * (double)sxa[xo];
+                            sxab[xo] = (R)(lf * (double)m);
+                        }
+                    }
+                    if (gm != 0.0) {
+                        Fb[0] += (R)gm;
+                        nz = true;
+                    }
                 }
             }
             if (!nz) {
@@ -451,6 +701,11 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 for (int v = 0; v < NV; ++v) {
                     Hb[s][d][v] = has ? bb[(s * NV + v) * S::Asize(d) + a] : R(0);
                     any |= Hb[s][d][v] != R(0);
+                }
+                if constexpr (FX) {
+                    for (int k = 0; k < nfx; ++k) {
+                        any |= has && sxab[k * AS::XA + AS::XAoff(d) + s * S::Asize(d) + a] != R(0);
+                    }
                 }
             }
         }
@@ -541,6 +796,100 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 }
             }
         }
+        // FX: reverse of the scalars' predicted face values
+        // x_p[s][ip] = (x_f[s][ip] rho_f[s][ip] + xinc) / rho_p[s][ip],
+        // xinc = sum_d (c_l x_f[0][d] m[0][d] - c_r x_f[1][d] m[1][d]): adjoints of the
+        // predicted face densities (Hb[.][.][0]), of the face densities (fpb[.][.][0]),
+        // of the face mass fluxes m (mfb, taken back through the flux's first
+        // component below) and of the scalars' slopes
+        R mfb[2][ND];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            mfb[0][d] = mfb[1][d] = R(0);
+        }
+        if constexpr (FX) {
+            R mf[2][ND], ccl[ND], ccr[ND];
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+                mf[0][d] = fp[0][d][0] * fp[0][d][1 + d];
+                mf[1][d] = fp[1][d][0] * fp[1][d][1 + d];
+                if constexpr (SPH) {
+                    const adj::SphGeo<R> sg = sph_geo(gi, gj, gk, d, dth);
+                    ccl[d] = sg.k * sg.dS;
+                    ccr[d] = sg.k * sg.dSp;
+                } else {
+                    ccl[d] = ccr[d] = cth[d];
+                }
+            }
+            for (int k = 0; k < nfx; ++k) {
+                R* xk = swx + k * S::NP;
+                R xf[2][ND], xgR[ND], xgL[ND];
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    const R xc = xk[lc];
+                    const R phi = adj::limiter(g.limiter, xk[lc + lstride[d]] - xc, xc - xk[lc - lstride[d]], &xgR[d],
+                                               &xgL[d]);
+                    xf[0][d] = xc - R(0.5) * phi;
+                    xf[1][d] = xc + R(0.5) * phi;
+                }
+                R xinc = R(0);
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    xinc += ccl[d] * (xf[0][d] * mf[0][d]) - ccr[d] * (xf[1][d] * mf[1][d]);
+                }
+                R xfb[2][ND];
+                R xincb = R(0);
+#pragma unroll
+                for (int ip = 0; ip < ND; ++ip) {
+                    xfb[0][ip] = xfb[1][ip] = R(0);
+                    if (own >= 0 && own != ip) {
+                        continue;
+                    }
+                    const int a = a_index(x, ip);
+                    const R* base = sa + S::Aoff(ip);
+#pragma unroll
+                    for (int s = 0; s < 2; ++s) {
+                        const R xpb = sxab[k * AS::XA + AS::XAoff(ip) + s * S::Asize(ip) + a];
+                        if (xpb == R(0)) {
+                            continue;
+                        }
+                        const R rp = base[s * NV * S::Asize(ip) + a]; // predicted face density
+                        const R inv = R(1) / rp;
+                        const R xp = (xf[s][ip] * fp[s][ip][0] + xinc) * inv;
+                        const R xrb = xpb * inv;
+                        Hb[s][ip][0] -= xrb * xp;
+                        xfb[s][ip] += xrb * fp[s][ip][0];
+                        fpb[s][ip][0] += xrb * xf[s][ip];
+                        xincb += xrb;
+                    }
+                }
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    xfb[0][d] += ccl[d] * xincb * mf[0][d];
+                    xfb[1][d] -= ccr[d] * xincb * mf[1][d];
+                    mfb[0][d] += ccl[d] * xincb * xf[0][d];
+                    mfb[1][d] -= ccr[d] * xincb * xf[1][d];
+                }
+                // slopes: x_f[0/1][d] = x_c -/+ phi/2
+                R* xkb = swxb + k * S::NP;
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    const R phib = R(0.5) * (xfb[1][d] - xfb[0][d]);
+                    const R dRb = phib * xgR[d];
+                    const R dLb = phib * xgL[d];
+                    const R own_b = xfb[0][d] + xfb[1][d] - dRb + dLb;
+                    if (own_b != R(0)) {
+                        atomicAdd(&xkb[lc], own_b);
+                    }
+                    if (dRb != R(0)) {
+                        atomicAdd(&xkb[lc + lstride[d]], dRb);
+                    }
+                    if (dLb != R(0)) {
+                        atomicAdd(&xkb[lc - lstride[d]], -dLb);
+                    }
+                }
+            }
+        }
         // H[s][ipos] = cons(fp[s][ipos]) + sum_d cth_d (F(fp[0][d]) - F(fp[1][d])) + gravity(cons(fp[s][ipos]))
         R Sb[NV];
 #pragma unroll
@@ -602,6 +951,10 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                     Fb1[v] = -cth[d] * Sb[v];
                 }
             }
+            if constexpr (FX) {
+                Fb0[0] += mfb[0][d];
+                Fb1[0] += mfb[1][d];
+            }
             adj::flux_prim_rev<ND>(eos, fp[0][d], d, Fb0, fpb[0][d]);
             adj::flux_prim_rev<ND>(eos, fp[1][d], d, Fb1, fpb[1][d]);
         }
@@ -651,6 +1004,9 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
         for (int v = 0; v < NV; ++v) {
             wb[v] = swb[v * S::NP + p];
             nz |= wb[v] != R(0);
+        }
+        for (int k = 0; k < nfx; ++k) {
+            nz |= swxb[k * S::NP + p] != R(0);
         }
         if (!nz) {
             continue;
@@ -709,6 +1065,27 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
             }
         }
         const int64_t oo = sidx(lam_in, g.n[1], si, sj, sk);
+        if constexpr (FX) {
+            // scalars: slopes and predictor; for an own cell also the identity
+            // part rho'x' = rho x + ... (its density part goes to outv[0], with the
+            // division's new-density adjoint, since rho' = rho + ...)
+            // (x1, x2 are -2 along the inactive dimensions)
+            const int tcell = own_cell ? x0 + S::T0 * ((ND >= 2 ? x1 : 0) + S::T1 * (ND >= 3 ? x2 : 0)) : -1;
+            if (own_cell) {
+                outv[0] += sgr[tcell]; // the density plane's atomic follows below
+            }
+            for (int k = 0; k < nfx; ++k) {
+                double xb = (double)swxb[k * S::NP + p];
+                if (own_cell) {
+                    const double lrx = sgx[k * S::TVOL + tcell];
+                    xb += lrx * U.q[o];
+                    outv[0] += lrx * U.q[o + U.plane * (NV + k)];
+                }
+                if (xb != 0.0) {
+                    atomicAdd(&lam_in.q[oo + lam_in.plane * (NV + k)], xb);
+                }
+            }
+        }
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             if (outv[v] != 0.0) {
@@ -728,13 +1105,14 @@ constexpr int adj_min_blocks()
     return sizeof(R) == 8 ? (NT <= 256 ? 2 : 1) : (NT <= 256 ? 3 : (NT <= 384 ? 3 : 1));
 }
 
-template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH, bool EXACTB>
-__global__ void __launch_bounds__(NT, adj_min_blocks<R, NT>())
+// FX (passive scalars): one CTA per SM (the scalars' shared arrays)
+template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH, bool EXACTB, bool FX = false>
+__global__ void __launch_bounds__(NT, FX ? 1 : adj_min_blocks<R, NT>())
 k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt, StateDev lam_zero, double* gbar)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    adjoint_tile<ND, R, TX, TY, TZ, NT, SPH, EXACTB>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw, &lam_zero, true,
-                                                     gbar);
+    adjoint_tile<ND, R, TX, TY, TZ, NT, SPH, EXACTB, FX>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw, &lam_zero,
+                                                         true, gbar);
 }
 
 // Transpose of the boundary fill: every interior cell gathers the adjoints of
@@ -783,6 +1161,9 @@ __device__ __forceinline__ void fold_cells(const GridDev& g, const StateDev& lam
                         acc[1 + d] += fl[d] ? -v : v;
                     }
                     acc[1 + ND] += lam.q[og + lam.plane * (1 + ND)];
+                    for (int k = 0; k < g.nfx; ++k) {
+                        lam.q[oc + lam.plane * (ND + 2 + k)] += lam.q[og + lam.plane * (ND + 2 + k)];
+                    }
                 }
             }
         }

@@ -1817,13 +1817,22 @@ int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p)
         return fail(HCL_ERR_CONFIG, "no state set");
     }
     const GridDev& g = h->g;
-    if (!g.uniform_dx || g.nfx > 0 || h->cfg.pressure_fix || g.eos != HCL_EOS_PERFECT_GAS) {
+    if (!g.uniform_dx || h->cfg.pressure_fix || g.eos != HCL_EOS_PERFECT_GAS) {
         return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian and spherical grids of uniform spacing, uniform, "
-                                    "point-mass or internal-mass gravity, every Riemann solver, nfx = 0, no pressure "
-                                    "fix, the perfect-gas EOS");
+                                    "point-mass or internal-mass gravity, every Riemann solver, passive scalars, no "
+                                    "pressure fix, the perfect-gas EOS");
     }
     if (p->precision != HCL_FP64 && p->precision != HCL_FP32_MIXED) {
         return fail(HCL_ERR_CONFIG, "the reverse sweep runs in HCL_FP64 or HCL_FP32_MIXED");
+    }
+    if (g.nfx > 0) {
+        size_t need = 0, avail = 0;
+        if (!hcl::adjoint::scalar_sweep_fits(g.ndim, p->precision == HCL_FP64, g.nfx, &need, &avail)) {
+            return fail(HCL_ERR_CONFIG,
+                        "the reverse sweep's tile with %d passive scalars needs %zu bytes of shared memory, the device "
+                        "allows %zu: use fewer scalars or the HCL_FP32_MIXED sweep",
+                        g.nfx, need, avail);
+        }
     }
     int rc;
     StepCtl ctl;
@@ -1841,7 +1850,7 @@ int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p)
     const int N = p->nsteps;
     const int k = p->checkpoint_every > 0 ? p->checkpoint_every : 32;
     const int nck = (N + k - 1) / k;
-    const size_t sz = (size_t)h->st[0].plane * (g.ndim + 2);
+    const size_t sz = (size_t)h->st[0].plane * (g.ndim + 2 + g.nfx);
     if (h->adj_cap_ck < nck) {
         cudaFree(h->adj_ckpt);
         h->adj_ckpt = nullptr;
@@ -1933,7 +1942,7 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
     const int nd = g.ndim;
     const int N = (int)h->adj_dts.size();
     const int k = h->adj_k;
-    const size_t sz = (size_t)h->st[0].plane * (nd + 2);
+    const size_t sz = (size_t)h->st[0].plane * (nd + 2 + g.nfx);
     int rc;
     // two segment buffers of k+1 states: the recompute of one overlaps the sweep of the other
     if (h->adj_cap_seg < 2 * (k + 1)) {
@@ -2008,6 +2017,13 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
     HCL_CUDA(cudaMemsetAsync(h->adj_lam, 0, sizeof(double) * sz * 3, s));
     hcl::fused::pack_state(g, lam[0], lam_final, lam_final + g.N, lam_final + g.N * (nd + 1),
                            memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
+    // the passive scalars' planes follow E in the caller's buffer
+    for (int f = 0; f < g.nfx; ++f) {
+        const size_t w = sizeof(double) * (size_t)g.n[0];
+        HCL_CUDA(cudaMemcpy2DAsync(lam[0].q + lam[0].plane * (nd + 2 + f), sizeof(double) * (size_t)lam[0].pitch,
+                                   lam_final + g.N * (nd + 2 + f), w, w, (size_t)g.n[1] * g.n[2],
+                                   memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    }
     // the reference layout packs rho, rhou (nd planes), E contiguously: rhou at +N, E at +N*(nd+1)
     hcl::adjoint::fold(g, lam[0], s);
     RunParamsDev rp;
@@ -2103,6 +2119,12 @@ static int adjoint_backward_impl(hcl_handle* h, const double* lam_final, double*
     hcl::adjoint::zero_ghosts(g, lam[ra], s);
     hcl::fused::unpack_state(g, lam[ra], grad, grad + g.N, grad + g.N * (nd + 1),
                              memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
+    for (int f = 0; f < g.nfx; ++f) {
+        const size_t w = sizeof(double) * (size_t)g.n[0];
+        HCL_CUDA(cudaMemcpy2DAsync(grad + g.N * (nd + 2 + f), w, lam[ra].q + lam[ra].plane * (nd + 2 + f),
+                                   sizeof(double) * (size_t)lam[ra].pitch, w, (size_t)g.n[1] * g.n[2],
+                                   memory == HCL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    }
     HCL_LAUNCH_CHECK();
     return HCL_OK;
 }

@@ -207,6 +207,9 @@ cudaError_t launch(int lim, int rs, int nw, int grid, const Prob* probs, const i
 namespace adjoint {
 
 void configure();
+// Whether the reverse sweep's tile with nfx passive scalars fits the current
+// device's shared memory: *need bytes against the opt-in *avail.
+int scalar_sweep_fits(int ndim, bool fp64, int nfx, size_t* need, size_t* avail);
 // One adjoint step: lam_in (zero on entry) += (dU^{n+1}/dU^n)^T lam_out, with
 // U = U^n and lam_out on interior cells (ghost entries zero); the
 // contributions to ghost cells land on the interior cells they are filled

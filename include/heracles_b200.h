@@ -336,11 +336,14 @@ int hcl_get_stream(const hcl_handle* h, void** stream);
  * (recorded by the forward pass or given).  Supported: Cartesian and
  * spherical grids of uniform spacing per coordinate (the spherical face areas,
  * volumes and geometric source terms included), uniform, point-mass and
- * internal-mass gravity, HLL/HLLC/Low Mach, every limiter, ndim 1-3, nfx = 0, no pressure
- * fix, the perfect-gas EOS; anything else returns HCL_ERR_CONFIG.  Branches
- * (limiter sign tests, wave-speed min/max, HLLC switches) are differentiated
- * along the branch the forward evaluation took.  No reference counterpart:
- * the reference has no adjoint. */
+ * internal-mass gravity, HLL/HLLC/Low Mach, every limiter, ndim 1-3, passive
+ * scalars (as many as the reverse tile's shared memory holds: 3-D FP64 sweeps
+ * take one), no pressure fix, the perfect-gas EOS; anything else returns
+ * HCL_ERR_CONFIG.  Branches (limiter sign tests, wave-speed min/max, HLLC
+ * switches) are differentiated along the branch the forward evaluation took;
+ * for the passive scalars (their limiters, the upwind choice of each face and
+ * the clamp of x' to [0, 1]) along the branch of the sweep's own
+ * recomputation.  No reference counterpart: the reference has no adjoint. */
 typedef struct hcl_adjoint_params {
     int nsteps;
     const double* dts;        /* host, nsteps values; NULL: CFL dt of this forward run (recorded) */
@@ -355,8 +358,9 @@ typedef struct hcl_adjoint_params {
 int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p);
 /* Reverse pass: given lam_final = dJ/dU^N, writes grad = dJ/dU^0 for the
  * interior cells (ghost entries are zero: ghosts are functions of the
- * interior).  Both are one contiguous buffer of (ndim+2)*N doubles holding
- * the full arrays rho, rhou (ndim planes), E in the layout above.  Each
+ * interior).  Both are one contiguous buffer of (ndim+2+nfx)*N doubles holding
+ * the full arrays rho, rhou (ndim planes), E and the nfx passive scalars (the
+ * mass fractions fx, not rho*fx) in the layout above.  Each
  * checkpoint segment is recomputed forward on the device, then swept
  * backward step by step. */
 int hcl_adjoint_backward(hcl_handle* h, const double* lam_final, double* grad, int memory);
