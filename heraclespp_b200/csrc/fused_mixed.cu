@@ -47,8 +47,8 @@ bool mixed_shape_valid(const GridDev& g, int shape)
                mixed_smem_bytes(g, shape) + kFusedStaticSmemMargin <= (size_t)smem_optin();
     }
     if (g.nfx > 0) {
-        // passive scalars ride in the shared-memory tiles and, one of them,
-        // in the 4-warp strips
+        // passive scalars ride in the shared-memory tiles and, one or two of
+        // them, in the 4-warp strips and the 3-D column march
         if (g.ndim == 2 && shape >= 3 && shape <= 6) {
             return strip2d_fx_eligible(g);
         }

@@ -14,7 +14,7 @@ namespace hcl::fused {
 bool strip3d_fx_eligible(const GridDev& g)
 {
     return g.ndim == 3 && g.uniform_cart && g.geom == GEOM_CARTESIAN && g.gravity == GRAV_UNIFORM && g.ng >= 2 &&
-           g.nfx == 1;
+           (g.nfx == 1 || g.nfx == 2);
 }
 
 bool strip3d_eligible(const GridDev& g)
@@ -71,7 +71,9 @@ template <int LIM, int RS>
 void launch_lr(const GridDev& g, const StateDev& in, const StateDev& out, StepCtl* ctl, const RunParamsDev& rp, int slot,
                int out_buf, int L, cudaStream_t s)
 {
-    if (g.nfx == 1) {
+    if (g.nfx == 2) {
+        launch_lrf<LIM, RS, 2>(g, in, out, ctl, rp, slot, out_buf, L, s);
+    } else if (g.nfx == 1) {
         launch_lrf<LIM, RS, 1>(g, in, out, ctl, rp, slot, out_buf, L, s);
     } else {
         launch_lrf<LIM, RS, 0>(g, in, out, ctl, rp, slot, out_buf, L, s);

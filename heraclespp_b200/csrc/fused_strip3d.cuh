@@ -85,11 +85,12 @@ __device__ __forceinline__ void cons_and_flux(const fast::Eos& e, const float w[
 // Hancock face states of one cell: minus/plus faces along x, y, z
 // (extrapolation_reconstruction.hpp:65-143, gravity :306-312).  wyd/wyu are
 // the y-neighbours, wzd/wzu the z-neighbours; x-neighbours come by shuffle.
-// NFX = 1: also the passive scalar's face values xo[0..2] (minus faces x, y,
-// z) and xo[3..5] (plus faces) from its primitives xw = {centre, y-, y+, z-,
-// z+}: limited slopes, times the face density before the predictor, plus the
-// predictor's increment from the face states' mass fluxes, divided by the
-// predicted face density (extrapolation_reconstruction.hpp:315-337, :329-339).
+// NFX > 0: also each passive scalar k's face values xo[6k..6k+2] (minus faces
+// x, y, z) and xo[6k+3..6k+5] (plus faces) from its primitives
+// xw[5k..5k+4] = {centre, y-, y+, z-, z+}: limited slopes, times the face
+// density before the predictor, plus the predictor's increment from the face
+// states' mass fluxes, divided by the predicted face density
+// (extrapolation_reconstruction.hpp:315-337, :329-339).
 template <int LIM, int NFX = 0>
 __device__ __forceinline__ void hancock(const Ctx& c, const float wc[5], const float wyd[5], const float wyu[5],
                                         const float wzd[5], const float wzu[5], float hm[3][5], float hp[3][5],
@@ -142,20 +143,23 @@ __device__ __forceinline__ void hancock(const Ctx& c, const float wc[5], const f
             }
         }
     }
-    if constexpr (NFX > 0) {
-        const float xl = __shfl_up_sync(0xffffffffu, xw[0], 1);
-        const float xr = __shfl_down_sync(0xffffffffu, xw[0], 1);
-        const float s[3] = {half_lim_fast<LIM>(xr - xw[0], xw[0] - xl), half_lim_fast<LIM>(xw[2] - xw[0], xw[0] - xw[1]),
-                            half_lim_fast<LIM>(xw[4] - xw[0], xw[0] - xw[3])};
+#pragma unroll
+    for (int k = 0; k < NFX; ++k) {
+        const float* xk = xw + 5 * k;
+        float* ok = xo + 6 * k;
+        const float xl = __shfl_up_sync(0xffffffffu, xk[0], 1);
+        const float xr = __shfl_down_sync(0xffffffffu, xk[0], 1);
+        const float s[3] = {half_lim_fast<LIM>(xr - xk[0], xk[0] - xl), half_lim_fast<LIM>(xk[2] - xk[0], xk[0] - xk[1]),
+                            half_lim_fast<LIM>(xk[4] - xk[0], xk[0] - xk[3])};
         float xinc = 0.f;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            xinc = fmaf(c.cth[d], (xw[0] - s[d]) * mfm[d] - (xw[0] + s[d]) * mfp[d], xinc);
+            xinc = fmaf(c.cth[d], (xk[0] - s[d]) * mfm[d] - (xk[0] + s[d]) * mfp[d], xinc);
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            xo[d] = __fdividef(fmaf(xw[0] - s[d], fm[d][0], xinc), hm[d][0]);
-            xo[3 + d] = __fdividef(fmaf(xw[0] + s[d], fp[d][0], xinc), hp[d][0]);
+            ok[d] = __fdividef(fmaf(xk[0] - s[d], fm[d][0], xinc), hm[d][0]);
+            ok[3 + d] = __fdividef(fmaf(xk[0] + s[d], fp[d][0], xinc), hp[d][0]);
         }
     }
 }
@@ -169,7 +173,7 @@ struct S3Shared {
     float yface[2][kS3Warps][2][5][32]; // [.][w][0: bottom (minus), 1: top (plus)]
     float gflux[2][kS3Warps][5][32];    // flux of the y-face above row w
 };
-// the same for one passive scalar
+// the same for each passive scalar
 struct S3SharedFx {
     float xprim[2][kS3Warps][32];
     float xyface[2][kS3Warps][2][32];
@@ -177,10 +181,10 @@ struct S3SharedFx {
 };
 template <int NFX>
 struct S3SharedT : S3Shared {
+    S3SharedFx fx[NFX];
 };
 template <>
-struct S3SharedT<1> : S3Shared {
-    S3SharedFx fx;
+struct S3SharedT<0> : S3Shared {
 };
 
 // Ghost images of one scalar plane q (no sign flips): the loops of
@@ -230,16 +234,20 @@ __device__ __forceinline__ void store_images_3d_scalar(double* __restrict__ q, i
     }
 }
 
-// NFX = 1: one passive scalar (state plane 5) rides along: face values from
-// hancock, upwind fluxes from the Riemann mass fluxes (godunov_scheme.hpp:
-// 262-301), the update in FP64 divided by the new density and clamped to
-// [0, 1], stored with the same ghost images.
+// NFX > 0: the passive scalars (state planes 5 .. 4 + NFX) ride along: face
+// values from hancock, upwind fluxes from the Riemann mass fluxes
+// (godunov_scheme.hpp:262-301), the update in FP64 divided by the new density
+// and clamped to [0, 1], stored with the same ghost images.
 template <int LIM, int RS, int NFX = 0>
 __global__ void __launch_bounds__(kS3Threads, 1)
 k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, int slot, int out_buf, int L)
 {
     extern __shared__ __align__(16) unsigned char s3_raw[];
     S3SharedT<NFX>& sh = *reinterpret_cast<S3SharedT<NFX>*>(s3_raw);
+    S3SharedFx* fxs = nullptr; // the scalars' shared planes
+    if constexpr (NFX > 0) {
+        fxs = sh.fx;
+    }
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     const Decision dec = decide(ctl, slot, rp);
@@ -310,23 +318,32 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
     double dFx[5];     // x-flux difference (left - right face) of plane z, exact in FP64
     float Gzlo[5];     // z-face flux z-1/2
     double qN[5 + NFX];
-    // passive scalar: primitives of planes z, z+1; z-plus face value of plane
-    // z; x-flux difference of plane z; upwind flux of the z-face z-1/2
-    float xC = 0.f, xD = 0.f, xzU = 0.f, gzx_lo = 0.f;
-    double dxx = 0.0;
+    // passive scalars (index k): primitives of planes z, z+1; z-plus face
+    // value of plane z; x-flux difference of plane z; upwind flux of the
+    // z-face z-1/2
+    constexpr int NX = NFX > 0 ? NFX : 1;
+    float xC[NX], xD[NX], xzU[NX], gzx_lo[NX];
+    double dxx[NX];
+#pragma unroll
+    for (int k = 0; k < NX; ++k) {
+        xC[k] = xD[k] = xzU[k] = gzx_lo[k] = 0.f;
+        dxx[k] = 0.0;
+    }
     {
         double q[5 + NFX];
         load(z0 - 2, q);
         s3::prim(gm1, q, wC);
-        if constexpr (NFX > 0) {
-            xC = (float)q[5];
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            xC[k] = (float)q[5 + k];
         }
         load(z0 - 1, q);
         s3::prim(gm1, q, wD);
         put_prim(z0 - 1, wD);
-        if constexpr (NFX > 0) {
-            xD = (float)q[5];
-            sh.fx.xprim[(z0 - 1) & 1][w][lane] = xD;
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            xD[k] = (float)q[5 + k];
+            fxs[k].xprim[(z0 - 1) & 1][w][lane] = xD[k];
         }
         load(z0, qN);
     }
@@ -349,10 +366,11 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
         float wN[5];
         s3::prim(gm1, qN, wN);
         put_prim(z + 2, wN);
-        float xN = 0.f;
-        if constexpr (NFX > 0) {
-            xN = (float)qN[5];
-            sh.fx.xprim[(z + 2) & 1][w][lane] = xN;
+        float xN[NX];
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            xN[k] = (float)qN[5 + k];
+            fxs[k].xprim[(z + 2) & 1][w][lane] = xN[k];
         }
         load(z + 3, qN);
         // 2. Hancock of plane z+1 (y-neighbours' primitives of plane z+1 were shared last step)
@@ -363,18 +381,27 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             wyu[v] = sh.prim[(z + 1) & 1][wu][v][lane];
         }
         float hm[3][5], hp[3][5];
-        float xw[5] = {xD, 0.f, 0.f, xC, xN};
-        if constexpr (NFX > 0) {
-            xw[1] = sh.fx.xprim[(z + 1) & 1][wd][lane];
-            xw[2] = sh.fx.xprim[(z + 1) & 1][wu][lane];
+        float xw[5 * NX];
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            xw[5 * k] = xD[k];
+            xw[5 * k + 1] = fxs[k].xprim[(z + 1) & 1][wd][lane];
+            xw[5 * k + 2] = fxs[k].xprim[(z + 1) & 1][wu][lane];
+            xw[5 * k + 3] = xC[k];
+            xw[5 * k + 4] = xN[k];
         }
-        float xo[6];
+        float xo[6 * NX];
         s3::hancock<LIM, NFX>(c, wD, wyd, wyu, wC, wN, hm, hp, xw, xo);
         // 3. x-faces of plane z+1: left face at this lane, right face from lane+1
         double dFxN[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        double dxxN = 0.0;
+        double dxxN[NX];
+        float gzx_hi[NX];
+#pragma unroll
+        for (int k = 0; k < NX; ++k) {
+            dxxN[k] = 0.0;
+            gzx_hi[k] = 0.f;
+        }
         float Gzhi[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-        float gzx_hi = 0.f;
         if (w_update) {
             float uL[5], Fl[5];
 #pragma unroll
@@ -386,16 +413,18 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             for (int v = 0; v < 5; ++v) {
                 dFxN[v] = (double)Fl[v] - (double)__shfl_down_sync(0xffffffffu, Fl[v], 1);
             }
-            if constexpr (NFX > 0) {
+#pragma unroll
+            for (int k = 0; k < NFX; ++k) {
                 // this cell's minus value when the mass flows left, else the left cell's plus value
-                const float up_left = __shfl_up_sync(0xffffffffu, xo[3], 1);
-                const float fl = (Fl[0] < 0.f ? xo[0] : up_left) * Fl[0];
-                dxxN = (double)fl - (double)__shfl_down_sync(0xffffffffu, fl, 1);
+                const float up_left = __shfl_up_sync(0xffffffffu, xo[6 * k + 3], 1);
+                const float fl = (Fl[0] < 0.f ? xo[6 * k] : up_left) * Fl[0];
+                dxxN[k] = (double)fl - (double)__shfl_down_sync(0xffffffffu, fl, 1);
             }
             // 4. z-face z+1/2
             fast::riemann<3>(c.eos, RS, hzU, hm[2], 2, Gzhi);
-            if constexpr (NFX > 0) {
-                gzx_hi = (Gzhi[0] < 0.f ? xo[2] : xzU) * Gzhi[0];
+#pragma unroll
+            for (int k = 0; k < NFX; ++k) {
+                gzx_hi[k] = (Gzhi[0] < 0.f ? xo[6 * k + 2] : xzU[k]) * Gzhi[0];
             }
         }
         // 5. y-face states of plane z+1 for the neighbours
@@ -404,9 +433,10 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             sh.yface[(z + 1) & 1][w][0][v][lane] = hm[1][v];
             sh.yface[(z + 1) & 1][w][1][v][lane] = hp[1][v];
         }
-        if constexpr (NFX > 0) {
-            sh.fx.xyface[(z + 1) & 1][w][0][lane] = xo[1];
-            sh.fx.xyface[(z + 1) & 1][w][1][lane] = xo[4];
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            fxs[k].xyface[(z + 1) & 1][w][0][lane] = xo[6 * k + 1];
+            fxs[k].xyface[(z + 1) & 1][w][1][lane] = xo[6 * k + 4];
         }
         // 6. y-face above this row, plane z
         const bool upd = z >= z0;
@@ -422,10 +452,12 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             for (int v = 0; v < 5; ++v) {
                 sh.gflux[z & 1][w][v][lane] = G[v];
             }
-            if constexpr (NFX > 0) {
+#pragma unroll
+            for (int k = 0; k < NFX; ++k) {
                 // the upper row's bottom value when the mass flows down, else this row's top value
-                const float xu = G[0] < 0.f ? sh.fx.xyface[z & 1][wu][0][lane] : sh.fx.xyface[z & 1][w][1][lane];
-                sh.fx.xgflux[z & 1][w][lane] = xu * G[0];
+                const float xu =
+                    G[0] < 0.f ? fxs[k].xyface[z & 1][wu][0][lane] : fxs[k].xyface[z & 1][w][1][lane];
+                fxs[k].xgflux[z & 1][w][lane] = xu * G[0];
             }
         }
         __syncthreads();
@@ -474,14 +506,16 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             for (int v = 0; v < 5; ++v) {
                 qout[oo + plane * v] = qn[v];
             }
-            double xnew = 0.0;
-            if constexpr (NFX > 0) {
-                const double gb = (double)sh.fx.xgflux[z & 1][wd][lane];
-                const double gt = (double)sh.fx.xgflux[z & 1][w][lane];
-                const double xn = fma(q[5], q[0], fma(cxyz[0], dxx, fma(cxyz[1], gb - gt, cxyz[2] * ((double)gzx_lo - (double)gzx_hi))));
-                xnew = xn / qn[0];
-                xnew = xnew < 0. ? 0. : (xnew > 1. ? 1. : xnew);
-                qout[oo + plane * 5] = xnew;
+            double xnew[NX];
+#pragma unroll
+            for (int k = 0; k < NFX; ++k) {
+                const double gb = (double)fxs[k].xgflux[z & 1][wd][lane];
+                const double gt = (double)fxs[k].xgflux[z & 1][w][lane];
+                const double xn = fma(q[5 + k], q[0], fma(cxyz[0], dxx[k], fma(cxyz[1], gb - gt, cxyz[2] * ((double)gzx_lo[k] - (double)gzx_hi[k]))));
+                double xv = xn / qn[0];
+                xv = xv < 0. ? 0. : (xv > 1. ? 1. : xv);
+                xnew[k] = xv;
+                qout[oo + plane * (5 + k)] = xv;
             }
             // ghost images of border cells (boundary_distribute.hpp:42-76)
             const unsigned zm = (z < 2 * g.ng || z >= g.n[2] - 2 * g.ng)
@@ -489,8 +523,10 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
                                     : 0u;
             if ((xym | zm) != 0u) {
                 store_images_3d(qout, plane, pitch, n0, n1, g.n[2], g.ng, col, row, z, xm, ym, zm, qn);
-                if constexpr (NFX > 0) {
-                    store_images_3d_scalar(qout + plane * 5, pitch, n0, n1, g.n[2], g.ng, col, row, z, xm, ym, zm, xnew);
+#pragma unroll
+                for (int k = 0; k < NFX; ++k) {
+                    store_images_3d_scalar(qout + plane * (5 + k), pitch, n0, n1, g.n[2], g.ng, col, row, z, xm, ym, zm,
+                                           xnew[k]);
                 }
             }
         }
@@ -503,12 +539,13 @@ k_strip3d(GridDev g, StateDev in, StateDev out, StepCtl* ctl, RunParamsDev rp, i
             dFx[v] = dFxN[v];
             Gzlo[v] = Gzhi[v];
         }
-        if constexpr (NFX > 0) {
-            xC = xD;
-            xD = xN;
-            xzU = xo[5];
-            dxx = dxxN;
-            gzx_lo = gzx_hi;
+#pragma unroll
+        for (int k = 0; k < NFX; ++k) {
+            xC[k] = xD[k];
+            xD[k] = xN[k];
+            xzU[k] = xo[6 * k + 5];
+            dxx[k] = dxxN[k];
+            gzx_lo[k] = gzx_hi[k];
         }
     }
 
