@@ -12,8 +12,6 @@ The FP64 gradient, including the scalars' planes, is checked against central
 differences of the FP64 forward along seeded random directions, the FP32 sweep
 against the FP64 one, and a 3-D FP64 sweep with more scalars than its tile's
 shared memory holds is refused."""
-import ctypes as C
-
 import numpy as np
 import pytest
 
