@@ -225,6 +225,41 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
         return sg;
     };
 
+    // Grids of non-uniform spacing (limited_linear_reconstruction.hpp:46-64):
+    // the face values are w -/+ (dl/2) lim(dR / hR, dL / hL) with the half
+    // spacings hR = (dl + dl_p)/2, hL = (dl_m + dl)/2, so phi = dl lim(...)
+    // and its partials carry dl/hR and dl/hL; on uniform grids (g.uniform_dx)
+    // the limiters' degree-1 homogeneity gives lim(dR, dL).  `gd` is the
+    // cell's global index along d; `exact`: the FP64 sweep's forward-rounded
+    // branch test.
+    auto limited_phi = [&](int d, int gd, R dR, R dL, R* gR, R* gL, bool exact) -> R {
+        if (g.uniform_dx) {
+            return adj::limiter(g.limiter, dR, dL, gR, gL);
+        }
+        const int c = min(max(gd, 1), g.n[d] - 2);
+        const double dl = g.dx[d][c];
+        const double hR = fwd::div(fwd::add(dl, g.dx[d][c + 1]), 2.0);
+        const double hL = fwd::div(fwd::add(g.dx[d][c - 1], dl), 2.0);
+        R a, b, sl;
+        if (exact) {
+            const bool active = fwd::mul(fwd::div((double)dL, hL), fwd::div((double)dR, hR)) > 0;
+            sl = adj::limiter_on(g.limiter, active, (R)(dR / hR), (R)(dL / hL), &a, &b);
+        } else {
+            sl = adj::limiter(g.limiter, (R)(dR / hR), (R)(dL / hL), &a, &b);
+        }
+        *gR = (R)(dl / hR) * a;
+        *gL = (R)(dl / hL) * b;
+        return (R)dl * sl;
+    };
+    // Cartesian predictor (dt/2) and update (dt) coefficients of the cell at
+    // global index gd along d: dt dS / dV = dt / dx_gd
+    auto cth_at = [&](int d, int gd) -> R {
+        return g.uniform_dx ? cth[d] : (R)(dth / g.dx[d][min(max(gd, 0), g.n[d] - 1)]);
+    };
+    auto cfull_at = [&](int d, int gd) -> double {
+        return g.uniform_dx ? dt * g.inv_dx[d] : dt / g.dx[d][min(max(gd, 0), g.n[d] - 1)];
+    };
+
     if (lam_zero) {
         // this tile's interior cells of the buffer the next step adds into
         for (int c = tid; c < S::TVOL; c += NT) {
@@ -347,8 +382,8 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 R gR, gL;
                 // the value only: a branch taken differently at a raw product
                 // that underflows changes it by less than 1e-270
-                const R phi = adj::limiter(g.limiter, sw[v * S::NP + lc + lstride[d]] - wc,
-                                           wc - sw[v * S::NP + lc - lstride[d]], &gR, &gL);
+                const R phi = limited_phi(d, gorg[d] + x[d], sw[v * S::NP + lc + lstride[d]] - wc,
+                                          wc - sw[v * S::NP + lc - lstride[d]], &gR, &gL, false);
                 fp[0][d][v] = wc - R(0.5) * phi;
                 fp[1][d][v] = wc + R(0.5) * phi;
             }
@@ -387,10 +422,11 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 }
                 adj::sph_source<ND>(sg, d, fp[0][d], fp[1][d], inc);
             } else {
-                ccl[d] = ccr[d] = cth[d];
+                const R ct = cth_at(d, gorg[d] + x[d]);
+                ccl[d] = ccr[d] = ct;
 #pragma unroll
                 for (int v = 0; v < NV; ++v) {
-                    inc[v] += cth[d] * (fL[v] - fR[v]);
+                    inc[v] += ct * (fL[v] - fR[v]);
                 }
             }
         }
@@ -406,7 +442,8 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 for (int d = 0; d < ND; ++d) {
                     const R xc = xk[lc];
                     R gR, gL;
-                    const R phi = adj::limiter(g.limiter, xk[lc + lstride[d]] - xc, xc - xk[lc - lstride[d]], &gR, &gL);
+                    const R phi =
+                        limited_phi(d, gorg[d] + x[d], xk[lc + lstride[d]] - xc, xc - xk[lc - lstride[d]], &gR, &gL, false);
                     xf[0][d] = xc - R(0.5) * phi;
                     xf[1][d] = xc + R(0.5) * phi;
                 }
@@ -415,7 +452,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                     if constexpr (SPH) {
                         xinc += ccl[d] * (xf[0][d] * mfl[d]) - ccr[d] * (xf[1][d] * mfr[d]);
                     } else {
-                        xinc += cth[d] * (xf[0][d] * mfl[d] - xf[1][d] * mfr[d]);
+                        xinc += ccl[d] * (xf[0][d] * mfl[d] - xf[1][d] * mfr[d]);
                     }
                 }
 #pragma unroll
@@ -484,7 +521,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
             const int64_t cf = side ? geo_cell(i1 + (d == 0), j1 + (d == 1), k1 + (d == 2)) : c;
             return dt / g.dv[c] * g.ds[cf + g.N * d];
         } else {
-            return dt * g.inv_dx[d];
+            return cfull_at(d, gorg[d] + x[d]);
         }
     };
     // A index along d of tile cell x (the H cells -1 .. T_d along d)
@@ -620,10 +657,20 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                     nz |= Fb[v] != R(0);
                 }
             } else {
+                if (g.uniform_dx) {
 #pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    Fb[v] = (R)(cfull[d] * (sl[v * S::NP + lcR] - sl[v * S::NP + lcL]));
-                    nz |= Fb[v] != R(0);
+                    for (int v = 0; v < NV; ++v) {
+                        Fb[v] = (R)(cfull[d] * (sl[v * S::NP + lcR] - sl[v * S::NP + lcL]));
+                        nz |= Fb[v] != R(0);
+                    }
+                } else {
+                    // the face enters U'_R with +dt/dx_R and U'_L with -dt/dx_L
+                    const double cR = cfull_at(d, gorg[d] + x[d]), cL = cfull_at(d, gorg[d] + x[d] - 1);
+#pragma unroll
+                    for (int v = 0; v < NV; ++v) {
+                        Fb[v] = (R)(cR * sl[v * S::NP + lcR] - cL * sl[v * S::NP + lcL]);
+                        nz |= Fb[v] != R(0);
+                    }
                 }
             }
             if constexpr (FX) {
@@ -767,7 +814,10 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 const R dR = sw[v * S::NP + lc + lstride[d]] - wc;
                 const R dL = wc - sw[v * S::NP + lc - lstride[d]];
                 R phi;
-                if constexpr (std::is_same<R, double>::value && EXACTB) {
+                if (!g.uniform_dx) {
+                    phi = limited_phi(d, gorg[d] + x[d], dR, dL, &gRs[d][v], &gLs[d][v],
+                                      std::is_same<R, double>::value && EXACTB);
+                } else if constexpr (std::is_same<R, double>::value && EXACTB) {
                     const double prod = dR * dL;
                     bool active = prod > 0;
                     if (fabs(prod) * (g.inv_dx[d] * g.inv_dx[d]) <= 1e-270) {
@@ -818,7 +868,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                     ccl[d] = sg.k * sg.dS;
                     ccr[d] = sg.k * sg.dSp;
                 } else {
-                    ccl[d] = ccr[d] = cth[d];
+                    ccl[d] = ccr[d] = cth_at(d, gorg[d] + x[d]);
                 }
             }
             for (int k = 0; k < nfx; ++k) {
@@ -827,8 +877,8 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
 #pragma unroll
                 for (int d = 0; d < ND; ++d) {
                     const R xc = xk[lc];
-                    const R phi = adj::limiter(g.limiter, xk[lc + lstride[d]] - xc, xc - xk[lc - lstride[d]], &xgR[d],
-                                               &xgL[d]);
+                    const R phi = limited_phi(d, gorg[d] + x[d], xk[lc + lstride[d]] - xc, xc - xk[lc - lstride[d]],
+                                              &xgR[d], &xgL[d], false);
                     xf[0][d] = xc - R(0.5) * phi;
                     xf[1][d] = xc + R(0.5) * phi;
                 }
@@ -945,10 +995,11 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 }
                 adj::sph_source_rev<ND>(sg, d, fp[0][d], fp[1][d], Sb, fpb[0][d], fpb[1][d]);
             } else {
+                const R ct = cth_at(d, gorg[d] + x[d]);
 #pragma unroll
                 for (int v = 0; v < NV; ++v) {
-                    Fb0[v] = cth[d] * Sb[v];
-                    Fb1[v] = -cth[d] * Sb[v];
+                    Fb0[v] = ct * Sb[v];
+                    Fb1[v] = -ct * Sb[v];
                 }
             }
             if constexpr (FX) {

@@ -1817,10 +1817,10 @@ int hcl_adjoint_forward(hcl_handle* h, const hcl_adjoint_params* p)
         return fail(HCL_ERR_CONFIG, "no state set");
     }
     const GridDev& g = h->g;
-    if (!g.uniform_dx || h->cfg.pressure_fix || g.eos != HCL_EOS_PERFECT_GAS) {
-        return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian and spherical grids of uniform spacing, uniform, "
-                                    "point-mass or internal-mass gravity, every Riemann solver, passive scalars, no "
-                                    "pressure fix, the perfect-gas EOS");
+    if (h->cfg.pressure_fix || g.eos != HCL_EOS_PERFECT_GAS) {
+        return fail(HCL_ERR_CONFIG, "the adjoint supports Cartesian and spherical grids, uniform, point-mass or "
+                                    "internal-mass gravity, every Riemann solver, passive scalars, no pressure fix, "
+                                    "the perfect-gas EOS");
     }
     if (p->precision != HCL_FP64 && p->precision != HCL_FP32_MIXED) {
         return fail(HCL_ERR_CONFIG, "the reverse sweep runs in HCL_FP64 or HCL_FP32_MIXED");

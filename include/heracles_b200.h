@@ -334,7 +334,7 @@ int hcl_get_stream(const hcl_handle* h, void** stream);
 /* ---- discrete adjoint of the fused step ------------------------------------ */
 /* Reverse-mode derivative of nsteps fused steps with dt held fixed per step
  * (recorded by the forward pass or given).  Supported: Cartesian and
- * spherical grids of uniform spacing per coordinate (the spherical face areas,
+ * spherical grids, regular or of user-defined nodes (the spherical face areas,
  * volumes and geometric source terms included), uniform, point-mass and
  * internal-mass gravity, HLL/HLLC/Low Mach, every limiter, ndim 1-3, passive
  * scalars (as many as the reverse tile's shared memory holds: 3-D FP64 sweeps
