@@ -1,6 +1,6 @@
 """GPU checks on grids of user-defined nodes (the reference's UserDefined grid
-type, grid_type.cpp:151-186): the FP64 fused step against the oracle, and
-the discrete adjoint against central differences.  On such grids the limited
+type, grid_type.cpp:151-186): the FP64, fast-FP64 and FP32-mixed fused steps
+against the oracle, and the discrete adjoint against central differences.  On such grids the limited
 slopes take the differences over the half spacings and the face values the
 half width of each cell (limited_linear_reconstruction.hpp:46-64), and the
 predictor and the update divide by each cell's own width (or volume).
@@ -92,6 +92,33 @@ def test_fp64_step_on_user_defined_nodes_matches_oracle(name):
     for k in range(fx.shape[0]):
         assert rel(fx_d[k], fx[k]) <= 1e-12, k
     d.close()
+
+
+@pytest.mark.parametrize("precision,bound", [("fp64_fast", 1e-12), ("fp32_mixed", 1e-5)])
+@pytest.mark.parametrize("name", list(CASES))
+def test_fast_and_mixed_steps_on_user_defined_nodes(name, precision, bound):
+    """The fast-FP64 and FP32-mixed steps on user-defined nodes (the fused tile
+    kernel's per-cell spacing path) against the oracle over the FP64 run's
+    dts: relative L1 per field within the bounds those precisions are held
+    to on regular grids."""
+    o, d, U0, dts, _ = problem(name)
+    d.close()
+    ndim, nx, nfx, kw, _ = CASES[name]
+    nd = ndim
+    rho, rhou, E, fx = (a.copy() for a in split(U0, nd))
+    o.run(rho, rhou, E, fx if fx.shape[0] else None, dts=dts, max_iter=len(dts))
+    dp = Domain(ndim, nx, nfx=nfx, nodes=stretched_nodes(ndim, nx, kw["xmin"], kw["xmax"]), precision=precision, **kw)
+    dp.set_state(*split(U0, nd))
+    dp.run(nsteps=len(dts), dts=dts)
+    fx_d = np.zeros_like(fx)
+    r_d, m_d, E_d = dp.get_state(fx=fx_d)
+    s = interior(nd)
+    rel = lambda a, b: float(np.abs(a[s] - b[s]).sum() / np.abs(b[s]).sum())  # noqa: E731
+    errs = [rel(r_d, rho), rel(E_d, E)] + [rel(m_d[k], rhou[k]) for k in range(nd)] + \
+        [rel(fx_d[k], fx[k]) for k in range(nfx)]
+    print(f"{name} {precision}: max rel L1 {max(errs):.2e}")
+    assert max(errs) <= bound, errs
+    dp.close()
 
 
 @pytest.mark.parametrize("name", list(CASES))
