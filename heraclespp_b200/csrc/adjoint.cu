@@ -31,6 +31,11 @@ struct Launcher {
         // with passive scalars the size depends on their count: allow the opt-in
         cudaFuncSetAttribute(k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());
+        // grids of user-defined nodes
+        cudaFuncSetAttribute(k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB, false, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
+        cudaFuncSetAttribute(k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB, true, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin());
     }
     static void launch(const GridDev& g, const StateDev& U, const StateDev& lo, const StateDev& li, double dt,
                        const StateDev& lz, double* gbar, cudaStream_t s)
@@ -38,12 +43,19 @@ struct Launcher {
         const int nt0 = (g.nx[0] + S::T0 - 1) / S::T0;
         const int nt1 = (g.nx[1] + S::T1 - 1) / S::T1;
         const int nt2 = (g.nx[2] + S::T2 - 1) / S::T2;
-        if (g.nfx > 0) {
-            k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB, true>
-                <<<nt0 * nt1 * nt2, NT, smem(g.nfx), s>>>(g, U, lo, li, dt, lz, gbar);
+        const dim3 grid(nt0 * nt1 * nt2);
+        if (!g.uniform_dx) {
+            if (g.nfx > 0) {
+                k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB, true, true>
+                    <<<grid, NT, smem(g.nfx), s>>>(g, U, lo, li, dt, lz, gbar);
+            } else {
+                k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB, false, true>
+                    <<<grid, NT, smem(), s>>>(g, U, lo, li, dt, lz, gbar);
+            }
+        } else if (g.nfx > 0) {
+            k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB, true><<<grid, NT, smem(g.nfx), s>>>(g, U, lo, li, dt, lz, gbar);
         } else {
-            k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB>
-                <<<nt0 * nt1 * nt2, NT, smem(), s>>>(g, U, lo, li, dt, lz, gbar);
+            k_adjoint_step<ND, R, TX, TY, TZ, NT, SPH, EXACTB><<<grid, NT, smem(), s>>>(g, U, lo, li, dt, lz, gbar);
         }
         ++g_launches;
     }

@@ -148,7 +148,11 @@ __device__ __forceinline__ double div(double a, double b)
 // values back to the face densities, the mass fluxes of the reconstructed
 // states and the scalars' slopes.  Branches (limiters, the upwind choice, the
 // clamp) are those of the sweep's own recomputation.
-template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH = false, bool EXACTB = true, bool FX = false>
+// NU: a grid of user-defined nodes (g.uniform_dx false); the regular-grid
+// instantiation keeps the homogeneous limiter forms and one coefficient per
+// direction, and carries none of the per-cell spacing code.
+template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH = false, bool EXACTB = true, bool FX = false,
+          bool NU = false>
 __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U, const StateDev& lam_out,
                                              const StateDev& lam_in, double dt, int tile, unsigned char* smem_raw,
                                              const StateDev* lam_zero = nullptr, bool redirect = false,
@@ -233,7 +237,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
     // cell's global index along d; `exact`: the FP64 sweep's forward-rounded
     // branch test.
     auto limited_phi = [&](int d, int gd, R dR, R dL, R* gR, R* gL, bool exact) -> R {
-        if (g.uniform_dx) {
+        if constexpr (!NU) {
             return adj::limiter(g.limiter, dR, dL, gR, gL);
         }
         const int c = min(max(gd, 1), g.n[d] - 2);
@@ -254,10 +258,16 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
     // Cartesian predictor (dt/2) and update (dt) coefficients of the cell at
     // global index gd along d: dt dS / dV = dt / dx_gd
     auto cth_at = [&](int d, int gd) -> R {
-        return g.uniform_dx ? cth[d] : (R)(dth / g.dx[d][min(max(gd, 0), g.n[d] - 1)]);
+        if constexpr (!NU) {
+            return cth[d];
+        }
+        return (R)(dth / g.dx[d][min(max(gd, 0), g.n[d] - 1)]);
     };
     auto cfull_at = [&](int d, int gd) -> double {
-        return g.uniform_dx ? dt * g.inv_dx[d] : dt / g.dx[d][min(max(gd, 0), g.n[d] - 1)];
+        if constexpr (!NU) {
+            return dt * g.inv_dx[d];
+        }
+        return dt / g.dx[d][min(max(gd, 0), g.n[d] - 1)];
     };
 
     if (lam_zero) {
@@ -657,7 +667,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                     nz |= Fb[v] != R(0);
                 }
             } else {
-                if (g.uniform_dx) {
+                if constexpr (!NU) {
 #pragma unroll
                     for (int v = 0; v < NV; ++v) {
                         Fb[v] = (R)(cfull[d] * (sl[v * S::NP + lcR] - sl[v * S::NP + lcL]));
@@ -814,7 +824,7 @@ __device__ __forceinline__ void adjoint_tile(const GridDev& g, const StateDev& U
                 const R dR = sw[v * S::NP + lc + lstride[d]] - wc;
                 const R dL = wc - sw[v * S::NP + lc - lstride[d]];
                 R phi;
-                if (!g.uniform_dx) {
+                if constexpr (NU) {
                     phi = limited_phi(d, gorg[d] + x[d], dR, dL, &gRs[d][v], &gLs[d][v],
                                       std::is_same<R, double>::value && EXACTB);
                 } else if constexpr (std::is_same<R, double>::value && EXACTB) {
@@ -1157,13 +1167,13 @@ constexpr int adj_min_blocks()
 }
 
 // FX (passive scalars): one CTA per SM (the scalars' shared arrays)
-template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH, bool EXACTB, bool FX = false>
+template <int ND, class R, int TX, int TY, int TZ, int NT, bool SPH, bool EXACTB, bool FX = false, bool NU = false>
 __global__ void __launch_bounds__(NT, FX ? 1 : adj_min_blocks<R, NT>())
 k_adjoint_step(GridDev g, StateDev U, StateDev lam_out, StateDev lam_in, double dt, StateDev lam_zero, double* gbar)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    adjoint_tile<ND, R, TX, TY, TZ, NT, SPH, EXACTB, FX>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw, &lam_zero,
-                                                         true, gbar);
+    adjoint_tile<ND, R, TX, TY, TZ, NT, SPH, EXACTB, FX, NU>(g, U, lam_out, lam_in, dt, blockIdx.x, smem_raw,
+                                                             &lam_zero, true, gbar);
 }
 
 // Transpose of the boundary fill: every interior cell gathers the adjoints of
